@@ -1,0 +1,308 @@
+// saru_core.cuh -- per-candidate banded alignment core (device code).
+//
+// One candidate = read r[0..m) against genome window g[0..L), DP matrix
+// D[0..L][0..m] (row = window position, column = read position) with the
+// reference's rules (src/cuda-functions.cu:413-497):
+//   D[0][j] = j;  D[i][0] = max(0, i - 2*so);
+//   D[i][j] = min(D[i-1][j-1] + (g[i-1] != r[j-1]),  D[i][j-1] + 1,
+//                 D[i-1][j] + 1 - [j == m && i-1 >= L - 2*eo])
+// for the unit costs match = 0, mismatch = 1.
+//
+// Fill: bit-parallel over a diagonal band.  For read column j the band holds
+// rows j - k + b for bit b in [0, BITS) (BITS = 32 or 64).  Every cell whose
+// value is <= k lies on a diagonal d = i - j in [-k, 2*so + k] (the value of
+// a cell is at least j - i, and at least i - j - 2*so off the last column),
+// so this band holds all of them whenever 2*so + k <= BITS - 1 - k.  Each
+// column is one step of the Myers/Hyyro vertical-delta recurrence, the
+// previous column's vectors shifted down one bit to follow the diagonal.
+// Cells outside the band enter as "+1 from a neighbour" (the cost of a real
+// path), so every band value is an upper bound and is exact when <= k.
+// Rows above row 0 are virtual (D[-r][j] = j + r), which gives row 0 = j.
+//
+// The last read column has free vertical moves below row L - 2*eo and is
+// evaluated with explicit values from the band of column m-1.
+//
+// For every band cell the traceback decision of the reference
+// (src/cuda-functions.cu:215-276) is recorded as 2 bits:
+//   DIAG if D[i-1][j-1] + 1 == v, or D[i-1][j-1] == v and the bytes match
+//   UP   else if D[i-1][j] + 1 - corr == v
+//   LEFT else if D[i][j-1] + 1 == v
+//   STOP otherwise
+// with corr = 1 on the last column below row L - 2eo and, when so != 0, on
+// the first column for rows <= 2so + 3 (src/cuda-functions.cu:181-190).
+// The traceback only visits cells with value <= k, where these decisions
+// equal the reference's: a neighbour that is > k (exact or bound) fails the
+// equality tests either way.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define SARU_HD __host__ __device__ __forceinline__
+#else
+#define SARU_HD inline
+#endif
+
+namespace saru {
+
+enum : int { OP_STOP = 0, OP_DIAG = 1, OP_UP = 2, OP_LEFT = 3 };
+
+// read-byte classes: A C G T, then up to MAX_EXTRA other bytes of the read
+constexpr int MAX_EXTRA = 4;
+constexpr int NCODES = 4 + MAX_EXTRA;
+
+SARU_HD uint32_t fshr32(uint32_t lo, uint32_t hi, uint32_t s) {
+#if defined(__CUDA_ARCH__)
+  return __funnelshift_r(lo, hi, s);
+#else
+  s &= 31;
+  return s ? (lo >> s) | (hi << (32 - s)) : lo;
+#endif
+}
+
+template <typename T>
+SARU_HD T lowmask(int n) {
+  constexpr int BITS = int(sizeof(T) * 8);
+  return n <= 0 ? T(0) : (n >= BITS ? ~T(0) : ((T(1) << n) - T(1)));
+}
+
+// bits [j, j + BITS) of a packed mask (words of 32 bits)
+template <typename T>
+SARU_HD T window_bits(const uint32_t *mask, int j);
+
+template <>
+SARU_HD uint32_t window_bits<uint32_t>(const uint32_t *mask, int j) {
+  int w = j >> 5;
+  return fshr32(mask[w], mask[w + 1], (uint32_t)j & 31u);
+}
+
+template <>
+SARU_HD uint64_t window_bits<uint64_t>(const uint32_t *mask, int j) {
+  int w = j >> 5;
+  uint32_t s = (uint32_t)j & 31u;
+  uint32_t lo = fshr32(mask[w], mask[w + 1], s);
+  uint32_t hi = fshr32(mask[w + 1], mask[w + 2], s);
+  return (uint64_t)lo | ((uint64_t)hi << 32);
+}
+
+SARU_HD int base_code(uint8_t c) {
+  switch (c) {
+    case 'A': return 0;
+    case 'C': return 1;
+    case 'G': return 2;
+    case 'T': return 3;
+    default: return -1;
+  }
+}
+
+// Number of 32-bit mask words per read class for a window of length L.
+SARU_HD int mask_words(int k, int L) { return ((k + 1 + L + 64) >> 5) + 1; }
+
+// Per-candidate scalar description.
+struct Cand {
+  int m, L, k, so, eo;
+  bool first_of_call;  // candidate 0 of a reference call: traceback stops on row 0
+};
+
+SARU_HD void flank_of(int dir, int k, int &so, int &eo) {
+  so = 0;
+  eo = 0;
+  switch (dir) {
+    case 1: case 5: eo = k; break;
+    case 2: case 6: so = k; break;
+    case 3: case 7: so = k; eo = k; break;
+    default: break;
+  }
+}
+
+// Builds the read-class codes (4 bits each, 8 per word) and the window
+// masks: bit (p + k + 1) of mask[c] is set iff window byte p belongs to
+// class c.  Returns false if the read has more than MAX_EXTRA distinct
+// non-ACGT bytes.  Reader/Writer abstract where bytes and words live.
+template <class ReadFn, class WinFn>
+SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, uint32_t *codes, uint32_t *mask,
+                         int mwords) {
+  uint8_t extra[MAX_EXTRA];
+  int nextra = 0;
+  for (int w = 0; w < (c.m + 7) / 8; ++w) codes[w] = 0;
+  for (int j = 0; j < c.m; ++j) {
+    uint8_t ch = rd(j);
+    int code = base_code(ch);
+    if (code < 0) {
+      int e = 0;
+      while (e < nextra && extra[e] != ch) ++e;
+      if (e == nextra) {
+        if (nextra == MAX_EXTRA) return false;
+        extra[nextra++] = ch;
+      }
+      code = 4 + e;
+    }
+    codes[j >> 3] |= (uint32_t)code << ((j & 7) * 4);
+  }
+  for (int w = 0; w < NCODES * mwords; ++w) mask[w] = 0;
+  for (int p = 0; p < c.L; ++p) {
+    uint8_t ch = wn(p);
+    int code = base_code(ch);
+    if (code < 0) {
+      code = -1;
+      for (int e = 0; e < nextra; ++e)
+        if (extra[e] == ch) code = 4 + e;
+      if (code < 0) continue;
+    }
+    int bit = p + c.k + 1;
+    mask[code * mwords + (bit >> 5)] |= 1u << (bit & 31);
+  }
+  return true;
+}
+
+SARU_HD int code_at(const uint32_t *codes, int j) { return (codes[j >> 3] >> ((j & 7) * 4)) & 15; }
+
+// Fill of one candidate.  `planes(j, A, B)` receives the decision planes of
+// read column j (1..m): code = A | 2B per band bit.  Returns D[L][m] if it
+// is <= k, otherwise k + 1.
+template <typename T, class PlaneSink>
+SARU_HD int fill_band(const Cand &c, const uint32_t *codes, const uint32_t *mask, int mwords,
+                      PlaneSink planes) {
+  constexpr int BITS = int(sizeof(T) * 8);
+  const int k = c.k, m = c.m;
+  // column 0: rows b - k; dv = -1 for rows <= 0, 0 for rows 1..2so, +1 after
+  T Mv = lowmask<T>(k + 1);
+  T Pv = ~lowmask<T>(k + 2 * c.so + 1);
+  int top = k;  // D[j - k][j] for the current column j (virtual rows: j + (k - j))
+  const T TOPBIT = T(1) << (BITS - 1);
+  // first-column quirk: rows <= 2so+3 <=> bits <= 2so + k + 2
+  const T col1_corr = c.so ? lowmask<T>(2 * c.so + k + 3) : T(0);
+  for (int j = 1; j < m; ++j) {
+    const T pv = (Pv >> 1) | TOPBIT;
+    const T mv = Mv >> 1;
+    const T eq = window_bits<T>(mask + code_at(codes, j - 1) * mwords, j);
+    const T xh = (((eq & pv) + pv) ^ pv) | eq;
+    const T d0 = xh | mv;
+    const T hp = mv | ~(d0 | pv);
+    const T hn = pv & d0;
+    const T hp1 = (hp << 1) | T(1);
+    const T hn1 = hn << 1;
+    Pv = hn1 | ~(d0 | hp1);
+    Mv = hp1 & d0;
+    const T diag = ~d0 | eq;
+    T up = Pv;
+    if (j == 1) up = (Pv & ~col1_corr) | (~(Pv | Mv) & col1_corr);
+    const T A = diag | (~up & hp);
+    const T B = ~diag & (up | hp);
+    planes(j, A, B);
+    top += (int)((~d0) & T(1));
+  }
+  // column m with explicit values; column m-1 band values from the deltas
+  int vprev[BITS + 1];
+  {
+    int v = top;
+    vprev[0] = v;
+    for (int b = 1; b < BITS; ++b) {
+      v += (int)((Pv >> b) & T(1)) - (int)((Mv >> b) & T(1));
+      vprev[b] = v;
+    }
+    vprev[BITS] = vprev[BITS - 1] + 1;
+  }
+  const T eqm = window_bits<T>(mask + code_at(codes, m - 1) * mwords, m);
+  const int bmax = c.L - m + k;  // band bit of row L in column m
+  T A = 0, B = 0;
+  int vcur_prev = vprev[0] + 1;  // D[m - k - 1][m], entering from the left
+  int score = k + 1;
+  for (int b = 0; b <= bmax && b < BITS; ++b) {
+    const int row = m - k + b;
+    const int dg = vprev[b], lf = vprev[b + 1], tp = vcur_prev;
+    const bool e = (eqm >> b) & T(1);
+    const int corr = (row - 1 >= c.L - 2 * c.eo) ? 1 : 0;
+    int v = dg + (e ? 0 : 1);
+    if (lf + 1 < v) v = lf + 1;
+    if (tp + 1 - corr < v) v = tp + 1 - corr;
+    int op;
+    if (dg + 1 == v || (dg == v && e)) op = OP_DIAG;
+    else if (tp + 1 - corr == v) op = OP_UP;
+    else if (lf + 1 == v) op = OP_LEFT;
+    else op = OP_STOP;
+    A |= T(op & 1) << b;
+    B |= T(op >> 1) << b;
+    vcur_prev = v;
+    if (b == bmax) score = v;
+  }
+  planes(m, A, B);
+  return score <= k ? score : k + 1;
+}
+
+// Traceback from (L, m).  plane(j, b) returns the 2-bit decision of band bit
+// b in column j.  emit(op, row, col) is called per step in traceback order
+// (from the alignment end) with the cell the step leaves.  Returns the
+// number of steps.
+template <class PlaneFn, class EmitFn>
+SARU_HD int traceback_band(const Cand &c, PlaneFn plane, EmitFn emit) {
+  int row = c.L, col = c.m, n = 0;
+  for (;;) {
+    int op;
+    if (col == 0) {
+      // column 0 holds max(0, row - 2so); only the vertical test can hold
+      if (row == 0) break;
+      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
+      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
+      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
+      op = (tp + 1 - corr == v) ? OP_UP : OP_STOP;
+    } else if (row == 0) {
+      // row 0 holds j.  The first candidate of a call leaves the loop here;
+      // the others see the previous matrix's last row as their diagonal and
+      // top neighbours, all > k when m > 3k, so only the left step holds.
+      op = c.first_of_call ? OP_STOP : OP_LEFT;
+    } else {
+      op = plane(col, row - col + c.k);
+    }
+    if (op == OP_STOP) break;
+    emit(op, row, col);
+    ++n;
+    if (op == OP_DIAG) {
+      --row;
+      --col;
+    } else if (op == OP_UP) {
+      --row;
+    } else {
+      --col;
+    }
+  }
+  return n;
+}
+
+}  // namespace saru
+
+namespace saru {
+
+// Maximum traceback length for a candidate: every step consumes a row or a
+// column, and a path of value <= k makes at most k left steps.
+SARU_HD int max_steps(const Cand &c) { return c.L + c.k; }
+
+// Writes the reference's slot bytes for one traceback: ops[0..n) in
+// traceback order (2 bits each, 16 per word), replayed from the cell where
+// the traceback stopped so the strings come out in reading order, as the
+// reference's in-place reversal leaves them (src/cuda-functions.cu:306-307).
+template <class ReadFn, class WinFn, class OutFn>
+SARU_HD void emit_forward(const Cand &c, const uint32_t *ops, int n, ReadFn rd, WinFn wn,
+                          OutFn out) {
+  int row = c.L, col = c.m;
+  for (int s = 0; s < n; ++s) {
+    int op = (ops[s >> 4] >> ((s & 15) * 2)) & 3;
+    if (op == OP_DIAG) { --row; --col; }
+    else if (op == OP_UP) { --row; }
+    else { --col; }
+  }
+  // (row, col) is now the cell after the last step; walk back up the path
+  for (int s = n - 1; s >= 0; --s) {
+    int op = (ops[s >> 4] >> ((s & 15) * 2)) & 3;
+    int r0 = row, c0 = col;
+    if (op == OP_DIAG) { r0 = row + 1; c0 = col + 1; }
+    else if (op == OP_UP) { r0 = row + 1; }
+    else { c0 = col + 1; }
+    uint8_t a = op == OP_UP ? (uint8_t)'_' : rd(c0 - 1);
+    uint8_t b = op == OP_LEFT ? (uint8_t)'_' : wn(r0 - 1);
+    out(n - 1 - s, a, b);
+    row = r0;
+    col = c0;
+  }
+}
+
+}  // namespace saru
