@@ -1,0 +1,440 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 alignment stage (libsaruman_b200.so).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2|c1|c4]
+
+Metric: candidate alignments per second (every candidate pair aligned,
+including those that score above k), with GCUPS (rectangle cells m*L per
+second) beside it.  Default workload: the microbial-scale configuration --
+5 Mbp seeded genome at 50 % GC with 40 repeat families of 1.5 kbp (5-50
+copies, 99 % identity), 2M reads of 100 bp from both strands with 3 % errors
+(70/15/15), k = 5; candidate windows are placed where the reference's q-gram
+filter places them (read origin, plus the same offset in every other copy of
+a repeat family), ~9.5 candidates per read as the reference's filter gives
+on this genome.  Synthetic data: there is no network for real data.
+
+One step aligns one such batch.  `value` times saru_align_device on inputs
+already resident in HBM (one kernel launch per step; inputs ~4 GB, larger
+than L2, so no flush is needed).  `e2e` times the same batch through the
+public API with host buffers: pinned H2D of the inputs, the kernel, D2H of
+the scores and both alignment-slot arrays, every step.
+
+With torchrun (N > 1) each rank aligns its own batch (replicas, weak
+scaling); rank 0 prints the max-over-ranks timing.  `--impl reference` times
+the reference's own alignment code (src/cuda-functions.cu compiled for the
+host, oracle/_ref) on all host cores over a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    "c2": dict(workload="microbial-scale plain kernel: 5 Mbp repeat-rich genome, 2M reads x 100 bp, "
+               "3% errors, k=5", genome=("repeat", 5_000_000, 201, "uniform"), reads=2_000_000,
+               m=100, k=5, rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0),
+    "c1": dict(workload="small: 1 Mbp uniform genome, 100k reads x 36 bp, 2% errors, k=2",
+               genome=("uniform", 1_000_000, 101), reads=100_000, m=36, k=2, rate=0.02,
+               mix=(0.70, 0.15, 0.15), unmapped=0.0),
+    "c4": dict(workload="long-read-end stress: 10 Mbp uniform genome, 1M reads x 250 bp, 4% errors "
+               "(60/20/20), 5% unmapped, k=15", genome=("uniform", 10_000_000, 401),
+               reads=1_000_000, m=250, k=15, rate=0.04, mix=(0.60, 0.20, 0.20), unmapped=0.05),
+}
+
+
+def build_batch(cfg: dict, rank: int):
+    from saruman_b200 import workloads as W
+    gs = cfg["genome"]
+    if gs[0] == "uniform":
+        g, rmap = W.uniform_genome(gs[1], seed=gs[2]), None
+    else:
+        g, rmap = W.repeat_genome_with_map(gs[1], seed=gs[2], copies=gs[3])
+    rd = W.sample_reads(g, cfg["reads"], cfg["m"], cfg["rate"], seed=1000 + rank, mix=cfg["mix"],
+                        unmapped=cfg["unmapped"])
+    return W.synthetic_candidates(g, rd, cfg["m"], cfg["k"], seed=2000 + rank, repeats=rmap)
+
+
+def band_cells(b) -> int:
+    """Cells of the band that must be evaluated per candidate: m*(2k+1)
+    when only the end gap is free (so = 0), m*(4k+1) otherwise."""
+    so_free = np.isin(b.dirs, (2, 3, 6, 7))
+    per = np.where(so_free, b.m * (4 * b.k + 1), b.m * (2 * b.k + 1))
+    return int(per.sum())
+
+
+def rect_cells(b) -> int:
+    return int((b.m * b.lengths).sum())
+
+
+def algorithmic_bytes(b) -> int:
+    """Bytes the stage must move per batch: read and window bytes, 9 bytes
+    of offsets/flag per candidate in, 4-byte score and both alignment slots
+    out."""
+    return int(len(b.reads) + len(b.genome) + 9 * b.n + 4 * b.n + 2 * b.total_genome)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.3)
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self) -> dict:
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+def profile_traffic() -> dict | None:
+    """DRAM bytes per candidate of the banded kernel from the committed ncu
+    summary (profiles/band_kernel_c2.json), if present."""
+    p = ROOT / "profiles" / "band_kernel_c2.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            return None
+    return None
+
+
+class Chunker:
+    """Consecutive sub-batches of a batch, each re-based as a call of its
+    own (the layout the reference's host code would build for it)."""
+
+    def __init__(self, b):
+        from saruman_b200 import workloads as W
+        self.b = b
+        self.W = W
+        self.L = b.lengths.astype(np.int64)
+        self.gend = np.cumsum(self.L)
+
+    def take(self, start: int, count: int):
+        b, W = self.b, self.W
+        e = min(b.n, start + count)
+        gs = int(self.gend[start - 1]) if start else 0
+        ge = int(self.gend[e - 1])
+        Ls = self.L[start:e]
+        go = np.cumsum(Ls).astype(np.int32)
+        ro = ((np.arange(e - start) + 1) * b.m).astype(np.int32)
+        esz = (b.m + 1) * (Ls + 1)
+        eo = (np.cumsum(esz) - esz).astype(np.int32)
+        return W.Batch(m=b.m, k=b.k, genome=b.genome[gs:ge], reads=b.reads[start * b.m:e * b.m],
+                       genome_offsets=go, read_offsets=ro, edit_offsets=eo, dirs=b.dirs[start:e],
+                       ids=b.ids[start:e], pos=b.pos[start:e])
+
+
+def cpu_reference_rate(b, seconds: float = 10.0, nthreads: int | None = None,
+                       chunker: Chunker | None = None) -> dict:
+    """The reference's own kernel code on the host (oracle/_ref), all host
+    threads, over consecutive sub-batches of the workload until `seconds`."""
+    import ctypes as C
+    lib_path = ROOT / "oracle" / "_ref" / "libref_emul.so"
+    if not lib_path.exists():
+        return {"value": None, "unavailable": "oracle/_ref/libref_emul.so not built"}
+    lib = C.CDLL(str(lib_path))
+    lib.ref_align_batch.restype = C.c_int
+    nthreads = nthreads or os.cpu_count() or 1
+    ch = chunker or Chunker(b)
+    P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    done = 0
+    chunk = max(2000, 500 * nthreads)
+    start = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds and start < b.n:
+        sb = ch.take(start, chunk)
+        sc = np.zeros(sb.n, np.int32)
+        ra = np.zeros(sb.total_genome + 64, np.uint8)
+        ga = np.zeros(sb.total_genome + 64, np.uint8)
+        rc = lib.ref_align_batch(C.c_int(0), C.c_int(1), P(sb.genome), P(sb.reads),
+                                 P(sb.genome_offsets), P(sb.read_offsets), P(sb.edit_offsets),
+                                 C.c_int(sb.n), P(sb.dirs), C.c_int(sb.k),
+                                 C.c_size_t(sb.total_genome), C.c_int(0), C.c_int(nthreads),
+                                 C.c_int(256), P(sc), P(ra), P(ga))
+        if rc != 0:
+            return {"value": None, "unavailable": "reference host run failed"}
+        done += sb.n
+        start += sb.n
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "cores": nthreads, "candidates": done, "seconds": dt}
+
+
+def run_reference_arm(args, cfg, rank: int) -> None:
+    if rank != 0:
+        return
+    b = build_batch(cfg, 0)
+    ch = Chunker(b)
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_rate(b, seconds=args.ref_seconds, chunker=ch)
+        if r.get("value") is None:
+            print(json.dumps({"impl": "reference", "unavailable": r.get("unavailable")}))
+            return
+        if i >= args.warmup:
+            per_step.append(r)
+    cand = sum(r["candidates"] for r in per_step)
+    secs = sum(r["seconds"] for r in per_step)
+    value = cand / secs
+    line = {
+        "impl": "reference", "metric": "alignments/s", "value": value, "unit": "alignments/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * secs / len(per_step), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "sample": "consecutive sub-batches of the "
+                   f"workload, {args.ref_seconds:.0f} s of host work per step"},
+        "cpu_baseline": {"value": value, "unit": "alignments/s", "cores": per_step[0]["cores"],
+                         "kind": "reference", "sample": f"{cand} candidates"},
+        "e2e": {"value": value, "unit": "alignments/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, cfg, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import saruman_b200 as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    b = build_batch(cfg, rank)
+    lib = S.load()
+    # inputs and outputs resident in HBM
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    g_d, r_d, go_d, ro_d, dir_d = (T(b.genome), T(b.reads), T(b.genome_offsets),
+                                   T(b.read_offsets), T(b.dirs))
+    scores = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    nscr = S.scratch_bytes(b.n, b.m, b.k)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
+    sb = S.SaruBatch(g_d.data_ptr(), r_d.data_ptr(), go_d.data_ptr(), ro_d.data_ptr(),
+                     dir_d.data_ptr(), b.n, b.k, 0, 1, 1, b.m, len(b.genome), b.total_genome)
+    sr = S.SaruResult(scores.data_ptr(), ra.data_ptr(), ga.data_ptr(), status.data_ptr())
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+
+    int_peak = S.int32_issue_peak() if rank == 0 else None
+
+    def step():
+        S.align_device(sb, sr, scratch.data_ptr(), nscr, sptr)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    stream.synchronize()
+    if int(status.item()) != 0:
+        raise SystemExit(f"kernel status {int(status.item())}")
+
+    # ---- device-resident timing ------------------------------------------
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = S.kernel_launches()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = S.kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * b.n / (ms_step * 1e-3)
+
+    # ---- end to end through the public API, host buffers ----------------
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    hg, hr, hgo, hro, hdir = pin(b.genome), pin(b.reads), pin(b.genome_offsets), pin(
+        b.read_offsets), pin(b.dirs)
+    hs = torch.empty(b.n, dtype=torch.int32).pin_memory()
+    hra = torch.empty(b.total_genome, dtype=torch.uint8).pin_memory()
+    hga = torch.empty(b.total_genome, dtype=torch.uint8).pin_memory()
+    h2d = sum(int(x.numel() * x.element_size()) for x in (hg, hr, hgo, hro, hdir))
+    d2h = int(hs.numel() * 4 + hra.numel() + hga.numel())
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            g_d.copy_(hg, non_blocking=True)
+            r_d.copy_(hr, non_blocking=True)
+            go_d.copy_(hgo, non_blocking=True)
+            ro_d.copy_(hro, non_blocking=True)
+            dir_d.copy_(hdir, non_blocking=True)
+            step()
+            hs.copy_(scores, non_blocking=True)
+            hra.copy_(ra[:b.total_genome], non_blocking=True)
+            hga.copy_(ga[:b.total_genome], non_blocking=True)
+
+    e2e_step()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    e1.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = world * b.n / (e_ms / e2e_steps * 1e-3)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    # ---- roofline --------------------------------------------------------
+    peaks = measured_peaks()
+    cells = band_cells(b)
+    ops = 6 * cells
+    achieved_ops = ops / (ms_step * 1e-3)
+    abytes = algorithmic_bytes(b)
+    prof = profile_traffic()
+    traffic = None
+    if prof and prof.get("dram_bytes_per_candidate"):
+        traffic = prof["dram_bytes_per_candidate"] * b.n
+    roofline = {
+        "bound": "int32",
+        "achieved": achieved_ops / 1e12, "peak": int_peak / 1e12 if int_peak and int_peak > 0 else None,
+        "unit": "Tops/s", "frac": (achieved_ops / int_peak) if int_peak and int_peak > 0 else None,
+        "traffic": traffic,
+        "peak_source": "measured live by saru_int32_issue_probe on this GPU",
+        "ops_per_candidate_definition": "band cells x 6 (m*(2k+1) or m*(4k+1) cells)",
+        "hbm": {"achieved_gbs": abytes / (ms_step * 1e-3) / 1e9,
+                "peak_gbs": peaks.get("hbm_gbs"),
+                "frac": abytes / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                "algorithmic_bytes_per_step": abytes,
+                "peak_source": "MEASURED_PEAKS.json" if not peaks.get("fallback") else "fallback"},
+    }
+    cpu = None
+    if world == 1:
+        r = cpu_reference_rate(b, seconds=args.cpu_seconds)
+        if r.get("value") is not None:
+            cpu = {"value": r["value"], "unit": "alignments/s", "cores": r["cores"],
+                   "kind": "reference",
+                   "sample": f"{r['candidates']} consecutive candidates of the workload, the "
+                             "reference's own kernel code compiled for the host"}
+        else:
+            cpu = {"value": None, "unavailable": r.get("unavailable")}
+    line = {
+        "metric": "alignments/s", "value": value, "unit": "alignments/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "candidates_per_step": b.n,
+                   "reads_per_step": cfg["reads"], "read_length": b.m, "k": b.k,
+                   "parallelism": f"replicas x{world}", "l2": "inputs 4+ GB > L2, no flush"},
+        "gcups_rect": world * rect_cells(b) / (ms_step * 1e-3) / 1e9,
+        "gpu_launches": int(launches),
+        "e2e": {"value": e2e_value, "unit": "alignments/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,154 @@
+/*
+ * saruman_b200.h -- C ABI of libsaruman_b200.so, a B200 (sm_100a) drop-in
+ * for the alignment stage of SARUMAN.
+ *
+ * Part 1 is the reference's own interface, unchanged, so the reference's
+ * host C (q-gram filter, candidate collection, src/hash.c:898-1111) links
+ * against this library instead of its src/cuda-functions.cu.
+ * Part 2 adds entry points with explicit arguments and return codes for
+ * callers that hold their batches in host or device memory themselves.
+ *
+ * Plain C types only; no CUDA or torch types appear in the signatures
+ * (streams are passed as void*).
+ */
+#ifndef SARUMAN_B200_H
+#define SARUMAN_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Part 1: the reference interface (src/cuda-functions.h:55-78).
+ * ---------------------------------------------------------------------- */
+
+/* Replaces cuda_needleman_wunsch (src/cuda-functions.h:55-63, implemented
+ * at src/cuda-functions.cu:584-1049).  Aligns sample_size candidates laid
+ * out as src/hash.c:1055-1059 builds them: windows back to back with
+ * genome_offsets their inclusive prefix sums, reads at read_offsets, one
+ * direction/flank flag each; error = k.  Prints one TSV line per candidate
+ * whose edit distance is <= k, in candidate order, exactly as the reference
+ * writer does (src/cuda-functions.cu:827-1006), updates the same counters
+ * and output-control arrays, and returns when the lines are written.  Safe
+ * to call from the forward (do_reverse = 0) and reverse (4) threads at once.
+ * Errors are reported on stderr and in saru_last_error(); the process is not
+ * terminated. */
+void cuda_needleman_wunsch(int match, int mismatch, char *genome_sequences_on_host,
+                           char *read_sequences_on_host, int *genome_offsets, int *read_offsets,
+                           int *edit_offsets, int sample_size, int *read_id_array,
+                           int *genome_pos_array, char *direction_array, int error,
+                           size_t total_genome_array_size, size_t total_read_sequence_array_size,
+                           size_t total_edit_matrix_size, int do_reverse);
+
+/* Replaces cuda_allocate_memory (src/cuda-functions.h:65-67,
+ * src/cuda-functions.cu:541-562): selects GPU use_gpu_value and prepares the
+ * stream and buffers of the forward (do_reverse != 4) or reverse (4) caller.
+ * Device memory grows on demand instead of taking cuda_memory_per_thread up
+ * front. */
+void cuda_allocate_memory(int do_reverse);
+
+/* Replaces cuda_free_memory (src/cuda-functions.h:69-71,
+ * src/cuda-functions.cu:564-575): releases the reverse caller's resources if
+ * do_reverse != 0, else the forward caller's. */
+void cuda_free_memory(int do_reverse);
+
+/* Replaces get_cuda_infos (src/cuda-functions.h:77-78,
+ * src/cuda-functions.cu:1051-1120): lists the GPUs on stderr, selects the
+ * one with the most free memory unless use_gpu_value names one, and returns
+ * that free memory in bytes.  Exits(1) like the reference when no GPU has
+ * 128 MB free. */
+unsigned long int get_cuda_infos(void);
+
+/* Defined by the reference's CUDA module (src/cuda-functions.cu:61) and read
+ * by its driver (src/saruman.c:321-397): milliseconds spent aligning, per
+ * strand (0 forward, 1 reverse).  This library accumulates into it. */
+extern float alignment_time[2];
+
+/* ------------------------------------------------------------------------
+ * Part 2: batch entry points (no counterpart in the reference; they take the
+ * same call layout with explicit arguments and return 0 or a SARU_E* code).
+ * ---------------------------------------------------------------------- */
+
+#define SARU_OK 0
+#define SARU_E_INVALID 1     /* malformed batch (offsets, lengths, sizes) */
+#define SARU_E_CUDA 2        /* CUDA runtime error */
+#define SARU_E_NOMEM 3       /* device or host allocation failed */
+#define SARU_E_OVERFLOW 4    /* a traceback left its slot (order-dependent in the reference) */
+
+/* One call's candidates in the reference layout.  All pointers are either
+ * all host or all device pointers, depending on the entry point. */
+typedef struct {
+  const char *genome;           /* windows back to back, genome_offsets[n-1] bytes */
+  const char *reads;            /* read bytes, read_offsets[n-1] bytes */
+  const int32_t *genome_offsets;/* inclusive prefix sums of the window lengths */
+  const int32_t *read_offsets;  /* inclusive prefix sums of the read lengths */
+  const int8_t *dirs;           /* direction/flank flags */
+  int32_t n;                    /* candidates */
+  int32_t k;                    /* error threshold */
+  int32_t match, mismatch;      /* DP costs */
+  int32_t first_of_call;        /* 1 if candidate 0 opens a reference call (its
+                                   traceback stops on row 0); 0 if the batch
+                                   continues an earlier one */
+  int32_t max_read_length;      /* upper bound of the read lengths (device entry
+                                   point; the host entry point computes it) */
+  int64_t genome_bytes;         /* genome_offsets[n-1] */
+  int64_t total_slots;          /* sum(L_t + k): size of each alignment array */
+} saru_batch;
+
+typedef struct {
+  int32_t *scores;              /* n: D[L][m] when <= k, else k + 1 */
+  char *read_aln;               /* total_slots bytes, reference slot layout */
+  char *genome_aln;             /* total_slots bytes */
+  int32_t *status;              /* optional (device entry point): OR of SARU_S_* */
+} saru_result;
+
+/* Status bits the device entry point ORs into result->status. */
+#define SARU_S_IRREGULAR 1  /* a window is not m + so + eo long, or m <= 3k */
+#define SARU_S_ALPHABET 2   /* a read holds more than 4 distinct non-ACGT bytes */
+#define SARU_S_OVERFLOW 4   /* a traceback left its band */
+
+/* Host buffers in, host buffers out: copies the batch to the GPU, aligns it
+ * and copies back the scores and both alignment-slot arrays exactly as the
+ * reference leaves them after its device-to-host copies
+ * (src/cuda-functions.cu:807-824).  Prints nothing.  `lane` (0 or 1)
+ * selects one of two independent streams/buffer sets. */
+int saru_align_host(const saru_batch *batch, saru_result *result, int lane);
+
+/* Device buffers in and out, enqueued on `stream` (a cudaStream_t, may be
+ * NULL for the legacy stream).  Returns after enqueueing; completion is
+ * ordered on the stream.  Runs the banded kernel only (unit costs, k <= 15,
+ * one read length m > 3k with m <= max_read_length <= 512); candidates it
+ * cannot take are reported in result->status, with score k + 1.  `scratch`
+ * must hold saru_scratch_bytes(n, max_read_length, k, k > 7) bytes of
+ * device memory.  Enqueues no allocation, so it can be captured in a CUDA
+ * graph. */
+int saru_align_device(const saru_batch *batch, saru_result *result, void *scratch,
+                      size_t scratch_bytes, void *stream);
+
+/* Device scratch the banded kernel needs for a batch (bytes). */
+size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
+
+/* Formats the reference's TSV lines for one aligned call into `out`
+ * (capacity cap) and returns the bytes needed.  names: n_names entries of
+ * name_stride bytes, indexed by read id. */
+int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
+                        const int32_t *read_ids, const int32_t *genome_pos, int32_t read_length,
+                        const char *names, int32_t name_stride, int32_t n_names, char *out,
+                        int64_t cap, int32_t *done_fwd, int32_t *done_rev);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char *saru_last_error(void);
+
+/* Number of kernels this library has launched (for accounting). */
+uint64_t saru_kernel_launches(void);
+
+/* Diagnostics: 32-bit integer operations per second the current GPU
+ * sustains on independent logic/add/shift chains at full occupancy (the
+ * denominator of the banded kernel's roofline); -1 on error. */
+double saru_int32_issue_probe(int iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,182 @@
+"""saruman_b200 -- B200 (sm_100a) alignment stage of SARUMAN behind its C ABI.
+
+The product is libsaruman_b200.so (built in-tree by saruman_b200.build):
+CUDA kernels plus the reference's four entry points (cuda_needleman_wunsch,
+cuda_allocate_memory, cuda_free_memory, get_cuda_infos; see
+include/saruman_b200.h).  This module is a thin ctypes view of that library
+for Python callers (tests, bench, the serving loop).  There is no Python or
+CPU implementation of the alignment: if the library is missing, loading
+fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from pathlib import Path
+
+import numpy as np
+
+from .workloads import Batch
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libsaruman_b200.so"
+
+SARU_OK, SARU_E_INVALID, SARU_E_CUDA, SARU_E_NOMEM, SARU_E_OVERFLOW = 0, 1, 2, 3, 4
+SARU_S_IRREGULAR, SARU_S_ALPHABET, SARU_S_OVERFLOW = 1, 2, 4
+
+# symbols include/saruman_b200.h declares
+ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_memory",
+                 "get_cuda_infos", "saru_align_host", "saru_align_device", "saru_scratch_bytes",
+                 "saru_format_tsv", "saru_last_error", "saru_kernel_launches",
+                 "saru_int32_issue_probe")
+ABI_DATA = ("alignment_time",)
+
+
+class SaruError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"saruman_b200 error {code}: {msg}")
+        self.code = code
+
+
+class SaruBatch(C.Structure):
+    _fields_ = [("genome", C.c_void_p), ("reads", C.c_void_p), ("genome_offsets", C.c_void_p),
+                ("read_offsets", C.c_void_p), ("dirs", C.c_void_p), ("n", C.c_int32),
+                ("k", C.c_int32), ("match", C.c_int32), ("mismatch", C.c_int32),
+                ("first_of_call", C.c_int32), ("max_read_length", C.c_int32),
+                ("genome_bytes", C.c_int64), ("total_slots", C.c_int64)]
+
+
+class SaruResult(C.Structure):
+    _fields_ = [("scores", C.c_void_p), ("read_aln", C.c_void_p), ("genome_aln", C.c_void_p),
+                ("status", C.c_void_p)]
+
+
+_lib = None
+
+
+def load(path: str | Path | None = None):
+    """Loads libsaruman_b200.so (in-tree).  Raises if it is not built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is not built; run `python -m saruman_b200.build` "
+                           "(there is no CPU fallback)")
+    lib = C.CDLL(str(p))
+    lib.saru_align_host.restype = C.c_int
+    lib.saru_align_host.argtypes = [C.POINTER(SaruBatch), C.POINTER(SaruResult), C.c_int]
+    lib.saru_align_device.restype = C.c_int
+    lib.saru_align_device.argtypes = [C.POINTER(SaruBatch), C.POINTER(SaruResult), C.c_void_p,
+                                      C.c_size_t, C.c_void_p]
+    lib.saru_scratch_bytes.restype = C.c_size_t
+    lib.saru_scratch_bytes.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int]
+    lib.saru_format_tsv.restype = C.c_int64
+    lib.saru_last_error.restype = C.c_char_p
+    lib.saru_kernel_launches.restype = C.c_uint64
+    lib.get_cuda_infos.restype = C.c_ulong
+    lib.saru_int32_issue_probe.restype = C.c_double
+    lib.saru_int32_issue_probe.argtypes = [C.c_int]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().saru_last_error().decode(errors="replace")
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def host_batch(b: Batch, first_of_call: bool = True) -> tuple[SaruBatch, list]:
+    """ctypes view of a host batch; the returned list keeps arrays alive."""
+    keep = [np.ascontiguousarray(b.genome, np.uint8), np.ascontiguousarray(b.reads, np.uint8),
+            np.ascontiguousarray(b.genome_offsets, np.int32),
+            np.ascontiguousarray(b.read_offsets, np.int32), np.ascontiguousarray(b.dirs, np.int8)]
+    sb = SaruBatch(_p(keep[0]), _p(keep[1]), _p(keep[2]), _p(keep[3]), _p(keep[4]), b.n, b.k,
+                   b.match, b.mismatch, 1 if first_of_call else 0, b.m, len(b.genome),
+                   b.total_genome)
+    return sb, keep
+
+
+@dataclasses.dataclass
+class AlignResult:
+    scores: np.ndarray      # int32, D[L][m] if <= k else k + 1
+    read_aln: np.ndarray    # uint8, sum(L + k), reference slot layout
+    genome_aln: np.ndarray  # uint8
+
+
+def align_host(b: Batch, lane: int = 0, first_of_call: bool = True,
+               out: AlignResult | None = None) -> AlignResult:
+    """Host arrays in, host arrays out (saru_align_host)."""
+    lib = load()
+    sb, keep = host_batch(b, first_of_call)
+    tot = b.total_genome
+    if out is None:
+        out = AlignResult(np.zeros(max(b.n, 1), np.int32), np.zeros(tot + 64, np.uint8),
+                          np.zeros(tot + 64, np.uint8))
+    res = SaruResult(_p(out.scores), _p(out.read_aln), _p(out.genome_aln), None)
+    rc = lib.saru_align_host(C.byref(sb), C.byref(res), lane)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+    return AlignResult(out.scores[:b.n], out.read_aln[:tot], out.genome_aln[:tot])
+
+
+def scratch_bytes(n: int, max_m: int, k: int) -> int:
+    return int(load().saru_scratch_bytes(n, max_m, k, 1 if k > 7 else 0))
+
+
+def align_device(batch: SaruBatch, result: SaruResult, scratch_ptr: int, scratch_len: int,
+                 stream_ptr: int = 0) -> None:
+    """Device pointers in and out, enqueued on a stream (saru_align_device)."""
+    rc = load().saru_align_device(C.byref(batch), C.byref(result), scratch_ptr, scratch_len,
+                                  stream_ptr)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+
+
+def name_table(names: dict[int, bytes] | list[bytes], stride: int = 60) -> np.ndarray:
+    if isinstance(names, dict):
+        n = max(names) + 1 if names else 1
+        items = names.items()
+    else:
+        n = max(len(names), 1)
+        items = enumerate(names)
+    tab = np.zeros((n, stride), np.uint8)
+    for i, nm in items:
+        raw = nm[:stride - 1]
+        tab[i, :len(raw)] = np.frombuffer(raw, np.uint8)
+    return tab
+
+
+def format_tsv(b: Batch, r: AlignResult, names: np.ndarray, read_length: int | None = None,
+               first_of_call: bool = True) -> tuple[bytes, int, int]:
+    """The reference writer's TSV for an aligned call (saru_format_tsv):
+    (text, forward alignments, reverse alignments)."""
+    lib = load()
+    sb, keep = host_batch(b, first_of_call)
+    scores = np.ascontiguousarray(r.scores, np.int32)
+    ra = np.concatenate([np.ascontiguousarray(r.read_aln, np.uint8), np.zeros(64, np.uint8)])
+    ga = np.concatenate([np.ascontiguousarray(r.genome_aln, np.uint8), np.zeros(64, np.uint8)])
+    res = SaruResult(_p(scores), _p(ra), _p(ga), None)
+    ids = np.ascontiguousarray(b.ids, np.int32)
+    pos = np.ascontiguousarray(b.pos, np.int32)
+    rl = b.m if read_length is None else read_length
+    df, dr = C.c_int32(), C.c_int32()
+    args = [C.byref(sb), C.byref(res), C.c_void_p(_p(ids)), C.c_void_p(_p(pos)), C.c_int32(rl),
+            C.c_void_p(_p(names)), C.c_int32(names.shape[1]), C.c_int32(names.shape[0])]
+    need = lib.saru_format_tsv(*args, None, C.c_int64(0), C.byref(df), C.byref(dr))
+    buf = np.zeros(need + 1, np.uint8)
+    lib.saru_format_tsv(*args, C.c_void_p(_p(buf)), C.c_int64(need + 1), C.byref(df), C.byref(dr))
+    return buf[:need].tobytes(), df.value, dr.value
+
+
+def kernel_launches() -> int:
+    return int(load().saru_kernel_launches())
+
+
+def int32_issue_peak(iters: int = 4096) -> float:
+    """Measured 32-bit integer ops/s of the current GPU (see probe.cu)."""
+    return float(load().saru_int32_issue_probe(iters))

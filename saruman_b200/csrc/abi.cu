@@ -1,0 +1,645 @@
+// abi.cu -- host side of libsaruman_b200.so: the reference's C entry points
+// (include/saruman_b200.h part 1) and the batch entry points (part 2).
+//
+// Flow of one call (reference: src/cuda-functions.cu:586-1049):
+//   validate the call layout on the host and pick the kernel path
+//   H2D of windows, reads, offsets and flags on the caller's lane stream
+//   banded kernel (or the exact full-rectangle kernels) writes scores and
+//     the two alignment-slot arrays, zero-filled, in the reference layout
+//   D2H of scores and slots; the TSV writer runs on the host
+// Each lane (forward / reverse caller) owns a stream and grow-only device
+// buffers, so the two reference threads run concurrently without locks on
+// the GPU path.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <atomic>
+#include <chrono>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/saruman_b200.h"
+#include "kernels.cuh"
+#include "saru_core.cuh"
+#include "writer.h"
+
+// ---------------------------------------------------------------------------
+// Globals of the reference's host program.  The reference defines them in
+// its headers (src/saruman.h:55-66, src/util.h:312-343, src/cuda-functions.h
+// :31-32); a program linked from those sources supplies its own copies,
+// which take precedence over these through ELF symbol interposition.  These
+// definitions let the library load on its own (tests, other callers).
+// ---------------------------------------------------------------------------
+extern "C" {
+struct read_name_hash;
+struct read_name_hash *read_names = nullptr;
+unsigned short int read_length_value = 0;
+unsigned short int be_verbose_value = 0;
+unsigned short int use_gpu_value = 5000;
+unsigned long int cuda_memory_per_thread = 0;
+unsigned int forward_alignments_done = 0;
+unsigned int reverse_alignments_done = 0;
+unsigned int forward_alignment_candidates = 0;
+unsigned int reverse_alignment_candidates = 0;
+char *forward_output_control = nullptr;
+char *reverse_output_control = nullptr;
+char *main_alloc_ptr_for = nullptr;
+char *main_alloc_ptr_rev = nullptr;
+float alignment_time[2] = {0.f, 0.f};
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+std::mutex g_out_mu;  // stdout lines and the shared counters
+
+void set_error(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+#define SARU_CUDA(call)                                                            \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      set_error("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return SARU_E_CUDA;                                                          \
+    }                                                                              \
+  } while (0)
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= n) return SARU_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t want = bytes + bytes / 8 + 4096;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMalloc of %zu bytes failed", want);
+      return SARU_E_NOMEM;
+    }
+    n = want;
+    return SARU_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <typename T>
+  T *as() const {
+    return reinterpret_cast<T *>(p);
+  }
+};
+
+struct Lane {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf genome, reads, goff, roff, dirs, scores, ra, ga, scratch, status, eoff, arena;
+  int *status_host = nullptr;  // pinned
+  std::mutex mu;
+
+  int init(int dev) {
+    if (device == dev && stream) return SARU_OK;
+    SARU_CUDA(cudaSetDevice(dev));
+    SARU_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    SARU_CUDA(cudaEventCreate(&ev0));
+    SARU_CUDA(cudaEventCreate(&ev1));
+    SARU_CUDA(cudaMallocHost(&status_host, sizeof(int)));
+    device = dev;
+    return SARU_OK;
+  }
+  void release() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    for (DevBuf *b : {&genome, &reads, &goff, &roff, &dirs, &scores, &ra, &ga, &scratch, &status,
+                      &eoff, &arena})
+      b->release();
+    if (status_host) cudaFreeHost(status_host);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+    status_host = nullptr;
+    ev0 = ev1 = nullptr;
+    stream = nullptr;
+    device = -1;
+  }
+};
+
+Lane g_lanes[2];
+
+int current_device() {
+  int d = 0;
+  if (use_gpu_value < 5000) d = use_gpu_value;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return -1;
+  }
+  if (d >= count) d = 0;
+  return d;
+}
+
+int sm_count(int dev) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+// ---------------------------------------------------------------------------
+// path selection
+// ---------------------------------------------------------------------------
+
+struct Plan {
+  bool band = false;   // banded kernel
+  bool wide = false;   // 64-bit band
+  int max_m = 0;
+  int64_t total_cells = 0;  // full-rectangle arena cells
+};
+
+// Host-side check of a host batch: the banded kernel needs unit costs, one
+// read length m > 3k with m <= kMaxBandM, k <= 15, and windows of exactly
+// m + so + eo bytes (the layout src/hash.c:986-1059 builds).
+int plan_host(const saru_batch *b, Plan *pl) {
+  if (b->n < 0 || b->k < 0) {
+    set_error("invalid batch: n=%d k=%d", b->n, b->k);
+    return SARU_E_INVALID;
+  }
+  const int n = b->n, k = b->k;
+  int64_t prev_g = 0, prev_r = 0, cells = 0;
+  int m0 = -1;
+  bool uniform = true, regular = true, any_start_gap = false;
+  int max_m = 0;
+  for (int t = 0; t < n; ++t) {
+    const int64_t L = (int64_t)b->genome_offsets[t] - prev_g;
+    const int64_t m = (int64_t)b->read_offsets[t] - prev_r;
+    if (L <= 0 || m <= 0 || L > 32000 || m > 32000) {
+      set_error("invalid batch: candidate %d has window %lld, read %lld", t, (long long)L,
+                (long long)m);
+      return SARU_E_INVALID;
+    }
+    prev_g = b->genome_offsets[t];
+    prev_r = b->read_offsets[t];
+    if (m0 < 0) m0 = (int)m;
+    if (m != m0) uniform = false;
+    if (m > max_m) max_m = (int)m;
+    int so, eo;
+    saru::flank_of(b->dirs[t], k, so, eo);
+    if (so) any_start_gap = true;
+    if (L != m + so + eo) regular = false;
+    cells += (m + 1) * (L + 1);
+  }
+  if (n > 0 && (prev_g != b->genome_bytes || prev_g > INT32_MAX || prev_r > INT32_MAX)) {
+    set_error("invalid batch: genome_bytes %lld does not match offsets (%lld)",
+              (long long)b->genome_bytes, (long long)prev_g);
+    return SARU_E_INVALID;
+  }
+  if (b->total_slots != prev_g + (int64_t)k * n) {
+    set_error("invalid batch: total_slots %lld != sum(L + k) = %lld", (long long)b->total_slots,
+              (long long)(prev_g + (int64_t)k * n));
+    return SARU_E_INVALID;
+  }
+  pl->max_m = max_m;
+  pl->total_cells = cells;
+  pl->band = b->match == 0 && b->mismatch == 1 && uniform && regular && k <= 15 &&
+             max_m > 3 * k && max_m <= saru::kMaxBandM && max_m >= 2;
+  pl->wide = k > 7 && any_start_gap;
+  return SARU_OK;
+}
+
+constexpr int kCta = 128;
+
+long band_grid(int dev, int n) {
+  // persistent grid: resident CTAs of the whole GPU
+  const long tiles = (n + kCta - 1) / kCta;
+  long g = (long)sm_count(dev) * 4;
+  return tiles < g ? tiles : g;
+}
+
+size_t band_scratch_bytes(long grid, int max_m, bool wide) {
+  return (size_t)grid * kCta * 2 * (size_t)(max_m + 1) * (wide ? 8 : 4);
+}
+
+// Enqueues the banded kernel on device buffers.
+int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
+             size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s) {
+  saru::KernelArgs a{};
+  a.genome = reinterpret_cast<const uint8_t *>(b->genome);
+  a.reads = reinterpret_cast<const uint8_t *>(b->reads);
+  a.goff = b->genome_offsets;
+  a.roff = b->read_offsets;
+  a.dirs = b->dirs;
+  a.n = b->n;
+  a.k = b->k;
+  a.max_m = pl.max_m;
+  a.first_of_call = b->first_of_call;
+  a.wide = pl.wide;
+  a.grid = band_grid(dev, b->n);
+  a.scores = r->scores;
+  a.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
+  a.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
+  a.scratch = scratch;
+  a.status = status_dev;
+  if (band_scratch_bytes(a.grid, pl.max_m, pl.wide) > scratch_bytes) {
+    set_error("scratch too small: %zu < %zu", scratch_bytes,
+              band_scratch_bytes(a.grid, pl.max_m, pl.wide));
+    return SARU_E_INVALID;
+  }
+  if (b->n == 0) return SARU_OK;
+  SARU_CUDA(saru::launch_band_kernel(a, kCta, sm_count(dev), s));
+  g_launches.fetch_add(1);
+  return SARU_OK;
+}
+
+// Host batch -> device buffers of `lane`, returns device-side view.
+int upload(Lane &L, const saru_batch *b, saru_batch *db) {
+  const size_t n = (size_t)b->n;
+  int rc;
+  if ((rc = L.genome.ensure((size_t)b->genome_bytes + 64))) return rc;
+  if ((rc = L.reads.ensure((size_t)(n ? b->read_offsets[n - 1] : 0) + 64))) return rc;
+  if ((rc = L.goff.ensure(4 * n + 64))) return rc;
+  if ((rc = L.roff.ensure(4 * n + 64))) return rc;
+  if ((rc = L.dirs.ensure(n + 64))) return rc;
+  cudaStream_t s = L.stream;
+  if (n) {
+    SARU_CUDA(cudaMemcpyAsync(L.genome.p, b->genome, (size_t)b->genome_bytes, cudaMemcpyHostToDevice, s));
+    SARU_CUDA(cudaMemcpyAsync(L.reads.p, b->reads, (size_t)b->read_offsets[n - 1], cudaMemcpyHostToDevice, s));
+    SARU_CUDA(cudaMemcpyAsync(L.goff.p, b->genome_offsets, 4 * n, cudaMemcpyHostToDevice, s));
+    SARU_CUDA(cudaMemcpyAsync(L.roff.p, b->read_offsets, 4 * n, cudaMemcpyHostToDevice, s));
+    SARU_CUDA(cudaMemcpyAsync(L.dirs.p, b->dirs, n, cudaMemcpyHostToDevice, s));
+  }
+  *db = *b;
+  db->genome = L.genome.as<const char>();
+  db->reads = L.reads.as<const char>();
+  db->genome_offsets = L.goff.as<const int32_t>();
+  db->read_offsets = L.roff.as<const int32_t>();
+  db->dirs = L.dirs.as<const int8_t>();
+  return SARU_OK;
+}
+
+// The exact full-rectangle path on lane buffers (whole call).
+int run_full(Lane &L, const saru_batch *hb, const saru_batch *db, const Plan &pl,
+             const saru_result *dr) {
+  const size_t n = (size_t)hb->n;
+  int rc;
+  std::vector<int64_t> eoff(n);
+  int64_t acc = 0;
+  for (size_t t = 0; t < n; ++t) {
+    eoff[t] = acc;
+    const int64_t L_ = (int64_t)hb->genome_offsets[t] - (t ? hb->genome_offsets[t - 1] : 0);
+    const int64_t m_ = (int64_t)hb->read_offsets[t] - (t ? hb->read_offsets[t - 1] : 0);
+    acc += (m_ + 1) * (L_ + 1);
+  }
+  if (acc > INT32_MAX) {
+    set_error("call too large for the reference's int cell index (%lld cells)", (long long)acc);
+    return SARU_E_INVALID;
+  }
+  if ((rc = L.eoff.ensure(8 * n + 64))) return rc;
+  if ((rc = L.arena.ensure(2 * (size_t)acc + 64))) return rc;
+  cudaStream_t s = L.stream;
+  SARU_CUDA(cudaMemcpyAsync(L.eoff.p, eoff.data(), 8 * n, cudaMemcpyHostToDevice, s));
+  SARU_CUDA(cudaMemsetAsync(dr->read_aln, 0, (size_t)hb->total_slots, s));
+  SARU_CUDA(cudaMemsetAsync(dr->genome_aln, 0, (size_t)hb->total_slots, s));
+  saru::FullArgs a{};
+  a.genome = reinterpret_cast<const uint8_t *>(db->genome);
+  a.reads = reinterpret_cast<const uint8_t *>(db->reads);
+  a.goff = db->genome_offsets;
+  a.roff = db->read_offsets;
+  a.dirs = db->dirs;
+  a.eoff = L.eoff.as<const int64_t>();
+  a.n = hb->n;
+  a.k = hb->k;
+  a.match = hb->match;
+  a.mismatch = hb->mismatch;
+  a.first_of_call = hb->first_of_call;
+  a.genome_bytes = hb->genome_bytes;
+  a.read_bytes = n ? hb->read_offsets[n - 1] : 0;
+  a.arena = L.arena.as<short>();
+  a.scores = dr->scores;
+  a.read_aln = reinterpret_cast<uint8_t *>(dr->read_aln);
+  a.genome_aln = reinterpret_cast<uint8_t *>(dr->genome_aln);
+  a.status = L.status.as<int>();
+  (void)pl;
+  SARU_CUDA(saru::launch_full_kernels(a, s));
+  g_launches.fetch_add(2);
+  return SARU_OK;
+}
+
+int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out) {
+  Plan pl;
+  int rc = plan_host(b, &pl);
+  if (rc) return rc;
+  const int dev = current_device();
+  if (dev < 0) {
+    set_error("no CUDA device");
+    return SARU_E_CUDA;
+  }
+  if ((rc = L.init(dev))) return rc;
+  SARU_CUDA(cudaSetDevice(dev));
+  if (b->n == 0) return SARU_OK;
+  cudaStream_t s = L.stream;
+  SARU_CUDA(cudaEventRecord(L.ev0, s));
+  saru_batch db;
+  if ((rc = upload(L, b, &db))) return rc;
+  const size_t n = (size_t)b->n;
+  if ((rc = L.scores.ensure(4 * n + 64))) return rc;
+  if ((rc = L.ra.ensure((size_t)b->total_slots + 64))) return rc;
+  if ((rc = L.ga.ensure((size_t)b->total_slots + 64))) return rc;
+  if ((rc = L.status.ensure(64))) return rc;
+  saru_result dr{L.scores.as<int32_t>(), L.ra.as<char>(), L.ga.as<char>(), L.status.as<int32_t>()};
+  SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
+  bool full = !pl.band;
+  if (pl.band) {
+    const long grid = band_grid(dev, b->n);
+    if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, pl.wide)))) return rc;
+    if ((rc = run_band(&db, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, s)))
+      return rc;
+    SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaStreamSynchronize(s));
+    const int st = *L.status_host;
+    if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
+      full = true;  // rare bytes or layouts: redo the call on the exact path
+      SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
+    } else if (st & saru::kStatusOverflow) {
+      set_error("banded traceback left its band (status %d)", st);
+      return SARU_E_OVERFLOW;
+    }
+  }
+  if (full) {
+    if ((rc = run_full(L, b, &db, pl, &dr))) return rc;
+    SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
+  SARU_CUDA(cudaMemcpyAsync(r->scores, dr.scores, 4 * n, cudaMemcpyDeviceToHost, s));
+  SARU_CUDA(cudaMemcpyAsync(r->read_aln, dr.read_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
+  SARU_CUDA(cudaMemcpyAsync(r->genome_aln, dr.genome_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
+  SARU_CUDA(cudaEventRecord(L.ev1, s));
+  SARU_CUDA(cudaStreamSynchronize(s));
+  if (full && (*L.status_host & saru::kStatusOverflow)) {
+    set_error("a traceback left its slot; the reference result depends on thread order");
+    return SARU_E_OVERFLOW;
+  }
+  if (ms_out) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, L.ev0, L.ev1);
+    *ms_out = ms;
+  }
+  return SARU_OK;
+}
+
+// uthash application-order walk of the caller's read_names table.  Element
+// layout of struct read_name_hash (src/util.h:350-354): int read_number;
+// char name[60]; UT_hash_handle hh; the handle's third pointer `next`
+// (src/uthash.h, UT_hash_handle) links the elements in insertion order.
+struct NameIndex {
+  std::vector<const char *> by_id;
+  static const char *lookup(void *ctx, int32_t id) {
+    auto *ni = static_cast<NameIndex *>(ctx);
+    if (id < 0 || (size_t)id >= ni->by_id.size()) return nullptr;
+    return ni->by_id[(size_t)id];
+  }
+  void build(const void *head) {
+    by_id.clear();
+    const char *e = static_cast<const char *>(head);
+    size_t guard = 0;
+    while (e && guard++ < (size_t)1 << 31) {
+      const int id = *reinterpret_cast<const int *>(e);
+      const char *name = e + sizeof(int);
+      if (id >= 0) {
+        if ((size_t)id >= by_id.size()) by_id.resize((size_t)id + 1, nullptr);
+        by_id[(size_t)id] = name;
+      }
+      const void *next = *reinterpret_cast<void *const *>(e + 64 + 2 * sizeof(void *));
+      e = static_cast<const char *>(next);
+    }
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char *saru_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t saru_kernel_launches(void) { return g_launches.load(); }
+
+size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide) {
+  (void)k;
+  int dev = current_device();
+  if (dev < 0) dev = 0;
+  return band_scratch_bytes(band_grid(dev, n), read_length, wide != 0);
+}
+
+int saru_align_host(const saru_batch *batch, saru_result *result, int lane) {
+  g_last_error.clear();
+  Lane &L = g_lanes[lane ? 1 : 0];
+  std::lock_guard<std::mutex> lk(L.mu);
+  return align_host_impl(batch, result, L, nullptr);
+}
+
+int saru_align_device(const saru_batch *batch, saru_result *result, void *scratch,
+                      size_t scratch_bytes, void *stream) {
+  g_last_error.clear();
+  if (batch->n < 0 || batch->k < 0 || batch->k > 15 || batch->match != 0 ||
+      batch->mismatch != 1 || batch->max_read_length < 2 ||
+      batch->max_read_length > saru::kMaxBandM || !result->status) {
+    set_error("saru_align_device: needs unit costs, k <= 15, 2 <= max_read_length <= %d and a "
+              "status word",
+              saru::kMaxBandM);
+    return SARU_E_INVALID;
+  }
+  int dev = 0;
+  SARU_CUDA(cudaGetDevice(&dev));
+  Plan pl;
+  pl.band = true;
+  pl.max_m = batch->max_read_length;
+  pl.wide = batch->k > 7;
+  return run_band(batch, pl, result, scratch, scratch_bytes, result->status, dev,
+                  reinterpret_cast<cudaStream_t>(stream));
+}
+
+int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
+                        const int32_t *read_ids, const int32_t *genome_pos, int32_t read_length,
+                        const char *names, int32_t name_stride, int32_t n_names, char *out,
+                        int64_t cap, int32_t *done_fwd, int32_t *done_rev) {
+  struct Tab {
+    const char *names;
+    int32_t stride, n;
+    static const char *get(void *c, int32_t id) {
+      auto *t = static_cast<Tab *>(c);
+      return (id >= 0 && id < t->n) ? t->names + (int64_t)id * t->stride : nullptr;
+    }
+  } tab{names, name_stride, n_names};
+  saru::WriterCall w{result->scores, result->read_aln, result->genome_aln, batch->total_slots,
+                     batch->genome_offsets, genome_pos, batch->dirs, read_ids, batch->k,
+                     read_length, &Tab::get, &tab};
+  std::string text;
+  int32_t df = 0, dr = 0;
+  saru::format_range(w, 0, batch->n, &text, &df, &dr);
+  if (done_fwd) *done_fwd = df;
+  if (done_rev) *done_rev = dr;
+  if (out && cap > 0) memcpy(out, text.data(), (size_t)((int64_t)text.size() < cap ? (int64_t)text.size() : cap));
+  return (int64_t)text.size();
+}
+
+void cuda_allocate_memory(int do_reverse) {
+  const int lane = do_reverse == 4 ? 1 : 0;
+  const int dev = current_device();
+  if (dev < 0) {
+    fprintf(stderr, "saruman_b200: no CUDA device\n");
+    return;
+  }
+  std::lock_guard<std::mutex> lk(g_lanes[lane].mu);
+  if (g_lanes[lane].init(dev) != SARU_OK) {
+    fprintf(stderr, "saruman_b200: %s\n", g_last_error.c_str());
+    return;
+  }
+  // the reference keeps its arena base in these globals; here they mark the
+  // lane as prepared (memory is allocated per call, on demand)
+  char *marker = reinterpret_cast<char *>(g_lanes[lane].stream);
+  if (lane) main_alloc_ptr_rev = marker;
+  else main_alloc_ptr_for = marker;
+}
+
+void cuda_free_memory(int do_reverse) {
+  const int lane = do_reverse ? 1 : 0;
+  std::lock_guard<std::mutex> lk(g_lanes[lane].mu);
+  g_lanes[lane].release();
+  if (lane) main_alloc_ptr_rev = nullptr;
+  else main_alloc_ptr_for = nullptr;
+}
+
+unsigned long int get_cuda_infos(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    cudaGetLastError();
+    count = 0;
+  }
+  fprintf(stderr, "\n=== CUDA hardware ===\n");
+  fprintf(stderr, "Detected %d GPU(s):\n\n", count);
+  size_t most_free = 0;
+  int best = 0, i;
+  for (i = 0; i < count; ++i) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, i);
+    size_t fr = 0, tot = 0;
+    cudaSetDevice(i);
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fprintf(stderr, "GPU %d: %s\t", i, prop.name);
+      fprintf(stderr, "Could not get memory information from GPU.\nShutting down.\n");
+      exit(-1);
+    }
+    if (fr > most_free) {
+      most_free = fr;
+      best = i;
+    }
+    fprintf(stderr, "GPU %d: %s\t", i, prop.name);
+    fprintf(stderr, "[%*lu/%*lu MB available]\n", 4, (unsigned long)(fr / (1024 * 1024)), 4,
+            (unsigned long)(tot / (1024 * 1024)));
+  }
+  if (most_free < 128000000UL) {
+    fprintf(stderr, "\n-> SARUMAN was not able to find a GPU with enough VRAM available! (available: %lu MB)\n",
+            (unsigned long)(most_free / (1024 * 1024)));
+    exit(1);
+  } else if (use_gpu_value <= i) {
+    fprintf(stderr, "\n-> SARUMAN was forced to run on GPU %d\n", use_gpu_value);
+  } else {
+    fprintf(stderr, "\n-> SARUMAN will run on GPU %d\n", best);
+    use_gpu_value = (unsigned short)best;
+  }
+  return (unsigned long)most_free;
+}
+
+void cuda_needleman_wunsch(int match, int mismatch, char *genome_sequences_on_host,
+                           char *read_sequences_on_host, int *genome_offsets, int *read_offsets,
+                           int *edit_offsets, int sample_size, int *read_id_array,
+                           int *genome_pos_array, char *direction_array, int error,
+                           size_t total_genome_array_size, size_t total_read_sequence_array_size,
+                           size_t total_edit_matrix_size, int do_reverse) {
+  (void)edit_offsets;
+  (void)total_read_sequence_array_size;
+  (void)total_edit_matrix_size;
+  g_last_error.clear();
+  fprintf(stderr, "\t\t-> starting CUDA kernel with %d samples from %s thread\n", sample_size,
+          (do_reverse ? "reverse" : "forward"));
+  {
+    std::lock_guard<std::mutex> lk(g_out_mu);
+    if (do_reverse) reverse_alignment_candidates += sample_size;
+    else forward_alignment_candidates += sample_size;
+  }
+  if (sample_size <= 0) return;
+  const int n = sample_size;
+  const size_t slots = total_genome_array_size;
+  // host result arrays with zeroed slack (the writer may scan past a slot)
+  std::vector<int32_t> scores((size_t)n);
+  std::vector<char> ra(slots + 64, 0), ga(slots + 64, 0);
+  saru_batch b{};
+  b.genome = genome_sequences_on_host;
+  b.reads = read_sequences_on_host;
+  b.genome_offsets = genome_offsets;
+  b.read_offsets = read_offsets;
+  b.dirs = reinterpret_cast<const int8_t *>(direction_array);
+  b.n = n;
+  b.k = error;
+  b.match = match;
+  b.mismatch = mismatch;
+  b.first_of_call = 1;
+  b.genome_bytes = genome_offsets[n - 1];
+  b.total_slots = (int64_t)slots;
+  saru_result r{scores.data(), ra.data(), ga.data(), nullptr};
+  const int lane = do_reverse ? 1 : 0;
+  float ms = 0.f;
+  int rc;
+  {
+    std::lock_guard<std::mutex> lk(g_lanes[lane].mu);
+    rc = align_host_impl(&b, &r, g_lanes[lane], &ms);
+  }
+  if (rc != SARU_OK) {
+    fprintf(stderr, "ERROR: saruman_b200 alignment failed: %s\n", g_last_error.c_str());
+    return;
+  }
+  NameIndex names;
+  names.build(read_names);
+  saru::WriterCall w{scores.data(), ra.data(), ga.data(), (int64_t)slots, genome_offsets,
+                     genome_pos_array, reinterpret_cast<const int8_t *>(direction_array),
+                     read_id_array, error, (int32_t)read_length_value, &NameIndex::lookup,
+                     &names};
+  std::string text;
+  text.reserve((size_t)n * 64);
+  int32_t df = 0, dr = 0;
+  saru::format_range(w, 0, n, &text, &df, &dr);
+  std::lock_guard<std::mutex> lk(g_out_mu);
+  fwrite(text.data(), 1, text.size(), stdout);
+  for (int v = 0; v < n; ++v) {
+    if (scores[(size_t)v] > error) continue;
+    const int id = read_id_array[v];
+    if (direction_array[v] > 3) {
+      if (reverse_output_control) reverse_output_control[id] = 1;
+    } else if (forward_output_control) {
+      forward_output_control[id] = 1;
+    }
+  }
+  forward_alignments_done += (unsigned)df;
+  reverse_alignments_done += (unsigned)dr;
+  alignment_time[lane] += ms;
+}
+
+}  // extern "C"

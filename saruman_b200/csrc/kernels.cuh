@@ -1,0 +1,58 @@
+// kernels.cuh -- launch interface of the alignment kernels (host <-> device).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace saru {
+
+// status bits written by the kernels
+constexpr int kStatusIrregular = 1;  // window length != m + so + eo, or m <= 3k
+constexpr int kStatusAlphabet = 2;   // a read with more distinct non-ACGT bytes than supported
+constexpr int kStatusOverflow = 4;   // a traceback left its slot / band
+constexpr int kStatusUndefined = 8;  // the reference would read outside its arrays
+
+constexpr int kMaxBandM = 512;  // longest read of the banded kernel
+constexpr int kMaxOpWords = (kMaxBandM + 3 * 15 + 15) / 16 + 1;
+
+struct KernelArgs {
+  const uint8_t *genome;
+  const uint8_t *reads;
+  const int32_t *goff;
+  const int32_t *roff;
+  const int8_t *dirs;
+  long n;
+  int k;
+  int max_m;
+  int first_of_call;
+  int wide;  // 64-bit band
+  long grid; // CTAs of the persistent grid (<= 0: one per tile)
+  int32_t *scores;
+  uint8_t *read_aln;
+  uint8_t *genome_aln;
+  void *scratch;  // decision planes: 2 * (max_m + 1) * grid * CTA band words
+  int *status;
+};
+
+struct FullArgs {
+  const uint8_t *genome;
+  const uint8_t *reads;
+  const int32_t *goff;
+  const int32_t *roff;
+  const int8_t *dirs;
+  const int64_t *eoff;  // cell offset of each matrix in the arena
+  long n;
+  int k, match, mismatch, first_of_call;
+  long genome_bytes, read_bytes;
+  short *arena;
+  int32_t *scores;
+  uint8_t *read_aln;
+  uint8_t *genome_aln;
+  int *status;
+};
+
+size_t band_smem_bytes(int max_m, int k, int cta);
+cudaError_t launch_band_kernel(const KernelArgs &a, int cta, int sms, cudaStream_t s);
+cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
+
+}  // namespace saru

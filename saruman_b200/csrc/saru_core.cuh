@@ -65,23 +65,43 @@ SARU_HD T lowmask(int n) {
   return n <= 0 ? T(0) : (n >= BITS ? ~T(0) : ((T(1) << n) - T(1)));
 }
 
+// Word arrays are addressed through P, either a plain uint32_t* or a
+// Strided view (word i of a thread at p[i * stride]) used for per-thread
+// tables interleaved across a thread block in shared memory.
+struct Strided {
+  uint32_t *p;
+  int stride;
+  SARU_HD uint32_t &operator[](int i) const { return p[i * stride]; }
+  SARU_HD Strided operator+(int i) const { return Strided{p + i * stride, stride}; }
+};
+
 // bits [j, j + BITS) of a packed mask (words of 32 bits)
-template <typename T>
-SARU_HD T window_bits(const uint32_t *mask, int j);
+template <typename T, class P>
+struct WindowBits;
 
-template <>
-SARU_HD uint32_t window_bits<uint32_t>(const uint32_t *mask, int j) {
-  int w = j >> 5;
-  return fshr32(mask[w], mask[w + 1], (uint32_t)j & 31u);
-}
+template <class P>
+struct WindowBits<uint32_t, P> {
+  static SARU_HD uint32_t get(P mask, int j) {
+    int w = j >> 5;
+    return fshr32(mask[w], mask[w + 1], (uint32_t)j & 31u);
+  }
+};
 
-template <>
-SARU_HD uint64_t window_bits<uint64_t>(const uint32_t *mask, int j) {
-  int w = j >> 5;
-  uint32_t s = (uint32_t)j & 31u;
-  uint32_t lo = fshr32(mask[w], mask[w + 1], s);
-  uint32_t hi = fshr32(mask[w + 1], mask[w + 2], s);
-  return (uint64_t)lo | ((uint64_t)hi << 32);
+template <class P>
+struct WindowBits<uint64_t, P> {
+  static SARU_HD uint64_t get(P mask, int j) {
+    int w = j >> 5;
+    uint32_t s = (uint32_t)j & 31u;
+    uint32_t a = mask[w], b = mask[w + 1], c = mask[w + 2];
+    uint32_t lo = fshr32(a, b, s);
+    uint32_t hi = fshr32(b, c, s);
+    return (uint64_t)lo | ((uint64_t)hi << 32);
+  }
+};
+
+template <typename T, class P>
+SARU_HD T window_bits(P mask, int j) {
+  return WindowBits<T, P>::get(mask, j);
 }
 
 SARU_HD int base_code(uint8_t c) {
@@ -118,9 +138,8 @@ SARU_HD void flank_of(int dir, int k, int &so, int &eo) {
 // masks: bit (p + k + 1) of mask[c] is set iff window byte p belongs to
 // class c.  Returns false if the read has more than MAX_EXTRA distinct
 // non-ACGT bytes.  Reader/Writer abstract where bytes and words live.
-template <class ReadFn, class WinFn>
-SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, uint32_t *codes, uint32_t *mask,
-                         int mwords) {
+template <class ReadFn, class WinFn, class P>
+SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, P codes, P mask, int mwords) {
   uint8_t extra[MAX_EXTRA];
   int nextra = 0;
   for (int w = 0; w < (c.m + 7) / 8; ++w) codes[w] = 0;
@@ -154,14 +173,16 @@ SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, uint32_t *codes, ui
   return true;
 }
 
-SARU_HD int code_at(const uint32_t *codes, int j) { return (codes[j >> 3] >> ((j & 7) * 4)) & 15; }
+template <class P>
+SARU_HD int code_at(P codes, int j) {
+  return (codes[j >> 3] >> ((j & 7) * 4)) & 15;
+}
 
 // Fill of one candidate.  `planes(j, A, B)` receives the decision planes of
 // read column j (1..m): code = A | 2B per band bit.  Returns D[L][m] if it
 // is <= k, otherwise k + 1.
-template <typename T, class PlaneSink>
-SARU_HD int fill_band(const Cand &c, const uint32_t *codes, const uint32_t *mask, int mwords,
-                      PlaneSink planes) {
+template <typename T, class P, class PlaneSink>
+SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink planes) {
   constexpr int BITS = int(sizeof(T) * 8);
   const int k = c.k, m = c.m;
   // column 0: rows b - k; dv = -1 for rows <= 0, 0 for rows 1..2so, +1 after

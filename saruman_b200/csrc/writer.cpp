@@ -1,0 +1,152 @@
+// writer.cpp -- the reference's TSV output for one aligned call.
+//
+// Reproduces src/cuda-functions.cu:827-1006 byte for byte from the scores
+// and the two alignment-slot arrays: for each candidate whose score is <= k
+//   start  = genome position + number of leading '_' in the read string
+//   stop_correction = number of '_' in the run of '_'/NUL that ends the slot
+//   a forward scan from the first non-gap byte counts '_' in the read
+//     (deletions) and in the window string (insertions) until a NUL, its
+//     bound growing by one per gap (z in the reference)
+//   chars  = (scan position of the NUL) - stop_correction, or
+//            read_length + deletions when no NUL was met
+//   line   = name, start, chars - insertions + start - 1, ">>" or "<<",
+//            both strings cut at chars bytes (or their NUL), score
+// with the reference's integer types (unsigned short counters, short chars,
+// unsigned positions printed with %d).  Bytes past the end of the arrays
+// read as 0; callers allocate the arrays with zeroed slack.
+#include <stdint.h>
+#include <string.h>
+
+#include "writer.h"
+
+namespace saru {
+
+static inline char *put_int(char *p, int v) {
+  char tmp[12];
+  int n = 0;
+  unsigned int u = v < 0 ? 0u - (unsigned int)v : (unsigned int)v;
+  do {
+    tmp[n++] = char('0' + u % 10u);
+    u /= 10u;
+  } while (u);
+  if (v < 0) *p++ = '-';
+  while (n) *p++ = tmp[--n];
+  return p;
+}
+
+struct ByteView {
+  const char *a;
+  int64_t n;
+  inline char operator[](int64_t i) const { return (i >= 0 && i < n) ? a[i] : 0; }
+};
+
+// Computes the fields of candidate v's line.  Returns false if the
+// candidate prints nothing (score > k).
+bool line_fields(const WriterCall &w, int64_t v, LineFields *f) {
+  if (w.scores[v] > w.k) return false;
+  const ByteView ra{w.read_aln, w.total_slots}, ga{w.genome_aln, w.total_slots};
+  unsigned short L;
+  int64_t gs, eb = 0;
+  if (v > 0) {
+    L = (unsigned short)(w.goff[v] - w.goff[v - 1]);
+    gs = w.goff[v - 1];
+    eb = (int64_t)w.k * v;
+  } else {
+    L = (unsigned short)w.goff[0];
+    gs = 0;
+  }
+  const int64_t slot = gs + eb;
+  unsigned int start = (unsigned int)w.pos[v];
+  unsigned short start_corr = 0, stop_corr = 0, deletion = 0, insertion = 0;
+  for (int64_t i = 0; ra[slot + i] == '_'; ++i) {
+    start++;
+    start_corr++;
+  }
+  for (int64_t i = slot + L + w.k - 1; i >= -1; --i) {
+    const char ch = ra[i];
+    if (ch != '_' && ch != 0) break;
+    if (ch == '_') stop_corr++;
+  }
+  int64_t i = 0, z = 0;
+  short end_of_read = 0;
+  while (i < (int64_t)L - stop_corr - start_corr + z) {
+    const char rc = ra[slot + start_corr + i];
+    if (rc == 0) {
+      end_of_read = (short)i;
+      break;
+    }
+    if (rc == '_') {
+      deletion++;
+      z++;
+      i++;
+      continue;
+    }
+    if (ga[slot + start_corr + i] == '_') {
+      insertion++;
+      z++;
+      i++;
+      continue;
+    }
+    i++;
+  }
+  const short chars =
+      end_of_read > 0 ? (short)(end_of_read - stop_corr) : (short)(w.read_length + deletion);
+  const char *name = w.name_of ? w.name_of(w.name_ctx, w.ids[v]) : "";
+  if (!name) name = "";
+  f->name = name;
+  f->name_len = (int64_t)strlen(name);
+  f->start = (int)start;
+  f->stop = (int)((unsigned int)(chars - insertion) + start - 1u);
+  f->from = slot + start_corr;
+  // "%.*s": up to chars bytes, or to the NUL (a negative precision is no limit)
+  int64_t la = 0, lb = 0;
+  while ((chars < 0 || la < chars) && ra[f->from + la]) ++la;
+  while ((chars < 0 || lb < chars) && ga[f->from + lb]) ++lb;
+  f->len_read = la;
+  f->len_genome = lb;
+  f->reverse = w.dirs[v] > 3;
+  f->score = w.scores[v];
+  f->bytes = f->name_len + la + lb + 3 * 12 + 8;
+  return true;
+}
+
+// Writes a line computed by line_fields; `out` has f.bytes of room.
+// Returns the bytes written.
+int64_t line_write(const WriterCall &w, const LineFields &f, char *out) {
+  const ByteView ra{w.read_aln, w.total_slots}, ga{w.genome_aln, w.total_slots};
+  char *p = out;
+  memcpy(p, f.name, (size_t)f.name_len);
+  p += f.name_len;
+  *p++ = '\t';
+  p = put_int(p, f.start);
+  *p++ = '\t';
+  p = put_int(p, f.stop);
+  memcpy(p, f.reverse ? "\t<<\t" : "\t>>\t", 4);
+  p += 4;
+  for (int64_t q = 0; q < f.len_read; ++q) *p++ = ra[f.from + q];
+  *p++ = '\t';
+  for (int64_t q = 0; q < f.len_genome; ++q) *p++ = ga[f.from + q];
+  *p++ = '\t';
+  p = put_int(p, f.score);
+  *p++ = '\n';
+  return p - out;
+}
+
+void format_range(const WriterCall &w, int64_t begin, int64_t end, std::string *out,
+                  int32_t *done_fwd, int32_t *done_rev) {
+  LineFields f;
+  for (int64_t v = begin; v < end; ++v) {
+    if (!line_fields(w, v, &f)) continue;
+    const size_t at = out->size();
+    out->resize(at + (size_t)f.bytes);
+    const int64_t n = line_write(w, f, &(*out)[at]);
+    out->resize(at + (size_t)n);
+    if (f.reverse) {
+      if (done_rev) ++*done_rev;
+    } else if (done_fwd) {
+      ++*done_fwd;
+    }
+  }
+}
+
+}  // namespace saru

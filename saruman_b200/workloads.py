@@ -35,6 +35,10 @@ for _a, _b in ((b"A", b"T"), (b"C", b"G"), (b"G", b"C"), (b"T", b"A")):
     _COMP[_a[0]] = _b[0]
 
 
+_CODE = np.zeros(256, dtype=np.uint8)
+_CODE[BASES] = np.arange(4, dtype=np.uint8)
+
+
 def reverse_complement(seqs: np.ndarray) -> np.ndarray:
     """Reverse complement of rows of ASCII bytes; only A/C/G/T are swapped
     and other bytes (N) are kept, as in the reference (src/util.c:35-57)."""
@@ -50,6 +54,16 @@ def uniform_genome(n: int, seed: int) -> np.ndarray:
     return BASES[rng.integers(0, 4, size=n, dtype=np.uint8)]
 
 
+@dataclasses.dataclass
+class RepeatMap:
+    """Where the inserted repeat copies are: copy i of family fam[i] starts
+    at start[i] and is family_len bases long (later copies may overwrite
+    parts of earlier ones)."""
+    fam: np.ndarray
+    start: np.ndarray
+    family_len: int
+
+
 def repeat_genome(n: int, seed: int, families: int = 40, family_len: int = 1500,
                   copies: str = "uniform", identity: float = 0.99,
                   gc: float = 0.5) -> np.ndarray:
@@ -57,22 +71,31 @@ def repeat_genome(n: int, seed: int, families: int = 40, family_len: int = 1500,
 
     copies="uniform": 5-50 copies per family (C2); copies="zipf": Zipf(1.5)
     capped at 500 (C3).  Each copy carries (1-identity) substitutions."""
+    return repeat_genome_with_map(n, seed, families, family_len, copies, identity, gc)[0]
+
+
+def repeat_genome_with_map(n: int, seed: int, families: int = 40, family_len: int = 1500,
+                           copies: str = "uniform", identity: float = 0.99,
+                           gc: float = 0.5) -> tuple[np.ndarray, RepeatMap]:
     rng = np.random.Generator(np.random.PCG64(seed))
+    cfam, cstart = [], []
     p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
     g = BASES[rng.choice(4, size=n, p=p).astype(np.uint8)]
-    for _ in range(families):
+    for fi in range(families):
         fam = BASES[rng.choice(4, size=family_len, p=p).astype(np.uint8)]
         if copies == "zipf":
             c = int(min(rng.zipf(1.5), 500))
         else:
             c = int(rng.integers(5, 51))
-        for _ in range(c):
+        for _c in range(c):
             cp = fam.copy()
             mut = rng.random(family_len) < (1.0 - identity)
             cp[mut] = BASES[(np.searchsorted(BASES, cp[mut]) + rng.integers(1, 4, mut.sum())) % 4]
             at = int(rng.integers(0, n - family_len))
             g[at:at + family_len] = cp
-    return g
+            cfam.append(fi)
+            cstart.append(at)
+    return g, RepeatMap(np.asarray(cfam, np.int64), np.asarray(cstart, np.int64), family_len)
 
 
 @dataclasses.dataclass
@@ -98,11 +121,13 @@ def sample_reads(genome: np.ndarray, n: int, m: int, rate: float, seed: int,
     for s in range(0, n, chunk):
         e = min(n, s + chunk)
         c = e - s
-        ev = rng.random((c, m)) < rate
-        kind = rng.choice(3, size=(c, m), p=np.asarray(mix))
-        ins = ev & (kind == 1)
-        dele = ev & (kind == 2)
-        sub = ev & (kind == 0)
+        u = rng.random((c, m))
+        ev = u < rate
+        # event type from the same uniform draw: [0, rate*mix0) substitution,
+        # then insertion, then deletion
+        sub = u < rate * mix[0]
+        ins = ev & ~sub & (u < rate * (mix[0] + mix[1]))
+        dele = ev & ~sub & ~ins
         step = np.where(ins, 0, np.where(dele, 2, 1)).astype(np.int64)
         # genome index consumed by read position t: origin + sum(step[:t]) + dele[t]
         before = np.cumsum(step, axis=1) - step
@@ -110,11 +135,9 @@ def sample_reads(genome: np.ndarray, n: int, m: int, rate: float, seed: int,
         org = rng.integers(0, G - int(span_c.max()) - 1, size=c)
         idx = org[:, None] + before + dele.astype(np.int64)
         r = genome[idx]
-        rnd = BASES[rng.integers(0, 4, size=(c, m), dtype=np.uint8)]
-        r = np.where(ins, rnd, r)
-        shift = rng.integers(1, 4, size=(c, m))
-        code = np.searchsorted(BASES, r)
-        r = np.where(sub, BASES[(code + shift) % 4], r)
+        r[ins] = BASES[rng.integers(0, 4, size=int(ins.sum()), dtype=np.uint8)]
+        r[sub] = BASES[(_CODE[r[sub]] + rng.integers(1, 4, size=int(sub.sum()),
+                                                     dtype=np.uint8)) % 4]
         out[s:e] = r
         origin[s:e] = org
         span[s:e] = span_c
@@ -223,57 +246,121 @@ def flank(flag: int, k: int) -> tuple[int, int]:
     return so, eo
 
 
-# flag mix of the reference filter, measured on its own output for C1/C2
-# (fraction of candidates with flank class 1 = end free, 2 = start free,
-# 3 = both free); see tests/golden/make_golden.py
-DEFAULT_FLANK_MIX = (0.60, 0.0, 0.40)
+# flank-class mix of the reference filter's candidates (1 = end gap free,
+# 2 = start gap free, 3 = both): about 60/0/40 on the uniform 36 bp shape and
+# 45/0/55 on the repeat-rich 100 bp shape, as counted from its own output
+DEFAULT_FLANK_MIX = (0.45, 0.0, 0.55)
+
+
+def repeat_hits(rd: Reads, rmap: RepeatMap, max_per_read: int = 1000):
+    """For reads whose source lies inside a repeat copy, the same offset in
+    every other copy of that family (where the q-gram filter finds exact
+    q-gram pairs).  Returns (read index, genome position) arrays."""
+    order = np.lexsort((rmap.start, rmap.fam))      # copies grouped by family
+    fs, cs = rmap.fam[order], rmap.start[order]
+    byst = np.argsort(cs)
+    o = rd.origin
+    i = np.searchsorted(cs[byst], o, side="right") - 1
+    ii = byst[np.maximum(i, 0)]
+    inside = (o >= 0) & (i >= 0) & (o + rd.span <= cs[ii] + rmap.family_len)
+    r = np.nonzero(inside)[0]
+    if r.size == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    c = ii[r]                                        # index of the source copy in (fs, cs)
+    f = fs[c]
+    first = np.searchsorted(fs, f, side="left")
+    cnt = np.minimum(np.searchsorted(fs, f, side="right") - first, max_per_read)
+    tot = int(cnt.sum())
+    rid = np.repeat(r, cnt)
+    within = np.arange(tot) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    src = np.repeat(first, cnt) + within
+    keep = src != np.repeat(c, cnt)
+    off = np.repeat(o[r] - cs[c], cnt)
+    return rid[keep], (cs[src] + off)[keep]
+
+
+def pack_windows(genome: np.ndarray, st: np.ndarray, L: np.ndarray,
+                 chunk: int = 1 << 20) -> np.ndarray:
+    """genome[st[t] : st[t] + L[t]] for all t, back to back."""
+    lmax = int(L.max()) if len(L) else 0
+    out = np.empty(int(L.sum()), dtype=np.uint8)
+    if lmax == 0:
+        return out
+    view = np.lib.stride_tricks.sliding_window_view(genome, lmax)
+    pos = 0
+    for s0 in range(0, len(st), chunk):
+        s1 = min(len(st), s0 + chunk)
+        rows = view[np.minimum(st[s0:s1], len(genome) - lmax)]
+        # rows too close to the end: fall back to exact slices
+        lens = L[s0:s1]
+        if (lmax == lens).all():
+            part = rows.reshape(-1)
+        else:
+            mask = np.arange(lmax)[None, :] < lens[:, None]
+            part = rows[mask]
+        near_end = st[s0:s1] > len(genome) - lmax
+        out[pos:pos + len(part)] = part
+        if near_end.any():
+            starts = pos + np.concatenate([[0], np.cumsum(lens)[:-1]])
+            for j in np.nonzero(near_end)[0]:
+                a = int(st[s0 + j])
+                out[starts[j]:starts[j] + lens[j]] = genome[a:a + lens[j]]
+        pos += len(part)
+    return out
 
 
 def synthetic_candidates(genome: np.ndarray, rd: Reads, m: int, k: int, seed: int,
                          flank_mix=DEFAULT_FLANK_MIX, extra_hits: float = 0.0,
+                         repeats: RepeatMap | None = None,
                          max_candidates: int | None = None) -> Batch:
     """Candidate windows placed as the q-gram filter places them: at the
-    read's origin, with a flank class drawn from `flank_mix`, plus
-    `extra_hits` decoy windows per read at random genome positions (the
-    multi-hit candidates of repeats and the rejections of unmapped reads)."""
+    read's origin, with a flank class drawn from `flank_mix`; with a repeat
+    map, also at the same offset of every other copy of the read's repeat
+    family; plus `extra_hits` decoy windows per read at random positions
+    (the rejections of reads without a true origin)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     n = rd.seqs.shape[0]
     G = len(genome)
     cls = rng.choice(3, size=n, p=np.asarray(flank_mix)) + 1
     so = np.where((cls == 2) | (cls == 3), k, 0)
-    eo = np.where((cls == 1) | (cls == 3), k, 0)
     org = np.where(rd.origin >= 0, rd.origin, rng.integers(k, G - m - 3 * k, size=n))
     start = org - so
     nx = rng.poisson(extra_hits, size=n) if extra_hits > 0 else np.zeros(n, np.int64)
     rid = np.concatenate([np.arange(n), np.repeat(np.arange(n), nx)])
     st = np.concatenate([start, rng.integers(k, G - m - 3 * k, size=int(nx.sum()))])
     cl = np.concatenate([cls, np.repeat(cls, nx)])
+    if repeats is not None:
+        hr, hp = repeat_hits(rd, repeats)
+        hc = rng.choice(3, size=len(hr), p=np.asarray(flank_mix)) + 1
+        hso = np.where((hc == 2) | (hc == 3), k, 0)
+        rid = np.concatenate([rid, hr])
+        st = np.concatenate([st, hp - hso])
+        cl = np.concatenate([cl, hc])
     s_o = np.where((cl == 2) | (cl == 3), k, 0)
     e_o = np.where((cl == 1) | (cl == 3), k, 0)
     st = np.clip(st, 0, G - (m + s_o + e_o))
-    order = rng.permutation(len(rid))
+    # candidates grouped by read, as the reference's collection loop emits
+    # them (src/hash.c:926-1082)
+    order = np.argsort(rid, kind="stable")
     if max_candidates is not None:
         order = order[:max_candidates]
     rid, st, cl, s_o, e_o = rid[order], st[order], cl[order], s_o[order], e_o[order]
     L = m + s_o + e_o
     go = np.cumsum(L)
-    gstart = go - L
-    total = int(go[-1]) if len(go) else 0
-    gbytes = np.empty(total, dtype=np.uint8)
-    # gather windows: index = st + (position within window)
-    seg = np.repeat(np.arange(len(st)), L)
-    within = np.arange(total) - np.repeat(gstart, L)
-    gbytes[:] = genome[np.repeat(st, L) + within] if total else gbytes
-    _ = seg
+    gbytes = pack_windows(genome, st, L)
     dirs = (cl + np.where(rd.reverse[rid], 4, 0)).astype(np.int8)
-    reads = rd.seqs[rid]
     # the reference aligns the reverse complement of reverse-strand reads
     # (src/hash.c:1027-1034); `rd.seqs` holds reads as sequenced, so undo it
-    reads = np.where(rd.reverse[rid][:, None], reverse_complement(reads), reads)
+    fwd = rd.seqs.copy()
+    fwd[rd.reverse] = reverse_complement(fwd[rd.reverse])
+    reads = fwd[rid]
     n_c = len(rid)
     ro = ((np.arange(n_c, dtype=np.int64) + 1) * m).astype(np.int32)
-    esz = (m + 1) * (L + 1)
-    eoff = (np.cumsum(esz) - esz).astype(np.int32) if n_c else np.zeros(0, np.int32)
+    esz = (m + 1) * (L.astype(np.int64) + 1)
+    ecum = np.cumsum(esz) - esz
+    # the reference's int edit offsets; batches past 2^31 cells cannot be one
+    # reference call and carry -1 (the banded path does not read them)
+    eoff = ecum.astype(np.int32) if n_c and ecum[-1] + esz[-1] < 2**31 else np.full(n_c, -1, np.int32)
     return Batch(m=m, k=k, genome=gbytes, reads=np.ascontiguousarray(reads.reshape(-1)),
                  genome_offsets=go.astype(np.int32), read_offsets=ro, edit_offsets=eoff,
                  dirs=dirs, ids=rid.astype(np.int32), pos=st.astype(np.int32))

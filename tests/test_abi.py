@@ -1,0 +1,70 @@
+"""CPU checks of the C ABI library: it loads, exports every symbol
+include/saruman_b200.h declares, and its host TSV writer reproduces the
+reference writer on the golden fixtures (host code only, no GPU call)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import golden_io as G
+import saruman_b200 as S
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "saruman_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    funcs = set(re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", text))
+    funcs -= {"sizeof", "defined"}
+    data = set(re.findall(r"extern\s+[a-z ]+\s+\**([a-z_][a-z0-9_]*)\s*\[", text))
+    return funcs, data
+
+
+def test_header_symbols_listed():
+    funcs, data = declared_symbols()
+    assert funcs == set(S.ABI_FUNCTIONS)
+    assert data == set(S.ABI_DATA)
+
+
+def test_library_exports_every_declared_symbol(saru_lib):
+    funcs, data = declared_symbols()
+    out = subprocess.run(["nm", "-D", "--defined-only", str(S.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = (funcs | data) - exported
+    assert not missing, missing
+    for name in funcs | data:
+        assert hasattr(saru_lib, name)
+
+
+def test_reference_globals_exported(saru_lib):
+    """The reference's host program reads and writes these through the
+    library (src/cuda-functions.h:15-28, src/saruman.h:55-66)."""
+    for name in ("read_names", "read_length_value", "be_verbose_value", "use_gpu_value",
+                 "cuda_memory_per_thread", "forward_alignments_done", "reverse_alignments_done",
+                 "forward_alignment_candidates", "reverse_alignment_candidates",
+                 "forward_output_control", "reverse_output_control", "main_alloc_ptr_for",
+                 "main_alloc_ptr_rev"):
+        C.c_int.in_dll(saru_lib, name)
+
+
+@pytest.mark.parametrize("name", G.fixture_names())
+def test_writer_matches_reference_writer(saru_lib, name):
+    b, names, do_rev, m, exp = G.load_fixture(name)
+    r = S.AlignResult(exp["scores"].astype(np.int32), exp["read_aln"], exp["genome_aln"])
+    tab = S.name_table(G.names_by_id(b, names))
+    tsv, df, dr = S.format_tsv(b, r, tab, read_length=m)
+    assert tsv == exp["tsv"]
+    assert df + dr == int((exp["scores"] <= b.k).sum())
+
+
+def test_load_fails_loudly_without_library(tmp_path):
+    with pytest.raises(RuntimeError, match="not built"):
+        S.load(tmp_path / "missing.so")
