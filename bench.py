@@ -260,8 +260,13 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--reads", type=int, default=None,
+                    help="override the reads per step (smaller cases for profiling)")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.reads:
+        cfg["reads"] = args.reads
+        cfg["workload"] += f" (reduced to {args.reads} reads)"
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

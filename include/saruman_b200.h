@@ -97,7 +97,9 @@ typedef struct {
 } saru_batch;
 
 typedef struct {
-  int32_t *scores;              /* n: D[L][m] when <= k, else k + 1 */
+  int32_t *scores;              /* n: D[L][m] when <= k; above k, k + 1 from the
+                                   banded kernel or the exact D[L][m] from the
+                                   full-rectangle path (never printed either way) */
   char *read_aln;               /* total_slots bytes, reference slot layout */
   char *genome_aln;             /* total_slots bytes */
   int32_t *status;              /* optional (device entry point): OR of SARU_S_* */

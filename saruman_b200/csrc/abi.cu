@@ -221,17 +221,19 @@ int plan_host(const saru_batch *b, Plan *pl) {
   return SARU_OK;
 }
 
-constexpr int kCta = 128;
+int smem_per_sm(int dev) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  return v > 0 ? v : 228 * 1024;
+}
 
-long band_grid(int dev, int n) {
-  // persistent grid: resident CTAs of the whole GPU
-  const long tiles = (n + kCta - 1) / kCta;
-  long g = (long)sm_count(dev) * 4;
-  return tiles < g ? tiles : g;
+// persistent grid of the banded kernel: as many CTAs as fit on the GPU
+long band_grid(int dev, long n, int max_m, int k) {
+  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k), smem_per_sm(dev));
 }
 
 size_t band_scratch_bytes(long grid, int max_m, bool wide) {
-  return (size_t)grid * kCta * 2 * (size_t)(max_m + 1) * (wide ? 8 : 4);
+  return saru::band_scratch_bytes(grid, max_m, wide);
 }
 
 // Enqueues the banded kernel on device buffers.
@@ -248,7 +250,7 @@ int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *sc
   a.max_m = pl.max_m;
   a.first_of_call = b->first_of_call;
   a.wide = pl.wide;
-  a.grid = band_grid(dev, b->n);
+  a.grid = band_grid(dev, b->n, pl.max_m, b->k);
   a.scores = r->scores;
   a.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
   a.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
@@ -260,7 +262,7 @@ int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *sc
     return SARU_E_INVALID;
   }
   if (b->n == 0) return SARU_OK;
-  SARU_CUDA(saru::launch_band_kernel(a, kCta, sm_count(dev), s));
+  SARU_CUDA(saru::launch_band_kernel(a, s));
   g_launches.fetch_add(1);
   return SARU_OK;
 }
@@ -364,7 +366,7 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
   SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
   bool full = !pl.band;
   if (pl.band) {
-    const long grid = band_grid(dev, b->n);
+    const long grid = band_grid(dev, b->n, pl.max_m, b->k);
     if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, pl.wide)))) return rc;
     if ((rc = run_band(&db, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, s)))
       return rc;
@@ -441,10 +443,9 @@ const char *saru_last_error(void) { return g_last_error.c_str(); }
 uint64_t saru_kernel_launches(void) { return g_launches.load(); }
 
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide) {
-  (void)k;
   int dev = current_device();
   if (dev < 0) dev = 0;
-  return band_scratch_bytes(band_grid(dev, n), read_length, wide != 0);
+  return band_scratch_bytes(band_grid(dev, n, read_length, k), read_length, wide != 0);
 }
 
 int saru_align_host(const saru_batch *batch, saru_result *result, int lane) {

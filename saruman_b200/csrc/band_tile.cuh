@@ -1,0 +1,262 @@
+// band_tile.cuh -- one warp tile of the banded kernel, as phases.
+//
+// A warp tile is 32 consecutive candidates, one per lane.  Their reads,
+// windows and output slots are three contiguous byte ranges, so the warp
+// stages the inputs into its shared-memory slice with 16-byte loads, aligns
+// out of shared memory, builds both alignment strings for the whole tile in
+// shared memory (zero-filled, as the reference's memset arena leaves them)
+// and writes the tile's slot range back with 16-byte stores.  Decision
+// planes (2 bits per band cell) go to a per-lane global scratch slice that
+// stays in L2; the traceback prefetches them two columns ahead.
+//
+// The phases are separated by warp barriers in the kernel; written as
+// functions of the lane so a host harness can run them lane by lane.
+//
+// Warp slice layout (bytes, each part 16-aligned):
+//   [reads staging RS][windows staging WS][region: codes+masks | outputs]
+// The region holds the lane-interleaved code/mask words during the fill
+// and the two output strings during the traceback.
+#pragma once
+#include <stdint.h>
+
+#include "saru_core.cuh"
+
+namespace saru {
+
+struct TileArgs {
+  const uint8_t *genome, *reads;
+  const int32_t *goff, *roff;
+  const int8_t *dirs;
+  long n;
+  int k, max_m, first_of_call;
+  int32_t *scores;
+  uint8_t *read_aln, *genome_aln;
+  void *planes;       // 2 * (max_m + 1) * pstride band words
+  long pstride;       // lanes of the whole grid
+  long rs_bytes, ws_bytes, region_bytes;
+};
+
+// Byte ranges of a tile in the three arrays.
+struct TileSpan {
+  long t0, t1;
+  long r_lo, r_hi, g_lo, g_hi, s_lo, s_hi;
+  long r_base, g_base, o_base_r, o_base_g, o_span_r;
+  bool fits;
+};
+
+SARU_HD long gstart_at(const int32_t *goff, long t) { return t ? goff[t - 1] : 0; }
+
+// Staging base of global range [lo, ...) of array `p`: byte x sits at
+// smem[x - base], with base chosen so that 16-byte aligned global addresses
+// map to 16-byte aligned smem offsets.
+SARU_HD long stage_base(const void *p, long lo) {
+  return lo - (long)(((uintptr_t)((const uint8_t *)p + lo)) & 15u);
+}
+
+SARU_HD TileSpan tile_span(const TileArgs &a, long wt) {
+  TileSpan s;
+  s.t0 = wt * 32;
+  s.t1 = s.t0 + 32 < a.n ? s.t0 + 32 : a.n;
+  s.r_lo = s.t0 ? a.roff[s.t0 - 1] : 0;
+  s.r_hi = a.roff[s.t1 - 1];
+  s.g_lo = gstart_at(a.goff, s.t0);
+  s.g_hi = a.goff[s.t1 - 1];
+  s.s_lo = s.g_lo + (long)a.k * s.t0;
+  s.s_hi = s.g_hi + (long)a.k * s.t1;
+  const long cnt = s.t1 - s.t0;
+  // a tile whose ranges exceed what regular candidates can span is not
+  // staged at all (its candidates are reported irregular)
+  s.fits = s.r_hi >= s.r_lo && s.g_hi >= s.g_lo && s.r_hi - s.r_lo <= cnt * (long)a.max_m &&
+           s.g_hi - s.g_lo <= cnt * (long)(a.max_m + 2 * a.k);
+  s.r_base = stage_base(a.reads, s.r_lo);
+  s.g_base = stage_base(a.genome, s.g_lo);
+  s.o_base_r = stage_base(a.read_aln, s.s_lo);
+  s.o_base_g = stage_base(a.genome_aln, s.s_lo);
+  s.o_span_r = ((s.s_hi - s.o_base_r) + 15) & ~15L;
+  return s;
+}
+
+// Copies global bytes [lo, hi) of src into dst (smem) at dst[x - base]:
+// 16-byte vectors where the global address is aligned, bytes at the edges.
+template <class Load16, class Load1>
+SARU_HD void stage_in(uint8_t *dst, const uint8_t *src, long lo, long hi, long base, int lane,
+                      Load16 ld16, Load1 ld1) {
+  const long a16 = base + ((lo - base + 15) & ~15L);
+  const long b16 = base + ((hi - base) & ~15L);
+  if (a16 >= b16) {
+    for (long x = lo + lane; x < hi; x += 32) dst[x - base] = ld1(src + x);
+    return;
+  }
+  for (long x = lo + lane; x < a16; x += 32) dst[x - base] = ld1(src + x);
+  const long nv = (b16 - a16) >> 4;
+  for (long i = lane; i < nv; i += 32) ld16(dst + (a16 - base) + 16 * i, src + a16 + 16 * i);
+  for (long x = b16 + lane; x < hi; x += 32) dst[x - base] = ld1(src + x);
+}
+
+// Writes smem src (holding byte x at src[x - base]) to global dst[lo, hi).
+template <class Store16>
+SARU_HD void stage_out(uint8_t *dst, const uint8_t *src, long lo, long hi, long base, int lane,
+                       Store16 st16) {
+  const long a16 = base + ((lo - base + 15) & ~15L);
+  const long b16 = base + ((hi - base) & ~15L);
+  if (a16 >= b16) {
+    for (long x = lo + lane; x < hi; x += 32) dst[x] = src[x - base];
+    return;
+  }
+  for (long x = lo + lane; x < a16; x += 32) dst[x] = src[x - base];
+  const long nv = (b16 - a16) >> 4;
+  for (long i = lane; i < nv; i += 32) st16(dst + a16 + 16 * i, src + (a16 - base) + 16 * i);
+  for (long x = b16 + lane; x < hi; x += 32) dst[x] = src[x - base];
+}
+
+// Per-lane state carried from the fill to the traceback.
+struct LaneState {
+  Cand c;
+  long gs, rs;
+  int score;
+  bool ok;
+};
+
+// Fill phase of one lane.  Returns status bits.
+template <typename T, class PlaneStore>
+SARU_HD int lane_fill(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
+                      const uint8_t *st_win, uint32_t *region32, LaneState &ls,
+                      PlaneStore store) {
+  const long t = s.t0 + lane;
+  ls.ok = false;
+  ls.score = a.k + 1;
+  if (t >= a.n) return 0;
+  int status = 0;
+  const int k = a.k;
+  const int code_words = (a.max_m + 7) / 8;
+  const int mwords = mask_words(k, a.max_m + 2 * k);
+  Strided codes{region32 + lane, 32};
+  Strided mask{region32 + code_words * 32 + lane, 32};
+  Cand &c = ls.c;
+  ls.gs = gstart_at(a.goff, t);
+  ls.rs = t ? a.roff[t - 1] : 0;
+  c.m = int(a.roff[t] - ls.rs);
+  c.L = int(a.goff[t] - ls.gs);
+  c.k = k;
+  flank_of(a.dirs[t], k, c.so, c.eo);
+  c.first_of_call = a.first_of_call && t == 0;
+  if (!s.fits || c.L != c.m + c.so + c.eo || c.m <= 3 * k || c.m > a.max_m || c.m < 2) {
+    status |= 1;  // irregular
+  } else {
+    const uint8_t *rd = st_reads + (ls.rs - s.r_base);
+    const uint8_t *wn = st_win + (ls.gs - s.g_base);
+    if (!build_codes(c, [&](int j) -> uint8_t { return rd[j]; },
+                     [&](int p) -> uint8_t { return wn[p]; }, codes, mask, mwords)) {
+      status |= 2;  // alphabet
+    } else {
+      ls.ok = true;
+      ls.score = fill_band<T>(c, codes, mask, mwords, store);
+    }
+  }
+  a.scores[t] = ls.score;
+  return status;
+}
+
+// Traceback phase of one lane: writes the lane's two strings into the
+// output staging (reversed in place, like the reference).  Returns status.
+template <typename T, class PlaneGet>
+SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
+                           const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
+                           const LaneState &ls, PlaneGet plane) {
+  const long t = s.t0 + lane;
+  if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
+  const Cand &c = ls.c;
+  const uint8_t *rd = st_reads + (ls.rs - s.r_base);
+  const uint8_t *wn = st_win + (ls.gs - s.g_base);
+  const long slot = ls.gs + (long)a.k * t;
+  uint8_t *orr = out_r + (slot - s.o_base_r);
+  uint8_t *og = out_g + (slot - s.o_base_g);
+  const int maxs = max_steps(c);
+  int n = 0;
+  bool bad = false;
+  traceback_band(
+      c,
+      [&](int j, int b) -> int {
+        if (b < 0 || b >= int(sizeof(T) * 8)) {
+          bad = true;
+          return OP_STOP;
+        }
+        return plane(j, b);
+      },
+      [&](int op, int row, int col) {
+        if (n < maxs) {
+          orr[n] = op == OP_UP ? uint8_t('_') : rd[col - 1];
+          og[n] = op == OP_LEFT ? uint8_t('_') : wn[row - 1];
+        }
+        ++n;
+      });
+  int status = 0;
+  if (bad || n > maxs) {
+    status |= 4;  // overflow
+    n = n > maxs ? maxs : n;
+  }
+  for (int i = 0, j = n - 1; i < j; ++i, --j) {
+    uint8_t x = orr[i];
+    orr[i] = orr[j];
+    orr[j] = x;
+    x = og[i];
+    og[i] = og[j];
+    og[j] = x;
+  }
+  return status;
+}
+
+// Decision planes of one lane, read column by column from m down to 1 with
+// the next two columns' words already requested.
+template <typename T>
+struct PlaneRing {
+  const T *planes;
+  long stride, slot;
+  int c0;
+  T A0, B0, A1, B1, A2, B2;
+  SARU_HD T ldA(int j) const { return planes[(2 * (long)j) * stride + slot]; }
+  SARU_HD T ldB(int j) const { return planes[(2 * (long)j + 1) * stride + slot]; }
+  SARU_HD void init(int m) {
+    c0 = m;
+    A0 = ldA(m);
+    B0 = ldB(m);
+    A1 = m >= 2 ? ldA(m - 1) : T(0);
+    B1 = m >= 2 ? ldB(m - 1) : T(0);
+    A2 = m >= 3 ? ldA(m - 2) : T(0);
+    B2 = m >= 3 ? ldB(m - 2) : T(0);
+  }
+  SARU_HD int get(int j, int b) {
+    if (j < c0) {  // the path moved one column left
+      A0 = A1;
+      B0 = B1;
+      A1 = A2;
+      B1 = B2;
+      --c0;
+      if (c0 >= 3) {
+        A2 = ldA(c0 - 2);
+        B2 = ldB(c0 - 2);
+      }
+    }
+    return int((A0 >> b) & T(1)) | (int((B0 >> b) & T(1)) << 1);
+  }
+};
+
+// Shared-memory slice sizes for a maximum read length and k.
+struct SliceLayout {
+  long rs_bytes, ws_bytes, region_bytes, warp_smem;
+};
+
+SARU_HD SliceLayout slice_layout(int max_m, int k) {
+  SliceLayout L;
+  const long code_words = (max_m + 7) / 8;
+  const long mwords = mask_words(k, max_m + 2 * k);
+  L.rs_bytes = (32L * max_m + 32 + 15) & ~15L;
+  L.ws_bytes = (32L * (max_m + 2 * k) + 32 + 15) & ~15L;
+  const long cm = 4L * 32 * (code_words + NCODES * mwords);
+  const long out = 2 * ((32L * (max_m + 3 * k) + 32 + 15) & ~15L);
+  L.region_bytes = ((cm > out ? cm : out) + 15) & ~15L;
+  L.warp_smem = L.rs_bytes + L.ws_bytes + L.region_bytes;
+  return L;
+}
+
+}  // namespace saru

@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "kernels.cuh"
+#include "band_tile.cuh"
 #include "saru_core.cuh"
 
 namespace saru {
@@ -21,109 +22,69 @@ namespace saru {
 __device__ __forceinline__ long gstart_of(const int32_t *goff, long t) { return t ? goff[t - 1] : 0; }
 
 // ---------------------------------------------------------------------------
-// banded kernel
+// banded kernel: persistent warps over warp tiles (band_tile.cuh)
 // ---------------------------------------------------------------------------
 
-// Cooperative zero fill of bytes [lo, hi): 16-byte stores for the aligned
-// middle, byte stores at the edges.
-__device__ __forceinline__ void zero_range(uint8_t *base, long lo, long hi, int tid, int nthr) {
-  const long a16 = (lo + 15) & ~15L, b16 = hi & ~15L;
-  if (a16 >= b16) {
-    for (long i = lo + tid; i < hi; i += nthr) base[i] = 0;
-    return;
-  }
-  for (long i = lo + tid; i < a16; i += nthr) base[i] = 0;
-  uint4 *v = reinterpret_cast<uint4 *>(base + a16);
-  const long nv = (b16 - a16) >> 4;
-  for (long i = tid; i < nv; i += nthr) v[i] = make_uint4(0, 0, 0, 0);
-  for (long i = b16 + tid; i < hi; i += nthr) base[i] = 0;
-}
-
-template <typename T, int CTA>
-__global__ void __launch_bounds__(CTA) saru_band_kernel(KernelArgs a) {
-  extern __shared__ uint32_t smem[];
-  const int tid = threadIdx.x;
-  const long slot_id = (long)blockIdx.x * CTA + tid;
-  const long sstride = (long)gridDim.x * CTA;
-  const int k = a.k;
-  const int code_words = (a.max_m + 7) / 8;
-  const int mwords = mask_words(k, a.max_m + 2 * k);
-  Strided codes{smem + tid, CTA};
-  Strided mask{smem + code_words * CTA + tid, CTA};
+template <typename T, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) saru_band_kernel(KernelArgs a) {
+  extern __shared__ uint4 smem_v[];
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  uint8_t *ws = reinterpret_cast<uint8_t *>(smem_v) + (long)wid * a.warp_smem;
+  uint8_t *st_reads = ws;
+  uint8_t *st_win = ws + a.rs_bytes;
+  uint8_t *region = st_win + a.ws_bytes;
+  uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
+  const long gwarp = (long)blockIdx.x * WARPS + wid;
+  const long nwarps = (long)gridDim.x * WARPS;
+  TileArgs ta{a.genome, a.reads, a.goff, a.roff, a.dirs, a.n, a.k, a.max_m, a.first_of_call,
+              a.scores, a.read_aln, a.genome_aln, a.scratch, nwarps * 32, a.rs_bytes, a.ws_bytes,
+              a.warp_smem - a.rs_bytes - a.ws_bytes};
   T *planes = reinterpret_cast<T *>(a.scratch);
-  uint32_t ops[kMaxOpWords];
+  const long pslot = gwarp * 32 + lane;
+  auto ld16 = [](uint8_t *d, const uint8_t *g) {
+    *reinterpret_cast<uint4 *>(d) = __ldg(reinterpret_cast<const uint4 *>(g));
+  };
+  auto ld1 = [](const uint8_t *g) -> uint8_t { return __ldg(g); };
+  auto st16 = [](uint8_t *g, const uint8_t *d) {
+    *reinterpret_cast<uint4 *>(g) = *reinterpret_cast<const uint4 *>(d);
+  };
 
-  for (long tile = blockIdx.x; tile * CTA < a.n; tile += gridDim.x) {
-    const long t = tile * CTA + tid;
+  for (long wt = gwarp; wt * 32 < a.n; wt += nwarps) {
+    const TileSpan s = tile_span(ta, wt);
+    if (!s.fits) {  // offsets no regular call can have: report, do not stage
+      const long t = s.t0 + lane;
+      if (t < a.n) a.scores[t] = a.k + 1;
+      if (lane == 0) atomicOr(a.status, kStatusIrregular);
+      continue;
+    }
+    stage_in(st_reads, a.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
+    stage_in(st_win, a.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
+    __syncwarp();
+    LaneState ls;
+    int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
+      planes[(2 * (long)j) * ta.pstride + pslot] = A;
+      planes[(2 * (long)j + 1) * ta.pstride + pslot] = B;
+    });
+    __syncwarp();
+    uint8_t *out_r = region;
+    uint8_t *out_g = region + s.o_span_r;
     {
-      // zero the tile's slot bytes (a contiguous range) before any thread
-      // writes its strings into them
-      const long t0 = tile * CTA, t1 = (t0 + CTA < a.n ? t0 + CTA : a.n);
-      const long lo = gstart_of(a.goff, t0) + (long)k * t0;
-      const long hi = (long)a.goff[t1 - 1] + (long)k * t1;
-      zero_range(a.read_aln, lo, hi, tid, CTA);
-      zero_range(a.genome_aln, lo, hi, tid, CTA);
-      __syncthreads();
+      uint4 *p4 = reinterpret_cast<uint4 *>(region);
+      const long nv = ta.region_bytes >> 4;
+      for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
     }
-    if (t >= a.n) continue;
-    const long gs = gstart_of(a.goff, t), rs = t ? a.roff[t - 1] : 0;
-    Cand c;
-    c.m = int(a.roff[t] - rs);
-    c.L = int(a.goff[t] - gs);
-    c.k = k;
-    flank_of(a.dirs[t], k, c.so, c.eo);
-    c.first_of_call = a.first_of_call && t == 0;
-    if (c.L != c.m + c.so + c.eo || c.m <= 3 * k || c.m > a.max_m) {
-      atomicOr(a.status, kStatusIrregular);
-      a.scores[t] = k + 1;
-      continue;
-    }
-    const uint8_t *rd = a.reads + rs;
-    const uint8_t *wn = a.genome + gs;
-    auto rdf = [&](int j) -> uint8_t { return __ldg(rd + j); };
-    auto wnf = [&](int p) -> uint8_t { return __ldg(wn + p); };
-    if (!build_codes(c, rdf, wnf, codes, mask, mwords)) {
-      atomicOr(a.status, kStatusAlphabet);
-      a.scores[t] = k + 1;
-      continue;
-    }
-    const int score = fill_band<T>(c, codes, mask, mwords, [&](int j, T A, T B) {
-      planes[(2 * (long)j) * sstride + slot_id] = A;
-      planes[(2 * (long)j + 1) * sstride + slot_id] = B;
-    });
-    a.scores[t] = score;
-    if (score > k) continue;
-    int nsteps = 0;
-    bool bad = false;
-    const int maxs = max_steps(c);
-    traceback_band(
-        c,
-        [&](int j, int b) -> int {
-          if (b < 0 || b >= int(sizeof(T) * 8)) {
-            bad = true;
-            return OP_STOP;
-          }
-          const T A = planes[(2 * (long)j) * sstride + slot_id];
-          const T B = planes[(2 * (long)j + 1) * sstride + slot_id];
-          return int((A >> b) & T(1)) | (int((B >> b) & T(1)) << 1);
-        },
-        [&](int op, int, int) {
-          if (nsteps < maxs) {
-            if ((nsteps & 15) == 0) ops[nsteps >> 4] = 0;
-            ops[nsteps >> 4] |= uint32_t(op) << ((nsteps & 15) * 2);
-          }
-          ++nsteps;
-        });
-    if (bad || nsteps > maxs) {
-      atomicOr(a.status, kStatusOverflow);
-      continue;
-    }
-    uint8_t *ra = a.read_aln + gs + (long)k * t;
-    uint8_t *ga = a.genome_aln + gs + (long)k * t;
-    emit_forward(c, ops, nsteps, rdf, wnf, [&](int pos, uint8_t x, uint8_t y) {
-      ra[pos] = x;
-      ga[pos] = y;
-    });
+    __syncwarp();
+    PlaneRing<T> ring{planes, ta.pstride, pslot};
+    if (ls.ok && ls.score <= a.k) ring.init(ls.c.m);
+    st |= lane_traceback<T>(ta, s, lane, st_reads, st_win, out_r, out_g, ls,
+                            [&](int j, int b) { return ring.get(j, b); });
+    if (st) atomicOr(a.status, (st & 1 ? kStatusIrregular : 0) | (st & 2 ? kStatusAlphabet : 0) |
+                                   (st & 4 ? kStatusOverflow : 0));
+    __syncwarp();
+    stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
+    stage_out(a.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
+    __syncwarp();
   }
 }
 
@@ -240,33 +201,49 @@ __global__ void saru_full_trace_kernel(FullArgs a) {
 // launchers
 // ---------------------------------------------------------------------------
 
-template <typename T, int CTA>
-static cudaError_t launch_band(const KernelArgs &a, int sms, cudaStream_t s) {
-  const size_t smem = band_smem_bytes(a.max_m, a.k, CTA);
-  auto kern = saru_band_kernel<T, CTA>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+constexpr int kWarps = 4;  // warps per CTA of the banded kernel
+
+BandLayout band_layout(int max_m, int k) {
+  const SliceLayout S = slice_layout(max_m, k);
+  BandLayout L;
+  L.rs_bytes = S.rs_bytes;
+  L.ws_bytes = S.ws_bytes;
+  L.region_bytes = S.region_bytes;
+  L.warp_smem = S.warp_smem;
+  L.cta_smem = S.warp_smem * kWarps;
+  return L;
+}
+
+template <typename T>
+static cudaError_t launch_band(KernelArgs a, const BandLayout &L, cudaStream_t s) {
+  auto kern = saru_band_kernel<T, kWarps>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.cta_smem);
   if (e != cudaSuccess) return e;
-  const long tiles = (a.n + CTA - 1) / CTA;
-  long grid = a.grid > 0 ? a.grid : tiles;
-  if (grid > tiles) grid = tiles;
-  (void)sms;
-  kern<<<(unsigned)grid, CTA, smem, s>>>(a);
+  a.rs_bytes = L.rs_bytes;
+  a.ws_bytes = L.ws_bytes;
+  a.warp_smem = L.warp_smem;
+  kern<<<(unsigned)a.grid, 32 * kWarps, L.cta_smem, s>>>(a);
   return cudaGetLastError();
 }
 
-size_t band_smem_bytes(int max_m, int k, int cta) {
-  const int code_words = (max_m + 7) / 8;
-  const int mwords = mask_words(k, max_m + 2 * k);
-  return sizeof(uint32_t) * (size_t)cta * (size_t)(code_words + NCODES * mwords);
+long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm) {
+  const long tiles = (n + 32 * kWarps - 1) / (32 * kWarps);
+  long per_sm = smem_per_sm / (L.cta_smem + 1024);
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 16) per_sm = 16;
+  const long g = (long)sms * per_sm;
+  return tiles < g ? (tiles > 0 ? tiles : 1) : g;
 }
 
-cudaError_t launch_band_kernel(const KernelArgs &a, int cta, int sms, cudaStream_t s) {
-  if (a.wide) {
-    if (cta == 64) return launch_band<uint64_t, 64>(a, sms, s);
-    return launch_band<uint64_t, 128>(a, sms, s);
-  }
-  if (cta == 64) return launch_band<uint32_t, 64>(a, sms, s);
-  return launch_band<uint32_t, 128>(a, sms, s);
+size_t band_scratch_bytes(long grid, int max_m, bool wide) {
+  return (size_t)grid * 32 * kWarps * 2 * (size_t)(max_m + 1) * (wide ? 8 : 4);
+}
+
+cudaError_t launch_band_kernel(const KernelArgs &a, cudaStream_t s) {
+  const BandLayout L = band_layout(a.max_m, a.k);
+  if (a.wide) return launch_band<uint64_t>(a, L, s);
+  return launch_band<uint32_t>(a, L, s);
 }
 
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s) {

@@ -26,12 +26,17 @@ struct KernelArgs {
   int max_m;
   int first_of_call;
   int wide;  // 64-bit band
-  long grid; // CTAs of the persistent grid (<= 0: one per tile)
+  long grid; // CTAs of the persistent grid
   int32_t *scores;
   uint8_t *read_aln;
   uint8_t *genome_aln;
   void *scratch;  // decision planes: 2 * (max_m + 1) * grid * CTA band words
   int *status;
+  long rs_bytes, ws_bytes, warp_smem;  // shared-memory slice layout (set by the launcher)
+};
+
+struct BandLayout {
+  long rs_bytes = 0, ws_bytes = 0, region_bytes = 0, warp_smem = 0, cta_smem = 0;
 };
 
 struct FullArgs {
@@ -51,8 +56,10 @@ struct FullArgs {
   int *status;
 };
 
-size_t band_smem_bytes(int max_m, int k, int cta);
-cudaError_t launch_band_kernel(const KernelArgs &a, int cta, int sms, cudaStream_t s);
+BandLayout band_layout(int max_m, int k);
+long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm);
+size_t band_scratch_bytes(long grid, int max_m, bool wide);
+cudaError_t launch_band_kernel(const KernelArgs &a, cudaStream_t s);
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
 
 }  // namespace saru

@@ -213,24 +213,17 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
     top += (int)((~d0) & T(1));
   }
   // column m with explicit values; column m-1 band values from the deltas
-  int vprev[BITS + 1];
-  {
-    int v = top;
-    vprev[0] = v;
-    for (int b = 1; b < BITS; ++b) {
-      v += (int)((Pv >> b) & T(1)) - (int)((Mv >> b) & T(1));
-      vprev[b] = v;
-    }
-    vprev[BITS] = vprev[BITS - 1] + 1;
-  }
   const T eqm = window_bits<T>(mask + code_at(codes, m - 1) * mwords, m);
   const int bmax = c.L - m + k;  // band bit of row L in column m
   T A = 0, B = 0;
-  int vcur_prev = vprev[0] + 1;  // D[m - k - 1][m], entering from the left
+  int vb = top;           // D[m-1-k+b][m-1]: column m-1 at band bit b
+  int vcur_prev = top + 1;  // D[m-k-1][m], entering from the left
   int score = k + 1;
   for (int b = 0; b <= bmax && b < BITS; ++b) {
+    const int vb1 = b + 1 < BITS ? vb + (int)((Pv >> (b + 1)) & T(1)) - (int)((Mv >> (b + 1)) & T(1))
+                                 : vb + 1;
     const int row = m - k + b;
-    const int dg = vprev[b], lf = vprev[b + 1], tp = vcur_prev;
+    const int dg = vb, lf = vb1, tp = vcur_prev;
     const bool e = (eqm >> b) & T(1);
     const int corr = (row - 1 >= c.L - 2 * c.eo) ? 1 : 0;
     int v = dg + (e ? 0 : 1);
@@ -244,6 +237,7 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
     A |= T(op & 1) << b;
     B |= T(op >> 1) << b;
     vcur_prev = v;
+    vb = vb1;
     if (b == bmax) score = v;
   }
   planes(m, A, B);

@@ -1,0 +1,92 @@
+// Host emulation of the banded kernel's warp loop (saruman_b200/csrc/
+// kernels.cu, saru_band_kernel) over band_tile.cuh, for CPU tests.  Each
+// warp's phases run lane by lane in the order the kernel's warp barriers
+// impose.  Built with AddressSanitizer and exactly-sized buffers (shared
+// slices, planes, inputs, outputs), it checks the kernel's index arithmetic
+// on the CPU before the kernel runs on a GPU.  Test infrastructure only.
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../saruman_b200/csrc/band_tile.cuh"
+
+using namespace saru;
+
+template <typename T>
+static int run(const TileArgs &a0, int nwarps_total) {
+  TileArgs a = a0;
+  const SliceLayout S = slice_layout(a.max_m, a.k);
+  a.rs_bytes = S.rs_bytes;
+  a.ws_bytes = S.ws_bytes;
+  a.region_bytes = S.region_bytes;
+  a.pstride = (long)nwarps_total * 32;
+  std::vector<T> planes_v((size_t)2 * (a.max_m + 1) * a.pstride);
+  T *planes = planes_v.data();
+  int status = 0;
+  auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
+  auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
+  auto st16 = [](uint8_t *g, const uint8_t *d) { memcpy(g, d, 16); };
+  for (int gwarp = 0; gwarp < nwarps_total; ++gwarp) {
+    // the three parts of a warp's shared slice, each its own exactly-sized
+    // 16-aligned allocation so an overrun of any part is caught
+    uint8_t *st_reads = (uint8_t *)aligned_alloc(16, (size_t)S.rs_bytes);
+    uint8_t *st_win = (uint8_t *)aligned_alloc(16, (size_t)S.ws_bytes);
+    uint8_t *region = (uint8_t *)aligned_alloc(16, (size_t)S.region_bytes);
+    memset(st_reads, 0xA5, (size_t)S.rs_bytes);
+    memset(st_win, 0xA5, (size_t)S.ws_bytes);
+    memset(region, 0xA5, (size_t)S.region_bytes);
+    uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
+    for (long wt = gwarp; wt * 32 < a.n; wt += nwarps_total) {
+      const TileSpan s = tile_span(a, wt);
+      if (!s.fits) {
+        for (int lane = 0; lane < 32; ++lane)
+          if (s.t0 + lane < a.n) a.scores[s.t0 + lane] = a.k + 1;
+        status |= 1;
+        continue;
+      }
+      for (int lane = 0; lane < 32; ++lane) {
+        stage_in(st_reads, a.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
+        stage_in(st_win, a.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
+      }
+      LaneState ls[32];
+      for (int lane = 0; lane < 32; ++lane) {
+        const long pslot = (long)gwarp * 32 + lane;
+        status |= lane_fill<T>(a, s, lane, st_reads, st_win, region32, ls[lane],
+                               [&](int j, T A, T B) {
+                                 planes[(2 * (long)j) * a.pstride + pslot] = A;
+                                 planes[(2 * (long)j + 1) * a.pstride + pslot] = B;
+                               });
+      }
+      uint8_t *out_r = region, *out_g = region + s.o_span_r;
+      memset(region, 0, (size_t)S.region_bytes);
+      for (int lane = 0; lane < 32; ++lane) {
+        const long pslot = (long)gwarp * 32 + lane;
+        PlaneRing<T> ring{planes, a.pstride, pslot};
+        if (ls[lane].ok && ls[lane].score <= a.k) ring.init(ls[lane].c.m);
+        status |= lane_traceback<T>(a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
+                                    [&](int j, int b) { return ring.get(j, b); });
+      }
+      for (int lane = 0; lane < 32; ++lane) {
+        stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
+        stage_out(a.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
+      }
+    }
+    free(st_reads);
+    free(st_win);
+    free(region);
+  }
+  return status;
+}
+
+// Aligns a call with the emulated kernel.  Buffers are the caller's (the
+// Python side passes exactly-sized copies, at chosen misalignments).
+extern "C" int tile_align_batch(const uint8_t *genome, const uint8_t *reads, const int *goff,
+                                const int *roff, const int8_t *dirs, long n, int k, int max_m,
+                                int wide, int first_of_call, int nwarps, int *scores,
+                                uint8_t *ra, uint8_t *ga) {
+  TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, ra, ga,
+             nullptr, 0, 0, 0, 0};
+  return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
+}

@@ -1,0 +1,81 @@
+"""Runs the host emulation of the banded kernel's warp loop under
+AddressSanitizer (child process of tests/test_tile_host.py).
+
+Every array is allocated at exactly its size and placed at a chosen
+misalignment, so any out-of-range shared-slice, plane, input or output
+access aborts the run; the outputs are compared with the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+import refkit as R  # noqa: E402
+from saruman_b200 import workloads as W  # noqa: E402
+
+
+def exact(a: np.ndarray, off: int) -> np.ndarray:
+    """Copy of `a` whose data ends exactly at the end of its allocation and
+    starts `off` bytes past a 16-byte boundary (when the allocator aligns)."""
+    raw = np.empty(a.nbytes + off, np.uint8)
+    v = raw[off:].view(a.dtype)
+    v[...] = a.reshape(-1)
+    return v
+
+
+def main():
+    lib = C.CDLL(sys.argv[1])
+    P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    cases = [(36, 2, 0.05), (100, 5, 0.04), (75, 5, 0.2), (150, 9, 0.05), (250, 15, 0.05),
+             (20, 1, 0.1), (40, 7, 0.1), (64, 15, 0.3)]
+    bad = 0
+    for ci, (m, k, err) in enumerate(cases):
+        for seed in range(2):
+            n = 97 + 31 * seed  # ragged last tile
+            b = W.random_batch(m, k, n, seed=seed + 5 * ci, err=err,
+                               alphabet=b"ACGT" if seed == 0 else b"ACGTN")
+            s1, ra1, ga1, _ = R.oracle_align(b)
+            wide = 1 if (k > 7) else 0
+            for off in (0, 3, 9):
+                g = exact(b.genome, off)
+                r = exact(b.reads, (off + 5) % 16)
+                go = exact(b.genome_offsets, 0)
+                ro = exact(b.read_offsets, 0)
+                d = exact(b.dirs, 1)
+                sc = np.zeros(n, np.int32)
+                ra = exact(np.zeros(b.total_genome, np.uint8), (off + 7) % 16)
+                ga = exact(np.zeros(b.total_genome, np.uint8), (off + 11) % 16)
+                st = lib.tile_align_batch(P(g), P(r), P(go), P(ro), P(d), C.c_long(n), C.c_int(k),
+                                          C.c_int(m), C.c_int(wide), C.c_int(1), C.c_int(3),
+                                          P(sc), P(ra), P(ga))
+                ok = (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
+                      and np.array_equal(ra1, ra) and np.array_equal(ga1, ga))
+                if not ok:
+                    bad += 1
+                    print("MISMATCH", m, k, seed, off, st, flush=True)
+    # an irregular tile (window far too long) must be rejected, not staged
+    b = W.random_batch(36, 2, 40, seed=1)
+    go = b.genome_offsets.copy()
+    go[5:] += 100000
+    g = np.zeros(int(go[-1]), np.uint8)
+    sc = np.zeros(b.n, np.int32)
+    ra = np.zeros(int(go[-1]) + 2 * b.n, np.uint8)
+    ga = np.zeros_like(ra)
+    st = lib.tile_align_batch(P(g), P(b.reads), P(go), P(b.read_offsets), P(b.dirs),
+                              C.c_long(b.n), C.c_int(2), C.c_int(36), C.c_int(0), C.c_int(1),
+                              C.c_int(3), P(sc), P(ra), P(ga))
+    if not (st & 1):
+        bad += 1
+        print("irregular tile not reported", st)
+    print("BAD", bad)
+    sys.exit(1 if bad else 0)
+
+
+if __name__ == "__main__":
+    main()
