@@ -232,8 +232,8 @@ long band_grid(int dev, long n, int max_m, int k) {
   return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k), smem_per_sm(dev));
 }
 
-size_t band_scratch_bytes(long grid, int max_m, bool wide) {
-  return saru::band_scratch_bytes(grid, max_m, wide);
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
+  return saru::band_scratch_bytes(grid, max_m, k, wide);
 }
 
 // Enqueues the banded kernel on device buffers.
@@ -256,9 +256,9 @@ int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *sc
   a.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
   a.scratch = scratch;
   a.status = status_dev;
-  if (band_scratch_bytes(a.grid, pl.max_m, pl.wide) > scratch_bytes) {
+  if (band_scratch_bytes(a.grid, pl.max_m, b->k, pl.wide) > scratch_bytes) {
     set_error("scratch too small: %zu < %zu", scratch_bytes,
-              band_scratch_bytes(a.grid, pl.max_m, pl.wide));
+              band_scratch_bytes(a.grid, pl.max_m, b->k, pl.wide));
     return SARU_E_INVALID;
   }
   if (b->n == 0) return SARU_OK;
@@ -367,7 +367,7 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
   bool full = !pl.band;
   if (pl.band) {
     const long grid = band_grid(dev, b->n, pl.max_m, b->k);
-    if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, pl.wide)))) return rc;
+    if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, b->k, pl.wide)))) return rc;
     if ((rc = run_band(&db, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, s)))
       return rc;
     SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -445,7 +445,7 @@ uint64_t saru_kernel_launches(void) { return g_launches.load(); }
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide) {
   int dev = current_device();
   if (dev < 0) dev = 0;
-  return band_scratch_bytes(band_grid(dev, n, read_length, k), read_length, wide != 0);
+  return band_scratch_bytes(band_grid(dev, n, read_length, k), read_length, k, wide != 0);
 }
 
 int saru_align_host(const saru_batch *batch, saru_result *result, int lane) {

@@ -25,11 +25,12 @@ __device__ __forceinline__ long gstart_of(const int32_t *goff, long t) { return 
 // banded kernel: persistent warps over warp tiles (band_tile.cuh)
 // ---------------------------------------------------------------------------
 
-template <typename T, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) saru_band_kernel(KernelArgs a) {
+template <typename T>
+__global__ void __launch_bounds__(128) saru_band_kernel(KernelArgs a) {
   extern __shared__ uint4 smem_v[];
   const int lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
+  const int WARPS = blockDim.x >> 5;
   uint8_t *ws = reinterpret_cast<uint8_t *>(smem_v) + (long)wid * a.warp_smem;
   uint8_t *st_reads = ws;
   uint8_t *st_win = ws + a.rs_bytes;
@@ -201,7 +202,7 @@ __global__ void saru_full_trace_kernel(FullArgs a) {
 // launchers
 // ---------------------------------------------------------------------------
 
-constexpr int kWarps = 4;  // warps per CTA of the banded kernel
+constexpr long kMaxCtaSmem = 227 * 1024;  // opt-in shared memory per block on sm_100
 
 BandLayout band_layout(int max_m, int k) {
   const SliceLayout S = slice_layout(max_m, k);
@@ -210,25 +211,29 @@ BandLayout band_layout(int max_m, int k) {
   L.ws_bytes = S.ws_bytes;
   L.region_bytes = S.region_bytes;
   L.warp_smem = S.warp_smem;
-  L.cta_smem = S.warp_smem * kWarps;
+  long w = kMaxCtaSmem / S.warp_smem;
+  L.warps = (int)(w >= 4 ? 4 : (w >= 2 ? 2 : (w >= 1 ? 1 : 0)));
+  L.cta_smem = S.warp_smem * L.warps;
   return L;
 }
 
 template <typename T>
 static cudaError_t launch_band(KernelArgs a, const BandLayout &L, cudaStream_t s) {
-  auto kern = saru_band_kernel<T, kWarps>;
+  if (L.warps < 1) return cudaErrorInvalidValue;
+  auto kern = saru_band_kernel<T>;
   cudaError_t e =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.cta_smem);
   if (e != cudaSuccess) return e;
   a.rs_bytes = L.rs_bytes;
   a.ws_bytes = L.ws_bytes;
   a.warp_smem = L.warp_smem;
-  kern<<<(unsigned)a.grid, 32 * kWarps, L.cta_smem, s>>>(a);
+  kern<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
   return cudaGetLastError();
 }
 
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm) {
-  const long tiles = (n + 32 * kWarps - 1) / (32 * kWarps);
+  const long per_cta = 32L * (L.warps > 0 ? L.warps : 1);
+  const long tiles = (n + per_cta - 1) / per_cta;
   long per_sm = smem_per_sm / (L.cta_smem + 1024);
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 16) per_sm = 16;
@@ -236,8 +241,10 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm) {
   return tiles < g ? (tiles > 0 ? tiles : 1) : g;
 }
 
-size_t band_scratch_bytes(long grid, int max_m, bool wide) {
-  return (size_t)grid * 32 * kWarps * 2 * (size_t)(max_m + 1) * (wide ? 8 : 4);
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
+  const BandLayout L = band_layout(max_m, k);
+  return (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 * (size_t)(max_m + 1) *
+         (wide ? 8 : 4);
 }
 
 cudaError_t launch_band_kernel(const KernelArgs &a, cudaStream_t s) {

@@ -37,6 +37,7 @@ struct KernelArgs {
 
 struct BandLayout {
   long rs_bytes = 0, ws_bytes = 0, region_bytes = 0, warp_smem = 0, cta_smem = 0;
+  int warps = 0;  // warps per CTA (0: a warp slice does not fit)
 };
 
 struct FullArgs {
@@ -58,7 +59,7 @@ struct FullArgs {
 
 BandLayout band_layout(int max_m, int k);
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm);
-size_t band_scratch_bytes(long grid, int max_m, bool wide);
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide);
 cudaError_t launch_band_kernel(const KernelArgs &a, cudaStream_t s);
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
 
