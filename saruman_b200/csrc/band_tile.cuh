@@ -109,6 +109,15 @@ SARU_HD void stage_out(uint8_t *dst, const uint8_t *src, long lo, long hi, long 
   for (long x = b16 + lane; x < hi; x += 32) dst[x] = src[x - base];
 }
 
+// Bytes p..p+3 (little endian) from a byte buffer at any alignment, with
+// two aligned 32-bit loads; reads up to 7 bytes past p, which the staging
+// slack covers.
+SARU_HD uint32_t load4(const uint8_t *p) {
+  const uintptr_t a = (uintptr_t)p;
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+  return fshr32(w[0], w[1], (uint32_t)(a & 3u) * 8u);
+}
+
 // Per-lane state carried from the fill to the traceback.
 struct LaneState {
   Cand c;
@@ -145,7 +154,9 @@ SARU_HD int lane_fill(const TileArgs &a, const TileSpan &s, int lane, const uint
   } else {
     const uint8_t *rd = st_reads + (ls.rs - s.r_base);
     const uint8_t *wn = st_win + (ls.gs - s.g_base);
-    if (!build_codes(c, [&](int j) -> uint8_t { return rd[j]; },
+    if (!build_codes_acgt(c, [&](int i) { return load4(rd + i); },
+                          [&](int i) { return load4(wn + i); }, codes, mask, mwords) &&
+        !build_codes(c, [&](int j) -> uint8_t { return rd[j]; },
                      [&](int p) -> uint8_t { return wn[p]; }, codes, mask, mwords)) {
       status |= 2;  // alphabet
     } else {
@@ -157,89 +168,131 @@ SARU_HD int lane_fill(const TileArgs &a, const TileSpan &s, int lane, const uint
   return status;
 }
 
-// Traceback phase of one lane: writes the lane's two strings into the
-// output staging (reversed in place, like the reference).  Returns status.
-template <typename T, class PlaneGet>
+// Traceback phase of one lane: writes the lane's two strings into its slot
+// of the output staging, in reading order (the reference emits from the
+// alignment end and reverses in place, src/cuda-functions.cu:306-307; here
+// the characters are written from the slot end downwards and the string is
+// then moved to the slot start, which leaves the same bytes).
+//
+// The walk visits columns m, m-1, ... one at a time (a diagonal or left step
+// moves exactly one column, an up step stays), so the decision planes of
+// column j are requested DEPTH columns before they are used, from a ring of
+// registers with static slots.  Decisions follow the reference's tests as
+// recorded by the fill; column 0 and row 0 follow the reference's rules for
+// the matrix border (see traceback_band in saru_core.cuh).
+template <typename T, int DEPTH, class LoadA, class LoadB>
 SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
                            const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
-                           const LaneState &ls, PlaneGet plane) {
+                           const LaneState &ls, LoadA ldA, LoadB ldB) {
+  constexpr int BITS = int(sizeof(T) * 8);
   const long t = s.t0 + lane;
   if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
   const Cand &c = ls.c;
   const uint8_t *rd = st_reads + (ls.rs - s.r_base);
   const uint8_t *wn = st_win + (ls.gs - s.g_base);
   const long slot = ls.gs + (long)a.k * t;
-  uint8_t *orr = out_r + (slot - s.o_base_r);
-  uint8_t *og = out_g + (slot - s.o_base_g);
-  const int maxs = max_steps(c);
-  int n = 0;
-  bool bad = false;
-  traceback_band(
-      c,
-      [&](int j, int b) -> int {
-        if (b < 0 || b >= int(sizeof(T) * 8)) {
-          bad = true;
-          return OP_STOP;
+  uint8_t *sr = out_r + (slot - s.o_base_r);
+  uint8_t *sg = out_g + (slot - s.o_base_g);
+  const int cap = c.L + c.k;  // slot bytes
+  uint8_t *er = sr + cap, *eg = sg + cap;
+  int row = c.L, col = c.m, b = c.L - c.m + c.k;
+  bool bad = false, done = false;
+  T ra[DEPTH], rb[DEPTH];
+#pragma unroll
+  for (int i = 0; i < DEPTH; ++i) {
+    ra[i] = col - i >= 1 ? ldA(col - i) : T(0);
+    rb[i] = col - i >= 1 ? ldB(col - i) : T(0);
+  }
+  while (!done && col >= 1) {
+#pragma unroll
+    for (int q = 0; q < DEPTH; ++q) {
+      if (done || col < 1) break;
+      const T A = ra[q], B = rb[q];
+      if (col - DEPTH >= 1) {  // refill this slot DEPTH columns ahead
+        ra[q] = ldA(col - DEPTH);
+        rb[q] = ldB(col - DEPTH);
+      }
+      // steps inside column col
+      for (;;) {
+        if (row == 0) {
+          // row 0: the first candidate of a call stops; later ones step left
+          // down to column 0 (their diagonal/top neighbours, the previous
+          // matrix's last row, are all > k when m > 3k)
+          if (c.first_of_call) {
+            done = true;
+            break;
+          }
+          if (er == sr) {
+            bad = done = true;
+            break;
+          }
+          *--er = rd[col - 1];
+          *--eg = '_';
+          --col;
+          ++b;
+          break;
         }
-        return plane(j, b);
-      },
-      [&](int op, int row, int col) {
-        if (n < maxs) {
-          orr[n] = op == OP_UP ? uint8_t('_') : rd[col - 1];
-          og[n] = op == OP_LEFT ? uint8_t('_') : wn[row - 1];
+        if ((unsigned)b >= (unsigned)BITS || er == sr) {
+          bad = done = true;
+          break;
         }
-        ++n;
-      });
-  int status = 0;
-  if (bad || n > maxs) {
-    status |= 4;  // overflow
-    n = n > maxs ? maxs : n;
-  }
-  for (int i = 0, j = n - 1; i < j; ++i, --j) {
-    uint8_t x = orr[i];
-    orr[i] = orr[j];
-    orr[j] = x;
-    x = og[i];
-    og[i] = og[j];
-    og[j] = x;
-  }
-  return status;
-}
-
-// Decision planes of one lane, read column by column from m down to 1 with
-// the next two columns' words already requested.
-template <typename T>
-struct PlaneRing {
-  const T *planes;
-  long stride, slot;
-  int c0;
-  T A0, B0, A1, B1, A2, B2;
-  SARU_HD T ldA(int j) const { return planes[(2 * (long)j) * stride + slot]; }
-  SARU_HD T ldB(int j) const { return planes[(2 * (long)j + 1) * stride + slot]; }
-  SARU_HD void init(int m) {
-    c0 = m;
-    A0 = ldA(m);
-    B0 = ldB(m);
-    A1 = m >= 2 ? ldA(m - 1) : T(0);
-    B1 = m >= 2 ? ldB(m - 1) : T(0);
-    A2 = m >= 3 ? ldA(m - 2) : T(0);
-    B2 = m >= 3 ? ldB(m - 2) : T(0);
-  }
-  SARU_HD int get(int j, int b) {
-    if (j < c0) {  // the path moved one column left
-      A0 = A1;
-      B0 = B1;
-      A1 = A2;
-      B1 = B2;
-      --c0;
-      if (c0 >= 3) {
-        A2 = ldA(c0 - 2);
-        B2 = ldB(c0 - 2);
+        const int op = int((A >> b) & T(1)) | (int((B >> b) & T(1)) << 1);
+        if (op == OP_UP) {
+          *--er = '_';
+          *--eg = wn[row - 1];
+          --row;
+          --b;
+          continue;
+        }
+        if (op == OP_DIAG) {
+          *--er = rd[col - 1];
+          *--eg = wn[row - 1];
+          --row;
+          --col;
+          break;
+        }
+        if (op == OP_LEFT) {
+          *--er = rd[col - 1];
+          *--eg = '_';
+          --col;
+          ++b;
+          break;
+        }
+        done = true;  // STOP
+        break;
       }
     }
-    return int((A0 >> b) & T(1)) | (int((B0 >> b) & T(1)) << 1);
   }
-};
+  if (!done && col == 0) {
+    // column 0 holds max(0, row - 2so); only the vertical test can hold
+    while (row >= 1) {
+      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
+      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
+      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
+      if (tp + 1 - corr != v) break;
+      if (er == sr) {
+        bad = true;
+        break;
+      }
+      *--er = '_';
+      *--eg = wn[row - 1];
+      --row;
+    }
+  }
+  // move the string to the slot start; clear what it vacated
+  const int n = (int)((sr + cap) - er);
+  if (n < cap) {
+    for (int i = 0; i < n; ++i) {
+      sr[i] = er[i];
+      sg[i] = eg[i];
+    }
+    for (int i = n; i < cap; ++i) {
+      sr[i] = 0;
+      sg[i] = 0;
+    }
+  }
+  return bad ? 4 : 0;
+}
 
 // Shared-memory slice sizes for a maximum read length and k.
 struct SliceLayout {
@@ -250,8 +303,10 @@ SARU_HD SliceLayout slice_layout(int max_m, int k) {
   SliceLayout L;
   const long code_words = (max_m + 7) / 8;
   const long mwords = mask_words(k, max_m + 2 * k);
-  L.rs_bytes = (32L * max_m + 32 + 15) & ~15L;
-  L.ws_bytes = (32L * (max_m + 2 * k) + 32 + 15) & ~15L;
+  // staged bytes, 16 bytes of alignment head and 96 of slack for the word
+  // readers (load4 and the 32-position chunks of build_codes_acgt)
+  L.rs_bytes = (32L * max_m + 16 + 96 + 15) & ~15L;
+  L.ws_bytes = (32L * (max_m + 2 * k) + 16 + 96 + 15) & ~15L;
   const long cm = 4L * 32 * (code_words + NCODES * mwords);
   const long out = 2 * ((32L * (max_m + 3 * k) + 32 + 15) & ~15L);
   L.region_bytes = ((cm > out ? cm : out) + 15) & ~15L;

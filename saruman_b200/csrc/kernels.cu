@@ -76,10 +76,10 @@ __global__ void __launch_bounds__(128) saru_band_kernel(KernelArgs a) {
       for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
     }
     __syncwarp();
-    PlaneRing<T> ring{planes, ta.pstride, pslot};
-    if (ls.ok && ls.score <= a.k) ring.init(ls.c.m);
-    st |= lane_traceback<T>(ta, s, lane, st_reads, st_win, out_r, out_g, ls,
-                            [&](int j, int b) { return ring.get(j, b); });
+    st |= lane_traceback<T, 8>(
+        ta, s, lane, st_reads, st_win, out_r, out_g, ls,
+        [&](int j) { return planes[(2 * (long)j) * ta.pstride + pslot]; },
+        [&](int j) { return planes[(2 * (long)j + 1) * ta.pstride + pslot]; });
     if (st) atomicOr(a.status, (st & 1 ? kStatusIrregular : 0) | (st & 2 ? kStatusAlphabet : 0) |
                                    (st & 4 ? kStatusOverflow : 0));
     __syncwarp();

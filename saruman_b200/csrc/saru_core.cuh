@@ -173,9 +173,107 @@ SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, P codes, P mask, in
   return true;
 }
 
+SARU_HD uint32_t byte_perm(uint32_t x, uint32_t y, uint32_t sel) {
+#if defined(__CUDA_ARCH__)
+  return __byte_perm(x, y, sel);
+#else
+  uint64_t v = (uint64_t)x | ((uint64_t)y << 32);
+  uint32_t r = 0;
+  for (int i = 0; i < 4; ++i) {
+    uint32_t s = (sel >> (4 * i)) & 7u;
+    r |= (uint32_t)((v >> (8 * s)) & 0xFFu) << (8 * i);
+  }
+  return r;
+#endif
+}
+
+// Four bytes of ASCII -> their base codes (A=0 C=1 G=2 T=3 in the low two
+// bits of each byte) and the ASCII those codes stand for; a byte is a base
+// exactly when it equals that ASCII.
+SARU_HD uint32_t base_codes4(uint32_t x) { return ((x >> 1) ^ (x >> 2)) & 0x03030303u; }
+SARU_HD uint32_t codes4_nibbles(uint32_t c4) { return byte_perm(c4 | (c4 >> 4), 0, 0x4420); }
+SARU_HD uint32_t ascii_of_nibbles(uint32_t nib) { return byte_perm(0x54474341u, 0, nib); }
+
+// Fast build of the codes and masks when the read and the window hold only
+// A/C/G/T (the common case).  rd4(i) / wn4(i) return bytes i..i+3 of the
+// read / window, little endian; bytes past the sequence may be anything.
+// Returns false (nothing guaranteed written) if a byte is not A/C/G/T.
+template <class Rd4, class Wn4, class P>
+SARU_HD bool build_codes_acgt(const Cand &c, Rd4 rd4, Wn4 wn4, P codes, P mask, int mwords) {
+  uint32_t bad = 0;
+  for (int w = 0; 8 * w < c.m; ++w) {
+    const uint32_t x0 = rd4(8 * w), x1 = rd4(8 * w + 4);
+    const uint32_t s0 = codes4_nibbles(base_codes4(x0));
+    const uint32_t s1 = codes4_nibbles(base_codes4(x1));
+    const int left = c.m - 8 * w;  // chars of this word inside the read
+    const uint32_t k0 = left >= 4 ? 0xFFFFFFFFu : ((1u << (8 * left)) - 1u);
+    const uint32_t k1 = left >= 8 ? 0xFFFFFFFFu : (left > 4 ? ((1u << (8 * (left - 4))) - 1u) : 0u);
+    bad |= ((ascii_of_nibbles(s0) ^ x0) & k0) | ((ascii_of_nibbles(s1) ^ x1) & k1);
+    codes[w] = s0 | (s1 << 16);
+  }
+  if (bad) return false;
+  // window bit-planes P0/P1 (code bits) over positions, 32 per word; mask
+  // bit (p + k + 1) of class c is set iff window byte p is base c
+  const int sh = c.k + 1;
+  uint32_t prevA = 0, prevC = 0, prevG = 0, prevT = 0;
+  const int words = (c.L + 31) >> 5;
+  for (int q = 0; q < mwords; ++q) {
+    uint32_t A = 0, C = 0, G = 0, T = 0;
+    if (q < words) {
+      uint32_t P0 = 0, P1 = 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const uint32_t x = wn4(32 * q + 4 * i);
+        const uint32_t c4 = base_codes4(x);
+        const int left = c.L - (32 * q + 4 * i);
+        const uint32_t keep =
+            left >= 4 ? 0xFFFFFFFFu : (left > 0 ? ((1u << (8 * left)) - 1u) : 0u);
+        bad |= (ascii_of_nibbles(codes4_nibbles(c4)) ^ x) & keep;
+        // bit 0 of each byte to bits 0..3, bit 1 to bits 4..7
+        const uint32_t t = (c4 & 0x01010101u) | ((c4 << 3) & 0x10101010u);
+        const uint32_t g = (t * 0x01020408u) >> 24;
+        P0 |= (g & 0xFu) << (4 * i);
+        P1 |= (g >> 4) << (4 * i);
+      }
+      const int inw = c.L - 32 * q;
+      const uint32_t V = inw >= 32 ? 0xFFFFFFFFu : ((1u << inw) - 1u);
+      A = ~P0 & ~P1 & V;
+      C = P0 & ~P1 & V;
+      G = ~P0 & P1 & V;
+      T = P0 & P1 & V;
+    }
+    // shift the planes up by k+1 bits into mask word q (and carry)
+    mask[0 * mwords + q] = sh >= 32 ? prevA : (A << sh) | (sh ? prevA >> (32 - sh) : 0u);
+    mask[1 * mwords + q] = sh >= 32 ? prevC : (C << sh) | (sh ? prevC >> (32 - sh) : 0u);
+    mask[2 * mwords + q] = sh >= 32 ? prevG : (G << sh) | (sh ? prevG >> (32 - sh) : 0u);
+    mask[3 * mwords + q] = sh >= 32 ? prevT : (T << sh) | (sh ? prevT >> (32 - sh) : 0u);
+    prevA = A;
+    prevC = C;
+    prevG = G;
+    prevT = T;
+  }
+  return bad == 0;
+}
+
 template <class P>
 SARU_HD int code_at(P codes, int j) {
   return (codes[j >> 3] >> ((j & 7) * 4)) & 15;
+}
+
+// One column of the bit-parallel recurrence.  In: the previous column's
+// vertical-delta vectors realigned to this column's rows (pv, mv) and the
+// match vector eq.  Out: this column's vectors (Pv, Mv), the diagonal-zero
+// vector d0 and the horizontal +1 vector hp.
+template <typename T>
+SARU_HD void myers_step(T pv, T mv, T eq, T &Pv, T &Mv, T &d0, T &hp) {
+  const T xh = (((eq & pv) + pv) ^ pv) | eq;
+  d0 = xh | mv;
+  hp = mv | ~(d0 | pv);
+  const T hn = pv & d0;
+  const T hp1 = (hp << 1) | T(1);
+  const T hn1 = hn << 1;
+  Pv = hn1 | ~(d0 | hp1);
+  Mv = hp1 & d0;
 }
 
 // Fill of one candidate.  `planes(j, A, B)` receives the decision planes of
@@ -185,32 +283,39 @@ template <typename T, class P, class PlaneSink>
 SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink planes) {
   constexpr int BITS = int(sizeof(T) * 8);
   const int k = c.k, m = c.m;
+  const T TOPBIT = T(1) << (BITS - 1);
   // column 0: rows b - k; dv = -1 for rows <= 0, 0 for rows 1..2so, +1 after
   T Mv = lowmask<T>(k + 1);
   T Pv = ~lowmask<T>(k + 2 * c.so + 1);
   int top = k;  // D[j - k][j] for the current column j (virtual rows: j + (k - j))
-  const T TOPBIT = T(1) << (BITS - 1);
-  // first-column quirk: rows <= 2so+3 <=> bits <= 2so + k + 2
-  const T col1_corr = c.so ? lowmask<T>(2 * c.so + k + 3) : T(0);
-  for (int j = 1; j < m; ++j) {
-    const T pv = (Pv >> 1) | TOPBIT;
-    const T mv = Mv >> 1;
-    const T eq = window_bits<T>(mask + code_at(codes, j - 1) * mwords, j);
-    const T xh = (((eq & pv) + pv) ^ pv) | eq;
-    const T d0 = xh | mv;
-    const T hp = mv | ~(d0 | pv);
-    const T hn = pv & d0;
-    const T hp1 = (hp << 1) | T(1);
-    const T hn1 = hn << 1;
-    Pv = hn1 | ~(d0 | hp1);
-    Mv = hp1 & d0;
+  {
+    // column 1, with the first-column quirk of the traceback: rows <= 2so+3
+    // (bits <= 2so + k + 2) take the vertical test with cost 0
+    const T eq = window_bits<T>(mask + (int)(codes[0] & 15u) * mwords, 1);
+    T d0, hp;
+    myers_step<T>((Pv >> 1) | TOPBIT, Mv >> 1, eq, Pv, Mv, d0, hp);
+    const T col1_corr = c.so ? lowmask<T>(2 * c.so + k + 3) : T(0);
+    const T up = (Pv & ~col1_corr) | (~(Pv | Mv) & col1_corr);
     const T diag = ~d0 | eq;
-    T up = Pv;
-    if (j == 1) up = (Pv & ~col1_corr) | (~(Pv | Mv) & col1_corr);
-    const T A = diag | (~up & hp);
-    const T B = ~diag & (up | hp);
-    planes(j, A, B);
+    planes(1, diag | (~up & hp), ~diag & (up | hp));
     top += (int)((~d0) & T(1));
+  }
+  // columns 2..m-1; column j matches read byte j-1 (code word (j-1)/8)
+  for (int w = 0; 8 * w + 1 < m; ++w) {
+    const uint32_t cw = codes[w];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = 8 * w + i + 1;
+      if (j < 2) continue;
+      if (j >= m) break;
+      const int code = (int)((cw >> (4 * i)) & 15u);
+      const T eq = window_bits<T>(mask + code * mwords, j);
+      T d0, hp;
+      myers_step<T>((Pv >> 1) | TOPBIT, Mv >> 1, eq, Pv, Mv, d0, hp);
+      const T diag = ~d0 | eq;
+      planes(j, diag | (~Pv & hp), ~diag & (Pv | hp));
+      top += (int)((~d0) & T(1));
+    }
   }
   // column m with explicit values; column m-1 band values from the deltas
   const T eqm = window_bits<T>(mask + code_at(codes, m - 1) * mwords, m);

@@ -15,7 +15,19 @@ static int run(const Cand &c, const uint8_t *read, const uint8_t *win, int *scor
                uint8_t *ga) {
   const int mw = mask_words(c.k, c.L);
   std::vector<uint32_t> codes((c.m + 7) / 8 + 1), mask(NCODES * mw);
-  if (!build_codes(c, [&](int j) { return read[j]; }, [&](int p) { return win[p]; },
+  // padded copies: the word readers look up to 40 bytes past the end
+  std::vector<uint8_t> rpad(c.m + 64, 0xEE), wpad(c.L + 64, 0xEE);
+  memcpy(rpad.data(), read, c.m);
+  memcpy(wpad.data(), win, c.L);
+  auto ld4 = [](const uint8_t *p) {
+    uint32_t v;
+    memcpy(&v, p, 4);
+    return v;
+  };
+  if (!build_codes_acgt(c, [&](int i) { return ld4(rpad.data() + i); },
+                        [&](int i) { return ld4(wpad.data() + i); }, codes.data(), mask.data(),
+                        mw) &&
+      !build_codes(c, [&](int j) { return read[j]; }, [&](int p) { return win[p]; },
                    codes.data(), mask.data(), mw))
     return 1;
   std::vector<T> PA(c.m + 1), PB(c.m + 1);

@@ -63,10 +63,10 @@ static int run(const TileArgs &a0, int nwarps_total) {
       memset(region, 0, (size_t)S.region_bytes);
       for (int lane = 0; lane < 32; ++lane) {
         const long pslot = (long)gwarp * 32 + lane;
-        PlaneRing<T> ring{planes, a.pstride, pslot};
-        if (ls[lane].ok && ls[lane].score <= a.k) ring.init(ls[lane].c.m);
-        status |= lane_traceback<T>(a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
-                                    [&](int j, int b) { return ring.get(j, b); });
+        status |= lane_traceback<T, 8>(
+            a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
+            [&](int j) { return planes[(2 * (long)j) * a.pstride + pslot]; },
+            [&](int j) { return planes[(2 * (long)j + 1) * a.pstride + pslot]; });
       }
       for (int lane = 0; lane < 32; ++lane) {
         stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
