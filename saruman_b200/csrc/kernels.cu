@@ -221,9 +221,11 @@ template <typename T>
 static cudaError_t launch_band(KernelArgs a, const BandLayout &L, cudaStream_t s) {
   if (L.warps < 1) return cudaErrorInvalidValue;
   auto kern = saru_band_kernel<T>;
-  cudaError_t e =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.cta_smem);
-  if (e != cudaSuccess) return e;
+  // allow the largest slice once; each launch asks for its own size (a
+  // per-launch attribute would race between concurrent callers)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxCtaSmem);
+  if (attr != cudaSuccess) return attr;
   a.rs_bytes = L.rs_bytes;
   a.ws_bytes = L.ws_bytes;
   a.warp_smem = L.warp_smem;
