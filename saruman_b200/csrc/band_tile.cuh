@@ -168,22 +168,30 @@ SARU_HD int lane_fill(const TileArgs &a, const TileSpan &s, int lane, const uint
   return status;
 }
 
+// Decision planes of one column for one lane, stored as an adjacent pair
+// so a single load fetches both.
+template <typename T>
+struct PlanePair {
+  T A, B;
+};
+
 // Traceback phase of one lane: writes the lane's two strings into its slot
 // of the output staging, in reading order (the reference emits from the
 // alignment end and reverses in place, src/cuda-functions.cu:306-307; here
 // the characters are written from the slot end downwards and the string is
 // then moved to the slot start, which leaves the same bytes).
 //
-// The walk visits columns m, m-1, ... one at a time (a diagonal or left step
-// moves exactly one column, an up step stays), so the decision planes of
-// column j are requested DEPTH columns before they are used, from a ring of
-// registers with static slots.  Decisions follow the reference's tests as
-// recorded by the fill; column 0 and row 0 follow the reference's rules for
-// the matrix border (see traceback_band in saru_core.cuh).
-template <typename T, int DEPTH, class LoadA, class LoadB>
+// One step per loop iteration for every lane (the warp stays converged): a
+// diagonal or left step moves one column left, and the planes of the next
+// column are already in registers; `prefetch(j)` is called for the column
+// PF columns ahead so its line sits in L1 by the time it is loaded.
+// Decisions follow the reference's tests as recorded by the fill; column 0
+// and row 0 follow the reference's rules for the matrix border (see
+// traceback_band in saru_core.cuh).
+template <typename T, int PF, class LoadPair, class Prefetch>
 SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
                            const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
-                           const LaneState &ls, LoadA ldA, LoadB ldB) {
+                           const LaneState &ls, LoadPair ld, Prefetch prefetch) {
   constexpr int BITS = int(sizeof(T) * 8);
   const long t = s.t0 + lane;
   if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
@@ -196,87 +204,50 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
   const int cap = c.L + c.k;  // slot bytes
   uint8_t *er = sr + cap, *eg = sg + cap;
   int row = c.L, col = c.m, b = c.L - c.m + c.k;
-  bool bad = false, done = false;
-  T ra[DEPTH], rb[DEPTH];
-#pragma unroll
-  for (int i = 0; i < DEPTH; ++i) {
-    ra[i] = col - i >= 1 ? ldA(col - i) : T(0);
-    rb[i] = col - i >= 1 ? ldB(col - i) : T(0);
-  }
-  while (!done && col >= 1) {
-#pragma unroll
-    for (int q = 0; q < DEPTH; ++q) {
-      if (done || col < 1) break;
-      const T A = ra[q], B = rb[q];
-      if (col - DEPTH >= 1) {  // refill this slot DEPTH columns ahead
-        ra[q] = ldA(col - DEPTH);
-        rb[q] = ldB(col - DEPTH);
-      }
-      // steps inside column col
-      for (;;) {
-        if (row == 0) {
-          // row 0: the first candidate of a call stops; later ones step left
-          // down to column 0 (their diagonal/top neighbours, the previous
-          // matrix's last row, are all > k when m > 3k)
-          if (c.first_of_call) {
-            done = true;
-            break;
-          }
-          if (er == sr) {
-            bad = done = true;
-            break;
-          }
-          *--er = rd[col - 1];
-          *--eg = '_';
-          --col;
-          ++b;
-          break;
-        }
-        if ((unsigned)b >= (unsigned)BITS || er == sr) {
-          bad = done = true;
-          break;
-        }
-        const int op = int((A >> b) & T(1)) | (int((B >> b) & T(1)) << 1);
-        if (op == OP_UP) {
-          *--er = '_';
-          *--eg = wn[row - 1];
-          --row;
-          --b;
-          continue;
-        }
-        if (op == OP_DIAG) {
-          *--er = rd[col - 1];
-          *--eg = wn[row - 1];
-          --row;
-          --col;
-          break;
-        }
-        if (op == OP_LEFT) {
-          *--er = rd[col - 1];
-          *--eg = '_';
-          --col;
-          ++b;
-          break;
-        }
-        done = true;  // STOP
-        break;
-      }
-    }
-  }
-  if (!done && col == 0) {
-    // column 0 holds max(0, row - 2so); only the vertical test can hold
-    while (row >= 1) {
-      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
-      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
-      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
-      if (tp + 1 - corr != v) break;
-      if (er == sr) {
+  bool bad = false;
+  PlanePair<T> cur = ld(col);
+  PlanePair<T> nxt = col >= 2 ? ld(col - 1) : PlanePair<T>{T(0), T(0)};
+  for (int j = col - 2; j >= 1 && j > col - 2 - PF; --j) prefetch(j);
+  for (;;) {
+    int op;
+    if (row >= 1 && col >= 1) {
+      if ((unsigned)b >= (unsigned)BITS) {
         bad = true;
         break;
       }
-      *--er = '_';
-      *--eg = wn[row - 1];
+      op = int((cur.A >> b) & T(1)) | (int((cur.B >> b) & T(1)) << 1);
+    } else if (col == 0) {
+      // column 0 holds max(0, row - 2so); only the vertical test can hold
+      if (row == 0) break;
+      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
+      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
+      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
+      op = tp + 1 - corr == v ? OP_UP : OP_STOP;
+    } else {
+      // row 0: the first candidate of a call stops; later ones step left to
+      // column 0 (their diagonal/top neighbours, the previous matrix's last
+      // row, are all > k when m > 3k)
+      op = c.first_of_call ? OP_STOP : OP_LEFT;
+    }
+    if (op == OP_STOP) break;
+    if (er == sr) {
+      bad = true;
+      break;
+    }
+    const uint8_t rch = rd[col >= 1 ? col - 1 : 0];
+    const uint8_t gch = wn[row >= 1 ? row - 1 : 0];
+    *--er = op == OP_UP ? uint8_t('_') : rch;
+    *--eg = op == OP_LEFT ? uint8_t('_') : gch;
+    if (op == OP_UP) {
       --row;
+      --b;
+    } else {
+      if (op == OP_DIAG) --row;
+      else ++b;
+      --col;
+      cur = nxt;
+      if (col >= 2) nxt = ld(col - 1);
+      if (col - 1 - PF >= 1) prefetch(col - 1 - PF);
     }
   }
   // move the string to the slot start; clear what it vacated

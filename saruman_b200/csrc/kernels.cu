@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(128) saru_band_kernel(KernelArgs a) {
   TileArgs ta{a.genome, a.reads, a.goff, a.roff, a.dirs, a.n, a.k, a.max_m, a.first_of_call,
               a.scores, a.read_aln, a.genome_aln, a.scratch, nwarps * 32, a.rs_bytes, a.ws_bytes,
               a.warp_smem - a.rs_bytes - a.ws_bytes};
-  T *planes = reinterpret_cast<T *>(a.scratch);
+  PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(a.scratch);
   const long pslot = gwarp * 32 + lane;
   auto ld16 = [](uint8_t *d, const uint8_t *g) {
     *reinterpret_cast<uint4 *>(d) = __ldg(reinterpret_cast<const uint4 *>(g));
@@ -64,8 +64,7 @@ __global__ void __launch_bounds__(128) saru_band_kernel(KernelArgs a) {
     __syncwarp();
     LaneState ls;
     int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
-      planes[(2 * (long)j) * ta.pstride + pslot] = A;
-      planes[(2 * (long)j + 1) * ta.pstride + pslot] = B;
+      planes[(long)j * ta.pstride + pslot] = PlanePair<T>{A, B};
     });
     __syncwarp();
     uint8_t *out_r = region;
@@ -78,8 +77,10 @@ __global__ void __launch_bounds__(128) saru_band_kernel(KernelArgs a) {
     __syncwarp();
     st |= lane_traceback<T, 8>(
         ta, s, lane, st_reads, st_win, out_r, out_g, ls,
-        [&](int j) { return planes[(2 * (long)j) * ta.pstride + pslot]; },
-        [&](int j) { return planes[(2 * (long)j + 1) * ta.pstride + pslot]; });
+        [&](int j) { return planes[(long)j * ta.pstride + pslot]; },
+        [&](int j) {
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + (long)j * ta.pstride + pslot));
+        });
     if (st) atomicOr(a.status, (st & 1 ? kStatusIrregular : 0) | (st & 2 ? kStatusAlphabet : 0) |
                                    (st & 4 ? kStatusOverflow : 0));
     __syncwarp();

@@ -22,8 +22,8 @@ static int run(const TileArgs &a0, int nwarps_total) {
   a.ws_bytes = S.ws_bytes;
   a.region_bytes = S.region_bytes;
   a.pstride = (long)nwarps_total * 32;
-  std::vector<T> planes_v((size_t)2 * (a.max_m + 1) * a.pstride);
-  T *planes = planes_v.data();
+  std::vector<PlanePair<T>> planes_v((size_t)(a.max_m + 1) * a.pstride);
+  PlanePair<T> *planes = planes_v.data();
   int status = 0;
   auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
   auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
@@ -55,8 +55,7 @@ static int run(const TileArgs &a0, int nwarps_total) {
         const long pslot = (long)gwarp * 32 + lane;
         status |= lane_fill<T>(a, s, lane, st_reads, st_win, region32, ls[lane],
                                [&](int j, T A, T B) {
-                                 planes[(2 * (long)j) * a.pstride + pslot] = A;
-                                 planes[(2 * (long)j + 1) * a.pstride + pslot] = B;
+                                 planes[(long)j * a.pstride + pslot] = PlanePair<T>{A, B};
                                });
       }
       uint8_t *out_r = region, *out_g = region + s.o_span_r;
@@ -65,8 +64,8 @@ static int run(const TileArgs &a0, int nwarps_total) {
         const long pslot = (long)gwarp * 32 + lane;
         status |= lane_traceback<T, 8>(
             a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
-            [&](int j) { return planes[(2 * (long)j) * a.pstride + pslot]; },
-            [&](int j) { return planes[(2 * (long)j + 1) * a.pstride + pslot]; });
+            [&](int j) { return planes[(long)j * a.pstride + pslot]; },
+            [&](int j) { (void)planes[(long)j * a.pstride + pslot]; });
       }
       for (int lane = 0; lane < 32; ++lane) {
         stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
