@@ -139,8 +139,8 @@ SARU_HD int lane_fill(const TileArgs &a, const TileSpan &s, int lane, const uint
   const int k = a.k;
   const int code_words = (a.max_m + 7) / 8;
   const int mwords = mask_words(k, a.max_m + 2 * k);
-  Strided codes{region32 + lane, 32};
-  Strided mask{region32 + code_words * 32 + lane, 32};
+  Strided codes{region32, lane};
+  Strided mask{region32, code_words * 32 + lane};
   Cand &c = ls.c;
   ls.gs = gstart_at(a.goff, t);
   ls.rs = t ? a.roff[t - 1] : 0;
@@ -181,13 +181,14 @@ struct PlanePair {
 // the characters are written from the slot end downwards and the string is
 // then moved to the slot start, which leaves the same bytes).
 //
-// One step per loop iteration for every lane (the warp stays converged): a
-// diagonal or left step moves one column left, and the planes of the next
-// column are already in registers; `prefetch(j)` is called for the column
-// PF columns ahead so its line sits in L1 by the time it is loaded.
-// Decisions follow the reference's tests as recorded by the fill; column 0
-// and row 0 follow the reference's rules for the matrix border (see
-// traceback_band in saru_core.cuh).
+// Interior cells (row >= 1, column >= 1) take a branch-free step per loop
+// iteration, so the warp stays converged: with the recorded decision as
+// bits (a, b) -- DIAG (1,0), UP (0,1), LEFT (1,1), STOP (0,0) -- the read
+// string gets a read byte iff a, the window string a window byte unless
+// a&b, the column drops iff a, the row drops unless a&b.  The planes of the
+// next column are already in registers and the column PF ahead is
+// prefetched.  Row 0 and column 0 follow the reference's border rules in a
+// short tail loop (see traceback_band in saru_core.cuh).
 template <typename T, int PF, class LoadPair, class Prefetch>
 SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
                            const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
@@ -196,70 +197,92 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
   const long t = s.t0 + lane;
   if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
   const Cand &c = ls.c;
-  const uint8_t *rd = st_reads + (ls.rs - s.r_base);
-  const uint8_t *wn = st_win + (ls.gs - s.g_base);
+  const int roff = (int)(ls.rs - s.r_base) - 1;  // read byte col-1 at st_reads[roff + col]
+  const int woff = (int)(ls.gs - s.g_base) - 1;  // window byte row-1 at st_win[woff + row]
   const long slot = ls.gs + (long)a.k * t;
-  uint8_t *sr = out_r + (slot - s.o_base_r);
-  uint8_t *sg = out_g + (slot - s.o_base_g);
-  const int cap = c.L + c.k;  // slot bytes
-  uint8_t *er = sr + cap, *eg = sg + cap;
+  const int sr = (int)(slot - s.o_base_r);  // slot start in out_r
+  const int sg = (int)(slot - s.o_base_g);
+  const int cap = c.L + c.k;                 // slot bytes
+  int n = 0;                                 // bytes written, from the slot end down
   int row = c.L, col = c.m, b = c.L - c.m + c.k;
-  bool bad = false;
+  bool bad = false, stop = false;
   PlanePair<T> cur = ld(col);
-  PlanePair<T> nxt = col >= 2 ? ld(col - 1) : PlanePair<T>{T(0), T(0)};
+  PlanePair<T> nxt = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
   for (int j = col - 2; j >= 1 && j > col - 2 - PF; --j) prefetch(j);
+  // interior: row >= 1 and col >= 1 hold on entry to every iteration
   for (;;) {
-    int op;
-    if (row >= 1 && col >= 1) {
-      if ((unsigned)b >= (unsigned)BITS) {
-        bad = true;
-        break;
-      }
-      op = int((cur.A >> b) & T(1)) | (int((cur.B >> b) & T(1)) << 1);
-    } else if (col == 0) {
-      // column 0 holds max(0, row - 2so); only the vertical test can hold
-      if (row == 0) break;
-      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
-      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
-      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
-      op = tp + 1 - corr == v ? OP_UP : OP_STOP;
-    } else {
-      // row 0: the first candidate of a call stops; later ones step left to
-      // column 0 (their diagonal/top neighbours, the previous matrix's last
-      // row, are all > k when m > 3k)
-      op = c.first_of_call ? OP_STOP : OP_LEFT;
-    }
-    if (op == OP_STOP) break;
-    if (er == sr) {
+    if ((unsigned)b >= (unsigned)BITS) {
       bad = true;
       break;
     }
-    const uint8_t rch = rd[col >= 1 ? col - 1 : 0];
-    const uint8_t gch = wn[row >= 1 ? row - 1 : 0];
-    *--er = op == OP_UP ? uint8_t('_') : rch;
-    *--eg = op == OP_LEFT ? uint8_t('_') : gch;
-    if (op == OP_UP) {
-      --row;
-      --b;
-    } else {
-      if (op == OP_DIAG) --row;
-      else ++b;
+    const uint32_t da = (uint32_t)((cur.A >> b) & T(1));
+    const uint32_t db = (uint32_t)((cur.B >> b) & T(1));
+    if ((da | db) == 0) {
+      stop = true;
+      break;
+    }
+    if (n >= cap) {
+      bad = true;
+      break;
+    }
+    const uint8_t rch = st_reads[roff + col];
+    const uint8_t gch = st_win[woff + row];
+    ++n;
+    out_r[sr + cap - n] = da ? rch : uint8_t('_');
+    out_g[sg + cap - n] = (da & db) ? uint8_t('_') : gch;
+    row -= (int)(1u - (da & db));
+    b += (int)db * ((int)da * 2 - 1);
+    if (da) {
       --col;
       cur = nxt;
       if (col >= 2) nxt = ld(col - 1);
       if (col - 1 - PF >= 1) prefetch(col - 1 - PF);
     }
+    if (row == 0 || col == 0) break;
+  }
+  if (!bad && !stop) {
+    // borders.  Row 0 (col >= 1): the first candidate of a call stops; later
+    // ones step left to column 0 (their diagonal/top neighbours are the
+    // previous matrix's last row, all > k when m > 3k).  Column 0 holds
+    // max(0, row - 2so); only the vertical test can hold there.
+    for (;;) {
+      if (row == 0) {
+        if (col == 0 || c.first_of_call) break;
+        if (n >= cap) {
+          bad = true;
+          break;
+        }
+        ++n;
+        out_r[sr + cap - n] = st_reads[roff + col];
+        out_g[sg + cap - n] = '_';
+        --col;
+        continue;
+      }
+      // col == 0, row >= 1
+      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
+      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
+      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
+      if (tp + 1 - corr != v) break;
+      if (n >= cap) {
+        bad = true;
+        break;
+      }
+      ++n;
+      out_r[sr + cap - n] = '_';
+      out_g[sg + cap - n] = st_win[woff + row];
+      --row;
+    }
   }
   // move the string to the slot start; clear what it vacated
-  const int n = (int)((sr + cap) - er);
   if (n < cap) {
+    const int from = cap - n;
     for (int i = 0; i < n; ++i) {
-      sr[i] = er[i];
-      sg[i] = eg[i];
+      out_r[sr + i] = out_r[sr + from + i];
+      out_g[sg + i] = out_g[sg + from + i];
     }
     for (int i = n; i < cap; ++i) {
-      sr[i] = 0;
-      sg[i] = 0;
+      out_r[sr + i] = 0;
+      out_g[sg + i] = 0;
     }
   }
   return bad ? 4 : 0;

@@ -26,7 +26,7 @@ __device__ __forceinline__ long gstart_of(const int32_t *goff, long t) { return 
 // ---------------------------------------------------------------------------
 
 template <typename T>
-__global__ void __launch_bounds__(128) saru_band_kernel(KernelArgs a) {
+__global__ void __launch_bounds__(128, 3) saru_band_kernel(KernelArgs a) {
   extern __shared__ uint4 smem_v[];
   const int lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;

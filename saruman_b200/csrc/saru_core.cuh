@@ -66,13 +66,14 @@ SARU_HD T lowmask(int n) {
 }
 
 // Word arrays are addressed through P, either a plain uint32_t* or a
-// Strided view (word i of a thread at p[i * stride]) used for per-thread
-// tables interleaved across a thread block in shared memory.
+// Strided view: word i of a lane at base[off + 32 * i], the per-lane tables
+// of a warp interleaved in shared memory (bank = lane for every access).
+// Offsets are 32-bit so address arithmetic stays in 32-bit registers.
 struct Strided {
-  uint32_t *p;
-  int stride;
-  SARU_HD uint32_t &operator[](int i) const { return p[i * stride]; }
-  SARU_HD Strided operator+(int i) const { return Strided{p + i * stride, stride}; }
+  uint32_t *base;
+  int off;
+  SARU_HD uint32_t &operator[](int i) const { return base[off + 32 * i]; }
+  SARU_HD Strided operator+(int i) const { return Strided{base, off + 32 * i}; }
 };
 
 // bits [j, j + BITS) of a packed mask (words of 32 bits)
