@@ -23,10 +23,6 @@
 
 namespace saru {
 
-// op words of the per-lane traceback buffer: paths are at most L + k <=
-// m + 3k long (m <= 512, k <= 15), 16 ops per word
-constexpr int kTraceOpWords = (512 + 45 + 15) / 16;
-
 struct TileArgs {
   const uint8_t *genome, *reads;
   const int32_t *goff, *roff;
@@ -179,40 +175,41 @@ struct PlanePair {
   T A, B;
 };
 
-// Traceback phase of one lane, in two passes.
+// Traceback phase of one lane: writes the lane's two strings into its slot
+// of the output staging, in reading order (the reference emits from the
+// alignment end and reverses in place, src/cuda-functions.cu:306-307; here
+// the characters are written from the slot end downwards and the string is
+// then moved to the slot start, which leaves the same bytes).
 //
-// Walk: from (L, m) the path is followed through the recorded decisions
-// (2 bits per band cell: DIAG (1,0), UP (0,1), LEFT (1,1), STOP (0,0), the
-// reference's tests in its order) and only the ops are kept, 2 bits each.
-// Interior steps are branch-free, so the warp stays converged: the column
-// drops iff bit a, the row unless a&b, the band bit moves by b*(2a-1); the
-// planes of column col-1 are loaded every step (the same L1 line until the
-// column changes) and the column PF ahead is prefetched.  Row 0 and column
-// 0 follow the reference's border rules in a short tail (see traceback_band
-// in saru_core.cuh).
-//
-// Emit: the ops replayed forward from the cell where the walk stopped write
-// both strings in reading order at the slot start -- the bytes the
-// reference leaves after its in-place reversal (src/cuda-functions.cu:
-// 306-307).  The staging is zero, so the rest of the slot stays zero.
+// Interior cells (row >= 1, column >= 1) take a branch-free step per loop
+// iteration, so the warp stays converged: with the recorded decision as
+// bits (a, b) -- DIAG (1,0), UP (0,1), LEFT (1,1), STOP (0,0) -- the read
+// string gets a read byte iff a, the window string a window byte unless
+// a&b, the column drops iff a, the row drops unless a&b.  The planes of the
+// next column are already in registers and the column PF ahead is
+// prefetched.  Row 0 and column 0 follow the reference's border rules in a
+// short tail loop (see traceback_band in saru_core.cuh).
 template <typename T, int PF, class LoadPair, class Prefetch>
 SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
                            const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
                            const LaneState &ls, LoadPair ld, Prefetch prefetch) {
   constexpr int BITS = int(sizeof(T) * 8);
-  constexpr int MAXW = kTraceOpWords;
   const long t = s.t0 + lane;
   if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
   const Cand &c = ls.c;
-  const int cap = c.L + c.k;  // slot bytes: no path is longer
-  uint32_t ops[MAXW];
-  uint32_t acc = 0;
-  int n = 0;
+  const int roff = (int)(ls.rs - s.r_base) - 1;  // read byte col-1 at st_reads[roff + col]
+  const int woff = (int)(ls.gs - s.g_base) - 1;  // window byte row-1 at st_win[woff + row]
+  const long slot = ls.gs + (long)a.k * t;
+  const int sr = (int)(slot - s.o_base_r);  // slot start in out_r
+  const int sg = (int)(slot - s.o_base_g);
+  const int cap = c.L + c.k;                 // slot bytes
+  int n = 0;                                 // bytes written, from the slot end down
   int row = c.L, col = c.m, b = c.L - c.m + c.k;
   bool bad = false, stop = false;
   PlanePair<T> cur = ld(col);
-  PlanePair<T> nxt = ld(col - 1);  // m >= 2
+  PlanePair<T> nxt = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
   for (int j = col - 2; j >= 1 && j > col - 2 - PF; --j) prefetch(j);
+  // interior: row >= 1 and col >= 1 hold on entry to every iteration
   for (;;) {
     if ((unsigned)b >= (unsigned)BITS) {
       bad = true;
@@ -228,18 +225,19 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
       bad = true;
       break;
     }
-    acc |= (da | (db << 1)) << (2 * (n & 15));
-    if ((n & 15) == 15) {
-      ops[n >> 4] = acc;
-      acc = 0;
-    }
+    const uint8_t rch = st_reads[roff + col];
+    const uint8_t gch = st_win[woff + row];
     ++n;
+    out_r[sr + cap - n] = da ? rch : uint8_t('_');
+    out_g[sg + cap - n] = (da & db) ? uint8_t('_') : gch;
     row -= (int)(1u - (da & db));
     b += (int)db * ((int)da * 2 - 1);
-    col -= (int)da;
-    cur = da ? nxt : cur;
-    nxt = ld(col >= 2 ? col - 1 : 1);
-    if (col - 1 - PF >= 1) prefetch(col - 1 - PF);
+    if (da) {
+      --col;
+      cur = nxt;
+      if (col >= 2) nxt = ld(col - 1);
+      if (col - 1 - PF >= 1) prefetch(col - 1 - PF);
+    }
     if (row == 0 || col == 0) break;
   }
   if (!bad && !stop) {
@@ -248,53 +246,46 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
     // previous matrix's last row, all > k when m > 3k).  Column 0 holds
     // max(0, row - 2so); only the vertical test can hold there.
     for (;;) {
-      uint32_t op;
       if (row == 0) {
         if (col == 0 || c.first_of_call) break;
-        op = OP_LEFT;
+        if (n >= cap) {
+          bad = true;
+          break;
+        }
+        ++n;
+        out_r[sr + cap - n] = st_reads[roff + col];
+        out_g[sg + cap - n] = '_';
         --col;
-      } else {
-        const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
-        const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
-        const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
-        if (tp + 1 - corr != v) break;
-        op = OP_UP;
-        --row;
+        continue;
       }
+      // col == 0, row >= 1
+      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
+      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
+      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
+      if (tp + 1 - corr != v) break;
       if (n >= cap) {
         bad = true;
         break;
       }
-      acc |= op << (2 * (n & 15));
-      if ((n & 15) == 15) {
-        ops[n >> 4] = acc;
-        acc = 0;
-      }
       ++n;
+      out_r[sr + cap - n] = '_';
+      out_g[sg + cap - n] = st_win[woff + row];
+      --row;
     }
   }
-  if (bad) return 4;
-  if (n & 15) ops[n >> 4] = acc;
-  // forward replay from the stop cell (row, col)
-  const uint8_t *rd = st_reads + (ls.rs - s.r_base);
-  const uint8_t *wn = st_win + (ls.gs - s.g_base);
-  const long slot = ls.gs + (long)a.k * t;
-  uint8_t *orr = out_r + (slot - s.o_base_r);
-  uint8_t *og = out_g + (slot - s.o_base_g);
-  int i = 0;
-  for (int w = (n - 1) >> 4; w >= 0; --w) {
-    const uint32_t word = ops[w];
-    const int hi = (w == (n - 1) >> 4) ? ((n - 1) & 15) : 15;
-    for (int q = hi; q >= 0; --q, ++i) {
-      const uint32_t op = (word >> (2 * q)) & 3u;
-      const uint32_t da = op & 1u, db = op >> 1;
-      orr[i] = da ? rd[col] : uint8_t('_');
-      og[i] = (da & db) ? uint8_t('_') : wn[row];
-      col += (int)da;
-      row += (int)(1u - (da & db));
+  // move the string to the slot start; clear what it vacated
+  if (n < cap) {
+    const int from = cap - n;
+    for (int i = 0; i < n; ++i) {
+      out_r[sr + i] = out_r[sr + from + i];
+      out_g[sg + i] = out_g[sg + from + i];
+    }
+    for (int i = n; i < cap; ++i) {
+      out_r[sr + i] = 0;
+      out_g[sg + i] = 0;
     }
   }
-  return 0;
+  return bad ? 4 : 0;
 }
 
 // Shared-memory slice sizes for a maximum read length and k.
