@@ -128,6 +128,24 @@ int saru_align_host(const saru_batch *batch, saru_result *result, int lane);
 int saru_align_device(const saru_batch *batch, saru_result *result, void *scratch,
                       size_t scratch_bytes, void *stream);
 
+/* saru_align_device without any allocation, for callers that cannot call
+ * cudaMalloc: a host program whose own allocator owns the device budget and
+ * forbids other allocations, or a code path that must not add an
+ * allocation's synchronisation and latency.  No counterpart in the
+ * reference.  Same batch, result and stream arguments and the same outputs
+ * as saru_align_device; the banded kernel's scratch comes from a device
+ * array inside the library of SARU_STATIC_SCRATCH_BYTES (32 MiB), present on
+ * every GPU that loads the library until the process exits.  Fewer thread
+ * blocks run when the planes of a full grid do not fit in it; a batch that
+ * cannot get even one block, or is outside the banded kernel's domain, is
+ * refused with SARU_E_INVALID and a message.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current), so make that first call before any stream capture.  All
+ * calls share the array: nothing in it needs to start at zero (each call
+ * writes what it reads), but calls that overlap on the GPU race. */
+#define SARU_STATIC_SCRATCH_BYTES (32u << 20)
+int saru_align_device_static(const saru_batch *batch, saru_result *result, void *stream);
+
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 

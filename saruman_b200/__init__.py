@@ -28,7 +28,7 @@ SARU_S_IRREGULAR, SARU_S_ALPHABET, SARU_S_OVERFLOW = 1, 2, 4
 ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_memory",
                  "get_cuda_infos", "saru_align_host", "saru_align_device", "saru_scratch_bytes",
                  "saru_format_tsv", "saru_last_error", "saru_kernel_launches",
-                 "saru_int32_issue_probe")
+                 "saru_int32_issue_probe", "saru_align_device_static")
 ABI_DATA = ("alignment_time",)
 
 

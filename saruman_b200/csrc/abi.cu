@@ -24,6 +24,10 @@
 #include <vector>
 
 #include "../../include/saruman_b200.h"
+
+#ifndef SARU_STATIC_SCRATCH_BYTES
+#define SARU_STATIC_SCRATCH_BYTES (32u << 20)
+#endif
 #include "kernels.cuh"
 #include "saru_core.cuh"
 #include "writer.h"
@@ -238,7 +242,8 @@ size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
 
 // Enqueues the banded kernel on device buffers.
 int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
-             size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s) {
+             size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
+             long max_grid = 0) {
   saru::KernelArgs a{};
   a.genome = reinterpret_cast<const uint8_t *>(b->genome);
   a.reads = reinterpret_cast<const uint8_t *>(b->reads);
@@ -251,6 +256,7 @@ int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *sc
   a.first_of_call = b->first_of_call;
   a.wide = pl.wide;
   a.grid = band_grid(dev, b->n, pl.max_m, b->k);
+  if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
   a.scores = r->scores;
   a.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
   a.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
@@ -474,6 +480,81 @@ int saru_align_device(const saru_batch *batch, saru_result *result, void *scratc
   pl.wide = batch->k > 7;
   return run_band(batch, pl, result, scratch, scratch_bytes, result->status, dev,
                   reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Entry point without any device allocation.  Its scratch (the banded
+// kernel's decision planes) is this file-scope device array, present on
+// every GPU that loads the library for the life of the process.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = SARU_STATIC_SCRATCH_BYTES;
+__device__ __align__(256) uint8_t g_static_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void *g_static_ptr[kMaxDevices] = {};
+
+// Device address of g_static_scratch on `dev` (the current device).  In host
+// code the array's name is only a stand-in, so the address is asked for once
+// per device with that device current.
+int static_scratch_ptr(int dev, void **out) {
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device %d out of range", dev);
+    return SARU_E_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("cudaGetSymbolAddress(g_static_scratch): %s", cudaGetErrorString(e));
+      return SARU_E_CUDA;
+    }
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return SARU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int saru_align_device_static(const saru_batch *batch, saru_result *result, void *stream) {
+  g_last_error.clear();
+  if (batch->n < 0 || batch->k < 0 || batch->k > 15 || batch->match != 0 ||
+      batch->mismatch != 1 || batch->max_read_length < 2 ||
+      batch->max_read_length > saru::kMaxBandM || !result->status) {
+    set_error("saru_align_device_static: needs unit costs, k <= 15, 2 <= max_read_length <= %d "
+              "and a status word",
+              saru::kMaxBandM);
+    return SARU_E_INVALID;
+  }
+  int dev = 0;
+  SARU_CUDA(cudaGetDevice(&dev));
+  void *scratch = nullptr;
+  int rc = static_scratch_ptr(dev, &scratch);
+  if (rc) return rc;
+  Plan pl;
+  pl.band = true;
+  pl.max_m = batch->max_read_length;
+  pl.wide = batch->k > 7;
+  // as many persistent CTAs as the array holds planes for (each CTA's warps
+  // need their own slice); a batch that cannot get even one CTA is refused
+  const size_t per_cta = band_scratch_bytes(1, pl.max_m, batch->k, pl.wide);
+  const long max_grid = (long)(kStaticScratchBytes / (per_cta ? per_cta : 1));
+  if (max_grid < 1) {
+    set_error("saru_align_device_static: one thread block needs %zu bytes of scratch, the "
+              "static array holds %zu",
+              per_cta, kStaticScratchBytes);
+    return SARU_E_INVALID;
+  }
+  return run_band(batch, pl, result, scratch, kStaticScratchBytes, result->status, dev,
+                  reinterpret_cast<cudaStream_t>(stream), max_grid);
 }
 
 int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
