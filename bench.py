@@ -52,19 +52,36 @@ CONFIGS = {
     "c4": dict(workload="long-read-end stress: 10 Mbp uniform genome, 1M reads x 250 bp, 4% errors "
                "(60/20/20), 5% unmapped, k=15", genome=("uniform", 10_000_000, 401),
                reads=1_000_000, m=250, k=15, rate=0.04, mix=(0.60, 0.20, 0.20), unmapped=0.05),
+    "c3": dict(workload="batching: 5 Mbp genome with Zipf(1.5, max 500) repeat copies, 4M reads of "
+               "lengths {36,75,100,150} (1M each), 3% errors, k=ceil(0.06 m); repeat hits capped at "
+               "25 per read (~22M candidates of uneven count per read); all length bins in one launch",
+               genome=("repeat", 5_000_000, 301, "zipf"), reads=4_000_000, lengths=(36, 75, 100, 150),
+               rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0, max_hits=25),
 }
 
 
-def build_batch(cfg: dict, rank: int):
+def build_batches(cfg: dict, rank: int):
+    """One batch per read-length bin (one for single-length configs)."""
     from saruman_b200 import workloads as W
     gs = cfg["genome"]
     if gs[0] == "uniform":
         g, rmap = W.uniform_genome(gs[1], seed=gs[2]), None
     else:
         g, rmap = W.repeat_genome_with_map(gs[1], seed=gs[2], copies=gs[3])
-    rd = W.sample_reads(g, cfg["reads"], cfg["m"], cfg["rate"], seed=1000 + rank, mix=cfg["mix"],
-                        unmapped=cfg["unmapped"])
-    return W.synthetic_candidates(g, rd, cfg["m"], cfg["k"], seed=2000 + rank, repeats=rmap)
+    lengths = cfg.get("lengths", (cfg.get("m"),))
+    per_bin = cfg["reads"] // len(lengths)
+    out = []
+    for i, m in enumerate(lengths):
+        k = cfg.get("k", W.k_for(m))
+        rd = W.sample_reads(g, per_bin, m, cfg["rate"], seed=1000 + 17 * rank + i, mix=cfg["mix"],
+                            unmapped=cfg["unmapped"])
+        out.append(W.synthetic_candidates(g, rd, m, k, seed=2000 + 17 * rank + i, repeats=rmap,
+                                          max_hits=cfg.get("max_hits", 1000)))
+    return out
+
+
+def build_batch(cfg: dict, rank: int):
+    return build_batches(cfg, rank)[0]
 
 
 def band_cells(b) -> int:
@@ -222,18 +239,23 @@ def cpu_reference_rate(b, seconds: float = 10.0, nthreads: int | None = None,
 def run_reference_arm(args, cfg, rank: int) -> None:
     if rank != 0:
         return
-    b = build_batch(cfg, 0)
-    ch = Chunker(b)
+    bs = build_batches(cfg, 0)
+    chs = [Chunker(b) for b in bs]
     per_step = []
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_rate(b, seconds=args.ref_seconds, chunker=ch)
-        if r.get("value") is None:
-            print(json.dumps({"impl": "reference", "unavailable": r.get("unavailable")}))
-            return
+        cand, secs = 0, 0.0
+        for b, ch in zip(bs, chs):
+            r = cpu_reference_rate(b, seconds=args.ref_seconds / len(bs), chunker=ch)
+            if r.get("value") is None:
+                print(json.dumps({"impl": "reference", "unavailable": r.get("unavailable")}))
+                return
+            cand += r["candidates"]
+            secs += r["seconds"]
+            cores = r["cores"]
         if i >= args.warmup:
-            per_step.append(r)
-    cand = sum(r["candidates"] for r in per_step)
-    secs = sum(r["seconds"] for r in per_step)
+            per_step.append((cand, secs))
+    cand = sum(c for c, _ in per_step)
+    secs = sum(t for _, t in per_step)
     value = cand / secs
     line = {
         "impl": "reference", "metric": "alignments/s", "value": value, "unit": "alignments/s",
@@ -242,12 +264,71 @@ def run_reference_arm(args, cfg, rank: int) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
         "config": {"workload": cfg["workload"], "sample": "consecutive sub-batches of the "
                    f"workload, {args.ref_seconds:.0f} s of host work per step"},
-        "cpu_baseline": {"value": value, "unit": "alignments/s", "cores": per_step[0]["cores"],
+        "cpu_baseline": {"value": value, "unit": "alignments/s", "cores": cores,
                          "kind": "reference", "sample": f"{cand} candidates"},
         "e2e": {"value": value, "unit": "alignments/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+class DeviceBatch:
+    """A batch's inputs and outputs resident on the device, with the C-ABI
+    views of them."""
+
+    def __init__(self, b, dev, S):
+        import torch
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        self.b = b
+        self.g, self.r, self.go, self.ro, self.d = (T(b.genome), T(b.reads), T(b.genome_offsets),
+                                                    T(b.read_offsets), T(b.dirs))
+        self.scores = torch.zeros(b.n, dtype=torch.int32, device=dev)
+        self.ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+        self.ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+        self.sb = S.SaruBatch(self.g.data_ptr(), self.r.data_ptr(), self.go.data_ptr(),
+                              self.ro.data_ptr(), self.d.data_ptr(), b.n, b.k, 0, 1, 1, b.m,
+                              len(b.genome), b.total_genome)
+        self.sr = S.SaruResult(self.scores.data_ptr(), self.ra.data_ptr(), self.ga.data_ptr(),
+                               None)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        self.h_in = [(self.g, pin(b.genome)), (self.r, pin(b.reads)), (self.go, pin(b.genome_offsets)),
+                     (self.ro, pin(b.read_offsets)), (self.d, pin(b.dirs))]
+        self.h_out = [(torch.empty(b.n, dtype=torch.int32).pin_memory(), self.scores),
+                      (torch.empty(b.total_genome, dtype=torch.uint8).pin_memory(),
+                       self.ra[:b.total_genome]),
+                      (torch.empty(b.total_genome, dtype=torch.uint8).pin_memory(),
+                       self.ga[:b.total_genome])]
+
+    def h2d(self):
+        for d, h in self.h_in:
+            d.copy_(h, non_blocking=True)
+
+    def d2h(self):
+        for h, d in self.h_out:
+            h.copy_(d, non_blocking=True)
+
+    def bytes_in(self):
+        return sum(int(h.numel() * h.element_size()) for _, h in self.h_in)
+
+    def bytes_out(self):
+        return sum(int(h.numel() * h.element_size()) for h, _ in self.h_out)
+
+
+def timed(stream, fn, steps, world, dist, dev):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms / steps
 
 
 def main() -> None:
@@ -286,102 +367,83 @@ def main() -> None:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
 
-    b = build_batch(cfg, rank)
-    lib = S.load()
-    # inputs and outputs resident in HBM
-    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    g_d, r_d, go_d, ro_d, dir_d = (T(b.genome), T(b.reads), T(b.genome_offsets),
-                                   T(b.read_offsets), T(b.dirs))
-    scores = torch.zeros(b.n, dtype=torch.int32, device=dev)
-    ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
-    ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    bs = build_batches(cfg, rank)
+    S.load()
+    dbs = [DeviceBatch(b, dev, S) for b in bs]
+    n_cand = sum(b.n for b in bs)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
-    nscr = S.scratch_bytes(b.n, b.m, b.k)
-    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
-    sb = S.SaruBatch(g_d.data_ptr(), r_d.data_ptr(), go_d.data_ptr(), ro_d.data_ptr(),
-                     dir_d.data_ptr(), b.n, b.k, 0, 1, 1, b.m, len(b.genome), b.total_genome)
-    sr = S.SaruResult(scores.data_ptr(), ra.data_ptr(), ga.data_ptr(), status.data_ptr())
+    for d in dbs:
+        d.sr.status = status.data_ptr()
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
+    multi = len(dbs) > 1
+    if multi:
+        nscr = S.multi_scratch_bytes([d.sb for d in dbs])
+    else:
+        nscr = S.scratch_bytes(bs[0].n, bs[0].m, bs[0].k)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
 
     int_peak = S.int32_issue_peak() if rank == 0 else None
 
-    def step():
-        S.align_device(sb, sr, scratch.data_ptr(), nscr, sptr)
+    def step_batched():
+        if multi:
+            S.align_multi_device([d.sb for d in dbs], [d.sr for d in dbs], status.data_ptr(),
+                                 scratch.data_ptr(), nscr, sptr)
+        else:
+            S.align_device(dbs[0].sb, dbs[0].sr, scratch.data_ptr(), nscr, sptr)
+
+    plain_scr = [S.scratch_bytes(d.b.n, d.b.m, d.b.k) for d in dbs] if multi else []
+    scratch_plain = (torch.empty(max(plain_scr), dtype=torch.uint8, device=dev)
+                     if multi else None)
+
+    def step_plain():  # one launch per length bin, in order
+        for d, n1 in zip(dbs, plain_scr):
+            S.align_device(d.sb, d.sr, scratch_plain.data_ptr(), n1, sptr)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            step()
+            step_batched()
     stream.synchronize()
     if int(status.item()) != 0:
         raise SystemExit(f"kernel status {int(status.item())}")
 
     # ---- device-resident timing ------------------------------------------
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
     launches0 = S.kernel_launches()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        ev1.synchronize()
+        ms_step = timed(stream, step_batched, args.steps, world, dist, dev)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     launches = S.kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    ms_step = ms_max / args.steps
-    value = world * b.n / (ms_step * 1e-3)
+    value = world * n_cand / (ms_step * 1e-3)
+    plain = None
+    if multi:
+        for _ in range(2):
+            step_plain()
+        stream.synchronize()
+        ms_plain = timed(stream, step_plain, args.steps, world, dist, dev)
+        plain = {"value": world * n_cand / (ms_plain * 1e-3), "ms_per_step": ms_plain,
+                 "launches_per_step": len(dbs),
+                 "what": "one launch per length bin (saru_align_device), bins in sequence"}
 
     # ---- end to end through the public API, host buffers ----------------
     e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-    hg, hr, hgo, hro, hdir = pin(b.genome), pin(b.reads), pin(b.genome_offsets), pin(
-        b.read_offsets), pin(b.dirs)
-    hs = torch.empty(b.n, dtype=torch.int32).pin_memory()
-    hra = torch.empty(b.total_genome, dtype=torch.uint8).pin_memory()
-    hga = torch.empty(b.total_genome, dtype=torch.uint8).pin_memory()
-    h2d = sum(int(x.numel() * x.element_size()) for x in (hg, hr, hgo, hro, hdir))
-    d2h = int(hs.numel() * 4 + hra.numel() + hga.numel())
 
     def e2e_step():
         with torch.cuda.stream(stream):
-            g_d.copy_(hg, non_blocking=True)
-            r_d.copy_(hr, non_blocking=True)
-            go_d.copy_(hgo, non_blocking=True)
-            ro_d.copy_(hro, non_blocking=True)
-            dir_d.copy_(hdir, non_blocking=True)
-            step()
-            hs.copy_(scores, non_blocking=True)
-            hra.copy_(ra[:b.total_genome], non_blocking=True)
-            hga.copy_(ga[:b.total_genome], non_blocking=True)
+            for d in dbs:
+                d.h2d()
+            step_batched()
+            for d in dbs:
+                d.d2h()
 
     e2e_step()
     stream.synchronize()
     if world > 1:
         dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    e1.record(stream)
-    e1.synchronize()
-    e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e2e_value = world * b.n / (e_ms / e2e_steps * 1e-3)
+    e_ms = timed(stream, e2e_step, e2e_steps, world, dist, dev)
+    e2e_value = world * n_cand / (e_ms * 1e-3)
 
     if world > 1:
         dist.barrier()
@@ -391,19 +453,20 @@ def main() -> None:
 
     # ---- roofline --------------------------------------------------------
     peaks = measured_peaks()
-    cells = band_cells(b)
-    ops = 6 * cells
-    achieved_ops = ops / (ms_step * 1e-3)
-    abytes = algorithmic_bytes(b)
-    prof = profile_traffic()
+    cells = sum(band_cells(b) for b in bs)
+    achieved_ops = 6 * cells / (ms_step * 1e-3)
+    abytes = sum(algorithmic_bytes(b) for b in bs)
+    prof = profile_traffic() if args.config == "c2" else None
     traffic = None
     if prof and prof.get("dram_bytes_per_candidate"):
-        traffic = prof["dram_bytes_per_candidate"] * b.n
+        traffic = prof["dram_bytes_per_candidate"] * n_cand
     roofline = {
         "bound": "int32",
         "achieved": achieved_ops / 1e12, "peak": int_peak / 1e12 if int_peak and int_peak > 0 else None,
         "unit": "Tops/s", "frac": (achieved_ops / int_peak) if int_peak and int_peak > 0 else None,
         "traffic": traffic,
+        "traffic_source": "profiles/band_kernel_c2.json (ncu dram bytes per candidate, small case, "
+                          "scaled by candidates)" if traffic else None,
         "peak_source": "measured live by saru_int32_issue_probe on this GPU",
         "ops_per_candidate_definition": "band cells x 6 (m*(2k+1) or m*(4k+1) cells)",
         "hbm": {"achieved_gbs": abytes / (ms_step * 1e-3) / 1e9,
@@ -414,30 +477,41 @@ def main() -> None:
     }
     cpu = None
     if world == 1:
-        r = cpu_reference_rate(b, seconds=args.cpu_seconds)
-        if r.get("value") is not None:
-            cpu = {"value": r["value"], "unit": "alignments/s", "cores": r["cores"],
+        cand, secs, cores = 0, 0.0, None
+        for b in bs:
+            r = cpu_reference_rate(b, seconds=args.cpu_seconds / len(bs))
+            if r.get("value") is None:
+                cpu = {"value": None, "unavailable": r.get("unavailable")}
+                break
+            cand += r["candidates"]
+            secs += r["seconds"]
+            cores = r["cores"]
+        if cpu is None:
+            cpu = {"value": cand / secs, "unit": "alignments/s", "cores": cores,
                    "kind": "reference",
-                   "sample": f"{r['candidates']} consecutive candidates of the workload, the "
-                             "reference's own kernel code compiled for the host"}
-        else:
-            cpu = {"value": None, "unavailable": r.get("unavailable")}
+                   "sample": f"{cand} consecutive candidates of the workload ({len(bs)} bins), "
+                             "the reference's own kernel code compiled for the host"}
     line = {
         "metric": "alignments/s", "value": value, "unit": "alignments/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
         "data": "synthetic",
-        "config": {"workload": cfg["workload"], "candidates_per_step": b.n,
-                   "reads_per_step": cfg["reads"], "read_length": b.m, "k": b.k,
-                   "parallelism": f"replicas x{world}", "l2": "inputs 4+ GB > L2, no flush"},
-        "gcups_rect": world * rect_cells(b) / (ms_step * 1e-3) / 1e9,
+        "config": {"workload": cfg["workload"], "candidates_per_step": n_cand,
+                   "reads_per_step": cfg["reads"], "read_lengths": [b.m for b in bs],
+                   "k": [b.k for b in bs], "parallelism": f"replicas x{world}",
+                   "l2": "inputs 4+ GB > L2, no flush"},
+        "gcups_rect": world * sum(rect_cells(b) for b in bs) / (ms_step * 1e-3) / 1e9,
         "gpu_launches": int(launches),
-        "e2e": {"value": e2e_value, "unit": "alignments/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+        "e2e": {"value": e2e_value, "unit": "alignments/s",
+                "h2d_bytes_per_step": sum(d.bytes_in() for d in dbs),
+                "d2h_bytes_per_step": sum(d.bytes_out() for d in dbs), "steps": e2e_steps},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
+    if plain:
+        line["plain"] = plain
+        line["batched_over_plain"] = plain["ms_per_step"] / ms_step
     print(json.dumps(line))
 
 

@@ -141,13 +141,25 @@ int saru_align_device(const saru_batch *batch, saru_result *result, void *scratc
  * refused with SARU_E_INVALID and a message.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress, with that
  * device current), so make that first call before any stream capture.  All
- * calls share the array: nothing in it needs to start at zero (each call
- * writes what it reads), but calls that overlap on the GPU race. */
+ * calls share the array: each call clears the work counter at its start
+ * and writes every other byte it reads, so nothing from an earlier call is
+ * used, but calls that overlap on the GPU race. */
 #define SARU_STATIC_SCRATCH_BYTES (32u << 20)
 int saru_align_device_static(const saru_batch *batch, saru_result *result, void *stream);
 
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
+
+/* Several calls in one launch of the banded kernel: each saru_batch is one
+ * reference-style call (its own read length, k, band width, first-of-call
+ * flag and output arrays, all device pointers); persistent warps take
+ * 32-candidate tiles of all calls from one work counter, heaviest calls
+ * first.  Up to 192 calls; conditions per call as for saru_align_device.
+ * The calls' status bits are ORed into *status (device).  `scratch` must hold
+ * saru_multi_scratch_bytes(calls, ncalls) bytes of device memory. */
+int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32_t ncalls,
+                            int32_t *status, void *scratch, size_t scratch_bytes, void *stream);
+size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls);
 
 /* Formats the reference's TSV lines for one aligned call into `out`
  * (capacity cap) and returns the bytes needed.  names: n_names entries of

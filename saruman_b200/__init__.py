@@ -28,7 +28,8 @@ SARU_S_IRREGULAR, SARU_S_ALPHABET, SARU_S_OVERFLOW = 1, 2, 4
 ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_memory",
                  "get_cuda_infos", "saru_align_host", "saru_align_device", "saru_scratch_bytes",
                  "saru_format_tsv", "saru_last_error", "saru_kernel_launches",
-                 "saru_int32_issue_probe", "saru_align_device_static")
+                 "saru_int32_issue_probe", "saru_align_device_static",
+                 "saru_align_multi_device", "saru_multi_scratch_bytes")
 ABI_DATA = ("alignment_time",)
 
 
@@ -75,6 +76,11 @@ def load(path: str | Path | None = None):
     lib.saru_last_error.restype = C.c_char_p
     lib.saru_kernel_launches.restype = C.c_uint64
     lib.get_cuda_infos.restype = C.c_ulong
+    lib.saru_align_multi_device.restype = C.c_int
+    lib.saru_align_multi_device.argtypes = [C.POINTER(SaruBatch), C.POINTER(SaruResult), C.c_int32,
+                                            C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+    lib.saru_multi_scratch_bytes.restype = C.c_size_t
+    lib.saru_multi_scratch_bytes.argtypes = [C.POINTER(SaruBatch), C.c_int32]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -180,3 +186,20 @@ def kernel_launches() -> int:
 def int32_issue_peak(iters: int = 4096) -> float:
     """Measured 32-bit integer ops/s of the current GPU (see probe.cu)."""
     return float(load().saru_int32_issue_probe(iters))
+
+
+def align_multi_device(batches: list[SaruBatch], results: list[SaruResult], status_ptr: int,
+                       scratch_ptr: int, scratch_len: int, stream_ptr: int = 0) -> None:
+    """Several calls (device pointers) in one launch (saru_align_multi_device)."""
+    n = len(batches)
+    arr_b = (SaruBatch * n)(*batches)
+    arr_r = (SaruResult * n)(*results)
+    rc = load().saru_align_multi_device(arr_b, arr_r, n, status_ptr, scratch_ptr, scratch_len,
+                                        stream_ptr)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+
+
+def multi_scratch_bytes(batches: list[SaruBatch]) -> int:
+    n = len(batches)
+    return int(load().saru_multi_scratch_bytes((SaruBatch * n)(*batches), n))

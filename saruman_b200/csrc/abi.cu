@@ -17,6 +17,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <mutex>
@@ -240,37 +241,80 @@ size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
   return saru::band_scratch_bytes(grid, max_m, k, wide);
 }
 
-// Enqueues the banded kernel on device buffers.
-int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
-             size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
-             long max_grid = 0) {
-  saru::KernelArgs a{};
-  a.genome = reinterpret_cast<const uint8_t *>(b->genome);
-  a.reads = reinterpret_cast<const uint8_t *>(b->reads);
-  a.goff = b->genome_offsets;
-  a.roff = b->read_offsets;
-  a.dirs = b->dirs;
-  a.n = b->n;
-  a.k = b->k;
-  a.max_m = pl.max_m;
-  a.first_of_call = b->first_of_call;
-  a.wide = pl.wide;
-  a.grid = band_grid(dev, b->n, pl.max_m, b->k);
-  if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
-  a.scores = r->scores;
-  a.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
-  a.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
-  a.scratch = scratch;
-  a.status = status_dev;
-  if (band_scratch_bytes(a.grid, pl.max_m, b->k, pl.wide) > scratch_bytes) {
-    set_error("scratch too small: %zu < %zu", scratch_bytes,
-              band_scratch_bytes(a.grid, pl.max_m, b->k, pl.wide));
+// Enqueues the banded kernel on device buffers: calls[0..ncalls) as the
+// segments of one launch (the single-call entry points pass one).  Scratch:
+// the tile counter, then the decision planes of the persistent grid.
+int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, const Plan &pl,
+                   void *scratch, size_t scratch_bytes, int *status_dev, int dev,
+                   cudaStream_t s, long max_grid = 0) {
+  if (ncalls < 1 || ncalls > saru::kMaxSegs) {
+    set_error("%d calls in one launch (1..%d)", ncalls, saru::kMaxSegs);
     return SARU_E_INVALID;
   }
-  if (b->n == 0) return SARU_OK;
+  // heavier segments first: the counter hands out tiles in segment order, so
+  // the tail of the launch is made of the cheapest tiles
+  std::vector<int> order((size_t)ncalls);
+  for (int i = 0; i < ncalls; ++i) order[(size_t)i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (long)calls[x].max_read_length * (calls[x].k + 1) >
+           (long)calls[y].max_read_length * (calls[y].k + 1);
+  });
+  static thread_local saru::KernelArgs a;  // ~19 KB: not on the stack
+  memset(&a, 0, sizeof(a));
+  long tiles = 0, total_n = 0;
+  int max_m = 0, max_k = 0, wide_any = 0;
+  for (int q = 0; q < ncalls; ++q) {
+    const saru_batch *b = &calls[order[(size_t)q]];
+    const saru_result *r = &res[order[(size_t)q]];
+    saru::Segment &g = a.segs[a.nseg++];
+    g.genome = reinterpret_cast<const uint8_t *>(b->genome);
+    g.reads = reinterpret_cast<const uint8_t *>(b->reads);
+    g.goff = b->genome_offsets;
+    g.roff = b->read_offsets;
+    g.dirs = b->dirs;
+    g.scores = r->scores;
+    g.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
+    g.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
+    g.n = b->n;
+    g.tile_begin = tiles;
+    g.k = b->k;
+    g.max_m = b->max_read_length;
+    g.first_of_call = b->first_of_call;
+    g.wide = b->k > 7 && (ncalls > 1 || pl.wide);
+    tiles += (b->n + 31) / 32;
+    total_n += b->n;
+    if (g.max_m > max_m) max_m = g.max_m;
+    if (g.k > max_k) max_k = g.k;
+    wide_any |= g.wide;
+  }
+  if (tiles == 0) return SARU_OK;
+  a.total_tiles = tiles;
+  a.max_m = max_m;
+  a.max_k = max_k;
+  a.wide_any = wide_any;
+  a.grid = saru::band_grid(sm_count(dev), total_n, saru::band_layout(max_m, max_k),
+                           smem_per_sm(dev));
+  if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
+  const size_t need = saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0);
+  if (need > scratch_bytes) {
+    set_error("scratch too small: %zu < %zu", scratch_bytes, need);
+    return SARU_E_INVALID;
+  }
+  a.counter = reinterpret_cast<int *>(scratch);
+  a.planes = reinterpret_cast<uint8_t *>(scratch) + saru::kCounterBytes;
+  a.status = status_dev;
   SARU_CUDA(saru::launch_band_kernel(a, s));
   g_launches.fetch_add(1);
   return SARU_OK;
+}
+
+int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
+             size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
+             long max_grid = 0) {
+  if (b->n == 0) return SARU_OK;
+  saru_batch one = *b;
+  one.max_read_length = pl.max_m;
+  return run_band_multi(&one, r, 1, pl, scratch, scratch_bytes, status_dev, dev, s, max_grid);
 }
 
 // Host batch -> device buffers of `lane`, returns device-side view.
@@ -555,6 +599,49 @@ int saru_align_device_static(const saru_batch *batch, saru_result *result, void 
   }
   return run_band(batch, pl, result, scratch, kStaticScratchBytes, result->status, dev,
                   reinterpret_cast<cudaStream_t>(stream), max_grid);
+}
+
+size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    dev = 0;
+  }
+  int max_m = 0, max_k = 0, wide = 0;
+  long n = 0;
+  for (int i = 0; i < ncalls; ++i) {
+    if (calls[i].max_read_length > max_m) max_m = calls[i].max_read_length;
+    if (calls[i].k > max_k) max_k = calls[i].k;
+    wide |= calls[i].k > 7;
+    n += calls[i].n;
+  }
+  const long grid = band_grid(dev, n, max_m, max_k);
+  return band_scratch_bytes(grid, max_m, max_k, wide != 0);
+}
+
+int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32_t ncalls,
+                            int32_t *status, void *scratch, size_t scratch_bytes, void *stream) {
+  g_last_error.clear();
+  if (ncalls < 1 || ncalls > saru::kMaxSegs || !status) {
+    set_error("saru_align_multi_device: 1..%d calls and a status word", saru::kMaxSegs);
+    return SARU_E_INVALID;
+  }
+  for (int i = 0; i < ncalls; ++i) {
+    const saru_batch *b = &calls[i];
+    if (b->n < 0 || b->k < 0 || b->k > 15 || b->match != 0 || b->mismatch != 1 ||
+        b->max_read_length < 2 || b->max_read_length > saru::kMaxBandM) {
+      set_error("saru_align_multi_device: call %d needs unit costs, k <= 15 and "
+                "2 <= max_read_length <= %d",
+                i, saru::kMaxBandM);
+      return SARU_E_INVALID;
+    }
+  }
+  int dev = 0;
+  SARU_CUDA(cudaGetDevice(&dev));
+  Plan pl;
+  pl.band = true;
+  return run_band_multi(calls, results, ncalls, pl, scratch, scratch_bytes, status, dev,
+                        reinterpret_cast<cudaStream_t>(stream));
 }
 
 int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,

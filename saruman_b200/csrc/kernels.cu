@@ -25,8 +25,58 @@ __device__ __forceinline__ long gstart_of(const int32_t *goff, long t) { return 
 // banded kernel: persistent warps over warp tiles (band_tile.cuh)
 // ---------------------------------------------------------------------------
 
+// One warp tile of one segment (the phases of band_tile.cuh).
 template <typename T>
-__global__ void __launch_bounds__(128, 3) saru_band_kernel(KernelArgs a) {
+__device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, uint8_t *st_reads,
+                                         uint8_t *st_win, uint8_t *region, void *planes_v,
+                                         long pslot) {
+  PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v);
+  uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
+  auto ld16 = [](uint8_t *d, const uint8_t *g) {
+    *reinterpret_cast<uint4 *>(d) = __ldg(reinterpret_cast<const uint4 *>(g));
+  };
+  auto ld1 = [](const uint8_t *g) -> uint8_t { return __ldg(g); };
+  auto st16 = [](uint8_t *g, const uint8_t *d) {
+    *reinterpret_cast<uint4 *>(g) = *reinterpret_cast<const uint4 *>(d);
+  };
+  const TileSpan s = tile_span(ta, wt);
+  if (!s.fits) {  // offsets no regular call can have: report, do not stage
+    const long t = s.t0 + lane;
+    if (t < ta.n) ta.scores[t] = ta.k + 1;
+    return 1;
+  }
+  stage_in(st_reads, ta.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
+  stage_in(st_win, ta.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
+  __syncwarp();
+  LaneState ls;
+  int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
+    planes[(long)j * ta.pstride + pslot] = PlanePair<T>{A, B};
+  });
+  __syncwarp();
+  uint8_t *out_r = region;
+  uint8_t *out_g = region + s.o_span_r;
+  {
+    uint4 *p4 = reinterpret_cast<uint4 *>(region);
+    const long nv = ta.region_bytes >> 4;
+    for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
+  }
+  __syncwarp();
+  st |= lane_traceback<T, 8>(
+      ta, s, lane, st_reads, st_win, out_r, out_g, ls,
+      [&](int j) { return planes[(long)j * ta.pstride + pslot]; },
+      [&](int j) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + (long)j * ta.pstride + pslot));
+      });
+  __syncwarp();
+  stage_out(ta.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
+  stage_out(ta.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
+  __syncwarp();
+  return st;
+}
+
+// Persistent warps take 32-candidate tiles from a launch-wide counter; a
+// tile belongs to one segment (a call with its own m, k and band width).
+__global__ void __launch_bounds__(128, 3) saru_band_kernel(const __grid_constant__ KernelArgs a) {
   extern __shared__ uint4 smem_v[];
   const int lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
@@ -35,59 +85,33 @@ __global__ void __launch_bounds__(128, 3) saru_band_kernel(KernelArgs a) {
   uint8_t *st_reads = ws;
   uint8_t *st_win = ws + a.rs_bytes;
   uint8_t *region = st_win + a.ws_bytes;
-  uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
   const long gwarp = (long)blockIdx.x * WARPS + wid;
-  const long nwarps = (long)gridDim.x * WARPS;
-  TileArgs ta{a.genome, a.reads, a.goff, a.roff, a.dirs, a.n, a.k, a.max_m, a.first_of_call,
-              a.scores, a.read_aln, a.genome_aln, a.scratch, nwarps * 32, a.rs_bytes, a.ws_bytes,
-              a.warp_smem - a.rs_bytes - a.ws_bytes};
-  PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(a.scratch);
+  const long pstride = (long)gridDim.x * WARPS * 32;
   const long pslot = gwarp * 32 + lane;
-  auto ld16 = [](uint8_t *d, const uint8_t *g) {
-    *reinterpret_cast<uint4 *>(d) = __ldg(reinterpret_cast<const uint4 *>(g));
-  };
-  auto ld1 = [](const uint8_t *g) -> uint8_t { return __ldg(g); };
-  auto st16 = [](uint8_t *g, const uint8_t *d) {
-    *reinterpret_cast<uint4 *>(g) = *reinterpret_cast<const uint4 *>(d);
-  };
-
-  for (long wt = gwarp; wt * 32 < a.n; wt += nwarps) {
-    const TileSpan s = tile_span(ta, wt);
-    if (!s.fits) {  // offsets no regular call can have: report, do not stage
-      const long t = s.t0 + lane;
-      if (t < a.n) a.scores[t] = a.k + 1;
-      if (lane == 0) atomicOr(a.status, kStatusIrregular);
-      continue;
+  int status = 0;
+  for (;;) {
+    int tile = 0;
+    if (lane == 0) tile = atomicAdd(a.counter, 1);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int lo = 0, hi = a.nseg - 1;  // last segment with tile_begin <= tile
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.segs[mid].tile_begin <= tile) lo = mid;
+      else hi = mid - 1;
     }
-    stage_in(st_reads, a.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
-    stage_in(st_win, a.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
-    __syncwarp();
-    LaneState ls;
-    int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
-      planes[(long)j * ta.pstride + pslot] = PlanePair<T>{A, B};
-    });
-    __syncwarp();
-    uint8_t *out_r = region;
-    uint8_t *out_g = region + s.o_span_r;
-    {
-      uint4 *p4 = reinterpret_cast<uint4 *>(region);
-      const long nv = ta.region_bytes >> 4;
-      for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
-    }
-    __syncwarp();
-    st |= lane_traceback<T, 8>(
-        ta, s, lane, st_reads, st_win, out_r, out_g, ls,
-        [&](int j) { return planes[(long)j * ta.pstride + pslot]; },
-        [&](int j) {
-          asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + (long)j * ta.pstride + pslot));
-        });
-    if (st) atomicOr(a.status, (st & 1 ? kStatusIrregular : 0) | (st & 2 ? kStatusAlphabet : 0) |
-                                   (st & 4 ? kStatusOverflow : 0));
-    __syncwarp();
-    stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
-    stage_out(a.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
-    __syncwarp();
+    const Segment &g = a.segs[lo];
+    const TileArgs ta{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
+                      g.first_of_call, g.scores, g.read_aln, g.genome_aln, a.planes, pstride,
+                      a.rs_bytes, a.ws_bytes, a.warp_smem - a.rs_bytes - a.ws_bytes};
+    const long wt = tile - g.tile_begin;
+    status |= g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
+                     : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);
   }
+  status = __reduce_or_sync(0xffffffffu, status);
+  if (status && lane == 0)
+    atomicOr(a.status, (status & 1 ? kStatusIrregular : 0) | (status & 2 ? kStatusAlphabet : 0) |
+                           (status & 4 ? kStatusOverflow : 0));
 }
 
 // ---------------------------------------------------------------------------
@@ -218,19 +242,20 @@ BandLayout band_layout(int max_m, int k) {
   return L;
 }
 
-template <typename T>
-static cudaError_t launch_band(KernelArgs a, const BandLayout &L, cudaStream_t s) {
-  if (L.warps < 1) return cudaErrorInvalidValue;
-  auto kern = saru_band_kernel<T>;
+cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
+  const BandLayout L = band_layout(a.max_m, a.max_k);
+  if (L.warps < 1 || a.nseg < 1 || a.nseg > kMaxSegs) return cudaErrorInvalidValue;
   // allow the largest slice once; each launch asks for its own size (a
   // per-launch attribute would race between concurrent callers)
-  static const cudaError_t attr =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxCtaSmem);
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      saru_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxCtaSmem);
   if (attr != cudaSuccess) return attr;
   a.rs_bytes = L.rs_bytes;
   a.ws_bytes = L.ws_bytes;
   a.warp_smem = L.warp_smem;
-  kern<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
+  cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  saru_band_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -246,14 +271,8 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm) {
 
 size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
   const BandLayout L = band_layout(max_m, k);
-  return (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 * (size_t)(max_m + 1) *
-         (wide ? 8 : 4);
-}
-
-cudaError_t launch_band_kernel(const KernelArgs &a, cudaStream_t s) {
-  const BandLayout L = band_layout(a.max_m, a.k);
-  if (a.wide) return launch_band<uint64_t>(a, L, s);
-  return launch_band<uint32_t>(a, L, s);
+  return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 *
+                             (size_t)(max_m + 1) * (wide ? 8 : 4);
 }
 
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s) {

@@ -15,23 +15,34 @@ constexpr int kStatusUndefined = 8;  // the reference would read outside its arr
 constexpr int kMaxBandM = 512;  // longest read of the banded kernel
 constexpr int kMaxOpWords = (kMaxBandM + 3 * 15 + 15) / 16 + 1;
 
-struct KernelArgs {
+// One reference-style call inside a launch: its own read length, k, band
+// width and output arrays; offsets are relative to its own arrays.
+struct Segment {
   const uint8_t *genome;
   const uint8_t *reads;
   const int32_t *goff;
   const int32_t *roff;
   const int8_t *dirs;
-  long n;
-  int k;
-  int max_m;
-  int first_of_call;
-  int wide;  // 64-bit band
-  long grid; // CTAs of the persistent grid
   int32_t *scores;
   uint8_t *read_aln;
   uint8_t *genome_aln;
-  void *scratch;  // decision planes: 2 * (max_m + 1) * grid * CTA band words
+  long n;
+  long tile_begin;  // first 32-candidate tile of this segment in the launch
+  int k, max_m, first_of_call, wide;
+};
+
+constexpr int kMaxSegs = 192;         // segments per launch (kernel parameter space)
+constexpr size_t kCounterBytes = 256;  // tile counter at the start of the scratch
+
+struct KernelArgs {
+  Segment segs[kMaxSegs];  // by value in the parameter space
+  int nseg;
+  long total_tiles;
+  int *counter;  // zeroed before the launch: next tile to take
+  void *planes;  // decision planes: (max_m + 1) * lanes pairs of the widest band word
   int *status;
+  long grid;
+  int max_m, max_k, wide_any;
   long rs_bytes, ws_bytes, warp_smem;  // shared-memory slice layout (set by the launcher)
 };
 
@@ -59,8 +70,8 @@ struct FullArgs {
 
 BandLayout band_layout(int max_m, int k);
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm);
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide);
-cudaError_t launch_band_kernel(const KernelArgs &a, cudaStream_t s);
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide);  // counter + planes
+cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s);
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
 
 }  // namespace saru

@@ -312,7 +312,7 @@ def pack_windows(genome: np.ndarray, st: np.ndarray, L: np.ndarray,
 def synthetic_candidates(genome: np.ndarray, rd: Reads, m: int, k: int, seed: int,
                          flank_mix=DEFAULT_FLANK_MIX, extra_hits: float = 0.0,
                          repeats: RepeatMap | None = None,
-                         max_candidates: int | None = None) -> Batch:
+                         max_candidates: int | None = None, max_hits: int = 1000) -> Batch:
     """Candidate windows placed as the q-gram filter places them: at the
     read's origin, with a flank class drawn from `flank_mix`; with a repeat
     map, also at the same offset of every other copy of the read's repeat
@@ -330,7 +330,7 @@ def synthetic_candidates(genome: np.ndarray, rd: Reads, m: int, k: int, seed: in
     st = np.concatenate([start, rng.integers(k, G - m - 3 * k, size=int(nx.sum()))])
     cl = np.concatenate([cls, np.repeat(cls, nx)])
     if repeats is not None:
-        hr, hp = repeat_hits(rd, repeats)
+        hr, hp = repeat_hits(rd, repeats, max_per_read=max_hits)
         hc = rng.choice(3, size=len(hr), p=np.asarray(flank_mix)) + 1
         hso = np.where((hc == 2) | (hc == 3), k, 0)
         rid = np.concatenate([rid, hr])

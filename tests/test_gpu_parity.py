@@ -220,3 +220,54 @@ def test_full_size_batch_sampled_against_oracle(saru_lib, shape):
         s = s[:np.argmax(s == 0)] if (s == 0).any() else s
         letters = s[s != ord("_")].tobytes()
         assert reads[i].tobytes().endswith(letters)
+
+
+def test_multi_call_launch_matches_each_call(saru_lib):
+    """Calls of different read lengths, k and band widths (and a call that
+    continues an earlier one) aligned in one launch give each call's own
+    reference bytes."""
+    import torch
+    dev = torch.device("cuda:0")
+    specs = [(36, 3, 3000, True), (75, 5, 2000, True), (100, 6, 2500, True), (150, 9, 1200, True),
+             (250, 15, 400, True), (100, 6, 700, False), (40, 2, 33, True)]
+    keep, sbs, srs, want = [], [], [], []
+    for i, (m, k, n, first) in enumerate(specs):
+        b = W.random_batch(m, k, n, seed=100 + i, err=0.05, alphabet=b"ACGT" if i % 3 else b"ACGTN")
+        if first:
+            s1, ra1, ga1, _ = R.oracle_align(b, nthreads=8)
+            want.append((b, s1, ra1, ga1, 0))
+        else:
+            # candidate 0 continues a call: compare with the oracle's view of
+            # the same candidates behind one extra leading candidate
+            lead = W.random_batch(m, k, 1, seed=999, err=0.05)
+            both = W.make_batch(m, k, [lead.genome] + [b.genome[b.genome_offsets[t] - b.lengths[t]:
+                                                                  b.genome_offsets[t]]
+                                                       for t in range(b.n)],
+                                np.concatenate([lead.reads, b.reads]).reshape(-1, m),
+                                np.concatenate([lead.dirs, b.dirs]))
+            s1, ra1, ga1, _ = R.oracle_align(both, nthreads=8)
+            off = int(both.slot_starts()[1])
+            want.append((b, s1[1:], ra1[off:], ga1[off:], 0))
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        bufs = dict(g=T(b.genome), r=T(b.reads), go=T(b.genome_offsets), ro=T(b.read_offsets),
+                    d=T(b.dirs), s=torch.zeros(b.n, dtype=torch.int32, device=dev),
+                    ra=torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev),
+                    ga=torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev))
+        keep.append(bufs)
+        sbs.append(S.SaruBatch(bufs["g"].data_ptr(), bufs["r"].data_ptr(), bufs["go"].data_ptr(),
+                               bufs["ro"].data_ptr(), bufs["d"].data_ptr(), b.n, b.k, 0, 1,
+                               1 if first else 0, m, len(b.genome), b.total_genome))
+        srs.append(S.SaruResult(bufs["s"].data_ptr(), bufs["ra"].data_ptr(), bufs["ga"].data_ptr(),
+                                None))
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    nscr = S.multi_scratch_bytes(sbs)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
+    S.align_multi_device(sbs, srs, status.data_ptr(), scratch.data_ptr(), nscr,
+                         torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    for (b, s1, ra1, ga1, _), bufs in zip(want, keep):
+        tot = b.total_genome
+        r = S.AlignResult(bufs["s"].cpu().numpy(), bufs["ra"][:tot].cpu().numpy(),
+                          bufs["ga"][:tot].cpu().numpy())
+        check_equal(b, s1, ra1, ga1, r)
