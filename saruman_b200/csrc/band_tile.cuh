@@ -31,8 +31,10 @@ struct TileArgs {
   int k, max_m, first_of_call;
   int32_t *scores;
   uint8_t *read_aln, *genome_aln;
-  void *planes;       // 2 * (max_m + 1) * pstride band words
+  void *planes;       // (max_m + 1) * pstride plane pairs
   long pstride;       // lanes of the whole grid
+  long pair_mul;      // plane-pair index multiplier: 2 when 32-bit pairs share a
+                      // launch with 64-bit ones (one slot size for every lane)
   long rs_bytes, ws_bytes, region_bytes;
 };
 

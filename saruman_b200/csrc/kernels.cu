@@ -49,8 +49,9 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
   stage_in(st_win, ta.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
   __syncwarp();
   LaneState ls;
+  const long mul = ta.pair_mul;
   int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
-    planes[(long)j * ta.pstride + pslot] = PlanePair<T>{A, B};
+    planes[((long)j * ta.pstride + pslot) * mul] = PlanePair<T>{A, B};
   });
   __syncwarp();
   uint8_t *out_r = region;
@@ -63,9 +64,9 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
   __syncwarp();
   st |= lane_traceback<T, 8>(
       ta, s, lane, st_reads, st_win, out_r, out_g, ls,
-      [&](int j) { return planes[(long)j * ta.pstride + pslot]; },
+      [&](int j) { return planes[((long)j * ta.pstride + pslot) * mul]; },
       [&](int j) {
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + (long)j * ta.pstride + pslot));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + ((long)j * ta.pstride + pslot) * mul));
       });
   __syncwarp();
   stage_out(ta.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
@@ -103,7 +104,8 @@ __global__ void __launch_bounds__(128, 3) saru_band_kernel(const __grid_constant
     const Segment &g = a.segs[lo];
     const TileArgs ta{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
                       g.first_of_call, g.scores, g.read_aln, g.genome_aln, a.planes, pstride,
-                      a.rs_bytes, a.ws_bytes, a.warp_smem - a.rs_bytes - a.ws_bytes};
+                      (!g.wide && a.wide_any) ? 2L : 1L, a.rs_bytes, a.ws_bytes,
+                      a.warp_smem - a.rs_bytes - a.ws_bytes};
     const long wt = tile - g.tile_begin;
     status |= g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
                      : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);

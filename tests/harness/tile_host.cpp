@@ -86,6 +86,131 @@ extern "C" int tile_align_batch(const uint8_t *genome, const uint8_t *reads, con
                                 int wide, int first_of_call, int nwarps, int *scores,
                                 uint8_t *ra, uint8_t *ga) {
   TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, ra, ga,
-             nullptr, 0, 0, 0, 0};
+             nullptr, 0, 1, 0, 0, 0};
   return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
+}
+
+// Multi-call launch (saru_band_kernel with a segment table): tiles of all
+// segments in table order, the shared slice sized for the largest read
+// length and k of the launch, one plane buffer for both band widths.
+struct HostSeg {
+  const uint8_t *genome, *reads;
+  const int *goff, *roff;
+  const int8_t *dirs;
+  int *scores;
+  uint8_t *ra, *ga;
+  long n;
+  int k, max_m, first_of_call, wide;
+};
+
+extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total) {
+  int max_m = 0, max_k = 0, wide_any = 0;
+  std::vector<long> tile_begin(nseg);
+  long tiles = 0;
+  for (int i = 0; i < nseg; ++i) {
+    tile_begin[i] = tiles;
+    tiles += (segs[i].n + 31) / 32;
+    if (segs[i].max_m > max_m) max_m = segs[i].max_m;
+    if (segs[i].k > max_k) max_k = segs[i].k;
+    wide_any |= segs[i].wide;
+  }
+  const SliceLayout S = slice_layout(max_m, max_k);
+  const long pstride = (long)nwarps_total * 32;
+  // exactly the bytes the launcher reserves for the planes
+  std::vector<uint8_t> planes_v((size_t)(max_m + 1) * pstride * 2 * (wide_any ? 8 : 4));
+  int status = 0;
+  auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
+  auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
+  auto st16 = [](uint8_t *g, const uint8_t *d) { memcpy(g, d, 16); };
+  struct Slice {
+    uint8_t *st_reads, *st_win, *region;
+    LaneState ls[32];
+    long tile = -1;
+    int seg = 0;
+    TileSpan span;
+  };
+  std::vector<Slice> W(nwarps_total);
+  for (auto &w : W) {
+    w.st_reads = (uint8_t *)aligned_alloc(16, (size_t)S.rs_bytes);
+    w.st_win = (uint8_t *)aligned_alloc(16, (size_t)S.ws_bytes);
+    w.region = (uint8_t *)aligned_alloc(16, (size_t)S.region_bytes);
+  }
+  auto targs = [&](int si) {
+    const HostSeg &g = segs[si];
+    return TileArgs{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
+                    g.first_of_call, g.scores, g.ra, g.ga, planes_v.data(), pstride,
+                    (!g.wide && wide_any) ? 2L : 1L, S.rs_bytes, S.ws_bytes, S.region_bytes};
+  };
+  // rounds: every warp takes a tile, all fills run, then all tracebacks --
+  // the interleaving in which one lane's planes could clobber another's
+  for (long base = 0; base < tiles; base += nwarps_total) {
+    for (int gw = 0; gw < nwarps_total; ++gw) {
+      Slice &w = W[gw];
+      w.tile = base + gw < tiles ? base + gw : -1;
+      if (w.tile < 0) continue;
+      int lo = 0, hi = nseg - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_begin[mid] <= w.tile) lo = mid;
+        else hi = mid - 1;
+      }
+      w.seg = lo;
+      const TileArgs a = targs(lo);
+      w.span = tile_span(a, w.tile - tile_begin[lo]);
+      if (!w.span.fits) {
+        status |= 1;
+        w.tile = -1;
+        continue;
+      }
+      auto fill = [&](auto tag) {
+        using T = decltype(tag);
+        PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
+        for (int lane = 0; lane < 32; ++lane) {
+          stage_in(w.st_reads, a.reads, w.span.r_lo, w.span.r_hi, w.span.r_base, lane, ld16, ld1);
+          stage_in(w.st_win, a.genome, w.span.g_lo, w.span.g_hi, w.span.g_base, lane, ld16, ld1);
+        }
+        for (int lane = 0; lane < 32; ++lane) {
+          const long pslot = (long)gw * 32 + lane;
+          status |= lane_fill<T>(a, w.span, lane, w.st_reads, w.st_win,
+                                 reinterpret_cast<uint32_t *>(w.region), w.ls[lane],
+                                 [&](int j, T A, T B) {
+                                   planes[((long)j * pstride + pslot) * a.pair_mul] =
+                                       PlanePair<T>{A, B};
+                                 });
+        }
+      };
+      if (segs[lo].wide) fill(uint64_t(0));
+      else fill(uint32_t(0));
+    }
+    for (int gw = 0; gw < nwarps_total; ++gw) {
+      Slice &w = W[gw];
+      if (w.tile < 0) continue;
+      const TileArgs a = targs(w.seg);
+      auto trace = [&](auto tag) {
+        using T = decltype(tag);
+        PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
+        memset(w.region, 0, (size_t)S.region_bytes);
+        uint8_t *out_r = w.region, *out_g = w.region + w.span.o_span_r;
+        for (int lane = 0; lane < 32; ++lane) {
+          const long pslot = (long)gw * 32 + lane;
+          status |= lane_traceback<T, 8>(
+              a, w.span, lane, w.st_reads, w.st_win, out_r, out_g, w.ls[lane],
+              [&](int j) { return planes[((long)j * pstride + pslot) * a.pair_mul]; },
+              [&](int j) { (void)planes[((long)j * pstride + pslot) * a.pair_mul]; });
+        }
+        for (int lane = 0; lane < 32; ++lane) {
+          stage_out(a.read_aln, out_r, w.span.s_lo, w.span.s_hi, w.span.o_base_r, lane, st16);
+          stage_out(a.genome_aln, out_g, w.span.s_lo, w.span.s_hi, w.span.o_base_g, lane, st16);
+        }
+      };
+      if (segs[w.seg].wide) trace(uint64_t(0));
+      else trace(uint32_t(0));
+    }
+  }
+  for (auto &w : W) {
+    free(w.st_reads);
+    free(w.st_win);
+    free(w.region);
+  }
+  return status;
 }

@@ -73,8 +73,46 @@ def main():
     if not (st & 1):
         bad += 1
         print("irregular tile not reported", st)
+    bad += multi_launch(lib)
     print("BAD", bad)
     sys.exit(1 if bad else 0)
+
+
+class HostSeg(C.Structure):
+    _fields_ = [("genome", C.c_void_p), ("reads", C.c_void_p), ("goff", C.c_void_p),
+                ("roff", C.c_void_p), ("dirs", C.c_void_p), ("scores", C.c_void_p),
+                ("ra", C.c_void_p), ("ga", C.c_void_p), ("n", C.c_long), ("k", C.c_int),
+                ("max_m", C.c_int), ("first_of_call", C.c_int), ("wide", C.c_int)]
+
+
+def multi_launch(lib) -> int:
+    """Calls of mixed read lengths and band widths in one emulated launch,
+    every warp's fill before any traceback (the interleaving in which lanes
+    could clobber each other's decision planes)."""
+    specs = [(36, 3, 300), (75, 5, 200), (100, 6, 250), (150, 9, 120), (250, 15, 40), (40, 2, 33)]
+    keep, segs = [], []
+    for i, (m, k, n) in enumerate(specs):
+        b = W.random_batch(m, k, n, seed=100 + i, err=0.05, alphabet=b"ACGT" if i % 3 else b"ACGTN")
+        sc = np.zeros(n, np.int32)
+        ra = exact(np.zeros(b.total_genome, np.uint8), i % 16)
+        ga = exact(np.zeros(b.total_genome, np.uint8), (i + 5) % 16)
+        g = exact(b.genome, (i + 3) % 16)
+        r = exact(b.reads, (i + 7) % 16)
+        keep.append((b, sc, ra, ga, g, r))
+        segs.append(HostSeg(g.ctypes.data, r.ctypes.data, b.genome_offsets.ctypes.data,
+                            b.read_offsets.ctypes.data, b.dirs.ctypes.data, sc.ctypes.data,
+                            ra.ctypes.data, ga.ctypes.data, n, k, m, 1, 1 if k > 7 else 0))
+    order = sorted(range(len(specs)), key=lambda i: -(specs[i][0] * (specs[i][1] + 1)))
+    arr = (HostSeg * len(segs))(*[segs[i] for i in order])
+    st = lib.tile_align_multi(arr, len(segs), 5)
+    bad = 1 if st else 0
+    for (b, sc, ra, ga, _, _), spec in zip(keep, specs):
+        s1, ra1, ga1, _ = R.oracle_align(b, nthreads=4)
+        if not (np.array_equal(np.minimum(s1, b.k + 1), sc) and np.array_equal(ra1, ra)
+                and np.array_equal(ga1, ga)):
+            print("MULTI MISMATCH", spec, flush=True)
+            bad += 1
+    return bad
 
 
 if __name__ == "__main__":
