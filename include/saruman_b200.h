@@ -150,11 +150,13 @@ int saru_align_device_static(const saru_batch *batch, saru_result *result, void 
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 
-/* Several calls in one launch of the banded kernel: each saru_batch is one
- * reference-style call (its own read length, k, band width, first-of-call
- * flag and output arrays, all device pointers); persistent warps take
- * 32-candidate tiles of all calls from one work counter, heaviest calls
- * first.  Up to 192 calls; conditions per call as for saru_align_device.
+/* Several calls at once: each saru_batch is one reference-style call (its
+ * own read length, k, band width, first-of-call flag and output arrays, all
+ * device pointers).  Calls of similar read length and band width share one
+ * persistent launch whose warps take 32-candidate tiles of all its calls
+ * from one work counter, heaviest first; the launches of different length
+ * classes run concurrently on streams forked from `stream` and joined back
+ * to it.  Up to 192 calls; conditions per call as for saru_align_device.
  * The calls' status bits are ORed into *status (device).  `scratch` must hold
  * saru_multi_scratch_bytes(calls, ncalls) bytes of device memory. */
 int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32_t ncalls,

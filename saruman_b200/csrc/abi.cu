@@ -308,6 +308,122 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   return SARU_OK;
 }
 
+// Calls of a multi-call request are grouped into layout classes (read-length
+// bucket x band width): one launch sizes its shared-memory slice for its
+// longest read, so mixing 36 bp and 150 bp calls in one launch would run the
+// short ones at the long ones' occupancy.  Each class gets its own persistent
+// launch; the launches run concurrently on forked streams.
+struct LaunchClass {
+  std::vector<int> calls;
+  int max_m = 0, max_k = 0;
+  bool wide = false;
+  long n = 0, grid = 0;
+  size_t scratch_off = 0, scratch_bytes = 0;
+};
+
+int length_bucket(int m) {
+  static const int edges[] = {48, 96, 160, 288, 512};
+  for (int e : edges)
+    if (m <= e) return e;
+  return m;
+}
+
+std::vector<LaunchClass> plan_classes(const saru_batch *calls, int ncalls, int dev) {
+  std::vector<LaunchClass> cls;
+  std::vector<std::pair<int, int>> keys;
+  for (int i = 0; i < ncalls; ++i) {
+    const std::pair<int, int> key(length_bucket(calls[i].max_read_length), calls[i].k > 7);
+    size_t c = 0;
+    while (c < keys.size() && keys[c] != key) ++c;
+    if (c == keys.size()) {
+      keys.push_back(key);
+      cls.emplace_back();
+    }
+    LaunchClass &L = cls[c];
+    L.calls.push_back(i);
+    L.max_m = std::max(L.max_m, calls[i].max_read_length);
+    L.max_k = std::max(L.max_k, calls[i].k);
+    L.wide = L.wide || calls[i].k > 7;
+    L.n += calls[i].n;
+  }
+  size_t off = 0;
+  for (auto &L : cls) {
+    L.grid = band_grid(dev, L.n, L.max_m, L.max_k);
+    L.scratch_bytes = band_scratch_bytes(L.grid, L.max_m, L.max_k, L.wide);
+    L.scratch_off = off;
+    off += (L.scratch_bytes + 255) & ~size_t(255);
+  }
+  return cls;
+}
+
+size_t classes_scratch_bytes(const std::vector<LaunchClass> &cls) {
+  size_t t = 0;
+  for (const auto &L : cls) t += (L.scratch_bytes + 255) & ~size_t(255);
+  return t;
+}
+
+// Streams and events for the concurrent class launches of one device.
+struct ClassStreams {
+  std::mutex mu;
+  int dev = -1;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  int ensure(int d, size_t n) {
+    if (dev != d) {
+      if (dev >= 0) return SARU_E_INVALID;
+      dev = d;
+      SARU_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    }
+    while (streams.size() < n) {
+      cudaStream_t st;
+      cudaEvent_t ev;
+      SARU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      SARU_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      streams.push_back(st);
+      joins.push_back(ev);
+    }
+    return SARU_OK;
+  }
+};
+ClassStreams g_class_streams[64];
+
+int run_band_classes(const saru_batch *calls, const saru_result *res, int ncalls, void *scratch,
+                     size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s) {
+  const std::vector<LaunchClass> cls = plan_classes(calls, ncalls, dev);
+  if (classes_scratch_bytes(cls) > scratch_bytes) {
+    set_error("scratch too small: %zu < %zu", scratch_bytes, classes_scratch_bytes(cls));
+    return SARU_E_INVALID;
+  }
+  Plan pl;
+  pl.band = true;
+  auto launch = [&](const LaunchClass &L, cudaStream_t st) {
+    std::vector<saru_batch> cb;
+    std::vector<saru_result> cr;
+    for (int i : L.calls) {
+      cb.push_back(calls[i]);
+      cr.push_back(res[i]);
+    }
+    return run_band_multi(cb.data(), cr.data(), (int)cb.size(), pl,
+                          static_cast<uint8_t *>(scratch) + L.scratch_off, L.scratch_bytes,
+                          status_dev, dev, st);
+  };
+  if (cls.size() == 1) return launch(cls[0], s);
+  if (dev < 0 || dev >= 64) return SARU_E_INVALID;
+  ClassStreams &CS = g_class_streams[dev];
+  std::lock_guard<std::mutex> lk(CS.mu);
+  int rc = CS.ensure(dev, cls.size());
+  if (rc) return rc;
+  SARU_CUDA(cudaEventRecord(CS.fork, s));
+  for (size_t c = 0; c < cls.size(); ++c) {
+    SARU_CUDA(cudaStreamWaitEvent(CS.streams[c], CS.fork, 0));
+    if ((rc = launch(cls[c], CS.streams[c]))) return rc;
+    SARU_CUDA(cudaEventRecord(CS.joins[c], CS.streams[c]));
+    SARU_CUDA(cudaStreamWaitEvent(s, CS.joins[c], 0));
+  }
+  return SARU_OK;
+}
+
 int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
              size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
              long max_grid = 0) {
@@ -607,16 +723,7 @@ size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls) {
     cudaGetLastError();
     dev = 0;
   }
-  int max_m = 0, max_k = 0, wide = 0;
-  long n = 0;
-  for (int i = 0; i < ncalls; ++i) {
-    if (calls[i].max_read_length > max_m) max_m = calls[i].max_read_length;
-    if (calls[i].k > max_k) max_k = calls[i].k;
-    wide |= calls[i].k > 7;
-    n += calls[i].n;
-  }
-  const long grid = band_grid(dev, n, max_m, max_k);
-  return band_scratch_bytes(grid, max_m, max_k, wide != 0);
+  return classes_scratch_bytes(plan_classes(calls, ncalls, dev));
 }
 
 int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32_t ncalls,
@@ -640,8 +747,9 @@ int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32
   SARU_CUDA(cudaGetDevice(&dev));
   Plan pl;
   pl.band = true;
-  return run_band_multi(calls, results, ncalls, pl, scratch, scratch_bytes, status, dev,
-                        reinterpret_cast<cudaStream_t>(stream));
+  (void)pl;
+  return run_band_classes(calls, results, ncalls, scratch, scratch_bytes, status, dev,
+                          reinterpret_cast<cudaStream_t>(stream));
 }
 
 int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
