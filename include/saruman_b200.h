@@ -75,6 +75,8 @@ extern float alignment_time[2];
 #define SARU_E_CUDA 2        /* CUDA runtime error */
 #define SARU_E_NOMEM 3       /* device or host allocation failed */
 #define SARU_E_OVERFLOW 4    /* a traceback left its slot (order-dependent in the reference) */
+#define SARU_E_TIMEOUT 5     /* saru_server_wait: the request is not done yet */
+#define SARU_MAX_CALLS 192   /* calls in one saru_align_multi_device request */
 
 /* One call's candidates in the reference layout.  All pointers are either
  * all host or all device pointers, depending on the entry point. */
@@ -156,12 +158,67 @@ size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
  * persistent launch whose warps take 32-candidate tiles of all its calls
  * from one work counter, heaviest first; the launches of different length
  * classes run concurrently on streams forked from `stream` and joined back
- * to it.  Up to 192 calls; conditions per call as for saru_align_device.
- * The calls' status bits are ORed into *status (device).  `scratch` must hold
+ * to it.  Up to 192 calls (SARU_MAX_CALLS); conditions per call as for
+ * saru_align_device.  Each call's status bits are ORed into its
+ * results[i].status when that is non-NULL, else into *status (device
+ * words the caller zeroes).  `scratch` must hold
  * saru_multi_scratch_bytes(calls, ncalls) bytes of device memory. */
 int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32_t ncalls,
                             int32_t *status, void *scratch, size_t scratch_bytes, void *stream);
 size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls);
+
+/* ---- request server (continuous batching on one GPU) ----------------------
+ * Not in the reference, whose alignment calls are synchronous
+ * (src/cuda-functions.cu:77-239).  A server owns one GPU, a device arena of
+ * device_budget_bytes for the inputs and outputs of admitted requests, and
+ * three streams (copy in, compute, copy out).  A request is a set of
+ * reference-style calls with HOST arrays (pinned memory lets the copies
+ * overlap; pageable memory works but serialises them) and host outputs.
+ * Requests are admitted in arrival order while the arena has room; all
+ * requests admitted together form one launch group, aligned by one
+ * saru_align_multi_device request, while the next group's inputs are copied
+ * in and the previous group's results are copied out.  Each request's
+ * results are those saru_align_host gives for each of its calls: calls the
+ * banded kernel flags (rare bytes, irregular windows, m <= 3k) are redone on
+ * the exact path before the request completes.
+ * pipeline = 0 processes one request at a time, one launch per call and no
+ * overlap: the plain per-request loop, for comparison.
+ * The caller keeps a request's host arrays alive until saru_server_wait
+ * returns something other than SARU_E_TIMEOUT for its ticket. */
+typedef struct saru_server saru_server;
+typedef struct {
+  int32_t device;
+  int32_t pipeline;                /* 1: continuous batching; 0: one request at a time */
+  int32_t max_requests_per_launch; /* cap on a launch group (>= 1) */
+  int32_t max_inflight;            /* launch groups queued on the GPU at once (>= 1) */
+  int64_t device_budget_bytes;     /* arena for request inputs and outputs */
+} saru_server_config;
+typedef struct {
+  const saru_batch *calls; /* host pointers */
+  saru_result *results;    /* host outputs; status unused */
+  int32_t ncalls;
+} saru_request;
+typedef struct {
+  int64_t submit_us, admit_us, done_us; /* steady clock, microseconds */
+  int32_t group;                        /* launch group the request ran in */
+  int32_t redone_calls;                 /* calls redone on the exact path */
+} saru_request_stats;
+
+/* NULL on failure (saru_last_error() says why). */
+saru_server *saru_server_create(const saru_server_config *cfg);
+/* Queues a request; *ticket identifies it.  SARU_E_INVALID for calls the
+ * banded kernel cannot take at all (costs, k, read length), SARU_E_NOMEM if
+ * it can never fit the arena. */
+int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket);
+/* Waits up to timeout_ms for a request: SARU_OK (results written),
+ * SARU_E_TIMEOUT (still running; wait again), or the error the request
+ * ended with.  A ticket is forgotten once a wait returns anything else
+ * than SARU_E_TIMEOUT. */
+int saru_server_wait(saru_server *s, int64_t ticket, int32_t timeout_ms, saru_request_stats *stats);
+/* Launch groups formed and kernel launches enqueued so far. */
+void saru_server_counters(saru_server *s, int64_t *groups, int64_t *launches);
+/* Finishes queued requests, then frees everything. */
+void saru_server_destroy(saru_server *s);
 
 /* Formats the reference's TSV lines for one aligned call into `out`
  * (capacity cap) and returns the bytes needed.  names: n_names entries of

@@ -22,6 +22,8 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libsaruman_b200.so"
 
 SARU_OK, SARU_E_INVALID, SARU_E_CUDA, SARU_E_NOMEM, SARU_E_OVERFLOW = 0, 1, 2, 3, 4
+SARU_E_TIMEOUT = 5
+SARU_MAX_CALLS = 192
 SARU_S_IRREGULAR, SARU_S_ALPHABET, SARU_S_OVERFLOW = 1, 2, 4
 
 # symbols include/saruman_b200.h declares
@@ -29,7 +31,9 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "get_cuda_infos", "saru_align_host", "saru_align_device", "saru_scratch_bytes",
                  "saru_format_tsv", "saru_last_error", "saru_kernel_launches",
                  "saru_int32_issue_probe", "saru_align_device_static",
-                 "saru_align_multi_device", "saru_multi_scratch_bytes")
+                 "saru_align_multi_device", "saru_multi_scratch_bytes", "saru_server_create",
+                 "saru_server_submit", "saru_server_wait", "saru_server_counters",
+                 "saru_server_destroy")
 ABI_DATA = ("alignment_time",)
 
 
@@ -50,6 +54,22 @@ class SaruBatch(C.Structure):
 class SaruResult(C.Structure):
     _fields_ = [("scores", C.c_void_p), ("read_aln", C.c_void_p), ("genome_aln", C.c_void_p),
                 ("status", C.c_void_p)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("pipeline", C.c_int32),
+                ("max_requests_per_launch", C.c_int32), ("max_inflight", C.c_int32),
+                ("device_budget_bytes", C.c_int64)]
+
+
+class SaruRequest(C.Structure):
+    _fields_ = [("calls", C.POINTER(SaruBatch)), ("results", C.POINTER(SaruResult)),
+                ("ncalls", C.c_int32)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("submit_us", C.c_int64), ("admit_us", C.c_int64), ("done_us", C.c_int64),
+                ("group", C.c_int32), ("redone_calls", C.c_int32)]
 
 
 _lib = None
@@ -81,6 +101,16 @@ def load(path: str | Path | None = None):
                                             C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
     lib.saru_multi_scratch_bytes.restype = C.c_size_t
     lib.saru_multi_scratch_bytes.argtypes = [C.POINTER(SaruBatch), C.c_int32]
+    lib.saru_server_create.restype = C.c_void_p
+    lib.saru_server_create.argtypes = [C.POINTER(ServerConfig)]
+    lib.saru_server_submit.restype = C.c_int
+    lib.saru_server_submit.argtypes = [C.c_void_p, C.POINTER(SaruRequest), C.POINTER(C.c_int64)]
+    lib.saru_server_wait.restype = C.c_int
+    lib.saru_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(RequestStats)]
+    lib.saru_server_counters.restype = None
+    lib.saru_server_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.saru_server_destroy.restype = None
+    lib.saru_server_destroy.argtypes = [C.c_void_p]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -203,3 +233,96 @@ def align_multi_device(batches: list[SaruBatch], results: list[SaruResult], stat
 def multi_scratch_bytes(batches: list[SaruBatch]) -> int:
     n = len(batches)
     return int(load().saru_multi_scratch_bytes((SaruBatch * n)(*batches), n))
+
+
+class HostRequest:
+    """Host arrays of one request for the server: the inputs of each call
+    (copied from Batch objects) and output arrays of the reference layout.
+    `alloc(nbytes)` gives the uint8 host buffers (pinned ones let the
+    server's copies overlap its kernels); numpy by default."""
+
+    def __init__(self, batches: list[Batch], first_of_call: list[bool] | None = None,
+                 alloc=None):
+        alloc = alloc or (lambda nbytes: np.zeros(nbytes, np.uint8))
+        first = first_of_call or [True] * len(batches)
+
+        def host(a: np.ndarray, dtype) -> np.ndarray:
+            a = np.ascontiguousarray(a, dtype)
+            buf = alloc(max(a.nbytes, 1)).view(np.uint8)[:max(a.nbytes, 1)]
+            buf[:a.nbytes] = a.view(np.uint8).reshape(-1)
+            return buf[:a.nbytes].view(dtype) if a.nbytes else buf[:0].view(dtype)
+
+        self.batches = batches
+        self.keep: list[np.ndarray] = []
+        self.outs: list[AlignResult] = []
+        calls, results = [], []
+        for b, f in zip(batches, first):
+            arrs = [host(b.genome, np.uint8), host(b.reads, np.uint8),
+                    host(b.genome_offsets, np.int32), host(b.read_offsets, np.int32),
+                    host(b.dirs, np.int8)]
+            self.keep += arrs
+            calls.append(SaruBatch(*[_p(a) if a.size else 0 for a in arrs], b.n, b.k, b.match,
+                                   b.mismatch, 1 if f else 0, b.m, len(b.genome),
+                                   b.total_genome))
+            out = AlignResult(alloc(4 * max(b.n, 1)).view(np.int32)[:max(b.n, 1)],
+                              alloc(b.total_genome + 64)[:b.total_genome + 64],
+                              alloc(b.total_genome + 64)[:b.total_genome + 64])
+            self.outs.append(out)
+            results.append(SaruResult(_p(out.scores), _p(out.read_aln), _p(out.genome_aln), None))
+        n = len(batches)
+        self.calls = (SaruBatch * n)(*calls)
+        self.results = (SaruResult * n)(*results)
+        self.req = SaruRequest(self.calls, self.results, n)
+
+    def result(self, i: int) -> AlignResult:
+        b, o = self.batches[i], self.outs[i]
+        return AlignResult(o.scores[:b.n], o.read_aln[:b.total_genome],
+                           o.genome_aln[:b.total_genome])
+
+
+class Server:
+    """Continuous-batching request server on one GPU (saru_server_*)."""
+
+    def __init__(self, device: int = 0, pipeline: bool = True, max_requests_per_launch: int = 64,
+                 max_inflight: int = 2, budget_bytes: int = 8 << 30):
+        self._lib = load()
+        cfg = ServerConfig(device, 1 if pipeline else 0, max_requests_per_launch, max_inflight,
+                           budget_bytes)
+        self._h = self._lib.saru_server_create(C.byref(cfg))
+        if not self._h:
+            raise SaruError(SARU_E_CUDA, last_error())
+        self._live: dict[int, HostRequest] = {}
+
+    def submit(self, req: HostRequest) -> int:
+        t = C.c_int64()
+        rc = self._lib.saru_server_submit(self._h, C.byref(req.req), C.byref(t))
+        if rc != SARU_OK:
+            raise SaruError(rc, last_error())
+        self._live[t.value] = req
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 600_000) -> tuple[int, RequestStats]:
+        """(status code, stats) once the request is done; raises TimeoutError."""
+        st = RequestStats()
+        rc = self._lib.saru_server_wait(self._h, ticket, timeout_ms, C.byref(st))
+        if rc == SARU_E_TIMEOUT:
+            raise TimeoutError(f"request {ticket} not done after {timeout_ms} ms")
+        self._live.pop(ticket, None)
+        return rc, st
+
+    def counters(self) -> tuple[int, int]:
+        g, l_ = C.c_int64(), C.c_int64()
+        self._lib.saru_server_counters(self._h, C.byref(g), C.byref(l_))
+        return g.value, l_.value
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.saru_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -62,6 +62,7 @@ namespace {
 
 thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
+thread_local uint64_t g_thread_launches = 0;  // launches enqueued by this thread
 std::mutex g_out_mu;  // stdout lines and the shared counters
 
 void set_error(const char *fmt, ...) {
@@ -145,7 +146,7 @@ struct Lane {
   }
 };
 
-Lane g_lanes[2];
+Lane g_lanes[3];  // legacy forward, legacy reverse, request server
 
 int current_device() {
   int d = 0;
@@ -275,6 +276,7 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
     g.scores = r->scores;
     g.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
     g.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
+    g.status = r->status ? r->status : status_dev;
     g.n = b->n;
     g.tile_begin = tiles;
     g.k = b->k;
@@ -302,9 +304,9 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   }
   a.counter = reinterpret_cast<int *>(scratch);
   a.planes = reinterpret_cast<uint8_t *>(scratch) + saru::kCounterBytes;
-  a.status = status_dev;
   SARU_CUDA(saru::launch_band_kernel(a, s));
   g_launches.fetch_add(1);
+  g_thread_launches += 1;
   return SARU_OK;
 }
 
@@ -395,9 +397,10 @@ int run_band_classes(const saru_batch *calls, const saru_result *res, int ncalls
     set_error("scratch too small: %zu < %zu", scratch_bytes, classes_scratch_bytes(cls));
     return SARU_E_INVALID;
   }
-  Plan pl;
-  pl.band = true;
   auto launch = [&](const LaunchClass &L, cudaStream_t st) {
+    Plan pl;  // a class of k > 7 calls runs 64-bit band words, even with one call
+    pl.band = true;
+    pl.wide = L.wide;
     std::vector<saru_batch> cb;
     std::vector<saru_result> cr;
     for (int i : L.calls) {
@@ -504,6 +507,7 @@ int run_full(Lane &L, const saru_batch *hb, const saru_batch *db, const Plan &pl
   (void)pl;
   SARU_CUDA(saru::launch_full_kernels(a, s));
   g_launches.fetch_add(2);
+  g_thread_launches += 2;
   return SARU_OK;
 }
 
@@ -597,6 +601,17 @@ struct NameIndex {
 };
 
 }  // namespace
+
+// hooks for the request server (server.cpp)
+namespace saru {
+uint64_t thread_launches() { return g_thread_launches; }
+void set_last_error(const char *msg) { g_last_error = msg; }
+int redo_on_host_path(const saru_batch *b, saru_result *r) {
+  Lane &L = g_lanes[2];
+  std::lock_guard<std::mutex> lk(L.mu);
+  return align_host_impl(b, r, L, nullptr);
+}
+}  // namespace saru
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -745,9 +760,6 @@ int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32
   }
   int dev = 0;
   SARU_CUDA(cudaGetDevice(&dev));
-  Plan pl;
-  pl.band = true;
-  (void)pl;
   return run_band_classes(calls, results, ncalls, scratch, scratch_bytes, status, dev,
                           reinterpret_cast<cudaStream_t>(stream));
 }

@@ -89,7 +89,6 @@ __global__ void __launch_bounds__(128, 3) saru_band_kernel(const __grid_constant
   const long gwarp = (long)blockIdx.x * WARPS + wid;
   const long pstride = (long)gridDim.x * WARPS * 32;
   const long pslot = gwarp * 32 + lane;
-  int status = 0;
   for (;;) {
     int tile = 0;
     if (lane == 0) tile = atomicAdd(a.counter, 1);
@@ -107,13 +106,13 @@ __global__ void __launch_bounds__(128, 3) saru_band_kernel(const __grid_constant
                       (!g.wide && a.wide_any) ? 2L : 1L, a.rs_bytes, a.ws_bytes,
                       a.warp_smem - a.rs_bytes - a.ws_bytes};
     const long wt = tile - g.tile_begin;
-    status |= g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
-                     : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);
+    int status = g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
+                        : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);
+    status = __reduce_or_sync(0xffffffffu, status);
+    if (status && lane == 0)
+      atomicOr(g.status, (status & 1 ? kStatusIrregular : 0) | (status & 2 ? kStatusAlphabet : 0) |
+                             (status & 4 ? kStatusOverflow : 0));
   }
-  status = __reduce_or_sync(0xffffffffu, status);
-  if (status && lane == 0)
-    atomicOr(a.status, (status & 1 ? kStatusIrregular : 0) | (status & 2 ? kStatusAlphabet : 0) |
-                           (status & 4 ? kStatusOverflow : 0));
 }
 
 // ---------------------------------------------------------------------------

@@ -26,6 +26,7 @@ struct Segment {
   int32_t *scores;
   uint8_t *read_aln;
   uint8_t *genome_aln;
+  int *status;      // this call's status word (device)
   long n;
   long tile_begin;  // first 32-candidate tile of this segment in the launch
   int k, max_m, first_of_call, wide;
@@ -40,7 +41,6 @@ struct KernelArgs {
   long total_tiles;
   int *counter;  // zeroed before the launch: next tile to take
   void *planes;  // decision planes: (max_m + 1) * lanes pairs of the widest band word
-  int *status;
   long grid;
   int max_m, max_k, wide_any;
   long rs_bytes, ws_bytes, warp_smem;  // shared-memory slice layout (set by the launcher)

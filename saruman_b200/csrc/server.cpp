@@ -1,0 +1,478 @@
+// server.cpp -- request loop with continuous batching on one GPU.
+//
+// A request is a set of reference-style calls (host arrays in, host arrays
+// out), typically one per read-length bin.  The scheduler thread admits
+// requests in arrival order while the device arena has room for their
+// inputs and outputs; the requests admitted together form a launch group
+// whose calls all go to one multi-call request of the banded kernel (one
+// persistent launch per read-length class, classes concurrent).  Three
+// streams overlap the work: the inputs of group i+1 are copied in while
+// group i computes, and the completion thread copies group i's results out
+// while group i+1 computes.  Requests that arrive while groups are on the GPU
+// join the next group as arena space and launch slots free up.
+//
+// Plain mode (pipeline = 0) processes one request at a time, one launch per
+// call and a full round trip before the next request: the per-request loop
+// the batched mode is measured against.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/saruman_b200.h"
+#include "kernels.cuh"
+#include "server_internal.h"
+
+namespace {
+
+int64_t now_us() {
+  return std::chrono::duration_cast<std::chrono::microseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// First-fit allocator over one device allocation (the admission budget).
+class Arena {
+ public:
+  bool init(size_t bytes) {
+    if (cudaMalloc(&base_, bytes) != cudaSuccess) {
+      base_ = nullptr;
+      return false;
+    }
+    size_ = bytes;
+    free_[0] = bytes;
+    return true;
+  }
+  void release() {
+    if (base_) cudaFree(base_);
+    base_ = nullptr;
+  }
+  long alloc(size_t bytes) {  // offset, or -1 when no free range is large enough
+    bytes = up256(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const size_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > bytes) free_[off + bytes] = len - bytes;
+      return (long)off;
+    }
+    return -1;
+  }
+  void free(size_t off, size_t bytes) {
+    bytes = up256(bytes);
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  uint8_t *ptr(size_t off) const { return static_cast<uint8_t *>(base_) + off; }
+  size_t size() const { return size_; }
+
+ private:
+  void *base_ = nullptr;
+  size_t size_ = 0;
+  std::map<size_t, size_t> free_;  // offset -> length
+};
+
+struct Request {
+  int64_t ticket = 0;
+  std::vector<saru_batch> calls;     // host views (caller's arrays)
+  std::vector<saru_result> results;  // host outputs (caller's arrays)
+  std::vector<saru_batch> dcalls;    // device views inside the arena
+  std::vector<saru_result> dres;
+  std::vector<int32_t> call_status;  // kernel status bits per call, read back
+  size_t dev_bytes = 0;
+  long dev_off = -1;
+  int32_t *dstatus = nullptr;  // one device word per call, inside the arena
+  int64_t t_submit = 0, t_admit = 0, t_done = 0;
+  int32_t group = -1, redone = 0;
+  int rc = SARU_OK;
+  bool done = false;
+};
+
+// Arena bytes one request takes: every device array up256-aligned.
+size_t request_bytes(const Request &r) {
+  size_t t = up256(4 * r.calls.size());  // status words
+  for (const auto &b : r.calls) {
+    const size_t n = (size_t)b.n;
+    t += up256((size_t)b.genome_bytes + 64);
+    t += up256((size_t)(n ? b.read_offsets[n - 1] : 0) + 64);
+    t += 3 * up256(4 * n + 64);  // genome_offsets, read_offsets, scores
+    t += up256(n + 64);          // dirs
+    t += 2 * up256((size_t)b.total_slots + 64);
+  }
+  return t;
+}
+
+}  // namespace
+
+struct saru_server {
+  saru_server_config cfg{};
+  Arena arena;
+  cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
+
+  struct Group {
+    std::vector<std::shared_ptr<Request>> reqs;
+    cudaEvent_t done_ev = nullptr;  // recorded on s_comp after the launch
+    int rc = SARU_OK;
+  };
+
+  std::mutex mu;
+  std::condition_variable cv_pending, cv_inflight, cv_freed, cv_done;
+  std::deque<std::shared_ptr<Request>> pending;
+  std::deque<Group> inflight;
+  std::unordered_map<int64_t, std::shared_ptr<Request>> tickets;
+  int64_t next_ticket = 1, groups = 0, launches = 0, free_gen = 0;
+  bool stop = false, sched_done = false;
+  std::thread sched_thr, done_thr;
+
+  // Carves a request's device arrays out of its arena range and copies its
+  // inputs in on s_in.
+  void stage(Request &r) {
+    uint8_t *p = arena.ptr((size_t)r.dev_off);
+    auto take = [&](size_t bytes) {
+      uint8_t *q = p;
+      p += up256(bytes);
+      return q;
+    };
+    const size_t nc = r.calls.size();
+    r.dstatus = reinterpret_cast<int32_t *>(take(4 * nc));
+    cudaMemsetAsync(r.dstatus, 0, 4 * nc, s_in);
+    r.dcalls.resize(nc);
+    r.dres.resize(nc);
+    for (size_t i = 0; i < nc; ++i) {
+      const saru_batch &h = r.calls[i];
+      const size_t n = (size_t)h.n;
+      const size_t rbytes = n ? (size_t)h.read_offsets[n - 1] : 0;
+      uint8_t *g = take((size_t)h.genome_bytes + 64), *rd = take(rbytes + 64);
+      uint8_t *go = take(4 * n + 64), *ro = take(4 * n + 64), *sc = take(4 * n + 64);
+      uint8_t *dr = take(n + 64);
+      uint8_t *ra = take((size_t)h.total_slots + 64), *ga = take((size_t)h.total_slots + 64);
+      if (n) {
+        cudaMemcpyAsync(g, h.genome, (size_t)h.genome_bytes, cudaMemcpyHostToDevice, s_in);
+        cudaMemcpyAsync(rd, h.reads, rbytes, cudaMemcpyHostToDevice, s_in);
+        cudaMemcpyAsync(go, h.genome_offsets, 4 * n, cudaMemcpyHostToDevice, s_in);
+        cudaMemcpyAsync(ro, h.read_offsets, 4 * n, cudaMemcpyHostToDevice, s_in);
+        cudaMemcpyAsync(dr, h.dirs, n, cudaMemcpyHostToDevice, s_in);
+      }
+      saru_batch &d = r.dcalls[i];
+      d = h;
+      d.genome = reinterpret_cast<const char *>(g);
+      d.reads = reinterpret_cast<const char *>(rd);
+      d.genome_offsets = reinterpret_cast<const int32_t *>(go);
+      d.read_offsets = reinterpret_cast<const int32_t *>(ro);
+      d.dirs = reinterpret_cast<const int8_t *>(dr);
+      r.dres[i] = saru_result{reinterpret_cast<int32_t *>(sc), reinterpret_cast<char *>(ra),
+                              reinterpret_cast<char *>(ga), r.dstatus + i};
+    }
+  }
+
+  int ensure_scratch(size_t bytes) {
+    if (bytes <= scratch_bytes) return SARU_OK;
+    // launches already enqueued on s_comp may still use the old scratch
+    cudaStreamSynchronize(s_comp);
+    if (scratch) cudaFree(scratch);
+    scratch = nullptr;
+    scratch_bytes = 0;
+    if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      saru::set_last_error("request server: scratch allocation failed");
+      return SARU_E_NOMEM;
+    }
+    scratch_bytes = bytes;
+    return SARU_OK;
+  }
+
+  // Next launch group: requests in arrival order while arena space, call
+  // slots and the group cap last.  Empty only when stopping.
+  std::vector<std::shared_ptr<Request>> admit() {
+    std::unique_lock<std::mutex> lk(mu);
+    std::vector<std::shared_ptr<Request>> grp;
+    const size_t cap = cfg.pipeline ? (size_t)cfg.max_requests_per_launch : 1;
+    const size_t max_inflight = cfg.pipeline ? (size_t)cfg.max_inflight : 1;
+    for (;;) {
+      cv_pending.wait(lk, [&] { return stop || !pending.empty(); });
+      if (pending.empty()) return grp;  // stopping, queue drained
+      cv_inflight.wait(lk, [&] { return inflight.size() < max_inflight; });
+      size_t ncalls = 0;
+      while (!pending.empty() && grp.size() < cap) {
+        auto &r = pending.front();
+        if (ncalls + r->calls.size() > (size_t)SARU_MAX_CALLS) break;
+        const long off = arena.alloc(r->dev_bytes);
+        if (off < 0) break;
+        r->dev_off = off;
+        r->t_admit = now_us();
+        r->group = (int32_t)groups;
+        ncalls += r->calls.size();
+        grp.push_back(r);
+        pending.pop_front();
+      }
+      if (!grp.empty()) {
+        groups += 1;
+        return grp;
+      }
+      // The head request waits for completed groups to free arena space.
+      // Something is in flight here: a request alone always fits the empty
+      // arena (submit checks it), and admitted requests hold arena space
+      // until the completion thread frees it.
+      const int64_t gen = free_gen;
+      cv_freed.wait(lk, [&] { return free_gen != gen; });
+    }
+  }
+
+  void scheduler() {
+    cudaSetDevice(cfg.device);
+    for (;;) {
+      std::vector<std::shared_ptr<Request>> grp = admit();
+      if (grp.empty()) break;
+      for (auto &r : grp) stage(*r);
+      cudaEvent_t in_ev = nullptr, done_ev = nullptr;
+      cudaEventCreateWithFlags(&in_ev, cudaEventDisableTiming);
+      cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming);
+      cudaEventRecord(in_ev, s_in);
+      cudaStreamWaitEvent(s_comp, in_ev, 0);
+      std::vector<saru_batch> calls;
+      std::vector<saru_result> res;
+      for (auto &r : grp)
+        for (size_t i = 0; i < r->dcalls.size(); ++i)
+          if (r->dcalls[i].n > 0) {
+            calls.push_back(r->dcalls[i]);
+            res.push_back(r->dres[i]);
+          }
+      int rc = SARU_OK;
+      const uint64_t l0 = saru::thread_launches();
+      if (!calls.empty() && cfg.pipeline) {
+        rc = ensure_scratch(saru_multi_scratch_bytes(calls.data(), (int)calls.size()));
+        if (!rc)  // every call has its own status word; res[0]'s is the unused fallback
+          rc = saru_align_multi_device(calls.data(), res.data(), (int)calls.size(), res[0].status,
+                                       scratch, scratch_bytes, s_comp);
+      } else {
+        for (size_t i = 0; i < calls.size() && !rc; ++i) {
+          rc = ensure_scratch(saru_scratch_bytes(calls[i].n, calls[i].max_read_length,
+                                                 calls[i].k, calls[i].k > 7));
+          if (!rc) rc = saru_align_device(&calls[i], &res[i], scratch, scratch_bytes, s_comp);
+        }
+      }
+      cudaEventRecord(done_ev, s_comp);
+      cudaEventDestroy(in_ev);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        launches += (int64_t)(saru::thread_launches() - l0);
+        inflight.push_back(Group{grp, done_ev, rc});
+      }
+      cv_inflight.notify_all();
+      if (!cfg.pipeline) {  // plain mode: one request's round trip at a time
+        std::unique_lock<std::mutex> lk(mu);
+        cv_done.wait(lk, [&] { return grp.back()->done; });
+      }
+    }
+  }
+
+  // Copies a group's results out, redoes flagged calls on the exact path,
+  // frees its arena ranges and completes its requests.
+  void completer() {
+    cudaSetDevice(cfg.device);
+    for (;;) {
+      Group g;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_inflight.wait(lk, [&] { return !inflight.empty() || sched_done; });
+        if (inflight.empty()) break;
+        g = inflight.front();
+      }
+      cudaStreamWaitEvent(s_out, g.done_ev, 0);
+      for (auto &r : g.reqs) {
+        r->call_status.assign(r->calls.size(), 0);
+        for (size_t i = 0; i < r->calls.size(); ++i) {
+          const saru_batch &h = r->calls[i];
+          if (h.n == 0) continue;
+          const saru_result &d = r->dres[i], &o = r->results[i];
+          cudaMemcpyAsync(o.scores, d.scores, 4 * (size_t)h.n, cudaMemcpyDeviceToHost, s_out);
+          cudaMemcpyAsync(o.read_aln, d.read_aln, (size_t)h.total_slots, cudaMemcpyDeviceToHost,
+                          s_out);
+          cudaMemcpyAsync(o.genome_aln, d.genome_aln, (size_t)h.total_slots,
+                          cudaMemcpyDeviceToHost, s_out);
+        }
+        cudaMemcpyAsync(r->call_status.data(), r->dstatus, 4 * r->calls.size(),
+                        cudaMemcpyDeviceToHost, s_out);
+      }
+      int rc = g.rc;
+      if (cudaStreamSynchronize(s_out) != cudaSuccess && rc == SARU_OK) {
+        saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
+        rc = SARU_E_CUDA;
+      }
+      cudaEventDestroy(g.done_ev);
+      for (auto &r : g.reqs) {
+        r->rc = rc;
+        for (size_t i = 0; i < r->calls.size() && r->rc == SARU_OK; ++i) {
+          const int st = r->call_status[i];
+          if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
+            // as saru_align_host does: the whole call again on the exact path
+            r->rc = saru::redo_on_host_path(&r->calls[i], &r->results[i]);
+            r->redone += 1;
+          } else if (st & saru::kStatusOverflow) {
+            saru::set_last_error("banded traceback left its band");
+            r->rc = SARU_E_OVERFLOW;
+          }
+        }
+      }
+      const int64_t t = now_us();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        inflight.pop_front();
+        for (auto &r : g.reqs) {
+          arena.free((size_t)r->dev_off, r->dev_bytes);
+          r->t_done = t;
+          r->done = true;
+        }
+        free_gen += 1;
+      }
+      cv_inflight.notify_all();
+      cv_freed.notify_all();
+      cv_done.notify_all();
+    }
+  }
+};
+
+extern "C" {
+
+saru_server *saru_server_create(const saru_server_config *cfg) {
+  if (!cfg || cfg->max_inflight < 1 || cfg->max_requests_per_launch < 1 ||
+      cfg->device_budget_bytes < (1 << 20)) {
+    saru::set_last_error("saru_server_create: max_inflight >= 1, max_requests_per_launch >= 1 "
+                         "and device_budget_bytes >= 1 MiB");
+    return nullptr;
+  }
+  auto *s = new saru_server();
+  s->cfg = *cfg;
+  if (cudaSetDevice(cfg->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->s_in, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->s_comp, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking) != cudaSuccess ||
+      !s->arena.init((size_t)cfg->device_budget_bytes)) {
+    saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
+    if (s->s_in) cudaStreamDestroy(s->s_in);
+    if (s->s_comp) cudaStreamDestroy(s->s_comp);
+    if (s->s_out) cudaStreamDestroy(s->s_out);
+    delete s;
+    return nullptr;
+  }
+  s->sched_thr = std::thread([s] { s->scheduler(); });
+  s->done_thr = std::thread([s] { s->completer(); });
+  return s;
+}
+
+int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket) {
+  if (!s || !req || !ticket || req->ncalls < 1 || req->ncalls > SARU_MAX_CALLS) {
+    saru::set_last_error("saru_server_submit: 1..SARU_MAX_CALLS calls and a ticket");
+    return SARU_E_INVALID;
+  }
+  auto r = std::make_shared<Request>();
+  r->calls.assign(req->calls, req->calls + req->ncalls);
+  r->results.assign(req->results, req->results + req->ncalls);
+  for (const auto &b : r->calls) {
+    if (b.n < 0 || b.k < 0 || b.k > 15 || b.match != 0 || b.mismatch != 1 ||
+        b.max_read_length < 2 || b.max_read_length > saru::kMaxBandM) {
+      saru::set_last_error("saru_server_submit: calls need unit costs, k <= 15 and "
+                           "2 <= max_read_length <= 512");
+      return SARU_E_INVALID;
+    }
+  }
+  r->dev_bytes = request_bytes(*r);
+  if (r->dev_bytes > s->arena.size()) {
+    saru::set_last_error("saru_server_submit: request larger than the device budget");
+    return SARU_E_NOMEM;
+  }
+  r->t_submit = now_us();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) {
+      saru::set_last_error("saru_server_submit: server is shutting down");
+      return SARU_E_INVALID;
+    }
+    r->ticket = s->next_ticket++;
+    s->tickets[r->ticket] = r;
+    s->pending.push_back(r);
+  }
+  *ticket = r->ticket;
+  s->cv_pending.notify_all();
+  return SARU_OK;
+}
+
+int saru_server_wait(saru_server *s, int64_t ticket, int32_t timeout_ms,
+                     saru_request_stats *stats) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) {
+    saru::set_last_error("saru_server_wait: unknown ticket");
+    return SARU_E_INVALID;
+  }
+  std::shared_ptr<Request> r = it->second;
+  if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms),
+                           [&] { return r->done; }))
+    return SARU_E_TIMEOUT;
+  if (stats) {
+    stats->submit_us = r->t_submit;
+    stats->admit_us = r->t_admit;
+    stats->done_us = r->t_done;
+    stats->group = r->group;
+    stats->redone_calls = r->redone;
+  }
+  s->tickets.erase(it);
+  return r->rc;
+}
+
+void saru_server_counters(saru_server *s, int64_t *groups, int64_t *launches) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (groups) *groups = s->groups;
+  if (launches) *launches = s->launches;
+}
+
+void saru_server_destroy(saru_server *s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_pending.notify_all();
+  if (s->sched_thr.joinable()) s->sched_thr.join();  // drains the pending queue first
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->sched_done = true;
+  }
+  s->cv_inflight.notify_all();
+  if (s->done_thr.joinable()) s->done_thr.join();
+  cudaSetDevice(s->cfg.device);
+  cudaStreamSynchronize(s->s_comp);
+  if (s->scratch) cudaFree(s->scratch);
+  s->arena.release();
+  cudaStreamDestroy(s->s_in);
+  cudaStreamDestroy(s->s_comp);
+  cudaStreamDestroy(s->s_out);
+  delete s;
+}
+
+}  // extern "C"
