@@ -57,6 +57,14 @@ CONFIGS = {
                "25 per read (~22M candidates of uneven count per read); all length bins in one launch",
                genome=("repeat", 5_000_000, 301, "zipf"), reads=4_000_000, lengths=(36, 75, 100, 150),
                rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0, max_hits=25),
+    "c5": dict(workload="serving: 5 Mbp genome with Zipf(1.5, max 500) repeat copies; Poisson "
+               "arrivals of requests of 1k-500k reads (log-uniform), read lengths {36,75,100,150} "
+               "in equal parts, k=ceil(0.06 m), repeat hits capped at 25 per read; 60 GB device "
+               "budget; continuous-batching server vs the plain per-request loop on one trace",
+               genome=("repeat", 5_000_000, 301, "zipf"), reads=2_000_000,
+               lengths=(36, 75, 100, 150), rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0,
+               max_hits=25, requests=96, min_reads=1_000, max_reads=500_000, budget=60 << 30,
+               load=0.8),
 }
 
 
@@ -331,6 +339,227 @@ def timed(stream, fn, steps, world, dist, dev):
     return ms / steps
 
 
+class RequestPool:
+    """Requests of the serving trace as C-ABI views into pinned host memory:
+    each request takes a contiguous range of reads from every length bin of
+    a pre-generated candidate pool (the host filter's output), one call per
+    bin, with its own re-based offsets; outputs come from a pinned ring that
+    requests release in completion order."""
+
+    def __init__(self, bs, S, ring_bytes: int):
+        import torch
+        self.S = S
+        self.bs = bs
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        self.pg = [pin(b.genome) for b in bs]
+        self.pr = [pin(b.reads) for b in bs]
+        self.pd = [pin(b.dirs) for b in bs]
+        self.gend = [np.concatenate([[0], b.genome_offsets.astype(np.int64)]) for b in bs]
+        self.per_bin = [int(b.ids.max()) + 1 for b in bs]
+        self.ring = torch.empty(ring_bytes, dtype=torch.uint8).pin_memory()
+        self.ring_ptr = self.ring.data_ptr()
+        self.ring_bytes = ring_bytes
+        self.live = []  # (start, end) of outstanding requests, oldest first
+
+    def make(self, reads: int, rng) -> dict:
+        import torch
+        S = self.S
+        calls, offs, cand = [], [], 0
+        out_bytes = 0
+        spans = []
+        for i, b in enumerate(self.bs):
+            r = max(1, reads // len(self.bs))
+            r0 = int(rng.integers(0, max(1, self.per_bin[i] - r)))
+            c0, c1 = (int(x) for x in np.searchsorted(b.ids, [r0, r0 + r]))
+            n = c1 - c0
+            if n == 0:
+                continue
+            base = int(self.gend[i][c0])
+            go = (self.gend[i][c0 + 1:c1 + 1] - base).astype(np.int32)
+            ro = ((np.arange(n, dtype=np.int64) + 1) * b.m).astype(np.int32)
+            t = torch.from_numpy(np.concatenate([go, ro])).pin_memory()
+            offs.append(t)
+            gbytes = int(go[-1])
+            slots = gbytes + b.k * n
+            spans.append((4 * n, slots + 64))
+            out_bytes += (4 * n + 255) // 256 * 256 + 2 * ((slots + 64 + 255) // 256 * 256)
+            calls.append(S.SaruBatch(self.pg[i].data_ptr() + base, self.pr[i].data_ptr() + c0 * b.m,
+                                     t.data_ptr(), t.data_ptr() + 4 * n,
+                                     self.pd[i].data_ptr() + c0, n, b.k, 0, 1, 1, b.m, gbytes,
+                                     slots))
+            cand += n
+        return dict(calls=calls, offs=offs, cand=cand, out_bytes=out_bytes, spans=spans,
+                    h2d=sum(int(c.genome_bytes) + c.n * (c.max_read_length + 9) for c in calls),
+                    d2h=sum(4 * c.n + 2 * int(c.total_slots) for c in calls))
+
+    def alloc(self, nbytes: int) -> int | None:
+        """Start offset in the ring, or None while the oldest requests hold it."""
+        if nbytes > self.ring_bytes:
+            raise ValueError("request larger than the output ring")
+        if not self.live:
+            return 0
+        tail, head = self.live[0][0], self.live[-1][1]
+        if self.live[-1][0] >= tail:  # not wrapped: free [head, end) and [0, tail)
+            if self.ring_bytes - head >= nbytes:
+                return head
+            return 0 if tail >= nbytes else None
+        return head if tail - head >= nbytes else None  # wrapped: free [head, tail)
+
+    def bind(self, req: dict, start: int):
+        S = self.S
+        p = self.ring_ptr + start
+        res = []
+        for n4, slots in req["spans"]:
+            sc = p
+            p += (n4 + 255) // 256 * 256
+            ra = p
+            p += (slots + 255) // 256 * 256
+            ga = p
+            p += (slots + 255) // 256 * 256
+            res.append(S.SaruResult(sc, ra, ga, None))
+        self.live.append((start, start + req["out_bytes"]))
+        n = len(req["calls"])
+        req["arr_c"] = (S.SaruBatch * n)(*req["calls"])
+        req["arr_r"] = (S.SaruResult * n)(*res)
+        req["creq"] = S.SaruRequest(req["arr_c"], req["arr_r"], n)
+
+    def release_oldest(self):
+        self.live.pop(0)
+
+
+def run_trace(S, pool: RequestPool, reqs: list, arrivals_s, pipeline: bool, budget: int,
+              max_per_launch: int = 64):
+    """Submits the requests at their arrival times (seconds after start;
+    None = all at once) to a fresh server and returns per-request latency
+    from arrival to results on the host, the makespan and the counters."""
+    import ctypes as C
+    import threading
+    srv = S.Server(pipeline=pipeline, max_requests_per_launch=max_per_launch, max_inflight=2,
+                   budget_bytes=budget)
+    lib = S.load()
+    tickets = [None] * len(reqs)
+    done_us = [0] * len(reqs)
+    lock = threading.Condition()
+    t0 = time.monotonic_ns() // 1000
+
+    def submitter():
+        for q, r in enumerate(reqs):
+            if arrivals_s is not None:
+                delay = t0 / 1e6 + arrivals_s[q] - time.monotonic()
+                if delay > 0:
+                    time.sleep(delay)
+            with lock:
+                while True:
+                    start = pool.alloc(r["out_bytes"])
+                    if start is not None:
+                        break
+                    lock.wait()
+                pool.bind(r, start)
+            t = C.c_int64()
+            rc = lib.saru_server_submit(srv._h, C.byref(r["creq"]), C.byref(t))
+            if rc != S.SARU_OK:
+                raise RuntimeError(S.last_error())
+            with lock:
+                tickets[q] = t.value
+                lock.notify_all()
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    st = S.RequestStats()
+    for q in range(len(reqs)):
+        with lock:
+            while tickets[q] is None:
+                lock.wait()
+            t = tickets[q]
+        rc = lib.saru_server_wait(srv._h, t, 3_600_000, C.byref(st))
+        if rc != S.SARU_OK:
+            raise RuntimeError(f"request {q}: {rc} {S.last_error()}")
+        done_us[q] = st.done_us
+        with lock:
+            pool.release_oldest()
+            lock.notify_all()
+    th.join()
+    groups, launches = srv.counters()
+    srv.close()
+    arr_us = [t0 + (int(a * 1e6) if arrivals_s is not None else 0) for a in
+              (arrivals_s if arrivals_s is not None else [0] * len(reqs))]
+    lat_ms = [(d - a) / 1000 for d, a in zip(done_us, arr_us)]
+    makespan = (max(done_us) - t0) / 1e6
+    return lat_ms, makespan, groups, launches
+
+
+def run_serving(args, cfg, rank: int) -> None:
+    """Serving workload: the same seeded Poisson trace through the batched
+    server and the plain per-request loop, plus both at saturation."""
+    import torch
+    import saruman_b200 as S
+    torch.cuda.set_device(0)
+    bs = build_batches(cfg, rank)
+    S.load()
+    rng = np.random.default_rng(4242)
+    nreq = args.requests or cfg["requests"]
+    sizes = np.exp(rng.uniform(np.log(cfg["min_reads"]), np.log(cfg["max_reads"]), nreq))
+    sizes = sizes.astype(np.int64)
+    pool = RequestPool(bs, S, ring_bytes=6 << 30)  # largest request: ~0.7 GB of outputs
+    reqs = [pool.make(int(s), rng) for s in sizes]
+    n_cand = sum(r["cand"] for r in reqs)
+    warm = [pool.make(100_000, rng) for _ in range(max(args.warmup, 3))]
+    budget = cfg["budget"]
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(budget, free - (8 << 30)))
+
+    # warm-up + plain capacity, closed loop
+    _, mk, _, _ = run_trace(S, pool, warm, None, False, budget)
+    plain_cap = sum(r["cand"] for r in warm) / mk
+    run_trace(S, pool, warm, None, True, budget)
+
+    mean_cand = n_cand / nreq
+    lam = cfg["load"] * plain_cap / mean_cand  # requests per second
+    gaps = rng.exponential(1.0 / lam, nreq)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    launches0 = S.kernel_launches()
+    with ClockSampler(0) as clk:
+        lat_b, mk_b, groups_b, launches_b = run_trace(S, pool, reqs, arrivals, True, budget)
+    lat_p, mk_p, groups_p, launches_p = run_trace(S, pool, reqs, arrivals, False, budget)
+    sat_b = run_trace(S, pool, reqs, None, True, budget)
+    sat_p = run_trace(S, pool, reqs, None, False, budget)
+    launches = S.kernel_launches() - launches0
+
+    def pct(v, p):
+        return float(np.percentile(np.asarray(v), p))
+
+    h2d = sum(r["h2d"] for r in reqs)
+    d2h = sum(r["d2h"] for r in reqs)
+    line = {
+        "metric": "alignments/s", "value": n_cand / sat_b[1], "unit": "alignments/s",
+        "n_gpus": 1, "steps": 1, "warmup": len(warm), "ms_per_step": 1000 * sat_b[1],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "requests": nreq, "candidates": n_cand,
+                   "reads": int(sizes.sum()), "device_budget_bytes": budget,
+                   "offered_load": {"requests_per_s": lam,
+                                    "alignments_per_s": lam * mean_cand,
+                                    "fraction_of_plain_capacity": cfg["load"]},
+                   "step": "the whole trace, submitted at once (saturation)",
+                   "timing": "host steady clock, arrival (or submit) to results in pinned host "
+                             "memory", "l2": "inputs > L2"},
+        "e2e": {"value": n_cand / sat_b[1], "unit": "alignments/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "latency_ms": {"p50": pct(lat_b, 50), "p99": pct(lat_b, 99), "max": max(lat_b),
+                       "throughput": n_cand / mk_b, "groups": groups_b,
+                       "launches": launches_b},
+        "plain": {"value": n_cand / sat_p[1], "latency_ms": {
+            "p50": pct(lat_p, 50), "p99": pct(lat_p, 99), "max": max(lat_p),
+            "throughput": n_cand / mk_p, "launches": launches_p},
+            "what": "one request at a time, one launch per length bin, no copy/compute overlap"},
+        "batched_over_plain": sat_p[1] / sat_b[1],
+        "p99_plain_over_batched": pct(lat_p, 99) / pct(lat_b, 99),
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -341,6 +570,8 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--requests", type=int, default=None,
+                    help="requests in the serving trace (c5)")
     ap.add_argument("--reads", type=int, default=None,
                     help="override the reads per step (smaller cases for profiling)")
     args = ap.parse_args()
@@ -354,6 +585,11 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, cfg, rank)
+        return
+    if args.config == "c5":
+        if world > 1:
+            raise SystemExit("the serving workload runs on one GPU")
+        run_serving(args, cfg, rank)
         return
 
     import torch

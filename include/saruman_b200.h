@@ -111,6 +111,35 @@ typedef struct {
 #define SARU_S_IRREGULAR 1  /* a window is not m + so + eo long, or m <= 3k */
 #define SARU_S_ALPHABET 2   /* a read holds more than 4 distinct non-ACGT bytes */
 #define SARU_S_OVERFLOW 4   /* a traceback left its band */
+#define SARU_S_GATHER 16    /* saru_gather_device: a candidate outside the genome or read
+                               table, a bad flag, or a window length that does not match */
+
+/* One call given as the reference's filter output instead of its windows:
+ * per candidate the read's row in a read table, the window's start in the
+ * genome and the flag; the windows and reads of the call are then gathered
+ * on the device (saru_gather_device, or the request server's resident
+ * genome) exactly as src/hash.c:986-1059 builds them on the host.  No
+ * counterpart in the reference, whose calls always ship the windows. */
+typedef struct {
+  const char *read_table;       /* nreads rows of read_length bytes, as sequenced */
+  const int32_t *read_index;    /* n: row of each candidate's read */
+  const int32_t *positions;     /* n: window start in the genome */
+  const int8_t *dirs;           /* n: flags 0..7 (4..7: reverse-complemented read) */
+  const int32_t *genome_offsets;/* n: inclusive prefix sums of the window lengths
+                                   m + so + eo, as in saru_batch */
+  int32_t n, nreads, k, match, mismatch, first_of_call, read_length;
+  int64_t genome_bytes;         /* genome_offsets[n-1] */
+  int64_t total_slots;          /* genome_bytes + k * n */
+} saru_gather_call;
+
+/* Device arrays in, enqueued on `stream`: writes the call's windows
+ * (genome_bytes bytes), reads (n * read_length bytes) and read offsets (n)
+ * into the caller's device buffers and fills *batch with the saru_batch
+ * that views them (for saru_align_device).  Candidates it cannot gather
+ * set SARU_S_GATHER in *status (device) and leave their bytes unwritten. */
+int saru_gather_device(const saru_gather_call *call, const char *genome, int64_t genome_len,
+                       char *windows, char *reads, int32_t *read_offsets, int32_t *status,
+                       saru_batch *batch, void *stream);
 
 /* Host buffers in, host buffers out: copies the batch to the GPU, aligns it
  * and copies back the scores and both alignment-slot arrays exactly as the
@@ -194,9 +223,11 @@ typedef struct {
   int64_t device_budget_bytes;     /* arena for request inputs and outputs */
 } saru_server_config;
 typedef struct {
-  const saru_batch *calls; /* host pointers */
-  saru_result *results;    /* host outputs; status unused */
+  const saru_batch *calls;        /* host pointers */
+  saru_result *results;           /* host outputs; status unused */
   int32_t ncalls;
+  const saru_gather_call *gather; /* if not NULL: the ncalls calls are these (host arrays),
+                                     gathered from the resident genome; `calls` is unused */
 } saru_request;
 typedef struct {
   int64_t submit_us, admit_us, done_us; /* steady clock, microseconds */
@@ -206,6 +237,10 @@ typedef struct {
 
 /* NULL on failure (saru_last_error() says why). */
 saru_server *saru_server_create(const saru_server_config *cfg);
+/* Copies the genome that gather requests index to the server's GPU, where
+ * it stays (outside the device budget) until replaced or the server is
+ * destroyed.  Refused (SARU_E_INVALID) while requests are unfinished. */
+int saru_server_set_genome(saru_server *s, const char *genome, int64_t genome_len);
 /* Queues a request; *ticket identifies it.  SARU_E_INVALID for calls the
  * banded kernel cannot take at all (costs, k, read length), SARU_E_NOMEM if
  * it can never fit the arena. */

@@ -24,7 +24,7 @@ LIB_PATH = PKG / "libsaruman_b200.so"
 SARU_OK, SARU_E_INVALID, SARU_E_CUDA, SARU_E_NOMEM, SARU_E_OVERFLOW = 0, 1, 2, 3, 4
 SARU_E_TIMEOUT = 5
 SARU_MAX_CALLS = 192
-SARU_S_IRREGULAR, SARU_S_ALPHABET, SARU_S_OVERFLOW = 1, 2, 4
+SARU_S_IRREGULAR, SARU_S_ALPHABET, SARU_S_OVERFLOW, SARU_S_GATHER = 1, 2, 4, 16
 
 # symbols include/saruman_b200.h declares
 ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_memory",
@@ -33,7 +33,7 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_int32_issue_probe", "saru_align_device_static",
                  "saru_align_multi_device", "saru_multi_scratch_bytes", "saru_server_create",
                  "saru_server_submit", "saru_server_wait", "saru_server_counters",
-                 "saru_server_destroy")
+                 "saru_server_destroy", "saru_server_set_genome", "saru_gather_device")
 ABI_DATA = ("alignment_time",)
 
 
@@ -62,9 +62,18 @@ class ServerConfig(C.Structure):
                 ("device_budget_bytes", C.c_int64)]
 
 
+class SaruGatherCall(C.Structure):
+    _fields_ = [("read_table", C.c_void_p), ("read_index", C.c_void_p), ("positions", C.c_void_p),
+                ("dirs", C.c_void_p), ("genome_offsets", C.c_void_p), ("n", C.c_int32),
+                ("nreads", C.c_int32), ("k", C.c_int32), ("match", C.c_int32),
+                ("mismatch", C.c_int32), ("first_of_call", C.c_int32),
+                ("read_length", C.c_int32), ("genome_bytes", C.c_int64),
+                ("total_slots", C.c_int64)]
+
+
 class SaruRequest(C.Structure):
     _fields_ = [("calls", C.POINTER(SaruBatch)), ("results", C.POINTER(SaruResult)),
-                ("ncalls", C.c_int32)]
+                ("ncalls", C.c_int32), ("gather", C.POINTER(SaruGatherCall))]
 
 
 class RequestStats(C.Structure):
@@ -110,6 +119,12 @@ def load(path: str | Path | None = None):
     lib.saru_server_counters.restype = None
     lib.saru_server_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.saru_server_destroy.restype = None
+    lib.saru_server_set_genome.restype = C.c_int
+    lib.saru_server_set_genome.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    lib.saru_gather_device.restype = C.c_int
+    lib.saru_gather_device.argtypes = [C.POINTER(SaruGatherCall), C.c_void_p, C.c_int64,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(SaruBatch), C.c_void_p]
     lib.saru_server_destroy.argtypes = [C.c_void_p]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
@@ -280,6 +295,45 @@ class HostRequest:
                            o.genome_aln[:b.total_genome])
 
 
+class GatherRequest(HostRequest):
+    """A request of gather calls: per call the read table (reads as
+    sequenced, `table` rows of m bytes) and per candidate its read's row,
+    window start and flag; the server gathers windows and reads from its
+    resident genome.  `batches` give the call shapes and the expected
+    layout (their genome/reads arrays are not sent)."""
+
+    def __init__(self, batches: list[Batch], tables: list[np.ndarray],
+                 first_of_call: list[bool] | None = None):
+        super().__init__(batches, first_of_call)
+        first = first_of_call or [True] * len(batches)
+        gcs = []
+        for b, tab, f in zip(batches, tables, first):
+            arrs = [np.ascontiguousarray(tab, np.uint8).reshape(-1),
+                    np.ascontiguousarray(b.ids, np.int32), np.ascontiguousarray(b.pos, np.int32),
+                    np.ascontiguousarray(b.dirs, np.int8),
+                    np.ascontiguousarray(b.genome_offsets, np.int32)]
+            self.keep += arrs
+            gcs.append(SaruGatherCall(*[_p(a) if a.size else 0 for a in arrs], b.n,
+                                      int(arrs[0].size // max(b.m, 1)), b.k, b.match, b.mismatch,
+                                      1 if f else 0, b.m, len(b.genome), b.total_genome))
+        n = len(batches)
+        self.gcalls = (SaruGatherCall * n)(*gcs)
+        self.req.gather = C.cast(self.gcalls, C.POINTER(SaruGatherCall))
+
+
+def gather_device(call: SaruGatherCall, genome_ptr: int, genome_len: int, windows_ptr: int,
+                  reads_ptr: int, read_offsets_ptr: int, status_ptr: int,
+                  stream_ptr: int = 0) -> SaruBatch:
+    """Windows and reads of a gather call built on the device
+    (saru_gather_device); returns the saru_batch that views them."""
+    out = SaruBatch()
+    rc = load().saru_gather_device(C.byref(call), genome_ptr, genome_len, windows_ptr, reads_ptr,
+                                   read_offsets_ptr, status_ptr, C.byref(out), stream_ptr)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+    return out
+
+
 class Server:
     """Continuous-batching request server on one GPU (saru_server_*)."""
 
@@ -292,6 +346,12 @@ class Server:
         if not self._h:
             raise SaruError(SARU_E_CUDA, last_error())
         self._live: dict[int, HostRequest] = {}
+
+    def set_genome(self, genome: np.ndarray) -> None:
+        g = np.ascontiguousarray(genome, np.uint8)
+        rc = self._lib.saru_server_set_genome(self._h, _p(g), g.size)
+        if rc != SARU_OK:
+            raise SaruError(rc, last_error())
 
     def submit(self, req: HostRequest) -> int:
         t = C.c_int64()

@@ -605,6 +605,10 @@ struct NameIndex {
 // hooks for the request server (server.cpp)
 namespace saru {
 uint64_t thread_launches() { return g_thread_launches; }
+void count_launch() {
+  g_launches.fetch_add(1);
+  g_thread_launches += 1;
+}
 void set_last_error(const char *msg) { g_last_error = msg; }
 int redo_on_host_path(const saru_batch *b, saru_result *r) {
   Lane &L = g_lanes[2];

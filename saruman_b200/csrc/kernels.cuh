@@ -11,6 +11,7 @@ constexpr int kStatusIrregular = 1;  // window length != m + so + eo, or m <= 3k
 constexpr int kStatusAlphabet = 2;   // a read with more distinct non-ACGT bytes than supported
 constexpr int kStatusOverflow = 4;   // a traceback left its slot / band
 constexpr int kStatusUndefined = 8;  // the reference would read outside its arrays
+constexpr int kStatusGather = 16;    // a gathered candidate lies outside the genome or read table
 
 constexpr int kMaxBandM = 512;  // longest read of the banded kernel
 constexpr int kMaxOpWords = (kMaxBandM + 3 * 15 + 15) / 16 + 1;
@@ -67,6 +68,23 @@ struct FullArgs {
   uint8_t *genome_aln;
   int *status;
 };
+
+// Windows and reads of one call gathered from a resident genome (gather.cu).
+struct GatherArgs {
+  const uint8_t *genome;  // resident genome
+  long genome_len;
+  const uint8_t *table;  // read table: nreads rows of m bytes, as sequenced
+  long nreads;
+  const int32_t *read_index, *positions, *goff;
+  const int8_t *dirs;
+  long n, genome_bytes;
+  int m, k;
+  uint8_t *windows, *reads;  // outputs in the reference call layout
+  int32_t *read_offsets;
+  int *status;
+};
+
+cudaError_t launch_gather(const GatherArgs &a, int sms, cudaStream_t s);
 
 BandLayout band_layout(int max_m, int k);
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm);

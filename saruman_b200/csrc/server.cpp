@@ -97,7 +97,9 @@ class Arena {
 
 struct Request {
   int64_t ticket = 0;
-  std::vector<saru_batch> calls;     // host views (caller's arrays)
+  bool gather = false;                  // calls given as saru_gather_call (resident genome)
+  std::vector<saru_gather_call> gcalls; // host views (caller's arrays), when gather
+  std::vector<saru_batch> calls;     // host views (caller's arrays); shapes only when gather
   std::vector<saru_result> results;  // host outputs (caller's arrays)
   std::vector<saru_batch> dcalls;    // device views inside the arena
   std::vector<saru_result> dres;
@@ -111,18 +113,36 @@ struct Request {
   bool done = false;
 };
 
+// Read bytes of call i (the gathered reads of a gather call).
+size_t read_bytes(const Request &r, size_t i) {
+  const saru_batch &b = r.calls[i];
+  if (r.gather) return (size_t)b.n * (size_t)b.max_read_length;
+  return b.n ? (size_t)b.read_offsets[b.n - 1] : 0;
+}
+
 // Arena bytes one request takes: every device array up256-aligned.
 size_t request_bytes(const Request &r) {
   size_t t = up256(4 * r.calls.size());  // status words
-  for (const auto &b : r.calls) {
+  for (size_t i = 0; i < r.calls.size(); ++i) {
+    const saru_batch &b = r.calls[i];
     const size_t n = (size_t)b.n;
     t += up256((size_t)b.genome_bytes + 64);
-    t += up256((size_t)(n ? b.read_offsets[n - 1] : 0) + 64);
+    t += up256(read_bytes(r, i) + 64);
     t += 3 * up256(4 * n + 64);  // genome_offsets, read_offsets, scores
     t += up256(n + 64);          // dirs
     t += 2 * up256((size_t)b.total_slots + 64);
+    if (r.gather)  // read table, read_index, positions
+      t += up256((size_t)r.gcalls[i].nreads * (size_t)b.max_read_length + 64) +
+           2 * up256(4 * n + 64);
   }
   return t;
+}
+
+// The saru_batch shape of a gather call (pointers unset).
+saru_batch shape_of(const saru_gather_call &g) {
+  return saru_batch{nullptr, nullptr, g.genome_offsets, nullptr, g.dirs, g.n, g.k,
+                    g.match, g.mismatch, g.first_of_call, g.read_length, g.genome_bytes,
+                    g.total_slots};
 }
 
 }  // namespace
@@ -133,6 +153,8 @@ struct saru_server {
   cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
+  char *genome = nullptr;  // resident genome of gather requests
+  int64_t genome_len = 0;
 
   struct Group {
     std::vector<std::shared_ptr<Request>> reqs;
@@ -166,18 +188,11 @@ struct saru_server {
     for (size_t i = 0; i < nc; ++i) {
       const saru_batch &h = r.calls[i];
       const size_t n = (size_t)h.n;
-      const size_t rbytes = n ? (size_t)h.read_offsets[n - 1] : 0;
+      const size_t rbytes = read_bytes(r, i);
       uint8_t *g = take((size_t)h.genome_bytes + 64), *rd = take(rbytes + 64);
       uint8_t *go = take(4 * n + 64), *ro = take(4 * n + 64), *sc = take(4 * n + 64);
       uint8_t *dr = take(n + 64);
       uint8_t *ra = take((size_t)h.total_slots + 64), *ga = take((size_t)h.total_slots + 64);
-      if (n) {
-        cudaMemcpyAsync(g, h.genome, (size_t)h.genome_bytes, cudaMemcpyHostToDevice, s_in);
-        cudaMemcpyAsync(rd, h.reads, rbytes, cudaMemcpyHostToDevice, s_in);
-        cudaMemcpyAsync(go, h.genome_offsets, 4 * n, cudaMemcpyHostToDevice, s_in);
-        cudaMemcpyAsync(ro, h.read_offsets, 4 * n, cudaMemcpyHostToDevice, s_in);
-        cudaMemcpyAsync(dr, h.dirs, n, cudaMemcpyHostToDevice, s_in);
-      }
       saru_batch &d = r.dcalls[i];
       d = h;
       d.genome = reinterpret_cast<const char *>(g);
@@ -187,7 +202,54 @@ struct saru_server {
       d.dirs = reinterpret_cast<const int8_t *>(dr);
       r.dres[i] = saru_result{reinterpret_cast<int32_t *>(sc), reinterpret_cast<char *>(ra),
                               reinterpret_cast<char *>(ga), r.dstatus + i};
+      if (!n) continue;
+      cudaMemcpyAsync(go, h.genome_offsets, 4 * n, cudaMemcpyHostToDevice, s_in);
+      cudaMemcpyAsync(dr, h.dirs, n, cudaMemcpyHostToDevice, s_in);
+      if (!r.gather) {
+        cudaMemcpyAsync(g, h.genome, (size_t)h.genome_bytes, cudaMemcpyHostToDevice, s_in);
+        cudaMemcpyAsync(rd, h.reads, rbytes, cudaMemcpyHostToDevice, s_in);
+        cudaMemcpyAsync(ro, h.read_offsets, 4 * n, cudaMemcpyHostToDevice, s_in);
+        continue;
+      }
+      // filter output in, windows and reads gathered from the resident genome
+      const saru_gather_call &hg = r.gcalls[i];
+      const size_t tbytes = (size_t)hg.nreads * (size_t)hg.read_length;
+      uint8_t *tab = take(tbytes + 64), *ri = take(4 * n + 64), *ps = take(4 * n + 64);
+      cudaMemcpyAsync(tab, hg.read_table, tbytes, cudaMemcpyHostToDevice, s_in);
+      cudaMemcpyAsync(ri, hg.read_index, 4 * n, cudaMemcpyHostToDevice, s_in);
+      cudaMemcpyAsync(ps, hg.positions, 4 * n, cudaMemcpyHostToDevice, s_in);
+      saru_gather_call dg = hg;
+      dg.read_table = reinterpret_cast<const char *>(tab);
+      dg.read_index = reinterpret_cast<const int32_t *>(ri);
+      dg.positions = reinterpret_cast<const int32_t *>(ps);
+      dg.dirs = d.dirs;
+      dg.genome_offsets = d.genome_offsets;
+      saru_batch gathered;
+      if (saru_gather_device(&dg, genome, genome_len, reinterpret_cast<char *>(g),
+                             reinterpret_cast<char *>(rd), reinterpret_cast<int32_t *>(ro),
+                             r.dstatus + i, &gathered, s_in) != SARU_OK)
+        r.rc = SARU_E_CUDA;
     }
+  }
+
+  // A flagged gather call, redone on the exact path: its gathered windows
+  // and reads come back from the arena first.
+  int redo_gather(Request &r, size_t i) {
+    const saru_batch &d = r.dcalls[i];
+    const size_t n = (size_t)d.n;
+    std::vector<char> win((size_t)d.genome_bytes), rd(read_bytes(r, i));
+    std::vector<int32_t> ro(n);
+    if (cudaMemcpy(win.data(), d.genome, win.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(rd.data(), d.reads, rd.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
+      return SARU_E_CUDA;
+    }
+    for (size_t t = 0; t < n; ++t) ro[t] = (int32_t)((t + 1) * (size_t)d.max_read_length);
+    saru_batch h = r.calls[i];
+    h.genome = win.data();
+    h.reads = rd.data();
+    h.read_offsets = ro.data();
+    return saru::redo_on_host_path(&h, &r.results[i]);
   }
 
   int ensure_scratch(size_t bytes) {
@@ -326,12 +388,17 @@ struct saru_server {
       }
       cudaEventDestroy(g.done_ev);
       for (auto &r : g.reqs) {
-        r->rc = rc;
+        if (r->rc == SARU_OK) r->rc = rc;
         for (size_t i = 0; i < r->calls.size() && r->rc == SARU_OK; ++i) {
           const int st = r->call_status[i];
-          if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
+          if (st & saru::kStatusGather) {
+            saru::set_last_error("a gathered candidate lies outside the genome or read table, "
+                                 "or its window length does not match its flag");
+            r->rc = SARU_E_INVALID;
+          } else if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
             // as saru_align_host does: the whole call again on the exact path
-            r->rc = saru::redo_on_host_path(&r->calls[i], &r->results[i]);
+            r->rc = r->gather ? redo_gather(*r, i)
+                              : saru::redo_on_host_path(&r->calls[i], &r->results[i]);
             r->redone += 1;
           } else if (st & saru::kStatusOverflow) {
             saru::set_last_error("banded traceback left its band");
@@ -391,8 +458,25 @@ int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket)
     return SARU_E_INVALID;
   }
   auto r = std::make_shared<Request>();
-  r->calls.assign(req->calls, req->calls + req->ncalls);
   r->results.assign(req->results, req->results + req->ncalls);
+  if (req->gather) {
+    r->gather = true;
+    r->gcalls.assign(req->gather, req->gather + req->ncalls);
+    for (const auto &g : r->gcalls) r->calls.push_back(shape_of(g));
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->genome) {
+      saru::set_last_error("saru_server_submit: gather request before saru_server_set_genome");
+      return SARU_E_INVALID;
+    }
+    for (const auto &g : r->gcalls)
+      if (g.nreads < 0 || g.total_slots != g.genome_bytes + (int64_t)g.k * g.n) {
+        saru::set_last_error("saru_server_submit: gather call with nreads < 0 or total_slots "
+                             "!= genome_bytes + k * n");
+        return SARU_E_INVALID;
+      }
+  } else {
+    r->calls.assign(req->calls, req->calls + req->ncalls);
+  }
   for (const auto &b : r->calls) {
     if (b.n < 0 || b.k < 0 || b.k > 15 || b.match != 0 || b.mismatch != 1 ||
         b.max_read_length < 2 || b.max_read_length > saru::kMaxBandM) {
@@ -445,6 +529,34 @@ int saru_server_wait(saru_server *s, int64_t ticket, int32_t timeout_ms,
   return r->rc;
 }
 
+int saru_server_set_genome(saru_server *s, const char *genome, int64_t genome_len) {
+  if (!s || !genome || genome_len < 1) {
+    saru::set_last_error("saru_server_set_genome: a genome of at least one byte");
+    return SARU_E_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->tickets.empty()) {
+    saru::set_last_error("saru_server_set_genome: requests are unfinished");
+    return SARU_E_INVALID;
+  }
+  cudaSetDevice(s->cfg.device);
+  if (s->genome) cudaFree(s->genome);
+  s->genome = nullptr;
+  s->genome_len = 0;
+  if (cudaMalloc(&s->genome, (size_t)genome_len + 64) != cudaSuccess) {
+    cudaGetLastError();
+    s->genome = nullptr;
+    saru::set_last_error("saru_server_set_genome: device allocation failed");
+    return SARU_E_NOMEM;
+  }
+  if (cudaMemcpy(s->genome, genome, (size_t)genome_len, cudaMemcpyHostToDevice) != cudaSuccess) {
+    saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
+    return SARU_E_CUDA;
+  }
+  s->genome_len = genome_len;
+  return SARU_OK;
+}
+
 void saru_server_counters(saru_server *s, int64_t *groups, int64_t *launches) {
   std::lock_guard<std::mutex> lk(s->mu);
   if (groups) *groups = s->groups;
@@ -468,6 +580,7 @@ void saru_server_destroy(saru_server *s) {
   cudaSetDevice(s->cfg.device);
   cudaStreamSynchronize(s->s_comp);
   if (s->scratch) cudaFree(s->scratch);
+  if (s->genome) cudaFree(s->genome);
   s->arena.release();
   cudaStreamDestroy(s->s_in);
   cudaStreamDestroy(s->s_comp);
