@@ -63,13 +63,14 @@ CONFIGS = {
                "budget; continuous-batching server vs the plain per-request loop on one trace",
                genome=("repeat", 5_000_000, 301, "zipf"), reads=2_000_000,
                lengths=(36, 75, 100, 150), rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0,
-               max_hits=25, requests=96, min_reads=1_000, max_reads=500_000, budget=60 << 30,
+               max_hits=25, requests=400, min_reads=1_000, max_reads=500_000, budget=60 << 30,
                load=0.8),
 }
 
 
-def build_batches(cfg: dict, rank: int):
-    """One batch per read-length bin (one for single-length configs)."""
+def build_batches(cfg: dict, rank: int, tables: list | None = None):
+    """One batch per read-length bin (one for single-length configs); the
+    sequenced reads of each bin go to `tables` when given."""
     from saruman_b200 import workloads as W
     gs = cfg["genome"]
     if gs[0] == "uniform":
@@ -85,6 +86,10 @@ def build_batches(cfg: dict, rank: int):
                             unmapped=cfg["unmapped"])
         out.append(W.synthetic_candidates(g, rd, m, k, seed=2000 + 17 * rank + i, repeats=rmap,
                                           max_hits=cfg.get("max_hits", 1000)))
+        if tables is not None:
+            tables.append(rd.seqs)
+    if tables is not None:
+        tables.append(g)  # the genome last
     return out
 
 
@@ -340,22 +345,24 @@ def timed(stream, fn, steps, world, dist, dev):
 
 
 class RequestPool:
-    """Requests of the serving trace as C-ABI views into pinned host memory:
-    each request takes a contiguous range of reads from every length bin of
-    a pre-generated candidate pool (the host filter's output), one call per
-    bin, with its own re-based offsets; outputs come from a pinned ring that
-    requests release in completion order."""
+    """Requests of the serving trace as C-ABI views into pinned host memory.
+    Each request takes a contiguous range of reads from every length bin of
+    a pre-generated candidate pool (the host filter's output), one gather
+    call per bin: the request's read table (reads as sequenced), and per
+    candidate its read's row, window start, flag and window end offset; the
+    server gathers windows and reads from its resident genome.  Outputs come
+    from a pinned ring that requests release in completion order."""
 
-    def __init__(self, bs, S, ring_bytes: int):
+    def __init__(self, bs, tables, S, ring_bytes: int):
         import torch
         self.S = S
         self.bs = bs
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-        self.pg = [pin(b.genome) for b in bs]
-        self.pr = [pin(b.reads) for b in bs]
+        self.pt = [pin(t.reshape(-1)) for t in tables]
+        self.pp = [pin(b.pos) for b in bs]
         self.pd = [pin(b.dirs) for b in bs]
         self.gend = [np.concatenate([[0], b.genome_offsets.astype(np.int64)]) for b in bs]
-        self.per_bin = [int(b.ids.max()) + 1 for b in bs]
+        self.per_bin = [t.shape[0] for t in tables]
         self.ring = torch.empty(ring_bytes, dtype=torch.uint8).pin_memory()
         self.ring_ptr = self.ring.data_ptr()
         self.ring_bytes = ring_bytes
@@ -364,9 +371,8 @@ class RequestPool:
     def make(self, reads: int, rng) -> dict:
         import torch
         S = self.S
-        calls, offs, cand = [], [], 0
-        out_bytes = 0
-        spans = []
+        calls, gcalls, keep, cand, out_bytes, spans = [], [], [], 0, 0, []
+        h2d = d2h = 0
         for i, b in enumerate(self.bs):
             r = max(1, reads // len(self.bs))
             r0 = int(rng.integers(0, max(1, self.per_bin[i] - r)))
@@ -376,21 +382,24 @@ class RequestPool:
                 continue
             base = int(self.gend[i][c0])
             go = (self.gend[i][c0 + 1:c1 + 1] - base).astype(np.int32)
-            ro = ((np.arange(n, dtype=np.int64) + 1) * b.m).astype(np.int32)
-            t = torch.from_numpy(np.concatenate([go, ro])).pin_memory()
-            offs.append(t)
+            ri = (b.ids[c0:c1] - r0).astype(np.int32)
+            t = torch.from_numpy(np.concatenate([go, ri])).pin_memory()
+            keep.append(t)
             gbytes = int(go[-1])
             slots = gbytes + b.k * n
             spans.append((4 * n, slots + 64))
             out_bytes += (4 * n + 255) // 256 * 256 + 2 * ((slots + 64 + 255) // 256 * 256)
-            calls.append(S.SaruBatch(self.pg[i].data_ptr() + base, self.pr[i].data_ptr() + c0 * b.m,
-                                     t.data_ptr(), t.data_ptr() + 4 * n,
-                                     self.pd[i].data_ptr() + c0, n, b.k, 0, 1, 1, b.m, gbytes,
-                                     slots))
+            calls.append(S.SaruBatch(0, 0, t.data_ptr(), 0, self.pd[i].data_ptr() + c0, n, b.k,
+                                     0, 1, 1, b.m, gbytes, slots))
+            gcalls.append(S.SaruGatherCall(self.pt[i].data_ptr() + r0 * b.m, t.data_ptr() + 4 * n,
+                                           self.pp[i].data_ptr() + 4 * c0,
+                                           self.pd[i].data_ptr() + c0, t.data_ptr(), n, r, b.k,
+                                           0, 1, 1, b.m, gbytes, slots))
             cand += n
-        return dict(calls=calls, offs=offs, cand=cand, out_bytes=out_bytes, spans=spans,
-                    h2d=sum(int(c.genome_bytes) + c.n * (c.max_read_length + 9) for c in calls),
-                    d2h=sum(4 * c.n + 2 * int(c.total_slots) for c in calls))
+            h2d += r * b.m + 13 * n
+            d2h += 4 * n + 2 * slots
+        return dict(calls=calls, gcalls=gcalls, keep=keep, cand=cand, out_bytes=out_bytes,
+                    spans=spans, h2d=h2d, d2h=d2h)
 
     def alloc(self, nbytes: int) -> int | None:
         """Start offset in the ring, or None while the oldest requests hold it."""
@@ -419,9 +428,12 @@ class RequestPool:
             res.append(S.SaruResult(sc, ra, ga, None))
         self.live.append((start, start + req["out_bytes"]))
         n = len(req["calls"])
+        import ctypes as C
         req["arr_c"] = (S.SaruBatch * n)(*req["calls"])
         req["arr_r"] = (S.SaruResult * n)(*res)
-        req["creq"] = S.SaruRequest(req["arr_c"], req["arr_r"], n)
+        req["arr_g"] = (S.SaruGatherCall * n)(*req["gcalls"])
+        req["creq"] = S.SaruRequest(req["arr_c"], req["arr_r"], n,
+                                    C.cast(req["arr_g"], C.POINTER(S.SaruGatherCall)))
 
     def release_oldest(self):
         self.live.pop(0)
@@ -436,6 +448,7 @@ def run_trace(S, pool: RequestPool, reqs: list, arrivals_s, pipeline: bool, budg
     import threading
     srv = S.Server(pipeline=pipeline, max_requests_per_launch=max_per_launch, max_inflight=2,
                    budget_bytes=budget)
+    srv.set_genome(pool.genome)
     lib = S.load()
     tickets = [None] * len(reqs)
     done_us = [0] * len(reqs)
@@ -494,13 +507,16 @@ def run_serving(args, cfg, rank: int) -> None:
     import torch
     import saruman_b200 as S
     torch.cuda.set_device(0)
-    bs = build_batches(cfg, rank)
+    tables = []
+    bs = build_batches(cfg, rank, tables)
+    genome = tables.pop()
     S.load()
     rng = np.random.default_rng(4242)
     nreq = args.requests or cfg["requests"]
     sizes = np.exp(rng.uniform(np.log(cfg["min_reads"]), np.log(cfg["max_reads"]), nreq))
     sizes = sizes.astype(np.int64)
-    pool = RequestPool(bs, S, ring_bytes=6 << 30)  # largest request: ~0.7 GB of outputs
+    pool = RequestPool(bs, tables, S, ring_bytes=6 << 30)  # largest request: ~0.7 GB out
+    pool.genome = genome
     reqs = [pool.make(int(s), rng) for s in sizes]
     n_cand = sum(r["cand"] for r in reqs)
     warm = [pool.make(100_000, rng) for _ in range(max(args.warmup, 3))]
@@ -536,6 +552,8 @@ def run_serving(args, cfg, rank: int) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
         "data": "synthetic",
         "config": {"workload": cfg["workload"], "requests": nreq, "candidates": n_cand,
+                   "genome": "resident on the device (saru_server_set_genome); requests carry "
+                             "reads and candidate (read, position, flag, window end) arrays",
                    "reads": int(sizes.sum()), "device_budget_bytes": budget,
                    "offered_load": {"requests_per_s": lam,
                                     "alignments_per_s": lam * mean_cand,
@@ -643,15 +661,28 @@ def main() -> None:
     if int(status.item()) != 0:
         raise SystemExit(f"kernel status {int(status.item())}")
 
-    # ---- device-resident timing ------------------------------------------
+    # ---- device-resident timing: the step captured once in a CUDA graph --
+    graph = torch.cuda.CUDAGraph()
     launches0 = S.kernel_launches()
+    with torch.cuda.graph(graph, stream=stream):
+        step_batched()
+    per_step_launches = S.kernel_launches() - launches0
+
+    def step_graph():
+        with torch.cuda.stream(stream):
+            graph.replay()
+
+    step_graph()
+    stream.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        ms_step = timed(stream, step_batched, args.steps, world, dist, dev)
+        ms_step = timed(stream, step_graph, args.steps, world, dist, dev)
     torch.cuda.synchronize()
-    launches = S.kernel_launches() - launches0
+    if int(status.item()) != 0:
+        raise SystemExit(f"kernel status {int(status.item())}")
+    launches = per_step_launches * args.steps
     value = world * n_cand / (ms_step * 1e-3)
     plain = None
     if multi:
@@ -738,6 +769,8 @@ def main() -> None:
                    "l2": "inputs 4+ GB > L2, no flush"},
         "gcups_rect": world * sum(rect_cells(b) for b in bs) / (ms_step * 1e-3) / 1e9,
         "gpu_launches": int(launches),
+        "launch": "one CUDA graph replay per step "
+                  f"({per_step_launches} kernel launch(es) captured)",
         "e2e": {"value": e2e_value, "unit": "alignments/s",
                 "h2d_bytes_per_step": sum(d.bytes_in() for d in dbs),
                 "d2h_bytes_per_step": sum(d.bytes_out() for d in dbs), "steps": e2e_steps},

@@ -178,6 +178,23 @@ int saru_align_device(const saru_batch *batch, saru_result *result, void *scratc
 #define SARU_STATIC_SCRATCH_BYTES (32u << 20)
 int saru_align_device_static(const saru_batch *batch, saru_result *result, void *stream);
 
+/* Launch shape of the banded kernel for calls of one (read length, k):
+ * the autotuner (saruman_b200.autotune) times the shapes on a sample and
+ * installs the fastest here; every entry point that launches the banded
+ * kernel for that class (saru_scratch_bytes included) then uses it.  0 in
+ * a field keeps the default: as many warps per CTA (up to 4) and CTAs per
+ * SM as fit, 32-bit band words when k <= 7 and 64-bit ones above.  A
+ * multi-call launch looks up its class by (longest read, largest k).
+ * Results do not depend on the shape.  Not in the reference. */
+typedef struct {
+  int32_t warps_per_cta; /* 1..4: alignments per CTA = 32 x warps */
+  int32_t ctas_per_sm;   /* cap on resident CTAs per SM */
+  int32_t word_bits;     /* 64: 64-bit band words for k <= 7 too; 32 only for k <= 7 */
+} saru_tuning;
+int saru_tuning_set(int32_t read_length, int32_t k, const saru_tuning *t); /* NULL: remove */
+int saru_tuning_get(int32_t read_length, int32_t k, saru_tuning *t);       /* 1 if set */
+void saru_tuning_clear(void);
+
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 

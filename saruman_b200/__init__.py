@@ -33,7 +33,8 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_int32_issue_probe", "saru_align_device_static",
                  "saru_align_multi_device", "saru_multi_scratch_bytes", "saru_server_create",
                  "saru_server_submit", "saru_server_wait", "saru_server_counters",
-                 "saru_server_destroy", "saru_server_set_genome", "saru_gather_device")
+                 "saru_server_destroy", "saru_server_set_genome", "saru_gather_device",
+                 "saru_tuning_set", "saru_tuning_get", "saru_tuning_clear")
 ABI_DATA = ("alignment_time",)
 
 
@@ -54,6 +55,11 @@ class SaruBatch(C.Structure):
 class SaruResult(C.Structure):
     _fields_ = [("scores", C.c_void_p), ("read_aln", C.c_void_p), ("genome_aln", C.c_void_p),
                 ("status", C.c_void_p)]
+
+
+class SaruTuning(C.Structure):
+    _fields_ = [("warps_per_cta", C.c_int32), ("ctas_per_sm", C.c_int32),
+                ("word_bits", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -126,6 +132,11 @@ def load(path: str | Path | None = None):
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.POINTER(SaruBatch), C.c_void_p]
     lib.saru_server_destroy.argtypes = [C.c_void_p]
+    lib.saru_tuning_set.restype = C.c_int
+    lib.saru_tuning_set.argtypes = [C.c_int32, C.c_int32, C.POINTER(SaruTuning)]
+    lib.saru_tuning_get.restype = C.c_int
+    lib.saru_tuning_get.argtypes = [C.c_int32, C.c_int32, C.POINTER(SaruTuning)]
+    lib.saru_tuning_clear.restype = None
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -386,3 +397,25 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def set_tuning(m: int, k: int, warps: int = 0, ctas_per_sm: int = 0, word_bits: int = 0) -> None:
+    """Launch shape of the banded kernel for (read length, k) (saru_tuning_set)."""
+    t = SaruTuning(warps, ctas_per_sm, word_bits)
+    rc = load().saru_tuning_set(m, k, C.byref(t))
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+
+
+def clear_tuning(m: int | None = None, k: int | None = None) -> None:
+    if m is None:
+        load().saru_tuning_clear()
+    else:
+        load().saru_tuning_set(m, k, None)
+
+
+def get_tuning(m: int, k: int) -> tuple[int, int, int] | None:
+    t = SaruTuning()
+    if load().saru_tuning_get(m, k, C.byref(t)):
+        return (t.warps_per_cta, t.ctas_per_sm, t.word_bits)
+    return None

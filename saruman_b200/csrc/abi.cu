@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -234,12 +235,26 @@ int smem_per_sm(int dev) {
 }
 
 // persistent grid of the banded kernel: as many CTAs as fit on the GPU
+// Launch shapes chosen per (read length, k) by the autotuner (saru_tuning_set);
+// classes without an entry keep the default shape.
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, saru::Tuning> g_tune;
+
+saru::Tuning tuning_for(int max_m, int k) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find({max_m, k});
+  return it == g_tune.end() ? saru::Tuning{} : it->second;
+}
+
 long band_grid(int dev, long n, int max_m, int k) {
-  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k), smem_per_sm(dev));
+  const saru::Tuning tn = tuning_for(max_m, k);
+  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k, tn.warps),
+                         smem_per_sm(dev), tn.ctas_per_sm);
 }
 
 size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
-  return saru::band_scratch_bytes(grid, max_m, k, wide);
+  const saru::Tuning tn = tuning_for(max_m, k);
+  return saru::band_scratch_bytes(grid, max_m, k, wide || tn.word_bits == 64, tn.warps);
 }
 
 // Enqueues the banded kernel on device buffers: calls[0..ncalls) as the
@@ -265,6 +280,11 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   long tiles = 0, total_n = 0;
   int max_m = 0, max_k = 0, wide_any = 0;
   for (int q = 0; q < ncalls; ++q) {
+    max_m = std::max(max_m, calls[q].max_read_length);
+    max_k = std::max(max_k, calls[q].k);
+  }
+  const saru::Tuning tn = tuning_for(max_m, max_k);
+  for (int q = 0; q < ncalls; ++q) {
     const saru_batch *b = &calls[order[(size_t)q]];
     const saru_result *r = &res[order[(size_t)q]];
     saru::Segment &g = a.segs[a.nseg++];
@@ -282,11 +302,9 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
     g.k = b->k;
     g.max_m = b->max_read_length;
     g.first_of_call = b->first_of_call;
-    g.wide = b->k > 7 && (ncalls > 1 || pl.wide);
+    g.wide = (b->k > 7 && (ncalls > 1 || pl.wide)) || tn.word_bits == 64;
     tiles += (b->n + 31) / 32;
     total_n += b->n;
-    if (g.max_m > max_m) max_m = g.max_m;
-    if (g.k > max_k) max_k = g.k;
     wide_any |= g.wide;
   }
   if (tiles == 0) return SARU_OK;
@@ -294,10 +312,11 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   a.max_m = max_m;
   a.max_k = max_k;
   a.wide_any = wide_any;
-  a.grid = saru::band_grid(sm_count(dev), total_n, saru::band_layout(max_m, max_k),
-                           smem_per_sm(dev));
+  a.warps_req = tn.warps;
+  a.grid = saru::band_grid(sm_count(dev), total_n, saru::band_layout(max_m, max_k, tn.warps),
+                           smem_per_sm(dev), tn.ctas_per_sm);
   if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
-  const size_t need = saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0);
+  const size_t need = saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0, tn.warps);
   if (need > scratch_bytes) {
     set_error("scratch too small: %zu < %zu", scratch_bytes, need);
     return SARU_E_INVALID;
@@ -626,6 +645,44 @@ extern "C" {
 const char *saru_last_error(void) { return g_last_error.c_str(); }
 
 uint64_t saru_kernel_launches(void) { return g_launches.load(); }
+
+int saru_tuning_set(int32_t read_length, int32_t k, const saru_tuning *t) {
+  g_last_error.clear();
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (!t) {
+    g_tune.erase({read_length, k});
+    return SARU_OK;
+  }
+  if (t->warps_per_cta < 0 || t->warps_per_cta > 4 || t->ctas_per_sm < 0 ||
+      t->ctas_per_sm > 16 || (t->word_bits != 0 && t->word_bits != 32 && t->word_bits != 64) ||
+      (t->word_bits == 32 && k > 7)) {
+    set_error("saru_tuning_set: warps_per_cta 0..4, ctas_per_sm 0..16, word_bits 0/32/64 "
+              "(32 only for k <= 7)");
+    return SARU_E_INVALID;
+  }
+  saru::Tuning tn;
+  tn.warps = t->warps_per_cta;
+  tn.ctas_per_sm = t->ctas_per_sm;
+  tn.word_bits = t->word_bits;
+  g_tune[{read_length, k}] = tn;
+  return SARU_OK;
+}
+
+int saru_tuning_get(int32_t read_length, int32_t k, saru_tuning *t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find({read_length, k});
+  if (it == g_tune.end()) {
+    if (t) *t = saru_tuning{0, 0, 0};
+    return 0;
+  }
+  if (t) *t = saru_tuning{it->second.warps, it->second.ctas_per_sm, it->second.word_bits};
+  return 1;
+}
+
+void saru_tuning_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
+}
 
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide) {
   int dev = current_device();

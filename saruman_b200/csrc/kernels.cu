@@ -230,7 +230,7 @@ __global__ void saru_full_trace_kernel(FullArgs a) {
 
 constexpr long kMaxCtaSmem = 227 * 1024;  // opt-in shared memory per block on sm_100
 
-BandLayout band_layout(int max_m, int k) {
+BandLayout band_layout(int max_m, int k, int warps_req) {
   const SliceLayout S = slice_layout(max_m, k);
   BandLayout L;
   L.rs_bytes = S.rs_bytes;
@@ -239,12 +239,13 @@ BandLayout band_layout(int max_m, int k) {
   L.warp_smem = S.warp_smem;
   long w = kMaxCtaSmem / S.warp_smem;
   L.warps = (int)(w >= 4 ? 4 : (w >= 2 ? 2 : (w >= 1 ? 1 : 0)));
+  if (warps_req >= 1 && warps_req < L.warps) L.warps = warps_req;
   L.cta_smem = S.warp_smem * L.warps;
   return L;
 }
 
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
-  const BandLayout L = band_layout(a.max_m, a.max_k);
+  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req);
   if (L.warps < 1 || a.nseg < 1 || a.nseg > kMaxSegs) return cudaErrorInvalidValue;
   // allow the largest slice once; each launch asks for its own size (a
   // per-launch attribute would race between concurrent callers)
@@ -260,18 +261,19 @@ cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm) {
+long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_cap) {
   const long per_cta = 32L * (L.warps > 0 ? L.warps : 1);
   const long tiles = (n + per_cta - 1) / per_cta;
   long per_sm = smem_per_sm / (L.cta_smem + 1024);
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 16) per_sm = 16;
+  if (ctas_cap >= 1 && per_sm > ctas_cap) per_sm = ctas_cap;
   const long g = (long)sms * per_sm;
   return tiles < g ? (tiles > 0 ? tiles : 1) : g;
 }
 
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
-  const BandLayout L = band_layout(max_m, k);
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req) {
+  const BandLayout L = band_layout(max_m, k, warps_req);
   return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 *
                              (size_t)(max_m + 1) * (wide ? 8 : 4);
 }

@@ -44,7 +44,17 @@ struct KernelArgs {
   void *planes;  // decision planes: (max_m + 1) * lanes pairs of the widest band word
   long grid;
   int max_m, max_k, wide_any;
+  int warps_req;                       // requested warps per CTA (0: as many as fit)
   long rs_bytes, ws_bytes, warp_smem;  // shared-memory slice layout (set by the launcher)
+};
+
+// Launch shape of the banded kernel for one (read length, k) class; 0 keeps
+// the default (as many warps per CTA and CTAs per SM as fit; 32-bit band
+// words when k <= 7).
+struct Tuning {
+  int warps = 0;        // warps per CTA, 1..4
+  int ctas_per_sm = 0;  // cap on resident CTAs per SM
+  int word_bits = 0;    // 64: 64-bit band words even when k <= 7
 };
 
 struct BandLayout {
@@ -86,9 +96,10 @@ struct GatherArgs {
 
 cudaError_t launch_gather(const GatherArgs &a, int sms, cudaStream_t s);
 
-BandLayout band_layout(int max_m, int k);
-long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm);
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide);  // counter + planes
+BandLayout band_layout(int max_m, int k, int warps_req = 0);
+long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_cap = 0);
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide,
+                          int warps_req = 0);  // counter + planes
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s);
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
 

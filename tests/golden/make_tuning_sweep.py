@@ -1,0 +1,50 @@
+"""Measures the banded kernel's time for every launch shape of the
+autotuner's search space over a grid of (read length, k, candidates) bins
+on the current GPU, and writes the table the cost-model tests train and
+evaluate on (tuning_sweep_b200.json).  Run on a B200:
+
+    python tests/golden/make_tuning_sweep.py OUT.json
+"""
+from __future__ import annotations
+
+import json
+import math
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import saruman_b200 as S  # noqa: E402
+from saruman_b200 import autotune as A  # noqa: E402
+
+LENGTHS = (36, 50, 75, 100, 125, 150, 200, 250)
+RATES = (0.03, 0.06, 0.10)
+SIZES = (16_000, 128_000, 1_000_000)
+
+
+def main(out: str) -> None:
+    S.load()
+    S.clear_tuning()
+    rows = []
+    t0 = time.time()
+    for m in LENGTHS:
+        ks = sorted({min(15, max(1, math.ceil(r * m))) for r in RATES})
+        for k in ks:
+            if m <= 3 * k:
+                continue
+            full = A.Sample.build(m, k, max(SIZES) // 4 + 1000, seed=1000 + m * 16 + k)
+            for n in SIZES:
+                smp = full.prefix(n)
+                for shape in A.search_space(k):
+                    ms = A.time_shape(smp, shape, reps=5)
+                    rows.append({"m": m, "k": k, "n": smp.batch.n,
+                                 "so_frac": smp.start_gap_fraction(), "shape": list(shape),
+                                 "ms": ms})
+            print(f"m={m} k={k} done, {len(rows)} rows, {time.time() - t0:.0f} s", flush=True)
+    Path(out).write_text(json.dumps({"gpu": A.gpu_name(), "rows": rows}) + "\n")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

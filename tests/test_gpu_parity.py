@@ -222,10 +222,9 @@ def test_full_size_batch_sampled_against_oracle(saru_lib, shape):
         assert reads[i].tobytes().endswith(letters)
 
 
-def test_multi_call_launch_matches_each_call(saru_lib):
-    """Calls of different read lengths, k and band widths (and a call that
-    continues an earlier one) aligned in one launch give each call's own
-    reference bytes."""
+def _multi_call_setup():
+    """Device buffers and expected bytes of seven calls of different read
+    lengths, k and band widths, one of them continuing an earlier call."""
     import torch
     dev = torch.device("cuda:0")
     specs = [(36, 3, 3000, True), (75, 5, 2000, True), (100, 6, 2500, True), (150, 9, 1200, True),
@@ -259,15 +258,59 @@ def test_multi_call_launch_matches_each_call(saru_lib):
                                1 if first else 0, m, len(b.genome), b.total_genome))
         srs.append(S.SaruResult(bufs["s"].data_ptr(), bufs["ra"].data_ptr(), bufs["ga"].data_ptr(),
                                 None))
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
-    nscr = S.multi_scratch_bytes(sbs)
-    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
-    S.align_multi_device(sbs, srs, status.data_ptr(), scratch.data_ptr(), nscr,
-                         torch.cuda.current_stream().cuda_stream)
-    torch.cuda.synchronize()
-    assert int(status.item()) == 0
+    return sbs, srs, keep, want
+
+
+def _check_multi(keep, want):
     for (b, s1, ra1, ga1, _), bufs in zip(want, keep):
         tot = b.total_genome
         r = S.AlignResult(bufs["s"].cpu().numpy(), bufs["ra"][:tot].cpu().numpy(),
                           bufs["ga"][:tot].cpu().numpy())
         check_equal(b, s1, ra1, ga1, r)
+
+
+def test_multi_call_launch_matches_each_call(saru_lib):
+    """Calls of different read lengths, k and band widths (and a call that
+    continues an earlier one) aligned in one launch give each call's own
+    reference bytes."""
+    import torch
+    sbs, srs, keep, want = _multi_call_setup()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+    nscr = S.multi_scratch_bytes(sbs)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device="cuda:0")
+    S.align_multi_device(sbs, srs, status.data_ptr(), scratch.data_ptr(), nscr,
+                         torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    _check_multi(keep, want)
+
+
+def test_multi_call_request_replays_from_a_cuda_graph(saru_lib):
+    """saru_align_multi_device captured once in a CUDA graph (its class
+    launches forked onto side streams and joined back inside the capture)
+    and replayed: every replay rewrites each call's reference bytes."""
+    import torch
+    sbs, srs, keep, want = _multi_call_setup()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+    nscr = S.multi_scratch_bytes(sbs)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device="cuda:0")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):  # first call outside capture: one-time setup
+        S.align_multi_device(sbs, srs, status.data_ptr(), scratch.data_ptr(), nscr,
+                             side.cuda_stream)
+    side.synchronize()
+    g = torch.cuda.CUDAGraph()
+    n0 = S.kernel_launches()
+    with torch.cuda.graph(g):
+        S.align_multi_device(sbs, srs, status.data_ptr(), scratch.data_ptr(), nscr,
+                             torch.cuda.current_stream().cuda_stream)
+    assert S.kernel_launches() - n0 >= 1
+    for _ in range(2):
+        for bufs in keep:
+            for key in ("s", "ra", "ga"):
+                bufs[key].zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        assert int(status.item()) == 0
+        _check_multi(keep, want)
+    del g

@@ -107,3 +107,120 @@ def test_submit_rejects_bad_requests(saru_lib):
         t = srv.submit(S.HostRequest([b]))
         rc, _ = srv.wait(t)
         assert rc == S.SARU_OK
+
+
+def gather_case(m: int, k: int, nreads: int, seed: int, n_alpha: bool = False):
+    """A genome, its sequenced reads and the candidate batch the filter's
+    host loop would build from them (windows + reverse-complemented reads)."""
+    g = W.uniform_genome(300_000, seed=seed)
+    if n_alpha:  # a few N runs in the genome
+        g = g.copy()
+        g[1000:1010] = ord("N")
+        g[50_000:50_003] = ord("N")
+    rd = W.sample_reads(g, nreads, m, 0.03, seed=seed + 1, unmapped=0.05)
+    b = W.synthetic_candidates(g, rd, m, k, seed=seed + 2, extra_hits=1.5)
+    return g, rd.seqs, b
+
+
+def test_gather_device_builds_the_reference_layout(saru_lib):
+    """saru_gather_device writes exactly the windows, reads and read offsets
+    of the host-built call, and aligning them gives saru_align_host's bytes."""
+    import torch
+    dev = torch.device("cuda:0")
+    g, table, b = gather_case(100, 5, 3000, seed=21, n_alpha=True)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    dg, dt, di, dp, dd, dgo = (T(g), T(table.reshape(-1)), T(b.ids), T(b.pos), T(b.dirs),
+                               T(b.genome_offsets))
+    win = torch.zeros(len(b.genome) + 64, dtype=torch.uint8, device=dev)
+    rds = torch.zeros(b.n * b.m + 64, dtype=torch.uint8, device=dev)
+    ro = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    call = S.SaruGatherCall(dt.data_ptr(), di.data_ptr(), dp.data_ptr(), dd.data_ptr(),
+                            dgo.data_ptr(), b.n, table.shape[0], b.k, 0, 1, 1, b.m,
+                            len(b.genome), b.total_genome)
+    sb = S.gather_device(call, dg.data_ptr(), len(g), win.data_ptr(), rds.data_ptr(),
+                         ro.data_ptr(), st.data_ptr())
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    np.testing.assert_array_equal(win[:len(b.genome)].cpu().numpy(), b.genome)
+    np.testing.assert_array_equal(rds[:b.n * b.m].cpu().numpy(), b.reads)
+    np.testing.assert_array_equal(ro.cpu().numpy(), b.read_offsets)
+    sc = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    res = S.SaruResult(sc.data_ptr(), ra.data_ptr(), ga.data_ptr(), st.data_ptr())
+    nscr = S.scratch_bytes(b.n, b.m, b.k)
+    scr = torch.empty(nscr, dtype=torch.uint8, device=dev)
+    S.align_device(sb, res, scr.data_ptr(), nscr)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    want = S.align_host(b)
+    assert_same(S.AlignResult(sc.cpu().numpy(), ra[:b.total_genome].cpu().numpy(),
+                              ga[:b.total_genome].cpu().numpy()), want)
+
+
+def test_gather_flags_candidates_outside_the_genome(saru_lib):
+    import torch
+    dev = torch.device("cuda:0")
+    g, table, b = gather_case(36, 2, 200, seed=3)
+    pos = b.pos.copy()
+    pos[7] = len(g) - 10  # window runs past the genome end
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    dg, dt, di, dp, dd, dgo = (T(g), T(table.reshape(-1)), T(b.ids), T(pos), T(b.dirs),
+                               T(b.genome_offsets))
+    win = torch.zeros(len(b.genome) + 64, dtype=torch.uint8, device=dev)
+    rds = torch.zeros(b.n * b.m + 64, dtype=torch.uint8, device=dev)
+    ro = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    call = S.SaruGatherCall(dt.data_ptr(), di.data_ptr(), dp.data_ptr(), dd.data_ptr(),
+                            dgo.data_ptr(), b.n, table.shape[0], b.k, 0, 1, 1, b.m,
+                            len(b.genome), b.total_genome)
+    S.gather_device(call, dg.data_ptr(), len(g), win.data_ptr(), rds.data_ptr(), ro.data_ptr(),
+                    st.data_ptr())
+    torch.cuda.synchronize()
+    assert int(st.item()) & S.SARU_S_GATHER
+
+
+def gather_case_on(g, m: int, k: int, nreads: int, seed: int):
+    rd = W.sample_reads(g, nreads, m, 0.03, seed=seed + 1, unmapped=0.05)
+    b = W.synthetic_candidates(g, rd, m, k, seed=seed + 2, extra_hits=1.5)
+    return rd.seqs, b
+
+
+def test_server_resident_genome_requests(saru_lib):
+    """Gather requests against the resident genome give saru_align_host's
+    bytes for the host-built calls, mixed with window requests; a call with
+    m <= 3k is redone on the exact path from its gathered windows."""
+    g = W.uniform_genome(300_000, seed=40)
+    shapes = [(36, 3, 2000), (75, 5, 1500), (100, 6, 1200), (150, 9, 800), (12, 5, 300)]
+    cases = [gather_case_on(g, m, k, n, seed=40 + 7 * i) for i, (m, k, n) in enumerate(shapes)]
+    with S.Server(pipeline=True, max_requests_per_launch=8, budget_bytes=1 << 30) as srv:
+        srv.set_genome(g)
+        reqs = []
+        for table, b in cases:
+            reqs.append(S.GatherRequest([b], [table]))
+            reqs.append(S.HostRequest([b]))
+        reqs.append(S.GatherRequest([b for _, b in cases], [t for t, _ in cases]))
+        tickets = [srv.submit(r) for r in reqs]
+        with pytest.raises(S.SaruError):  # requests are unfinished until waited for
+            srv.set_genome(g)
+        redone = 0
+        for t in tickets:
+            rc, st = srv.wait(t)
+            assert rc == S.SARU_OK, S.last_error()
+            redone += st.redone_calls
+        assert redone >= 3  # the m <= 3k call, alone twice and inside the last request
+        srv.set_genome(g)
+    for i, (table, b) in enumerate(cases):
+        want = S.align_host(b)
+        assert_same(reqs[2 * i].result(0), want)
+        assert_same(reqs[2 * i + 1].result(0), want)
+        assert_same(reqs[-1].result(i), want)
+
+
+def test_gather_request_needs_a_genome(saru_lib):
+    g, table, b = gather_case(36, 2, 100, seed=5)
+    with S.Server(budget_bytes=1 << 24) as srv:
+        with pytest.raises(S.SaruError) as e:
+            srv.submit(S.GatherRequest([b], [table]))
+        assert e.value.code == S.SARU_E_INVALID
