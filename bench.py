@@ -344,6 +344,28 @@ def timed(stream, fn, steps, world, dist, dev):
     return ms / steps
 
 
+def tune_bins(bs, dbs, status, sample: int = 1_000_000) -> dict:
+    """Autotunes the launch shape of every (read length, k) bin on the
+    first `sample` candidates of the bin itself: the cost model (trained on
+    the GPU from the committed B200 sweep) ranks the shapes, the tuner
+    times its top 3 and the default, and installs the fastest."""
+    from saruman_b200 import autotune as A
+    from saruman_b200 import costmodel as CM
+    t0 = time.perf_counter()
+    model = CM.trained_on_sweep()
+    t_train = time.perf_counter() - t0
+    out = {}
+    for b, d in zip(bs, dbs):
+        smp = A.Sample.wrap(b, d.sb, d.sr, status).prefix(min(b.n, sample))
+        r = A.tune_bin(smp, model=model, top=3)
+        out[f"{b.m},{b.k}"] = {"shape": list(r["best"]), "trials": len(r["ms"]),
+                               "ms_sample": r["ms"][r["best"]],
+                               "default_ms_sample": r["default_ms"]}
+    out["cost_model_train_s"] = t_train
+    out["tune_s"] = time.perf_counter() - t0
+    return out
+
+
 class RequestPool:
     """Requests of the serving trace as C-ABI views into pinned host memory.
     Each request takes a contiguous range of reads from every length bin of
@@ -520,6 +542,15 @@ def run_serving(args, cfg, rank: int) -> None:
     reqs = [pool.make(int(s), rng) for s in sizes]
     n_cand = sum(r["cand"] for r in reqs)
     warm = [pool.make(100_000, rng) for _ in range(max(args.warmup, 3))]
+    status = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+    tuning = {}
+    if not args.no_tune:
+        dbs = [DeviceBatch(b, torch.device("cuda:0"), S) for b in bs]
+        for d in dbs:
+            d.sr.status = status.data_ptr()
+        tuning = tune_bins(bs, dbs, status)
+        del dbs
+        torch.cuda.empty_cache()
     budget = cfg["budget"]
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(budget, free - (8 << 30)))
@@ -559,6 +590,7 @@ def run_serving(args, cfg, rank: int) -> None:
                                     "alignments_per_s": lam * mean_cand,
                                     "fraction_of_plain_capacity": cfg["load"]},
                    "step": "the whole trace, submitted at once (saturation)",
+                   "tuning": tuning or "default shapes",
                    "timing": "host steady clock, arrival (or submit) to results in pinned host "
                              "memory", "l2": "inputs > L2"},
         "e2e": {"value": n_cand / sat_b[1], "unit": "alignments/s", "h2d_bytes_per_step": h2d,
@@ -588,6 +620,8 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--requests", type=int, default=None,
                     help="requests in the serving trace (c5)")
     ap.add_argument("--reads", type=int, default=None,
@@ -631,13 +665,15 @@ def main() -> None:
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     multi = len(dbs) > 1
+    int_peak = S.int32_issue_peak() if rank == 0 else None
+    # launch shapes first: the scratch sizes depend on them
+    tuning = tune_bins(bs, dbs, status) if not args.no_tune else {}
+    status.zero_()
     if multi:
         nscr = S.multi_scratch_bytes([d.sb for d in dbs])
     else:
         nscr = S.scratch_bytes(bs[0].n, bs[0].m, bs[0].k)
     scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
-
-    int_peak = S.int32_issue_peak() if rank == 0 else None
 
     def step_batched():
         if multi:
@@ -766,7 +802,8 @@ def main() -> None:
         "config": {"workload": cfg["workload"], "candidates_per_step": n_cand,
                    "reads_per_step": cfg["reads"], "read_lengths": [b.m for b in bs],
                    "k": [b.k for b in bs], "parallelism": f"replicas x{world}",
-                   "l2": "inputs 4+ GB > L2, no flush"},
+                   "l2": "inputs 4+ GB > L2, no flush",
+                   "tuning": tuning or "default shapes"},
         "gcups_rect": world * sum(rect_cells(b) for b in bs) / (ms_step * 1e-3) / 1e9,
         "gpu_launches": int(launches),
         "launch": "one CUDA graph replay per step "

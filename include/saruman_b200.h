@@ -195,6 +195,26 @@ int saru_tuning_set(int32_t read_length, int32_t k, const saru_tuning *t); /* NU
 int saru_tuning_get(int32_t read_length, int32_t k, saru_tuning *t);       /* 1 if set */
 void saru_tuning_clear(void);
 
+/* ---- cost model of the autotuner (costmodel.cu) -----------------------------
+ * A fully connected network, dims[0] inputs -> ... -> dims[nlayers] = 1
+ * output, tanh hidden layers, fp32, that predicts the banded kernel's log
+ * time per candidate from a bin's features and a launch shape; the
+ * autotuner times only the shapes it ranks best.  Parameters: per layer
+ * W (fan_out x fan_in, row-major) then the bias.  x: n rows of dims[0]
+ * features.  All arrays are device arrays; `work` holds
+ * saru_mlp_work_floats(dims, nlayers, n) floats.  Gradients are exact
+ * (fixed-order sums) for the mean squared error over the n rows.  Not in the
+ * reference. */
+int64_t saru_mlp_param_count(const int32_t *dims, int32_t nlayers);
+int64_t saru_mlp_work_floats(const int32_t *dims, int32_t nlayers, int32_t n);
+int saru_mlp_forward(const int32_t *dims, int32_t nlayers, const float *params, const float *x,
+                     int32_t n, float *y, float *work, void *stream);
+int saru_mlp_loss_grad(const int32_t *dims, int32_t nlayers, const float *params, const float *x,
+                       const float *y, int32_t n, float *loss, float *grad, float *work,
+                       void *stream);
+int saru_mlp_adam_step(float *params, const float *grad, float *m, float *v, int64_t count,
+                       float lr, float beta1, float beta2, float eps, int32_t step, void *stream);
+
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 

@@ -34,7 +34,9 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_align_multi_device", "saru_multi_scratch_bytes", "saru_server_create",
                  "saru_server_submit", "saru_server_wait", "saru_server_counters",
                  "saru_server_destroy", "saru_server_set_genome", "saru_gather_device",
-                 "saru_tuning_set", "saru_tuning_get", "saru_tuning_clear")
+                 "saru_tuning_set", "saru_tuning_get", "saru_tuning_clear",
+                 "saru_mlp_param_count", "saru_mlp_work_floats", "saru_mlp_forward",
+                 "saru_mlp_loss_grad", "saru_mlp_adam_step")
 ABI_DATA = ("alignment_time",)
 
 
@@ -137,6 +139,21 @@ def load(path: str | Path | None = None):
     lib.saru_tuning_get.restype = C.c_int
     lib.saru_tuning_get.argtypes = [C.c_int32, C.c_int32, C.POINTER(SaruTuning)]
     lib.saru_tuning_clear.restype = None
+    I32P = C.POINTER(C.c_int32)
+    lib.saru_mlp_param_count.restype = C.c_int64
+    lib.saru_mlp_param_count.argtypes = [I32P, C.c_int32]
+    lib.saru_mlp_work_floats.restype = C.c_int64
+    lib.saru_mlp_work_floats.argtypes = [I32P, C.c_int32, C.c_int32]
+    lib.saru_mlp_forward.restype = C.c_int
+    lib.saru_mlp_forward.argtypes = [I32P, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.saru_mlp_loss_grad.restype = C.c_int
+    lib.saru_mlp_loss_grad.argtypes = [I32P, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.saru_mlp_adam_step.restype = C.c_int
+    lib.saru_mlp_adam_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                       C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32,
+                                       C.c_void_p]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:

@@ -58,6 +58,14 @@ class Sample:
         s.sr = S.SaruResult(*[x.data_ptr() for x in bufs[5:9]])
         return s
 
+    @staticmethod
+    def wrap(batch: W.Batch, sb, sr, status) -> "Sample":
+        """A sample over buffers the caller already holds on the device
+        (`status`: a device int32 tensor the launches OR their status into)."""
+        s = Sample(batch, [None] * 8 + [status])
+        s.sb, s.sr = sb, sr
+        return s
+
     def prefix(self, n: int) -> "Sample":
         """The first n candidates (a valid call of their own), same buffers."""
         import saruman_b200 as S
@@ -108,17 +116,20 @@ def time_shape(sample: Sample, shape: tuple[int, int, int], reps: int = 5,
 
 
 def tune_bin(sample: Sample, shapes: list[tuple[int, int, int]] | None = None,
-             reps: int = 5) -> dict:
-    """Times `shapes` (the whole search space by default) and installs the
-    fastest.  Returns {"best": shape, "ms": {shape: ms}, "default_ms": ms}."""
+             reps: int = 5, model=None, top: int = 3) -> dict:
+    """Times `shapes` (the whole search space by default; with a trained
+    cost model, only its `top` best-ranked shapes) and installs the fastest.
+    Returns {"best": shape, "ms": {shape: ms}, "default_ms": ms}."""
     import saruman_b200 as S
     b = sample.batch
     space = shapes or search_space(b.k)
+    if model is not None:
+        space = model.rank(b.m, b.k, sample.start_gap_fraction(), b.n, space)[:top]
     ms = {sh: time_shape(sample, sh, reps) for sh in space}
     dflt = default_shape(b.k)
     if dflt not in ms:
         ms[dflt] = time_shape(sample, dflt, reps)
-    best = min(space, key=lambda sh: ms[sh])
+    best = min(ms, key=lambda sh: ms[sh])  # the default shape competes too
     S.set_tuning(b.m, b.k, *best)
     return {"m": b.m, "k": b.k, "n": b.n, "best": best, "ms": ms, "default_ms": ms[dflt]}
 

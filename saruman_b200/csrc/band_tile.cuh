@@ -208,9 +208,13 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
   int n = 0;                                 // bytes written, from the slot end down
   int row = c.L, col = c.m, b = c.L - c.m + c.k;
   bool bad = false, stop = false;
+  // planes of the current column and the next three to the left in
+  // registers, so a load is issued three column moves before its use
   PlanePair<T> cur = ld(col);
-  PlanePair<T> nxt = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
-  for (int j = col - 2; j >= 1 && j > col - 2 - PF; --j) prefetch(j);
+  PlanePair<T> n1 = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
+  PlanePair<T> n2 = col >= 3 ? ld(col - 2) : PlanePair<T>{};
+  PlanePair<T> n3 = col >= 4 ? ld(col - 3) : PlanePair<T>{};
+  for (int j = col - 4; j >= 1 && j > col - 4 - PF; --j) prefetch(j);
   // interior: row >= 1 and col >= 1 hold on entry to every iteration
   for (;;) {
     if ((unsigned)b >= (unsigned)BITS) {
@@ -236,9 +240,11 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
     b += (int)db * ((int)da * 2 - 1);
     if (da) {
       --col;
-      cur = nxt;
-      if (col >= 2) nxt = ld(col - 1);
-      if (col - 1 - PF >= 1) prefetch(col - 1 - PF);
+      cur = n1;
+      n1 = n2;
+      n2 = n3;
+      if (col >= 4) n3 = ld(col - 3);
+      if (col - 3 - PF >= 1) prefetch(col - 3 - PF);
     }
     if (row == 0 || col == 0) break;
   }

@@ -1,9 +1,11 @@
 """Measures the banded kernel's time for every launch shape of the
 autotuner's search space over a grid of (read length, k, candidates) bins
-on the current GPU, and writes the table the cost-model tests train and
-evaluate on (tuning_sweep_b200.json).  Run on a B200:
+on the current GPU: the training data of the autotuner's cost model
+(tuning_sweep_b200.json beside this file was made on a B200 with
 
-    python tests/golden/make_tuning_sweep.py OUT.json
+    python -m saruman_b200.sweep OUT.json
+
+and copied here).
 """
 from __future__ import annotations
 
@@ -13,11 +15,8 @@ import sys
 import time
 from pathlib import Path
 
-ROOT = Path(__file__).resolve().parents[2]
-sys.path.insert(0, str(ROOT))
-
-import saruman_b200 as S  # noqa: E402
-from saruman_b200 import autotune as A  # noqa: E402
+import saruman_b200 as S
+from saruman_b200 import autotune as A
 
 LENGTHS = (36, 50, 75, 100, 125, 150, 200, 250)
 RATES = (0.03, 0.06, 0.10)
