@@ -343,7 +343,8 @@ struct LaunchClass {
 };
 
 int length_bucket(int m) {
-  static const int edges[] = {48, 96, 160, 288, 512};
+  // about 25% apart: a class's slice is at most ~25% larger than a member needs
+  static const int edges[] = {40, 48, 64, 80, 96, 112, 128, 160, 192, 240, 288, 352, 416, 512};
   for (int e : edges)
     if (m <= e) return e;
   return m;

@@ -6,8 +6,8 @@
 // out of shared memory, builds both alignment strings for the whole tile in
 // shared memory (zero-filled, as the reference's memset arena leaves them)
 // and writes the tile's slot range back with 16-byte stores.  Decision
-// planes (2 bits per band cell) go to a per-lane global scratch slice that
-// stays in L2; the traceback prefetches them two columns ahead.
+// planes (2 bits per band cell) go to a global scratch that stays in L2;
+// the traceback keeps the next three columns' planes in registers.
 //
 // The phases are separated by warp barriers in the kernel; written as
 // functions of the lane so a host harness can run them lane by lane.
@@ -31,7 +31,7 @@ struct TileArgs {
   int k, max_m, first_of_call;
   int32_t *scores;
   uint8_t *read_aln, *genome_aln;
-  void *planes;       // (max_m + 1) * pstride plane pairs
+  void *planes;       // plane_columns(max_m) * pstride plane pairs (plane_index)
   long pstride;       // lanes of the whole grid
   long pair_mul;      // plane-pair index multiplier: 2 when 32-bit pairs share a
                       // launch with 64-bit ones (one slot size for every lane)
@@ -176,6 +176,17 @@ template <typename T>
 struct PlanePair {
   T A, B;
 };
+
+// Decision planes in the scratch: [column][lane], so the fill's store of a
+// column is one contiguous 256-byte (512-byte) run per warp.  (Runs of
+// columns per lane would give the traceback's walk better L1 locality, but
+// their fill stores touch a sector per lane and measured twice as slow.)
+// `mul` spaces 32-bit pairs like 64-bit ones when a launch mixes both.
+SARU_HD long plane_columns(int max_m) { return (long)max_m + 1; }  // columns 0..max_m
+
+SARU_HD long plane_index(int j, long pstride, long pslot, long mul) {
+  return ((long)j * pstride + pslot) * mul;
+}
 
 // Traceback phase of one lane: writes the lane's two strings into its slot
 // of the output staging, in reading order (the reference emits from the

@@ -19,6 +19,15 @@
 
 namespace saru {
 
+// Columns ahead that the traceback prefetches into L1 beyond the next one.
+// 0 (none) measured fastest: the lanes of a warp walk different columns, and
+// prefetched lines evict each other from the L1 left beside the
+// shared-memory slices.
+#ifndef SARU_TRACE_PREFETCH
+#define SARU_TRACE_PREFETCH 0
+#endif
+constexpr int kTracePrefetch = SARU_TRACE_PREFETCH;
+
 __device__ __forceinline__ long gstart_of(const int32_t *goff, long t) { return t ? goff[t - 1] : 0; }
 
 // ---------------------------------------------------------------------------
@@ -51,7 +60,7 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
   LaneState ls;
   const long mul = ta.pair_mul;
   int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
-    planes[((long)j * ta.pstride + pslot) * mul] = PlanePair<T>{A, B};
+    planes[plane_index(j, ta.pstride, pslot, mul)] = PlanePair<T>{A, B};
   });
   __syncwarp();
   uint8_t *out_r = region;
@@ -62,12 +71,12 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
     for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
   }
   __syncwarp();
-  st |= lane_traceback<T, 8>(
-      ta, s, lane, st_reads, st_win, out_r, out_g, ls,
-      [&](int j) { return planes[((long)j * ta.pstride + pslot) * mul]; },
-      [&](int j) {
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + ((long)j * ta.pstride + pslot) * mul));
-      });
+  auto ld_pair = [&](int j) { return planes[plane_index(j, ta.pstride, pslot, mul)]; };
+  auto pf_pair = [&](int j) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + plane_index(j, ta.pstride, pslot, mul)));
+  };
+  st |= lane_traceback<T, kTracePrefetch>(
+      ta, s, lane, st_reads, st_win, out_r, out_g, ls, ld_pair, pf_pair);
   __syncwarp();
   stage_out(ta.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
   stage_out(ta.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
@@ -275,7 +284,7 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_c
 size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req) {
   const BandLayout L = band_layout(max_m, k, warps_req);
   return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 *
-                             (size_t)(max_m + 1) * (wide ? 8 : 4);
+                             (size_t)plane_columns(max_m) * (wide ? 8 : 4);
 }
 
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s) {

@@ -22,7 +22,7 @@ static int run(const TileArgs &a0, int nwarps_total) {
   a.ws_bytes = S.ws_bytes;
   a.region_bytes = S.region_bytes;
   a.pstride = (long)nwarps_total * 32;
-  std::vector<PlanePair<T>> planes_v((size_t)(a.max_m + 1) * a.pstride);
+  std::vector<PlanePair<T>> planes_v((size_t)plane_columns(a.max_m) * a.pstride);
   PlanePair<T> *planes = planes_v.data();
   int status = 0;
   auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
@@ -55,7 +55,7 @@ static int run(const TileArgs &a0, int nwarps_total) {
         const long pslot = (long)gwarp * 32 + lane;
         status |= lane_fill<T>(a, s, lane, st_reads, st_win, region32, ls[lane],
                                [&](int j, T A, T B) {
-                                 planes[(long)j * a.pstride + pslot] = PlanePair<T>{A, B};
+                                 planes[plane_index(j, a.pstride, pslot, 1)] = PlanePair<T>{A, B};
                                });
       }
       uint8_t *out_r = region, *out_g = region + s.o_span_r;
@@ -64,8 +64,8 @@ static int run(const TileArgs &a0, int nwarps_total) {
         const long pslot = (long)gwarp * 32 + lane;
         status |= lane_traceback<T, 8>(
             a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
-            [&](int j) { return planes[(long)j * a.pstride + pslot]; },
-            [&](int j) { (void)planes[(long)j * a.pstride + pslot]; });
+            [&](int j) { return planes[plane_index(j, a.pstride, pslot, 1)]; },
+            [&](int j) { (void)planes[plane_index(j, a.pstride, pslot, 1)]; });
       }
       for (int lane = 0; lane < 32; ++lane) {
         stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
@@ -117,7 +117,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
   const SliceLayout S = slice_layout(max_m, max_k);
   const long pstride = (long)nwarps_total * 32;
   // exactly the bytes the launcher reserves for the planes
-  std::vector<uint8_t> planes_v((size_t)(max_m + 1) * pstride * 2 * (wide_any ? 8 : 4));
+  std::vector<uint8_t> planes_v((size_t)plane_columns(max_m) * pstride * 2 * (wide_any ? 8 : 4));
   int status = 0;
   auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
   auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
@@ -174,7 +174,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
           status |= lane_fill<T>(a, w.span, lane, w.st_reads, w.st_win,
                                  reinterpret_cast<uint32_t *>(w.region), w.ls[lane],
                                  [&](int j, T A, T B) {
-                                   planes[((long)j * pstride + pslot) * a.pair_mul] =
+                                   planes[plane_index(j, pstride, pslot, a.pair_mul)] =
                                        PlanePair<T>{A, B};
                                  });
         }
@@ -195,8 +195,8 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
           const long pslot = (long)gw * 32 + lane;
           status |= lane_traceback<T, 8>(
               a, w.span, lane, w.st_reads, w.st_win, out_r, out_g, w.ls[lane],
-              [&](int j) { return planes[((long)j * pstride + pslot) * a.pair_mul]; },
-              [&](int j) { (void)planes[((long)j * pstride + pslot) * a.pair_mul]; });
+              [&](int j) { return planes[plane_index(j, pstride, pslot, a.pair_mul)]; },
+              [&](int j) { (void)planes[plane_index(j, pstride, pslot, a.pair_mul)]; });
         }
         for (int lane = 0; lane < 32; ++lane) {
           stage_out(a.read_aln, out_r, w.span.s_lo, w.span.s_hi, w.span.o_base_r, lane, st16);
