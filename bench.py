@@ -748,6 +748,44 @@ def main() -> None:
     e_ms = timed(stream, e2e_step, e2e_steps, world, dist, dev)
     e2e_value = world * n_cand / (e_ms * 1e-3)
 
+    # ---- compact result records instead of slot strings (single-bin) -----
+    compact = None
+    if not multi:
+        d0, b0 = dbs[0], bs[0]
+        rbytes = S.compact_record_bytes(b0.m, b0.k)
+        rec = torch.empty(b0.n * rbytes, dtype=torch.uint8, device=dev)
+        h_rec = torch.empty(b0.n * rbytes, dtype=torch.uint8).pin_memory()
+
+        def step_compact():
+            S.align_device_compact(d0.sb, d0.scores.data_ptr(), rec.data_ptr(), rbytes,
+                                   status.data_ptr(), scratch.data_ptr(), nscr, sptr)
+
+        for _ in range(2):
+            step_compact()
+        stream.synchronize()
+        c_ms = timed(stream, step_compact, args.steps, world, dist, dev)
+
+        def e2e_compact():
+            with torch.cuda.stream(stream):
+                d0.h2d()
+                step_compact()
+                d0.h_out[0][0].copy_(d0.scores, non_blocking=True)
+                h_rec.copy_(rec, non_blocking=True)
+
+        e2e_compact()
+        stream.synchronize()
+        ce_ms = timed(stream, e2e_compact, e2e_steps, world, dist, dev)
+        if int(status.item()) != 0:
+            raise SystemExit(f"kernel status {int(status.item())} (compact)")
+        compact = {"value": world * n_cand / (c_ms * 1e-3), "ms_per_step": c_ms,
+                   "record_bytes": rbytes,
+                   "e2e": {"value": world * n_cand / (ce_ms * 1e-3), "unit": "alignments/s",
+                           "h2d_bytes_per_step": d0.bytes_in(),
+                           "d2h_bytes_per_step": 4 * b0.n + b0.n * rbytes},
+                   "what": "saru_align_device_compact: 2-bit traceback records per candidate "
+                           "instead of the slot strings; saru_expand_compact rebuilds the "
+                           "slots on the host"}
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -818,6 +856,10 @@ def main() -> None:
     if plain:
         line["plain"] = plain
         line["batched_over_plain"] = plain["ms_per_step"] / ms_step
+    if compact:
+        compact["roofline_frac"] = (6 * cells / (compact["ms_per_step"] * 1e-3) / int_peak
+                                    if int_peak and int_peak > 0 else None)
+        line["compact"] = compact
     print(json.dumps(line))
 
 

@@ -215,6 +215,27 @@ int saru_mlp_loss_grad(const int32_t *dims, int32_t nlayers, const float *params
 int saru_mlp_adam_step(float *params, const float *grad, float *m, float *v, int64_t count,
                        float lr, float beta1, float beta2, float eps, int32_t step, void *stream);
 
+/* ---- compact results (no counterpart in the reference) ---------------------
+ * The banded kernel can return, instead of the two slot strings of each
+ * candidate (2(L + k) bytes), a fixed-size record of its traceback steps,
+ * 2 bits each: record_bytes = saru_compact_record_bytes(m, k), 48 bytes for
+ * m = 100, k = 5 against ~230 for the slots.  Word 0 of a record: the step
+ * count n (bits 0-15) and an overflow flag (bit 16); words 1..: the steps
+ * in traceback order, 16 per word (1 DIAG, 2 UP = gap in the read, 3 LEFT =
+ * gap in the window).  saru_expand_compact rebuilds on the host, from the
+ * records and the call's own reads and windows, exactly the slot strings the
+ * slot mode writes (the reference's layout).  Same conditions as
+ * saru_align_device; `records` holds n * record_bytes bytes (device). */
+int64_t saru_compact_record_bytes(int32_t max_read_length, int32_t k);
+int saru_align_device_compact(const saru_batch *batch, int32_t *scores, uint8_t *records,
+                              int64_t record_bytes, int32_t *status, void *scratch,
+                              size_t scratch_bytes, void *stream);
+/* Host arrays: the call (host batch), its scores and records -> both slot
+ * arrays (total_slots bytes each).  nthreads <= 0: all hardware threads. */
+int saru_expand_compact(const saru_batch *batch, const int32_t *scores, const uint8_t *records,
+                        int64_t record_bytes, char *read_aln, char *genome_aln,
+                        int32_t nthreads);
+
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 

@@ -36,7 +36,8 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_server_destroy", "saru_server_set_genome", "saru_gather_device",
                  "saru_tuning_set", "saru_tuning_get", "saru_tuning_clear",
                  "saru_mlp_param_count", "saru_mlp_work_floats", "saru_mlp_forward",
-                 "saru_mlp_loss_grad", "saru_mlp_adam_step")
+                 "saru_mlp_loss_grad", "saru_mlp_adam_step", "saru_compact_record_bytes",
+                 "saru_align_device_compact", "saru_expand_compact")
 ABI_DATA = ("alignment_time",)
 
 
@@ -154,6 +155,15 @@ def load(path: str | Path | None = None):
     lib.saru_mlp_adam_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                        C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32,
                                        C.c_void_p]
+    lib.saru_compact_record_bytes.restype = C.c_int64
+    lib.saru_compact_record_bytes.argtypes = [C.c_int32, C.c_int32]
+    lib.saru_align_device_compact.restype = C.c_int
+    lib.saru_align_device_compact.argtypes = [C.POINTER(SaruBatch), C.c_void_p, C.c_void_p,
+                                              C.c_int64, C.c_void_p, C.c_void_p, C.c_size_t,
+                                              C.c_void_p]
+    lib.saru_expand_compact.restype = C.c_int
+    lib.saru_expand_compact.argtypes = [C.POINTER(SaruBatch), C.c_void_p, C.c_void_p, C.c_int64,
+                                        C.c_void_p, C.c_void_p, C.c_int32]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -436,3 +446,33 @@ def get_tuning(m: int, k: int) -> tuple[int, int, int] | None:
     if load().saru_tuning_get(m, k, C.byref(t)):
         return (t.warps_per_cta, t.ctas_per_sm, t.word_bits)
     return None
+
+
+def compact_record_bytes(m: int, k: int) -> int:
+    return int(load().saru_compact_record_bytes(m, k))
+
+
+def align_device_compact(batch: SaruBatch, scores_ptr: int, records_ptr: int, record_bytes: int,
+                         status_ptr: int, scratch_ptr: int, scratch_len: int,
+                         stream_ptr: int = 0) -> None:
+    """Device pointers; compact records instead of slot strings."""
+    rc = load().saru_align_device_compact(C.byref(batch), scores_ptr, records_ptr, record_bytes,
+                                          status_ptr, scratch_ptr, scratch_len, stream_ptr)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+
+
+def expand_compact(b: Batch, scores: np.ndarray, records: np.ndarray, record_bytes: int,
+                   nthreads: int = 0, first_of_call: bool = True) -> AlignResult:
+    """The reference slot strings rebuilt on the host from compact records."""
+    sb, keep = host_batch(b, first_of_call)
+    tot = b.total_genome
+    ra = np.zeros(tot + 64, np.uint8)
+    ga = np.zeros(tot + 64, np.uint8)
+    sc = np.ascontiguousarray(scores, np.int32)
+    rec = np.ascontiguousarray(records, np.uint8)
+    rc = load().saru_expand_compact(C.byref(sb), _p(sc), _p(rec), record_bytes, _p(ra), _p(ga),
+                                    nthreads)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+    return AlignResult(sc[:b.n], ra[:tot], ga[:tot])

@@ -19,8 +19,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libsaruman_b200.so"
-SOURCES = ["kernels.cu", "gather.cu", "abi.cu", "writer.cpp", "server.cpp", "costmodel.cu",
-           "probe.cu"]
+SOURCES = ["kernels.cu", "gather.cu", "abi.cu", "writer.cpp", "server.cpp", "compact.cpp",
+           "costmodel.cu", "probe.cu"]
 HEADERS = ["kernels.cuh", "saru_core.cuh", "band_tile.cuh", "writer.h", "server_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler",

@@ -30,6 +30,7 @@
 #ifndef SARU_STATIC_SCRATCH_BYTES
 #define SARU_STATIC_SCRATCH_BYTES (32u << 20)
 #endif
+#include "band_tile.cuh"
 #include "kernels.cuh"
 #include "saru_core.cuh"
 #include "writer.h"
@@ -260,9 +261,15 @@ size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
 // Enqueues the banded kernel on device buffers: calls[0..ncalls) as the
 // segments of one launch (the single-call entry points pass one).  Scratch:
 // the tile counter, then the decision planes of the persistent grid.
+// Compact records of a call (instead of its slot strings).
+struct CompactOut {
+  uint8_t *records;
+  long rec_bytes;
+};
+
 int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, const Plan &pl,
                    void *scratch, size_t scratch_bytes, int *status_dev, int dev,
-                   cudaStream_t s, long max_grid = 0) {
+                   cudaStream_t s, long max_grid = 0, const CompactOut *cmp = nullptr) {
   if (ncalls < 1 || ncalls > saru::kMaxSegs) {
     set_error("%d calls in one launch (1..%d)", ncalls, saru::kMaxSegs);
     return SARU_E_INVALID;
@@ -297,6 +304,10 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
     g.read_aln = reinterpret_cast<uint8_t *>(r->read_aln);
     g.genome_aln = reinterpret_cast<uint8_t *>(r->genome_aln);
     g.status = r->status ? r->status : status_dev;
+    if (cmp) {
+      g.records = cmp[order[(size_t)q]].records;
+      g.rec_bytes = cmp[order[(size_t)q]].rec_bytes;
+    }
     g.n = b->n;
     g.tile_begin = tiles;
     g.k = b->k;
@@ -449,11 +460,12 @@ int run_band_classes(const saru_batch *calls, const saru_result *res, int ncalls
 
 int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
              size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
-             long max_grid = 0) {
+             long max_grid = 0, const CompactOut *cmp = nullptr) {
   if (b->n == 0) return SARU_OK;
   saru_batch one = *b;
   one.max_read_length = pl.max_m;
-  return run_band_multi(&one, r, 1, pl, scratch, scratch_bytes, status_dev, dev, s, max_grid);
+  return run_band_multi(&one, r, 1, pl, scratch, scratch_bytes, status_dev, dev, s, max_grid,
+                        cmp);
 }
 
 // Host batch -> device buffers of `lane`, returns device-side view.
@@ -792,6 +804,39 @@ int saru_align_device_static(const saru_batch *batch, saru_result *result, void 
   }
   return run_band(batch, pl, result, scratch, kStaticScratchBytes, result->status, dev,
                   reinterpret_cast<cudaStream_t>(stream), max_grid);
+}
+
+int64_t saru_compact_record_bytes(int32_t max_read_length, int32_t k) {
+  if (max_read_length < 1 || k < 0) return -1;
+  return saru::compact_record_bytes(max_read_length, k);
+}
+
+int saru_align_device_compact(const saru_batch *batch, int32_t *scores, uint8_t *records,
+                              int64_t record_bytes, int32_t *status, void *scratch,
+                              size_t scratch_bytes, void *stream) {
+  g_last_error.clear();
+  if (batch->n < 0 || batch->k < 0 || batch->k > 15 || batch->match != 0 ||
+      batch->mismatch != 1 || batch->max_read_length < 2 ||
+      batch->max_read_length > saru::kMaxBandM || !status || !scores ||
+      (batch->n > 0 && !records) ||
+      record_bytes < saru::compact_record_bytes(batch->max_read_length, batch->k) ||
+      (record_bytes & 15)) {
+    set_error("saru_align_device_compact: needs unit costs, k <= 15, 2 <= max_read_length <= "
+              "%d, scores, records of at least saru_compact_record_bytes (a multiple of 16) "
+              "and a status word",
+              saru::kMaxBandM);
+    return SARU_E_INVALID;
+  }
+  int dev = 0;
+  SARU_CUDA(cudaGetDevice(&dev));
+  Plan pl;
+  pl.band = true;
+  pl.max_m = batch->max_read_length;
+  pl.wide = batch->k > 7;
+  const saru_result r{scores, nullptr, nullptr, status};
+  const CompactOut cmp{records, (long)record_bytes};
+  return run_band(batch, pl, &r, scratch, scratch_bytes, status, dev,
+                  reinterpret_cast<cudaStream_t>(stream), 0, &cmp);
 }
 
 size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls) {

@@ -36,6 +36,8 @@ struct TileArgs {
   long pair_mul;      // plane-pair index multiplier: 2 when 32-bit pairs share a
                       // launch with 64-bit ones (one slot size for every lane)
   long rs_bytes, ws_bytes, region_bytes;
+  uint8_t *records;  // compact result records instead of slot strings (nullptr: slots)
+  long rec_bytes;    // bytes per record (compact_record_bytes)
 };
 
 // Byte ranges of a tile in the three arrays.
@@ -304,6 +306,102 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
       out_g[sg + i] = 0;
     }
   }
+  return bad ? 4 : 0;
+}
+
+// Compact result record of one candidate (the alternative to its two slot
+// strings): word 0 = number of traceback steps n (bits 0-15) and an
+// overflow flag (bit 16); words 1.. = the steps in traceback order (from
+// the alignment end), 2 bits each, 16 per word: 1 DIAG (read byte against
+// window byte), 2 UP (gap in the read), 3 LEFT (gap in the window).  With
+// the call's reads and windows the host rebuilds the slot strings exactly
+// (saru_expand_compact).  A candidate with score > k has n = 0.
+constexpr int kCompactHeaderBytes = 4;
+
+SARU_HD long compact_record_bytes(int max_m, int k) {
+  const long steps = (long)max_m + 3L * k;  // L + k <= m + 3k
+  return (kCompactHeaderBytes + 4 * ((steps + 15) / 16) + 15) & ~15L;
+}
+
+// Traceback of one lane into its compact record (same walk and border rules
+// as lane_traceback).  store(w, v) writes word w of candidate t's record.
+template <typename T, class LoadPair, class StoreWord>
+SARU_HD int lane_traceback_ops(const TileArgs &a, const TileSpan &s, int lane,
+                               const LaneState &ls, LoadPair ld, StoreWord store) {
+  constexpr int BITS = int(sizeof(T) * 8);
+  const long t = s.t0 + lane;
+  if (t >= a.n) return 0;
+  if (!ls.ok || ls.score > a.k) {
+    store(0, 0u);
+    return 0;
+  }
+  const Cand &c = ls.c;
+  const int cap = c.L + c.k;
+  int n = 0;
+  uint32_t acc = 0;
+  int row = c.L, col = c.m, b = c.L - c.m + c.k;
+  bool bad = false, stop = false;
+  auto push = [&](uint32_t op) {
+    acc |= op << (2 * (n & 15));
+    ++n;
+    if ((n & 15) == 0) {
+      store(n >> 4, acc);  // words 1.. hold steps 16(w-1) .. 16w-1
+      acc = 0;
+    }
+  };
+  PlanePair<T> cur = ld(col);
+  PlanePair<T> nxt = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
+  for (;;) {
+    if ((unsigned)b >= (unsigned)BITS) {
+      bad = true;
+      break;
+    }
+    const uint32_t da = (uint32_t)((cur.A >> b) & T(1));
+    const uint32_t db = (uint32_t)((cur.B >> b) & T(1));
+    if ((da | db) == 0) {
+      stop = true;
+      break;
+    }
+    if (n >= cap) {
+      bad = true;
+      break;
+    }
+    push(da | (db << 1));
+    row -= (int)(1u - (da & db));
+    b += (int)db * ((int)da * 2 - 1);
+    if (da) {
+      --col;
+      cur = nxt;
+      if (col >= 2) nxt = ld(col - 1);
+    }
+    if (row == 0 || col == 0) break;
+  }
+  if (!bad && !stop) {
+    for (;;) {  // borders, as in lane_traceback
+      if (row == 0) {
+        if (col == 0 || c.first_of_call) break;
+        if (n >= cap) {
+          bad = true;
+          break;
+        }
+        push(3u);
+        --col;
+        continue;
+      }
+      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
+      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
+      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
+      if (tp + 1 - corr != v) break;
+      if (n >= cap) {
+        bad = true;
+        break;
+      }
+      push(2u);
+      --row;
+    }
+  }
+  if (n & 15) store((n >> 4) + 1, acc);
+  store(0, (uint32_t)n | (bad ? 0x10000u : 0u));
   return bad ? 4 : 0;
 }
 

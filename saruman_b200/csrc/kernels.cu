@@ -63,6 +63,14 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
     planes[plane_index(j, ta.pstride, pslot, mul)] = PlanePair<T>{A, B};
   });
   __syncwarp();
+  if (ta.records) {  // compact records straight to global memory
+    uint32_t *rec = reinterpret_cast<uint32_t *>(ta.records + (s.t0 + lane) * ta.rec_bytes);
+    st |= lane_traceback_ops<T>(
+        ta, s, lane, ls, [&](int j) { return planes[plane_index(j, ta.pstride, pslot, mul)]; },
+        [&](int w, uint32_t v) { rec[w] = v; });
+    __syncwarp();
+    return st;
+  }
   uint8_t *out_r = region;
   uint8_t *out_g = region + s.o_span_r;
   {
@@ -113,7 +121,7 @@ __global__ void __launch_bounds__(128, 3) saru_band_kernel(const __grid_constant
     const TileArgs ta{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
                       g.first_of_call, g.scores, g.read_aln, g.genome_aln, a.planes, pstride,
                       (!g.wide && a.wide_any) ? 2L : 1L, a.rs_bytes, a.ws_bytes,
-                      a.warp_smem - a.rs_bytes - a.ws_bytes};
+                      a.warp_smem - a.rs_bytes - a.ws_bytes, g.records, g.rec_bytes};
     const long wt = tile - g.tile_begin;
     int status = g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
                         : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);

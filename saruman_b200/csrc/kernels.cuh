@@ -28,6 +28,8 @@ struct Segment {
   uint8_t *read_aln;
   uint8_t *genome_aln;
   int *status;      // this call's status word (device)
+  uint8_t *records;  // compact result records instead of slot strings (nullptr: slots)
+  long rec_bytes;
   long n;
   long tile_begin;  // first 32-candidate tile of this segment in the launch
   int k, max_m, first_of_call, wide;

@@ -58,6 +58,17 @@ static int run(const TileArgs &a0, int nwarps_total) {
                                  planes[plane_index(j, a.pstride, pslot, 1)] = PlanePair<T>{A, B};
                                });
       }
+      if (a.records) {  // compact records straight to the (exactly sized) output
+        for (int lane = 0; lane < 32; ++lane) {
+          const long pslot = (long)gwarp * 32 + lane;
+          uint32_t *rec = reinterpret_cast<uint32_t *>(a.records + (s.t0 + lane) * a.rec_bytes);
+          status |= lane_traceback_ops<T>(
+              a, s, lane, ls[lane],
+              [&](int j) { return planes[plane_index(j, a.pstride, pslot, 1)]; },
+              [&](int w, uint32_t v) { rec[w] = v; });
+        }
+        continue;
+      }
       uint8_t *out_r = region, *out_g = region + s.o_span_r;
       memset(region, 0, (size_t)S.region_bytes);
       for (int lane = 0; lane < 32; ++lane) {
@@ -87,6 +98,17 @@ extern "C" int tile_align_batch(const uint8_t *genome, const uint8_t *reads, con
                                 uint8_t *ra, uint8_t *ga) {
   TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, ra, ga,
              nullptr, 0, 1, 0, 0, 0};
+  return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
+}
+
+// The same call with compact records (rec_bytes per candidate) instead of
+// slot strings.
+extern "C" int tile_align_compact(const uint8_t *genome, const uint8_t *reads, const int *goff,
+                                  const int *roff, const int8_t *dirs, long n, int k, int max_m,
+                                  int wide, int first_of_call, int nwarps, int *scores,
+                                  uint8_t *records, long rec_bytes) {
+  TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, nullptr,
+             nullptr, nullptr, 0, 1, 0, 0, 0, records, rec_bytes};
   return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
 }
 

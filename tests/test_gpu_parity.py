@@ -314,3 +314,46 @@ def test_multi_call_request_replays_from_a_cuda_graph(saru_lib):
         assert int(status.item()) == 0
         _check_multi(keep, want)
     del g
+
+
+def _compact_roundtrip(b):
+    """saru_align_device_compact on the GPU, records expanded on the host."""
+    import torch
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    g, r, go, ro, d = T(b.genome), T(b.reads), T(b.genome_offsets), T(b.read_offsets), T(b.dirs)
+    R_ = S.compact_record_bytes(b.m, b.k)
+    sc = torch.zeros(max(b.n, 1), dtype=torch.int32, device=dev)
+    rec = torch.zeros(max(b.n, 1) * R_, dtype=torch.uint8, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    sb = S.SaruBatch(g.data_ptr(), r.data_ptr(), go.data_ptr(), ro.data_ptr(), d.data_ptr(), b.n,
+                     b.k, 0, 1, 1, b.m, len(b.genome), b.total_genome)
+    nscr = S.scratch_bytes(b.n, b.m, b.k)
+    scr = torch.empty(nscr, dtype=torch.uint8, device=dev)
+    S.align_device_compact(sb, sc.data_ptr(), rec.data_ptr(), R_, st.data_ptr(), scr.data_ptr(),
+                           nscr)
+    torch.cuda.synchronize()
+    return int(st.item()), S.expand_compact(b, sc.cpu().numpy()[:b.n], rec.cpu().numpy(), R_)
+
+
+@pytest.mark.parametrize("name", G.fixture_names())
+def test_compact_records_rebuild_the_golden_slots(saru_lib, name):
+    b, names, do_rev, m, exp = G.load_fixture(name)
+    if not (b.m > 3 * b.k and b.k <= 15 and b.match == 0 and b.mismatch == 1):
+        pytest.skip("outside the banded kernel's domain")
+    st, r = _compact_roundtrip(b)
+    if st & (S.SARU_S_IRREGULAR | S.SARU_S_ALPHABET):
+        pytest.skip("fixture takes the exact path")
+    assert st == 0
+    check_equal(b, exp["scores"], exp["read_aln"], exp["genome_aln"], r)
+
+
+@pytest.mark.parametrize("m,k", [(36, 3), (100, 5), (150, 9), (250, 15)])
+def test_compact_records_match_slot_mode(saru_lib, m, k):
+    b = W.random_batch(m, k, 1500, seed=m * 7 + k, err=0.05, alphabet=b"ACGTN")
+    st, r = _compact_roundtrip(b)
+    assert st == 0
+    want = S.align_host(b)
+    assert np.array_equal(r.scores, want.scores)
+    assert np.array_equal(r.read_aln, want.read_aln)
+    assert np.array_equal(r.genome_aln, want.genome_aln)

@@ -29,6 +29,23 @@ def exact(a: np.ndarray, off: int) -> np.ndarray:
     return v
 
 
+def compact_case(lib, b, g, r, go, ro, d, wide, s1, ra1, ga1) -> int:
+    import saruman_b200 as S
+    P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    R_ = S.compact_record_bytes(b.m, b.k)
+    rec = exact(np.zeros(b.n * R_, np.uint8), 0)
+    sc = np.zeros(b.n, np.int32)
+    st = lib.tile_align_compact(P(g), P(r), P(go), P(ro), P(d), C.c_long(b.n), C.c_int(b.k),
+                                C.c_int(b.m), C.c_int(wide), C.c_int(1), C.c_int(3), P(sc),
+                                P(rec), C.c_long(R_))
+    out = S.expand_compact(b, sc, rec, R_, nthreads=2)
+    ok = (st == 0 and np.array_equal(np.minimum(s1, b.k + 1), sc)
+          and np.array_equal(ra1, out.read_aln) and np.array_equal(ga1, out.genome_aln))
+    if not ok:
+        print("COMPACT MISMATCH", b.m, b.k, st, flush=True)
+    return 0 if ok else 1
+
+
 def main():
     lib = C.CDLL(sys.argv[1])
     P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
@@ -59,6 +76,8 @@ def main():
                 if not ok:
                     bad += 1
                     print("MISMATCH", m, k, seed, off, st, flush=True)
+                if off == 3:  # compact records, expanded on the host by the library
+                    bad += compact_case(lib, b, g, r, go, ro, d, wide, s1, ra1, ga1)
     # an irregular tile (window far too long) must be rejected, not staged
     b = W.random_batch(36, 2, 40, seed=1)
     go = b.genome_offsets.copy()
