@@ -394,7 +394,7 @@ class RequestPool:
         import torch
         S = self.S
         calls, gcalls, keep, cand, out_bytes, spans = [], [], [], 0, 0, []
-        h2d = d2h = 0
+        h2d = d2h = out_compact = d2h_compact = 0
         for i, b in enumerate(self.bs):
             r = max(1, reads // len(self.bs))
             r0 = int(rng.integers(0, max(1, self.per_bin[i] - r)))
@@ -409,8 +409,11 @@ class RequestPool:
             keep.append(t)
             gbytes = int(go[-1])
             slots = gbytes + b.k * n
-            spans.append((4 * n, slots + 64))
+            recs = n * S.compact_record_bytes(b.m, b.k)
+            spans.append((4 * n, slots + 64, recs))
             out_bytes += (4 * n + 255) // 256 * 256 + 2 * ((slots + 64 + 255) // 256 * 256)
+            out_compact += (4 * n + 255) // 256 * 256 + (recs + 255) // 256 * 256
+            d2h_compact += 4 * n + recs
             calls.append(S.SaruBatch(0, 0, t.data_ptr(), 0, self.pd[i].data_ptr() + c0, n, b.k,
                                      0, 1, 1, b.m, gbytes, slots))
             gcalls.append(S.SaruGatherCall(self.pt[i].data_ptr() + r0 * b.m, t.data_ptr() + 4 * n,
@@ -421,7 +424,8 @@ class RequestPool:
             h2d += r * b.m + 13 * n
             d2h += 4 * n + 2 * slots
         return dict(calls=calls, gcalls=gcalls, keep=keep, cand=cand, out_bytes=out_bytes,
-                    spans=spans, h2d=h2d, d2h=d2h)
+                    out_compact=out_compact, spans=spans, h2d=h2d, d2h=d2h,
+                    d2h_compact=d2h_compact)
 
     def alloc(self, nbytes: int) -> int | None:
         """Start offset in the ring, or None while the oldest requests hold it."""
@@ -436,33 +440,38 @@ class RequestPool:
             return 0 if tail >= nbytes else None
         return head if tail - head >= nbytes else None  # wrapped: free [head, tail)
 
-    def bind(self, req: dict, start: int):
+    def bind(self, req: dict, start: int, compact: bool = False):
         S = self.S
         p = self.ring_ptr + start
         res = []
-        for n4, slots in req["spans"]:
+        for n4, slots, recs in req["spans"]:
             sc = p
             p += (n4 + 255) // 256 * 256
+            if compact:
+                res.append(S.SaruResult(sc, p, 0, None))
+                p += (recs + 255) // 256 * 256
+                continue
             ra = p
             p += (slots + 255) // 256 * 256
             ga = p
             p += (slots + 255) // 256 * 256
             res.append(S.SaruResult(sc, ra, ga, None))
-        self.live.append((start, start + req["out_bytes"]))
+        self.live.append((start, start + (req["out_compact"] if compact else req["out_bytes"])))
         n = len(req["calls"])
         import ctypes as C
         req["arr_c"] = (S.SaruBatch * n)(*req["calls"])
         req["arr_r"] = (S.SaruResult * n)(*res)
         req["arr_g"] = (S.SaruGatherCall * n)(*req["gcalls"])
         req["creq"] = S.SaruRequest(req["arr_c"], req["arr_r"], n,
-                                    C.cast(req["arr_g"], C.POINTER(S.SaruGatherCall)))
+                                    C.cast(req["arr_g"], C.POINTER(S.SaruGatherCall)),
+                                    1 if compact else 0)
 
     def release_oldest(self):
         self.live.pop(0)
 
 
 def run_trace(S, pool: RequestPool, reqs: list, arrivals_s, pipeline: bool, budget: int,
-              max_per_launch: int = 64):
+              max_per_launch: int = 64, compact: bool = False):
     """Submits the requests at their arrival times (seconds after start;
     None = all at once) to a fresh server and returns per-request latency
     from arrival to results on the host, the makespan and the counters."""
@@ -485,11 +494,11 @@ def run_trace(S, pool: RequestPool, reqs: list, arrivals_s, pipeline: bool, budg
                     time.sleep(delay)
             with lock:
                 while True:
-                    start = pool.alloc(r["out_bytes"])
+                    start = pool.alloc(r["out_compact"] if compact else r["out_bytes"])
                     if start is not None:
                         break
                     lock.wait()
-                pool.bind(r, start)
+                pool.bind(r, start, compact)
             t = C.c_int64()
             rc = lib.saru_server_submit(srv._h, C.byref(r["creq"]), C.byref(t))
             if rc != S.SARU_OK:
@@ -570,6 +579,11 @@ def run_serving(args, cfg, rank: int) -> None:
     lat_p, mk_p, groups_p, launches_p = run_trace(S, pool, reqs, arrivals, False, budget)
     sat_b = run_trace(S, pool, reqs, None, True, budget)
     sat_p = run_trace(S, pool, reqs, None, False, budget)
+    # compact records instead of slot strings, same trace and arrivals
+    lat_bc, mk_bc, _, _ = run_trace(S, pool, reqs, arrivals, True, budget, compact=True)
+    lat_pc, mk_pc, _, _ = run_trace(S, pool, reqs, arrivals, False, budget, compact=True)
+    sat_bc = run_trace(S, pool, reqs, None, True, budget, compact=True)
+    sat_pc = run_trace(S, pool, reqs, None, False, budget, compact=True)
     launches = S.kernel_launches() - launches0
 
     def pct(v, p):
@@ -604,6 +618,16 @@ def run_serving(args, cfg, rank: int) -> None:
             "what": "one request at a time, one launch per length bin, no copy/compute overlap"},
         "batched_over_plain": sat_p[1] / sat_b[1],
         "p99_plain_over_batched": pct(lat_p, 99) / pct(lat_b, 99),
+        "compact": {
+            "what": "the same trace with compact records (saru_request.compact) returned "
+                    "instead of slot strings",
+            "d2h_bytes_per_step": sum(r["d2h_compact"] for r in reqs),
+            "value": n_cand / sat_bc[1], "plain_value": n_cand / sat_pc[1],
+            "batched_over_plain": sat_pc[1] / sat_bc[1],
+            "latency_ms": {"p50": pct(lat_bc, 50), "p99": pct(lat_bc, 99),
+                           "throughput": n_cand / mk_bc},
+            "plain_latency_ms": {"p50": pct(lat_pc, 50), "p99": pct(lat_pc, 99),
+                                 "throughput": n_cand / mk_pc}},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
@@ -622,6 +646,8 @@ def main() -> None:
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--shape", default=None,
+                    help="W,C,B: install this launch shape for every bin instead of tuning")
     ap.add_argument("--requests", type=int, default=None,
                     help="requests in the serving trace (c5)")
     ap.add_argument("--reads", type=int, default=None,
@@ -667,7 +693,13 @@ def main() -> None:
     multi = len(dbs) > 1
     int_peak = S.int32_issue_peak() if rank == 0 else None
     # launch shapes first: the scratch sizes depend on them
-    tuning = tune_bins(bs, dbs, status) if not args.no_tune else {}
+    if args.shape:
+        shape = tuple(int(x) for x in args.shape.split(","))
+        for b in bs:
+            S.set_tuning(b.m, b.k, *shape)
+        tuning = {f"{b.m},{b.k}": {"shape": list(shape), "trials": 0} for b in bs}
+    else:
+        tuning = tune_bins(bs, dbs, status) if not args.no_tune else {}
     status.zero_()
     if multi:
         nscr = S.multi_scratch_bytes([d.sb for d in dbs])

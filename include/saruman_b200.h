@@ -286,6 +286,9 @@ typedef struct {
   int32_t ncalls;
   const saru_gather_call *gather; /* if not NULL: the ncalls calls are these (host arrays),
                                      gathered from the resident genome; `calls` is unused */
+  int32_t compact;                /* 1: results[i].read_aln receives the call's compact
+                                     records (n x saru_compact_record_bytes(m, k) bytes;
+                                     genome_aln unused) instead of the slot strings */
 } saru_request;
 typedef struct {
   int64_t submit_us, admit_us, done_us; /* steady clock, microseconds */

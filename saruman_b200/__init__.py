@@ -82,7 +82,8 @@ class SaruGatherCall(C.Structure):
 
 class SaruRequest(C.Structure):
     _fields_ = [("calls", C.POINTER(SaruBatch)), ("results", C.POINTER(SaruResult)),
-                ("ncalls", C.c_int32), ("gather", C.POINTER(SaruGatherCall))]
+                ("ncalls", C.c_int32), ("gather", C.POINTER(SaruGatherCall)),
+                ("compact", C.c_int32)]
 
 
 class RequestStats(C.Structure):
@@ -295,9 +296,11 @@ class HostRequest:
     server's copies overlap its kernels); numpy by default."""
 
     def __init__(self, batches: list[Batch], first_of_call: list[bool] | None = None,
-                 alloc=None):
+                 alloc=None, compact: bool = False):
         alloc = alloc or (lambda nbytes: np.zeros(nbytes, np.uint8))
         first = first_of_call or [True] * len(batches)
+        self.compact = compact
+        self.first = first
 
         def host(a: np.ndarray, dtype) -> np.ndarray:
             a = np.ascontiguousarray(a, dtype)
@@ -317,18 +320,28 @@ class HostRequest:
             calls.append(SaruBatch(*[_p(a) if a.size else 0 for a in arrs], b.n, b.k, b.match,
                                    b.mismatch, 1 if f else 0, b.m, len(b.genome),
                                    b.total_genome))
-            out = AlignResult(alloc(4 * max(b.n, 1)).view(np.int32)[:max(b.n, 1)],
-                              alloc(b.total_genome + 64)[:b.total_genome + 64],
-                              alloc(b.total_genome + 64)[:b.total_genome + 64])
+            if compact:  # records in read_aln, genome_aln unused
+                nrec = max(b.n, 1) * compact_record_bytes(b.m, b.k)
+                out = AlignResult(alloc(4 * max(b.n, 1)).view(np.int32)[:max(b.n, 1)],
+                                  alloc(nrec)[:nrec], np.zeros(0, np.uint8))
+            else:
+                out = AlignResult(alloc(4 * max(b.n, 1)).view(np.int32)[:max(b.n, 1)],
+                                  alloc(b.total_genome + 64)[:b.total_genome + 64],
+                                  alloc(b.total_genome + 64)[:b.total_genome + 64])
             self.outs.append(out)
-            results.append(SaruResult(_p(out.scores), _p(out.read_aln), _p(out.genome_aln), None))
+            results.append(SaruResult(_p(out.scores), _p(out.read_aln),
+                                      _p(out.genome_aln) if out.genome_aln.size else 0, None))
         n = len(batches)
         self.calls = (SaruBatch * n)(*calls)
         self.results = (SaruResult * n)(*results)
-        self.req = SaruRequest(self.calls, self.results, n)
+        self.req = SaruRequest(self.calls, self.results, n, None, 1 if compact else 0)
 
     def result(self, i: int) -> AlignResult:
+        """Call i's scores and slot strings (compact records are expanded)."""
         b, o = self.batches[i], self.outs[i]
+        if self.compact:
+            return expand_compact(b, o.scores[:b.n], o.read_aln, compact_record_bytes(b.m, b.k),
+                                  first_of_call=self.first[i])
         return AlignResult(o.scores[:b.n], o.read_aln[:b.total_genome],
                            o.genome_aln[:b.total_genome])
 
@@ -341,8 +354,8 @@ class GatherRequest(HostRequest):
     layout (their genome/reads arrays are not sent)."""
 
     def __init__(self, batches: list[Batch], tables: list[np.ndarray],
-                 first_of_call: list[bool] | None = None):
-        super().__init__(batches, first_of_call)
+                 first_of_call: list[bool] | None = None, compact: bool = False):
+        super().__init__(batches, first_of_call, compact=compact)
         first = first_of_call or [True] * len(batches)
         gcs = []
         for b, tab, f in zip(batches, tables, first):

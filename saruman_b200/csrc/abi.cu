@@ -33,6 +33,7 @@
 #include "band_tile.cuh"
 #include "kernels.cuh"
 #include "saru_core.cuh"
+#include "server_internal.h"
 #include "writer.h"
 
 // ---------------------------------------------------------------------------
@@ -261,11 +262,7 @@ size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
 // Enqueues the banded kernel on device buffers: calls[0..ncalls) as the
 // segments of one launch (the single-call entry points pass one).  Scratch:
 // the tile counter, then the decision planes of the persistent grid.
-// Compact records of a call (instead of its slot strings).
-struct CompactOut {
-  uint8_t *records;
-  long rec_bytes;
-};
+using saru::CompactOut;
 
 int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, const Plan &pl,
                    void *scratch, size_t scratch_bytes, int *status_dev, int dev,
@@ -422,7 +419,8 @@ struct ClassStreams {
 ClassStreams g_class_streams[64];
 
 int run_band_classes(const saru_batch *calls, const saru_result *res, int ncalls, void *scratch,
-                     size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s) {
+                     size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
+                     const CompactOut *cmp = nullptr) {
   const std::vector<LaunchClass> cls = plan_classes(calls, ncalls, dev);
   if (classes_scratch_bytes(cls) > scratch_bytes) {
     set_error("scratch too small: %zu < %zu", scratch_bytes, classes_scratch_bytes(cls));
@@ -434,13 +432,15 @@ int run_band_classes(const saru_batch *calls, const saru_result *res, int ncalls
     pl.wide = L.wide;
     std::vector<saru_batch> cb;
     std::vector<saru_result> cr;
+    std::vector<CompactOut> cc;
     for (int i : L.calls) {
       cb.push_back(calls[i]);
       cr.push_back(res[i]);
+      if (cmp) cc.push_back(cmp[i]);
     }
     return run_band_multi(cb.data(), cr.data(), (int)cb.size(), pl,
                           static_cast<uint8_t *>(scratch) + L.scratch_off, L.scratch_bytes,
-                          status_dev, dev, st);
+                          status_dev, dev, st, 0, cmp ? cc.data() : nullptr);
   };
   if (cls.size() == 1) return launch(cls[0], s);
   if (dev < 0 || dev >= 64) return SARU_E_INVALID;
@@ -646,6 +646,14 @@ int redo_on_host_path(const saru_batch *b, saru_result *r) {
   Lane &L = g_lanes[2];
   std::lock_guard<std::mutex> lk(L.mu);
   return align_host_impl(b, r, L, nullptr);
+}
+int align_multi_mixed(const saru_batch *calls, const saru_result *results,
+                      const CompactOut *cmp, int32_t ncalls, int32_t *status, void *scratch,
+                      size_t scratch_bytes, void *stream) {
+  int dev = 0;
+  SARU_CUDA(cudaGetDevice(&dev));
+  return run_band_classes(calls, results, ncalls, scratch, scratch_bytes, status, dev,
+                          reinterpret_cast<cudaStream_t>(stream), cmp);
 }
 }  // namespace saru
 

@@ -53,6 +53,40 @@ bool expand_one(const uint32_t *rec, const char *read, const char *win, int m, i
 
 }  // namespace
 
+namespace saru {
+
+// Records from slot strings (the inverse of expand_one): the steps are the
+// string's columns in reverse (traceback) order -- '_' in the read string an
+// UP step, '_' in the window string a LEFT step, else DIAG.
+int records_from_slots(const saru_batch *b, const int32_t *scores, const char *read_aln,
+                       const char *genome_aln, uint8_t *records, long record_bytes) {
+  for (int64_t t = 0; t < b->n; ++t) {
+    const int64_t gs = t ? b->genome_offsets[t - 1] : 0;
+    const int L = (int)(b->genome_offsets[t] - gs);
+    const int cap = L + b->k;
+    const char *sr = read_aln + gs + (int64_t)b->k * t;
+    const char *sg = genome_aln + gs + (int64_t)b->k * t;
+    uint32_t *rec = reinterpret_cast<uint32_t *>(records + t * record_bytes);
+    memset(rec, 0, (size_t)record_bytes);
+    if (scores[t] > b->k) continue;
+    int n = 0;
+    while (n < cap && sr[n] != 0) ++n;
+    if (4 + 4 * ((n + 15) / 16) > record_bytes) {
+      set_last_error("records_from_slots: a string longer than its record");
+      return SARU_E_INVALID;
+    }
+    for (int i = 0; i < n; ++i) {
+      const uint32_t op = sr[i] == '_' ? 2u : (sg[i] == '_' ? 3u : 1u);
+      const int st = n - 1 - i;
+      rec[1 + (st >> 4)] |= op << (2 * (st & 15));
+    }
+    rec[0] = (uint32_t)n;
+  }
+  return SARU_OK;
+}
+
+}  // namespace saru
+
 extern "C" int saru_expand_compact(const saru_batch *b, const int32_t *scores,
                                    const uint8_t *records, int64_t record_bytes, char *read_aln,
                                    char *genome_aln, int32_t nthreads) {

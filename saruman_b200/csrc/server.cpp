@@ -98,11 +98,13 @@ class Arena {
 struct Request {
   int64_t ticket = 0;
   bool gather = false;                  // calls given as saru_gather_call (resident genome)
+  bool compact = false;                 // compact records instead of slot strings
   std::vector<saru_gather_call> gcalls; // host views (caller's arrays), when gather
   std::vector<saru_batch> calls;     // host views (caller's arrays); shapes only when gather
   std::vector<saru_result> results;  // host outputs (caller's arrays)
   std::vector<saru_batch> dcalls;    // device views inside the arena
   std::vector<saru_result> dres;
+  std::vector<saru::CompactOut> dcmp;  // device records per call (compact requests)
   std::vector<int32_t> call_status;  // kernel status bits per call, read back
   size_t dev_bytes = 0;
   long dev_off = -1;
@@ -120,6 +122,16 @@ size_t read_bytes(const Request &r, size_t i) {
   return b.n ? (size_t)b.read_offsets[b.n - 1] : 0;
 }
 
+size_t record_bytes(const saru_batch &b) {
+  return (size_t)saru_compact_record_bytes(b.max_read_length, b.k);
+}
+
+// Device bytes of a call's results: two slot arrays, or its records.
+size_t output_bytes(const Request &r, const saru_batch &b) {
+  return r.compact ? up256((size_t)b.n * record_bytes(b) + 64)
+                   : 2 * up256((size_t)b.total_slots + 64);
+}
+
 // Arena bytes one request takes: every device array up256-aligned.
 size_t request_bytes(const Request &r) {
   size_t t = up256(4 * r.calls.size());  // status words
@@ -130,7 +142,7 @@ size_t request_bytes(const Request &r) {
     t += up256(read_bytes(r, i) + 64);
     t += 3 * up256(4 * n + 64);  // genome_offsets, read_offsets, scores
     t += up256(n + 64);          // dirs
-    t += 2 * up256((size_t)b.total_slots + 64);
+    t += output_bytes(r, b);
     if (r.gather)  // read table, read_index, positions
       t += up256((size_t)r.gcalls[i].nreads * (size_t)b.max_read_length + 64) +
            2 * up256(4 * n + 64);
@@ -185,6 +197,7 @@ struct saru_server {
     cudaMemsetAsync(r.dstatus, 0, 4 * nc, s_in);
     r.dcalls.resize(nc);
     r.dres.resize(nc);
+    r.dcmp.assign(nc, saru::CompactOut{nullptr, 0});
     for (size_t i = 0; i < nc; ++i) {
       const saru_batch &h = r.calls[i];
       const size_t n = (size_t)h.n;
@@ -192,7 +205,14 @@ struct saru_server {
       uint8_t *g = take((size_t)h.genome_bytes + 64), *rd = take(rbytes + 64);
       uint8_t *go = take(4 * n + 64), *ro = take(4 * n + 64), *sc = take(4 * n + 64);
       uint8_t *dr = take(n + 64);
-      uint8_t *ra = take((size_t)h.total_slots + 64), *ga = take((size_t)h.total_slots + 64);
+      uint8_t *ra = nullptr, *ga = nullptr;
+      if (r.compact) {
+        ra = take(n * record_bytes(h) + 64);
+        r.dcmp[i] = saru::CompactOut{ra, (long)record_bytes(h)};
+      } else {
+        ra = take((size_t)h.total_slots + 64);
+        ga = take((size_t)h.total_slots + 64);
+      }
       saru_batch &d = r.dcalls[i];
       d = h;
       d.genome = reinterpret_cast<const char *>(g);
@@ -232,24 +252,37 @@ struct saru_server {
     }
   }
 
-  // A flagged gather call, redone on the exact path: its gathered windows
-  // and reads come back from the arena first.
-  int redo_gather(Request &r, size_t i) {
-    const saru_batch &d = r.dcalls[i];
-    const size_t n = (size_t)d.n;
-    std::vector<char> win((size_t)d.genome_bytes), rd(read_bytes(r, i));
-    std::vector<int32_t> ro(n);
-    if (cudaMemcpy(win.data(), d.genome, win.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(rd.data(), d.reads, rd.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
-      saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
-      return SARU_E_CUDA;
-    }
-    for (size_t t = 0; t < n; ++t) ro[t] = (int32_t)((t + 1) * (size_t)d.max_read_length);
+  // A flagged call, redone on the exact path as saru_align_host does.  A
+  // gather call's windows and reads come back from the arena first; a
+  // compact request gets the exact path's slot strings as records.
+  int redo_call(Request &r, size_t i) {
     saru_batch h = r.calls[i];
-    h.genome = win.data();
-    h.reads = rd.data();
-    h.read_offsets = ro.data();
-    return saru::redo_on_host_path(&h, &r.results[i]);
+    const size_t n = (size_t)h.n;
+    std::vector<char> win, rd;
+    std::vector<int32_t> ro;
+    if (r.gather) {
+      const saru_batch &d = r.dcalls[i];
+      win.resize((size_t)d.genome_bytes);
+      rd.resize(read_bytes(r, i));
+      ro.resize(n);
+      if (cudaMemcpy(win.data(), d.genome, win.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(rd.data(), d.reads, rd.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
+        return SARU_E_CUDA;
+      }
+      for (size_t t = 0; t < n; ++t) ro[t] = (int32_t)((t + 1) * (size_t)d.max_read_length);
+      h.genome = win.data();
+      h.reads = rd.data();
+      h.read_offsets = ro.data();
+    }
+    if (!r.compact) return saru::redo_on_host_path(&h, &r.results[i]);
+    std::vector<char> sr((size_t)h.total_slots + 64), sg((size_t)h.total_slots + 64);
+    saru_result tmp{r.results[i].scores, sr.data(), sg.data(), nullptr};
+    const int rc = saru::redo_on_host_path(&h, &tmp);
+    if (rc) return rc;
+    return saru::records_from_slots(&h, tmp.scores, sr.data(), sg.data(),
+                                    reinterpret_cast<uint8_t *>(r.results[i].read_aln),
+                                    (long)record_bytes(h));
   }
 
   int ensure_scratch(size_t bytes) {
@@ -318,24 +351,31 @@ struct saru_server {
       cudaStreamWaitEvent(s_comp, in_ev, 0);
       std::vector<saru_batch> calls;
       std::vector<saru_result> res;
+      std::vector<saru::CompactOut> cmp;
       for (auto &r : grp)
         for (size_t i = 0; i < r->dcalls.size(); ++i)
           if (r->dcalls[i].n > 0) {
             calls.push_back(r->dcalls[i]);
             res.push_back(r->dres[i]);
+            cmp.push_back(r->dcmp[i]);
           }
       int rc = SARU_OK;
       const uint64_t l0 = saru::thread_launches();
       if (!calls.empty() && cfg.pipeline) {
         rc = ensure_scratch(saru_multi_scratch_bytes(calls.data(), (int)calls.size()));
         if (!rc)  // every call has its own status word; res[0]'s is the unused fallback
-          rc = saru_align_multi_device(calls.data(), res.data(), (int)calls.size(), res[0].status,
-                                       scratch, scratch_bytes, s_comp);
+          rc = saru::align_multi_mixed(calls.data(), res.data(), cmp.data(), (int)calls.size(),
+                                       res[0].status, scratch, scratch_bytes, s_comp);
       } else {
         for (size_t i = 0; i < calls.size() && !rc; ++i) {
           rc = ensure_scratch(saru_scratch_bytes(calls[i].n, calls[i].max_read_length,
                                                  calls[i].k, calls[i].k > 7));
-          if (!rc) rc = saru_align_device(&calls[i], &res[i], scratch, scratch_bytes, s_comp);
+          if (rc) break;
+          rc = cmp[i].records
+                   ? saru_align_device_compact(&calls[i], res[i].scores, cmp[i].records,
+                                               cmp[i].rec_bytes, res[i].status, scratch,
+                                               scratch_bytes, s_comp)
+                   : saru_align_device(&calls[i], &res[i], scratch, scratch_bytes, s_comp);
         }
       }
       cudaEventRecord(done_ev, s_comp);
@@ -373,6 +413,11 @@ struct saru_server {
           if (h.n == 0) continue;
           const saru_result &d = r->dres[i], &o = r->results[i];
           cudaMemcpyAsync(o.scores, d.scores, 4 * (size_t)h.n, cudaMemcpyDeviceToHost, s_out);
+          if (r->compact) {
+            cudaMemcpyAsync(o.read_aln, d.read_aln, (size_t)h.n * record_bytes(h),
+                            cudaMemcpyDeviceToHost, s_out);
+            continue;
+          }
           cudaMemcpyAsync(o.read_aln, d.read_aln, (size_t)h.total_slots, cudaMemcpyDeviceToHost,
                           s_out);
           cudaMemcpyAsync(o.genome_aln, d.genome_aln, (size_t)h.total_slots,
@@ -397,8 +442,7 @@ struct saru_server {
             r->rc = SARU_E_INVALID;
           } else if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
             // as saru_align_host does: the whole call again on the exact path
-            r->rc = r->gather ? redo_gather(*r, i)
-                              : saru::redo_on_host_path(&r->calls[i], &r->results[i]);
+            r->rc = redo_call(*r, i);
             r->redone += 1;
           } else if (st & saru::kStatusOverflow) {
             saru::set_last_error("banded traceback left its band");
@@ -458,6 +502,7 @@ int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket)
     return SARU_E_INVALID;
   }
   auto r = std::make_shared<Request>();
+  r->compact = req->compact != 0;
   r->results.assign(req->results, req->results + req->ncalls);
   if (req->gather) {
     r->gather = true;

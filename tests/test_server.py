@@ -224,3 +224,28 @@ def test_gather_request_needs_a_genome(saru_lib):
         with pytest.raises(S.SaruError) as e:
             srv.submit(S.GatherRequest([b], [table]))
         assert e.value.code == S.SARU_E_INVALID
+
+
+def test_compact_requests_expand_to_the_same_bytes(saru_lib):
+    """Requests asking for compact records (window and gather calls, an
+    m <= 3k call redone on the exact path) expand on the host to exactly
+    saru_align_host's slots, mixed with slot-string requests."""
+    g = W.uniform_genome(300_000, seed=60)
+    shapes = [(36, 3, 1500), (100, 6, 1200), (150, 9, 700), (12, 5, 200)]
+    cases = [gather_case_on(g, m, k, n, seed=60 + 5 * i) for i, (m, k, n) in enumerate(shapes)]
+    for pipeline in (True, False):
+        with S.Server(pipeline=pipeline, max_requests_per_launch=8, budget_bytes=1 << 30) as srv:
+            srv.set_genome(g)
+            reqs = []
+            for table, b in cases:
+                reqs.append(S.GatherRequest([b], [table], compact=True))
+                reqs.append(S.HostRequest([b], compact=True))
+                reqs.append(S.HostRequest([b]))
+            tickets = [srv.submit(r) for r in reqs]
+            for t in tickets:
+                rc, _ = srv.wait(t)
+                assert rc == S.SARU_OK, S.last_error()
+        for i, (table, b) in enumerate(cases):
+            want = S.align_host(b)
+            for r in reqs[3 * i:3 * i + 3]:
+                assert_same(r.result(0), want)
