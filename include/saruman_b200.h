@@ -236,6 +236,18 @@ int saru_expand_compact(const saru_batch *batch, const int32_t *scores, const ui
                         int64_t record_bytes, char *read_aln, char *genome_aln,
                         int32_t nthreads);
 
+/* The reference writer's TSV lines (as saru_format_tsv) straight from host
+ * compact records, without the call's slot arrays: each thread expands only
+ * the slots its lines and the writer's scans reach.  Returns the bytes
+ * needed (-1 on invalid input) and writes min(needed, cap) bytes to out.
+ * nthreads <= 0: all hardware threads. */
+int64_t saru_format_tsv_compact(const saru_batch *batch, const int32_t *scores,
+                                const uint8_t *records, int64_t record_bytes,
+                                const int32_t *read_ids, const int32_t *genome_pos,
+                                int32_t read_length, const char *names, int32_t name_stride,
+                                int32_t n_names, char *out, int64_t cap, int32_t *done_fwd,
+                                int32_t *done_rev, int32_t nthreads);
+
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 

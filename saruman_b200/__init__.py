@@ -37,7 +37,7 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_tuning_set", "saru_tuning_get", "saru_tuning_clear",
                  "saru_mlp_param_count", "saru_mlp_work_floats", "saru_mlp_forward",
                  "saru_mlp_loss_grad", "saru_mlp_adam_step", "saru_compact_record_bytes",
-                 "saru_align_device_compact", "saru_expand_compact")
+                 "saru_align_device_compact", "saru_expand_compact", "saru_format_tsv_compact")
 ABI_DATA = ("alignment_time",)
 
 
@@ -165,6 +165,12 @@ def load(path: str | Path | None = None):
     lib.saru_expand_compact.restype = C.c_int
     lib.saru_expand_compact.argtypes = [C.POINTER(SaruBatch), C.c_void_p, C.c_void_p, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.c_int32]
+    lib.saru_format_tsv_compact.restype = C.c_int64
+    lib.saru_format_tsv_compact.argtypes = [C.POINTER(SaruBatch), C.c_void_p, C.c_void_p,
+                                            C.c_int64, C.c_void_p, C.c_void_p, C.c_int32,
+                                            C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                            C.c_int64, C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_int32), C.c_int32]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -489,3 +495,31 @@ def expand_compact(b: Batch, scores: np.ndarray, records: np.ndarray, record_byt
     if rc != SARU_OK:
         raise SaruError(rc, last_error())
     return AlignResult(sc[:b.n], ra[:tot], ga[:tot])
+
+
+def format_tsv_compact(b: Batch, scores: np.ndarray, records: np.ndarray, record_bytes: int,
+                       names: np.ndarray, read_length: int | None = None,
+                       first_of_call: bool = True, nthreads: int = 0) -> tuple[bytes, int, int]:
+    """The reference writer's TSV straight from compact records
+    (saru_format_tsv_compact): (text, forward alignments, reverse alignments)."""
+    lib = load()
+    sb, keep = host_batch(b, first_of_call)
+    sc = np.ascontiguousarray(scores, np.int32)
+    rec = np.ascontiguousarray(records, np.uint8)
+    ids = np.ascontiguousarray(b.ids, np.int32)
+    pos = np.ascontiguousarray(b.pos, np.int32)
+    rl = b.m if read_length is None else read_length
+    df, dr = C.c_int32(), C.c_int32()
+    est = int((sc <= b.k).sum()) * (names.shape[1] + 2 * (b.m + 3 * b.k) + 64) + 64
+    buf = np.zeros(est, np.uint8)
+    need = lib.saru_format_tsv_compact(C.byref(sb), _p(sc), _p(rec), record_bytes, _p(ids),
+                                       _p(pos), rl, _p(names), names.shape[1], names.shape[0],
+                                       _p(buf), est, C.byref(df), C.byref(dr), nthreads)
+    if need < 0:
+        raise SaruError(SARU_E_INVALID, last_error())
+    if need > est:  # the estimate was short: once more with the exact size
+        buf = np.zeros(need, np.uint8)
+        lib.saru_format_tsv_compact(C.byref(sb), _p(sc), _p(rec), record_bytes, _p(ids), _p(pos),
+                                    rl, _p(names), names.shape[1], names.shape[0], _p(buf), need,
+                                    C.byref(df), C.byref(dr), nthreads)
+    return buf[:need].tobytes(), df.value, dr.value

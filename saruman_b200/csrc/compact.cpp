@@ -10,6 +10,7 @@
 
 #include "../../include/saruman_b200.h"
 #include "server_internal.h"
+#include "writer.h"
 
 namespace {
 
@@ -130,4 +131,134 @@ extern "C" int saru_expand_compact(const saru_batch *b, const int32_t *scores,
       return SARU_E_INVALID;
     }
   return SARU_OK;
+}
+
+namespace {
+
+struct Shape {
+  const saru_batch *b;
+  const int32_t *scores;
+  const uint8_t *records;
+  int64_t rb;
+  int64_t slot_start(int64_t t) const {
+    return (t ? b->genome_offsets[t - 1] : 0) + (int64_t)b->k * t;
+  }
+  int cap(int64_t t) const {
+    return (int)(b->genome_offsets[t] - (t ? b->genome_offsets[t - 1] : 0)) + b->k;
+  }
+  const uint32_t *rec(int64_t t) const {
+    return reinterpret_cast<const uint32_t *>(records + t * rb);
+  }
+  bool reported(int64_t t) const { return scores[t] <= b->k; }
+  // the slot has no NUL: the writer's forward scans run into the next slot
+  bool full(int64_t t) const { return reported(t) && (int)(rec(t)[0] & 0xFFFFu) >= cap(t); }
+  // the read string holds a read byte (a DIAG or LEFT step): the writer's
+  // backward scan stops inside the slot
+  bool has_letter(int64_t t) const {
+    if (!reported(t)) return false;
+    const int n = (int)(rec(t)[0] & 0xFFFFu);
+    for (int w = 0; 16 * w < n; ++w) {
+      uint32_t x = rec(t)[1 + w];
+      const int left = n - 16 * w;
+      if (left < 16) x &= (1u << (2 * left)) - 1u;
+      if (x & 0x55555555u) return true;
+    }
+    return false;
+  }
+};
+
+struct NameTab {
+  const char *names;
+  int32_t stride, n;
+};
+
+const char *table_name(void *ctx, int32_t id) {
+  auto *t = static_cast<NameTab *>(ctx);
+  return (id >= 0 && id < t->n) ? t->names + (int64_t)id * t->stride : nullptr;
+}
+
+}  // namespace
+
+// TSV lines of a call straight from compact records: each thread expands
+// the slots of its candidate range -- widened to the slots the reference
+// writer's scans can reach (backwards until a slot with a read byte,
+// forwards while a slot has no NUL) -- into its own buffer and runs the
+// writer there.  Output in candidate order; returns the bytes needed and
+// writes min(needed, cap) bytes to out.
+extern "C" int64_t saru_format_tsv_compact(const saru_batch *b, const int32_t *scores,
+                                           const uint8_t *records, int64_t record_bytes,
+                                           const int32_t *read_ids, const int32_t *genome_pos,
+                                           int32_t read_length, const char *names,
+                                           int32_t name_stride, int32_t n_names, char *out,
+                                           int64_t cap, int32_t *done_fwd, int32_t *done_rev,
+                                           int32_t nthreads) {
+  saru::set_last_error("");
+  if (!b || b->n < 0 || (b->n > 0 && (!scores || !records || !read_ids || !genome_pos)) ||
+      record_bytes < 4 || (record_bytes & 3)) {
+    saru::set_last_error("saru_format_tsv_compact: invalid arguments");
+    return -1;
+  }
+  const int64_t n = b->n;
+  int nt = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+  nt = std::max(1, std::min(nt, 64));
+  if ((int64_t)nt * 64 > n) nt = (int)std::max<int64_t>(1, n / 64);
+  const Shape sh{b, scores, records, record_bytes};
+  NameTab tab{names, name_stride, n_names};
+  std::vector<std::string> text((size_t)nt);
+  std::vector<int32_t> df((size_t)nt, 0), dr((size_t)nt, 0);
+  std::vector<int> bad((size_t)nt, 0);
+  auto work = [&](int w) {
+    const int64_t lo = n * w / nt, hi = n * (w + 1) / nt;
+    if (lo >= hi) return;
+    int64_t s = lo;  // back to a slot whose read string holds a read byte
+    while (s > 0 && !sh.has_letter(s)) --s;
+    int64_t e = hi;  // on while the last slot has no NUL
+    while (e < n && sh.full(e - 1)) ++e;
+    const int64_t wlo = sh.slot_start(s), whi = sh.slot_start(e - 1) + sh.cap(e - 1);
+    std::vector<char> ra((size_t)(whi - wlo)), ga((size_t)(whi - wlo));
+    for (int64_t t = s; t < e; ++t) {
+      const int64_t at = sh.slot_start(t) - wlo;
+      const int64_t gs = t ? b->genome_offsets[t - 1] : 0;
+      const int64_t rs = t ? b->read_offsets[t - 1] : 0;
+      const int L = (int)(b->genome_offsets[t] - gs), m = (int)(b->read_offsets[t] - rs);
+      if (!sh.reported(t)) {
+        memset(&ra[(size_t)at], 0, (size_t)(L + b->k));
+        memset(&ga[(size_t)at], 0, (size_t)(L + b->k));
+      } else if (!expand_one(sh.rec(t), b->reads + rs, b->genome + gs, m, L, b->k,
+                             &ra[(size_t)at], &ga[(size_t)at])) {
+        bad[(size_t)w] = 1;
+        return;
+      }
+    }
+    saru::WriterCall wc{scores, ra.data(), ga.data(), b->total_slots, b->genome_offsets,
+                        genome_pos, b->dirs, read_ids, b->k, read_length, &table_name, &tab};
+    wc.window_lo = wlo;
+    wc.window_hi = whi;
+    saru::format_range(wc, lo, hi, &text[(size_t)w], &df[(size_t)w], &dr[(size_t)w]);
+  };
+  std::vector<std::thread> th;
+  for (int w = 1; w < nt; ++w) th.emplace_back(work, w);
+  work(0);
+  for (auto &x : th) x.join();
+  for (int v : bad)
+    if (v) {
+      saru::set_last_error("saru_format_tsv_compact: a record does not fit its candidate");
+      return -1;
+    }
+  int64_t total = 0, at = 0;
+  int32_t f = 0, r = 0;
+  for (int w = 0; w < nt; ++w) {
+    total += (int64_t)text[(size_t)w].size();
+    f += df[(size_t)w];
+    r += dr[(size_t)w];
+  }
+  if (out && cap > 0)
+    for (int w = 0; w < nt && at < cap; ++w) {
+      const int64_t len = std::min<int64_t>((int64_t)text[(size_t)w].size(), cap - at);
+      memcpy(out + at, text[(size_t)w].data(), (size_t)len);
+      at += len;
+    }
+  if (done_fwd) *done_fwd = f;
+  if (done_rev) *done_rev = r;
+  return total;
 }

@@ -34,17 +34,25 @@ static inline char *put_int(char *p, int v) {
   return p;
 }
 
+// Byte i of a slot array: 0 outside the call (the reference's memset
+// arena), a[i - lo] inside the window the caller holds.
 struct ByteView {
   const char *a;
-  int64_t n;
-  inline char operator[](int64_t i) const { return (i >= 0 && i < n) ? a[i] : 0; }
+  int64_t n, lo, hi;
+  inline char operator[](int64_t i) const {
+    return (i >= 0 && i < n && i >= lo && i < hi) ? a[i - lo] : 0;
+  }
 };
+
+static inline ByteView view(const WriterCall &w, const char *a) {
+  return ByteView{a, w.total_slots, w.window_lo, w.window_hi < 0 ? w.total_slots : w.window_hi};
+}
 
 // Computes the fields of candidate v's line.  Returns false if the
 // candidate prints nothing (score > k).
 bool line_fields(const WriterCall &w, int64_t v, LineFields *f) {
   if (w.scores[v] > w.k) return false;
-  const ByteView ra{w.read_aln, w.total_slots}, ga{w.genome_aln, w.total_slots};
+  const ByteView ra = view(w, w.read_aln), ga = view(w, w.genome_aln);
   unsigned short L;
   int64_t gs, eb = 0;
   if (v > 0) {
@@ -113,7 +121,7 @@ bool line_fields(const WriterCall &w, int64_t v, LineFields *f) {
 // Writes a line computed by line_fields; `out` has f.bytes of room.
 // Returns the bytes written.
 int64_t line_write(const WriterCall &w, const LineFields &f, char *out) {
-  const ByteView ra{w.read_aln, w.total_slots}, ga{w.genome_aln, w.total_slots};
+  const ByteView ra = view(w, w.read_aln), ga = view(w, w.genome_aln);
   char *p = out;
   memcpy(p, f.name, (size_t)f.name_len);
   p += f.name_len;

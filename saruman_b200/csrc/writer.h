@@ -20,6 +20,11 @@ struct WriterCall {
   int32_t read_length;
   const char *(*name_of)(void *ctx, int32_t id);
   void *name_ctx;
+  // read_aln/genome_aln hold slot bytes [window_lo, window_hi) of the call
+  // (window_hi < 0: the whole call, [0, total_slots)); the writer's scans
+  // never leave the window when it covers the slots they reach
+  int64_t window_lo = 0;
+  int64_t window_hi = -1;
 };
 
 struct LineFields {

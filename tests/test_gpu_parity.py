@@ -333,6 +333,7 @@ def _compact_roundtrip(b):
     S.align_device_compact(sb, sc.data_ptr(), rec.data_ptr(), R_, st.data_ptr(), scr.data_ptr(),
                            nscr)
     torch.cuda.synchronize()
+    _compact_roundtrip.last = (sc.cpu().numpy()[:b.n], rec.cpu().numpy(), R_)
     return int(st.item()), S.expand_compact(b, sc.cpu().numpy()[:b.n], rec.cpu().numpy(), R_)
 
 
@@ -346,6 +347,11 @@ def test_compact_records_rebuild_the_golden_slots(saru_lib, name):
         pytest.skip("fixture takes the exact path")
     assert st == 0
     check_equal(b, exp["scores"], exp["read_aln"], exp["genome_aln"], r)
+    # the reference's TSV straight from the device's records
+    sc, rec, rb = _compact_roundtrip.last
+    text, _, _ = S.format_tsv_compact(b, sc, rec, rb, S.name_table(G.names_by_id(b, names)),
+                                      read_length=m, nthreads=4)
+    assert text == exp["tsv"]
 
 
 @pytest.mark.parametrize("m,k", [(36, 3), (100, 5), (150, 9), (250, 15)])
