@@ -249,3 +249,53 @@ def test_compact_requests_expand_to_the_same_bytes(saru_lib):
             want = S.align_host(b)
             for r in reqs[3 * i:3 * i + 3]:
                 assert_same(r.result(0), want)
+
+
+def test_a_bad_request_fails_alone(saru_lib):
+    """A gather request with a candidate outside the genome ends with
+    SARU_E_INVALID; the requests around it, in the same launch groups,
+    still get saru_align_host's bytes."""
+    g = W.uniform_genome(200_000, seed=70)
+    good = [gather_case_on(g, 100, 5, 600, seed=71 + i) for i in range(4)]
+    table, bad = gather_case_on(g, 100, 5, 300, seed=90)
+    bad.pos = bad.pos.copy()
+    bad.pos[10] = len(g) - 20  # its window runs past the genome end
+    with S.Server(pipeline=True, max_requests_per_launch=8, budget_bytes=1 << 28) as srv:
+        srv.set_genome(g)
+        reqs = [S.GatherRequest([b], [t]) for t, b in good[:2]]
+        reqs.append(S.GatherRequest([bad], [table]))
+        reqs += [S.GatherRequest([b], [t]) for t, b in good[2:]]
+        tickets = [srv.submit(r) for r in reqs]
+        rcs = [srv.wait(t)[0] for t in tickets]
+    assert rcs == [S.SARU_OK, S.SARU_OK, S.SARU_E_INVALID, S.SARU_OK, S.SARU_OK]
+    for r, (t, b) in zip(reqs[:2] + reqs[3:], good):
+        assert_same(r.result(0), S.align_host(b))
+
+
+def test_concurrent_clients(saru_lib):
+    """Four client threads submit and wait on their own requests at once;
+    every request's bytes equal saru_align_host's."""
+    import threading
+    reqs = make_requests(32, seed=11)
+    want = [alone(calls) for calls in reqs]
+    hrs = [S.HostRequest(calls) for calls in reqs]
+    errors = []
+    with S.Server(pipeline=True, max_requests_per_launch=16, budget_bytes=1 << 29) as srv:
+        def client(c):
+            try:
+                mine = list(range(c, len(hrs), 4))
+                tickets = [srv.submit(hrs[q]) for q in mine]
+                for t in tickets:
+                    rc, _ = srv.wait(t)
+                    assert rc == S.SARU_OK
+            except Exception as e:  # surfaced in the main thread
+                errors.append(e)
+        th = [threading.Thread(target=client, args=(c,)) for c in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join(300)
+    assert not errors, errors
+    for h, w in zip(hrs, want):
+        for i in range(len(w)):
+            assert_same(h.result(i), w[i])
