@@ -809,6 +809,17 @@ def main() -> None:
         ce_ms = timed(stream, e2e_compact, e2e_steps, world, dist, dev)
         if int(status.item()) != 0:
             raise SystemExit(f"kernel status {int(status.item())} (compact)")
+        # the reference's TSV lines from the records, on the host cores
+        names = S.name_table([b"read%d" % i for i in range(int(b0.ids.max()) + 1)])
+        t0 = time.perf_counter()
+        tsv, nf, nr = S.format_tsv_compact(b0, d0.h_out[0][0].numpy(), h_rec.numpy(), rbytes,
+                                           names)
+        tsv_s = time.perf_counter() - t0
+        tsv_leg = {"value": n_cand / tsv_s, "unit": "alignments/s", "lines": nf + nr,
+                   "bytes": len(tsv), "seconds": tsv_s, "threads": os.cpu_count(),
+                   "what": "saru_format_tsv_compact on the host cores (host clock): the "
+                           "reference writer's lines straight from the records"}
+        del tsv
         compact = {"value": world * n_cand / (c_ms * 1e-3), "ms_per_step": c_ms,
                    "record_bytes": rbytes,
                    "e2e": {"value": world * n_cand / (ce_ms * 1e-3), "unit": "alignments/s",
@@ -816,7 +827,8 @@ def main() -> None:
                            "d2h_bytes_per_step": 4 * b0.n + b0.n * rbytes},
                    "what": "saru_align_device_compact: 2-bit traceback records per candidate "
                            "instead of the slot strings; saru_expand_compact rebuilds the "
-                           "slots on the host"}
+                           "slots on the host",
+                   "tsv": tsv_leg}
 
     if world > 1:
         dist.barrier()

@@ -17,6 +17,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <vector>
+
 #include "writer.h"
 
 namespace saru {
@@ -37,15 +39,23 @@ static inline char *put_int(char *p, int v) {
 // Byte i of a slot array: 0 outside the call (the reference's memset
 // arena), a[i - lo] inside the window the caller holds.
 struct ByteView {
-  const char *a;
-  int64_t n, lo, hi;
+  const char *a;  // byte lo
+  int64_t lo;
+  uint64_t len;   // the window clipped to the call: [lo, lo + len)
   inline char operator[](int64_t i) const {
-    return (i >= 0 && i < n && i >= lo && i < hi) ? a[i - lo] : 0;
+    return (uint64_t)(i - lo) < len ? a[i - lo] : 0;
   }
 };
 
 static inline ByteView view(const WriterCall &w, const char *a) {
-  return ByteView{a, w.total_slots, w.window_lo, w.window_hi < 0 ? w.total_slots : w.window_hi};
+  int64_t lo = w.window_lo, hi = w.window_hi < 0 ? w.total_slots : w.window_hi;
+  if (hi > w.total_slots) hi = w.total_slots;
+  const char *base = a;
+  if (lo < 0) {  // the call starts at 0: bytes before it read as 0
+    base -= lo;
+    lo = 0;
+  }
+  return ByteView{base, lo, (uint64_t)(hi > lo ? hi - lo : 0)};
 }
 
 // Computes the fields of candidate v's line.  Returns false if the
@@ -143,12 +153,12 @@ int64_t line_write(const WriterCall &w, const LineFields &f, char *out) {
 void format_range(const WriterCall &w, int64_t begin, int64_t end, std::string *out,
                   int32_t *done_fwd, int32_t *done_rev) {
   LineFields f;
+  std::vector<char> line;
   for (int64_t v = begin; v < end; ++v) {
     if (!line_fields(w, v, &f)) continue;
-    const size_t at = out->size();
-    out->resize(at + (size_t)f.bytes);
-    const int64_t n = line_write(w, f, &(*out)[at]);
-    out->resize(at + (size_t)n);
+    if ((int64_t)line.size() < f.bytes) line.resize((size_t)f.bytes * 2);
+    const int64_t n = line_write(w, f, line.data());
+    out->append(line.data(), (size_t)n);
     if (f.reverse) {
       if (done_rev) ++*done_rev;
     } else if (done_fwd) {
