@@ -1,0 +1,102 @@
+// filter_calls.h -- the reference's alignment calls from the filter's
+// per-read positions (host code).
+//
+// The reference keeps each read's positions in a result hash (reads in the
+// order they first keep a position), adds every kept position > 0 to an
+// alignment queue, and after each read, once the queue exceeds the chunk
+// value, submits one call (src/hash.c:840-850): every read of the hash in
+// order, every position > 0 whose window m + so + eo fits the genome
+// (src/hash.c:982), which it then negates so no later call repeats it.
+// Positions whose window does not fit stay positive and are skipped again
+// by every later call.  After the last read the rest goes out as a final
+// call (src/hash.c:462).  Perfect hits (flag 0, negative positions) are
+// printed by the filter itself and never aligned.
+#pragma once
+#include <stdint.h>
+
+#include <vector>
+
+#include "filter_core.cuh"
+
+namespace saru {
+
+struct FilterCalls {
+  std::vector<int64_t> call_begin;  // candidate index where each call starts (+ the end)
+  std::vector<int32_t> ids, pos;
+  std::vector<int8_t> dirs;
+  std::vector<int32_t> perfect_ids, perfect_pos;  // in print order; pos = start (0-based)
+};
+
+class CallAssembler {
+ public:
+  CallAssembler(int m, int k, int64_t genome_len, uint32_t chunk_value)
+      : m_(m), k_(k), glen_(genome_len), chunk_(chunk_value) {
+    out.call_begin.push_back(0);
+  }
+
+  // The read's kept positions, in the order the filter kept them.
+  void add_read(int32_t id, const int32_t *pos, const int8_t *flag, int n, int queue) {
+    if (n > 0) {
+      Entry e;
+      e.id = id;
+      e.pos.assign(pos, pos + n);
+      e.flag.assign(flag, flag + n);
+      for (int i = 0; i < n; ++i)
+        if (flag[i] == 0) {  // a perfect hit (kept only with a negative position)
+          out.perfect_ids.push_back(id);
+          out.perfect_pos.push_back(-pos[i]);
+        }
+      entries_.push_back(std::move(e));
+    }
+    queue_ += (uint32_t)queue;
+    if (queue_ > chunk_) flush();
+  }
+
+  void finish() {
+    if (queue_ > 0) flush();
+  }
+
+  FilterCalls out;
+
+ private:
+  struct Entry {
+    int32_t id;
+    std::vector<int32_t> pos;
+    std::vector<int8_t> flag;
+  };
+
+  void flush() {
+    const int64_t before = (int64_t)out.ids.size();
+    size_t keep = 0;
+    for (size_t e = 0; e < entries_.size(); ++e) {
+      Entry &E = entries_[e];
+      bool pending = false;
+      for (size_t i = 0; i < E.pos.size(); ++i) {
+        if (E.pos[i] <= 0) continue;
+        int so = 0, eo = 0;
+        flank_of(E.flag[i], k_, so, eo);
+        if ((int64_t)(uint32_t)E.pos[i] + m_ + so + eo > glen_) {
+          pending = true;  // stays positive: looked at again by later calls
+          continue;
+        }
+        out.ids.push_back(E.id);
+        out.pos.push_back(E.pos[i]);
+        out.dirs.push_back(E.flag[i]);
+        E.pos[i] = -E.pos[i];
+      }
+      // reads left with nothing positive can never contribute again
+      if (pending) entries_[keep++] = std::move(E);
+    }
+    entries_.resize(keep);
+    if ((int64_t)out.ids.size() > before) out.call_begin.push_back((int64_t)out.ids.size());
+    queue_ = 0;
+  }
+
+  int m_, k_;
+  int64_t glen_;
+  uint32_t chunk_;
+  uint32_t queue_ = 0;
+  std::vector<Entry> entries_;
+};
+
+}  // namespace saru

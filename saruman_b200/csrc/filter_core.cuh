@@ -1,0 +1,205 @@
+// filter_core.cuh -- the q-gram pair filter of one read (host and device).
+//
+// The reference's filter (src/hash.c:348-839) emits, per read and strand,
+// the genome positions the aligner is asked to check, with a flag that sets
+// the free gaps of the window (1/5: end gap, 2/6: start gap, 3/7: both).
+// Its candidate stream decides which alignments exist, their order inside a
+// call and, through the queue flushes, where calls begin (and with them the
+// first-of-call rule of the traceback), so it is restated here step by step:
+//
+//  * q-grams of the read at q-gram start positions qpos[0..P): the first
+//    half at 0, q, 2q, ...; the second at m - q, m - 2q, ... (src/saruman.c
+//    :46-75); their genome positions come from the q-gram index in genome
+//    order (src/util.c:462-480), laid out per read chunk as the reference's
+//    data array: each list, then a 0 (src/hash.c:404-457).  A position 0
+//    reads as the end of its list, as it does there.
+//  * for each first-half q-gram a and each of its positions: the read's
+//    start genome_start = pos - (a q + 1); a perfect match of the read at
+//    genome_start + 1 is recorded as a hit at -(genome_start + 1) (flag 0);
+//    then pairs with the later first-half q-grams (error zones -k..k; the
+//    scan of each pair's list starts at the index of a's current position,
+//    not at 0, exactly as the reference indexes it) and with every
+//    second-half q-gram (zones of half-width |half - 1 - b - a|); every pair
+//    found raises a counter, and the candidate is recorded when the counter
+//    reaches the threshold (src/hash.c:472-807).
+//  * recording (src/hash.c:43-176): a read's first position is kept; a later
+//    one is dropped if it lies within -k..k of a kept one (or of its negation)
+//    with a flag not above its own, replaces the flag of an equal position on
+//    the same strand with a lower one, is dropped on an equal position (or
+//    negation) on the same strand, else appended; every kept position > 0
+//    adds 1 to the alignment queue.
+// Comparisons follow the reference's unsigned 32-bit arithmetic.
+#pragma once
+#include <math.h>
+#include <stdint.h>
+
+#include "saru_core.cuh"
+
+namespace saru {
+
+constexpr int kFilterMaxQgrams = 64;
+
+struct FilterShape {
+  int m, k, q, P, half, rest, tresh;
+  int qpos[kFilterMaxQgrams];
+};
+
+// The filter's parameters for reads of length m with up to k errors, in
+// the reference's float arithmetic (src/saruman.c:46-75,119).  Returns
+// false if the q-gram layout does not fit (q < 1 or more than 64 q-grams).
+SARU_HD bool filter_shape(int m, int k, FilterShape *S) {
+  S->m = m;
+  S->k = k;
+  S->q = (int)ceilf((float)m / (float)(k + 1)) - 1;
+  if (S->q < 1) return false;
+  S->rest = m % S->q;
+  const int n1 = m / S->q;
+  S->P = S->rest ? 2 * n1 : n1;
+  if (S->P > kFilterMaxQgrams) return false;
+  S->half = S->P / 2;
+  int x = 0;
+  for (; x < n1; ++x) S->qpos[x] = x * S->q;
+  for (int z = 1; z <= n1 && x < S->P; ++z, ++x) S->qpos[x] = m - z * S->q;
+  S->tresh = (int)floorf((float)m / (float)S->q) - k + 1;
+  return true;
+}
+
+// Positions kept for one read, in the order the reference keeps them.
+struct ReadHits {
+  int32_t *pos;   // capacity cap
+  int8_t *flag;
+  int cap;
+  int n;          // kept positions
+  int queue;      // of them > 0 (the alignment queue increments)
+  int overflow;   // more than cap positions
+};
+
+// add_start_position (src/hash.c:43-176): 0 new, 1 dropped, 2 appended or
+// flag replaced.
+SARU_HD int filter_record(ReadHits &h, int k, int tresh, int start, int flag, int possible) {
+  if (possible != tresh) return 1;
+  const int dir = flag > 3 ? 1 : 0;
+  if (h.n == 0) {
+    if (h.cap < 1) {
+      h.overflow = 1;
+      return 1;
+    }
+    h.pos[0] = start;
+    h.flag[0] = (int8_t)flag;
+    h.n = 1;
+    if (start > 0) ++h.queue;
+    return 0;
+  }
+  for (int c = 0; c < h.n; ++c) {
+    const int pc = h.pos[c], fc = h.flag[c];
+    const int dc = fc > 3 ? 1 : 0;
+    for (int i = -k; i <= k; ++i)
+      if ((start + i == pc || start + i == -pc) && fc <= flag) return 1;
+    if (pc == start && dc == dir && fc > flag) {
+      h.flag[c] = (int8_t)flag;
+      return 2;
+    }
+    if ((pc == start && dc == dir) || (pc == -start && dc == dir)) return 1;
+  }
+  if (h.n >= h.cap) {
+    h.overflow = 1;
+    return 1;
+  }
+  h.pos[h.n] = start;
+  h.flag[h.n] = (int8_t)flag;
+  ++h.n;
+  if (start > 0) ++h.queue;
+  return 2;
+}
+
+// One read (read bytes as sequenced; reversed and complemented here when
+// dr == 4).  val(x, i): element i of the data array from the start of this
+// read's list for q-gram x (past the list: its 0, then what follows).
+// perfect(gs1): the genome at gs1 (0-based) spells the read (strand-adjusted)
+// over m bytes.
+template <class Val, class Perfect>
+SARU_HD void filter_read(const FilterShape &S, int dr, Val val, Perfect perfect, ReadHits &h) {
+  const int k = S.k, half = S.half, q = S.q;
+  for (int a = 0; a < half; ++a) {
+    const int first = a == 0 ? 1 : 0;
+    const uint32_t in_read = (uint32_t)a * q + 1;
+    uint32_t off = 0;
+    uint32_t pa = val(a, off);
+    while (pa > 0) {
+      const int gs = (int)(pa - in_read);
+      if (gs + 1 > 0) {
+        if (perfect(gs + 1)) filter_record(h, k, S.tresh, -(gs + 1), 0, S.tresh);
+        int possible = 1;
+        // pairs with the later first-half q-grams
+        for (int b = a + 1; b < half; ++b) {
+          const uint32_t rs = (uint32_t)b * q + 1;
+          for (int ez = -k; ez <= k; ++ez) {
+            const uint32_t want = (uint32_t)gs + rs + (uint32_t)ez;
+            uint32_t v = val(b, off);  // the reference starts this scan at a's index
+            uint32_t vo = 0;
+            while (v > 0) {
+              if (v == want) {
+                int flag, start;
+                if (b == half - 1 && first) {
+                  flag = 1 + dr;
+                  start = gs + 1;
+                } else if (a == half - 1) {
+                  flag = ((int)(pa + q) > S.m ? 3 : 2) + dr;
+                  start = gs - k + 1;
+                } else if (first) {
+                  flag = 1 + dr;
+                  start = gs + 1;
+                } else {
+                  flag = 3 + dr;
+                  start = gs - k + 1;
+                }
+                ++possible;
+                filter_record(h, k, S.tresh, start, flag, possible);
+              }
+              ++vo;
+              v = val(b, vo);
+            }
+          }
+        }
+        // pairs with the second-half q-grams
+        for (int b = 0; b < half; ++b) {
+          int lim = half - 1 - b - a;
+          if (lim < 0) lim = -lim;
+          const uint32_t ns = (uint32_t)(half - b - 1) * q + 1 + S.rest;
+          for (int err = -lim; err <= lim; ++err) {
+            const int ae = (b - a < 0) ? -err : err;
+            const uint32_t want = (uint32_t)gs + ns + (uint32_t)ae;
+            uint32_t so = 0;
+            uint32_t v = val(half + b, so);
+            while (v > 0) {
+              if (v == want) {
+                int flag, start;
+                if (b == 0 && first) {
+                  flag = 1 + dr;
+                  start = gs + 1;
+                } else if (b == 0) {
+                  flag = ((int)(ns + q) > S.m ? 3 : 2) + dr;
+                  start = gs - k + 1;
+                } else if (first) {
+                  flag = 1 + dr;
+                  start = gs + 1;
+                } else {
+                  flag = 3 + dr;
+                  start = gs - k + 1;
+                }
+                ++possible;
+                filter_record(h, k, S.tresh, start, flag, possible);
+              }
+              ++so;
+              v = val(half + b, so);
+            }
+          }
+        }
+      }
+      ++off;
+      pa = val(a, off);
+    }
+  }
+}
+
+}  // namespace saru
