@@ -248,6 +248,35 @@ int64_t saru_format_tsv_compact(const saru_batch *batch, const int32_t *scores,
                                 int32_t n_names, char *out, int64_t cap, int32_t *done_fwd,
                                 int32_t *done_rev, int32_t nthreads);
 
+/* ---- candidate generation on the device (no counterpart in the reference,
+ * whose filter runs on the host: src/hash.c:348-839) ---------------------------
+ * The reference's q-gram pair filter for one strand and one batch of reads
+ * (the reads it loads at a time, its -c option; read ids count from 0 in
+ * each batch), one thread per read, against a q-gram index of the genome
+ * held on the device.  The kept positions are assembled into exactly the
+ * calls the reference would submit: read ids, positions, flags and call
+ * boundaries, set by chunk_value (its -s option: the queue threshold, which
+ * is also the number of reads per chunk of its data array).  Perfect hits,
+ * which the reference prints from the filter, come back as (read id,
+ * 0-based start).  The genome must be one chunk (the reference's -G at
+ * least its length). */
+typedef struct saru_filter saru_filter;
+saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t read_length,
+                                int32_t k, int32_t device);
+/* reads: nreads x read_length bytes (host), as the reference reads them.
+ * counts[0..2] = calls, candidates, perfect hits.  SARU_E_OVERFLOW if a read
+ * keeps more than 4096 positions on one strand. */
+int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t do_reverse,
+                    uint32_t chunk_value, int64_t *counts);
+/* The last run's calls: call_begin (calls + 1 entries), ids, pos, dirs
+ * (candidates), perfect_ids, perfect_pos (perfect hits); NULL skips one. */
+int saru_filter_results(const saru_filter *f, int64_t *call_begin, int32_t *ids, int32_t *pos,
+                        int8_t *dirs, int32_t *perfect_ids, int32_t *perfect_pos);
+/* Device time of the last run's filter (ms), and the resident genome (device). */
+double saru_filter_last_ms(const saru_filter *f);
+const char *saru_filter_genome(const saru_filter *f);
+void saru_filter_destroy(saru_filter *f);
+
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 

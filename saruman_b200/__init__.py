@@ -37,7 +37,9 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_tuning_set", "saru_tuning_get", "saru_tuning_clear",
                  "saru_mlp_param_count", "saru_mlp_work_floats", "saru_mlp_forward",
                  "saru_mlp_loss_grad", "saru_mlp_adam_step", "saru_compact_record_bytes",
-                 "saru_align_device_compact", "saru_expand_compact", "saru_format_tsv_compact")
+                 "saru_align_device_compact", "saru_expand_compact", "saru_format_tsv_compact",
+                 "saru_filter_create", "saru_filter_run", "saru_filter_results",
+                 "saru_filter_last_ms", "saru_filter_genome", "saru_filter_destroy")
 ABI_DATA = ("alignment_time",)
 
 
@@ -171,6 +173,19 @@ def load(path: str | Path | None = None):
                                             C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                             C.c_int64, C.POINTER(C.c_int32),
                                             C.POINTER(C.c_int32), C.c_int32]
+    lib.saru_filter_create.restype = C.c_void_p
+    lib.saru_filter_create.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32]
+    lib.saru_filter_run.restype = C.c_int
+    lib.saru_filter_run.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_uint32,
+                                    C.c_void_p]
+    lib.saru_filter_results.restype = C.c_int
+    lib.saru_filter_results.argtypes = [C.c_void_p] + [C.c_void_p] * 6
+    lib.saru_filter_last_ms.restype = C.c_double
+    lib.saru_filter_last_ms.argtypes = [C.c_void_p]
+    lib.saru_filter_genome.restype = C.c_void_p
+    lib.saru_filter_genome.argtypes = [C.c_void_p]
+    lib.saru_filter_destroy.restype = None
+    lib.saru_filter_destroy.argtypes = [C.c_void_p]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -523,3 +538,75 @@ def format_tsv_compact(b: Batch, scores: np.ndarray, records: np.ndarray, record
                                     rl, _p(names), names.shape[1], names.shape[0], _p(buf), need,
                                     C.byref(df), C.byref(dr), nthreads)
     return buf[:need].tobytes(), df.value, dr.value
+
+
+@dataclasses.dataclass
+class FilterCalls:
+    """One strand's calls as the reference would submit them: call c holds
+    candidates call_begin[c]..call_begin[c+1] (ids, pos, dirs); perfect hits
+    (read id, 0-based start) are printed by the filter, not aligned."""
+    call_begin: np.ndarray
+    ids: np.ndarray
+    pos: np.ndarray
+    dirs: np.ndarray
+    perfect_ids: np.ndarray
+    perfect_pos: np.ndarray
+    ms: float
+
+    def call(self, genome: np.ndarray, reads: np.ndarray, m: int, k: int, c: int) -> Batch:
+        """Call c in the reference's call layout (windows cut from the genome,
+        reads reverse-complemented for flags 4-7)."""
+        from .workloads import flank, make_batch, reverse_complement
+        lo, hi = int(self.call_begin[c]), int(self.call_begin[c + 1])
+        ids, pos, dirs = self.ids[lo:hi], self.pos[lo:hi], self.dirs[lo:hi]
+        wins = []
+        for p, d in zip(pos, dirs):
+            so, eo = flank(int(d), k)
+            wins.append(genome[int(p):int(p) + m + so + eo])
+        rd = reads[ids].copy()
+        rev = dirs > 3
+        if rev.any():
+            rd[rev] = reverse_complement(rd[rev])
+        return make_batch(m, k, wins, rd, dirs, ids=ids, pos=pos)
+
+
+class Filter:
+    """The reference's q-gram pair filter on the device (saru_filter_*)."""
+
+    def __init__(self, genome: np.ndarray, m: int, k: int, device: int = 0):
+        self._lib = load()
+        g = np.ascontiguousarray(genome, np.uint8)
+        self.m, self.k = m, k
+        self._h = self._lib.saru_filter_create(_p(g), g.size, m, k, device)
+        if not self._h:
+            raise SaruError(SARU_E_INVALID, last_error())
+
+    def run(self, reads: np.ndarray, do_reverse: int, chunk_value: int) -> FilterCalls:
+        """One batch of reads (ids from 0), one strand (do_reverse 0 or 4)."""
+        r = np.ascontiguousarray(reads, np.uint8).reshape(-1)
+        n = r.size // self.m
+        cnt = np.zeros(3, np.int64)
+        rc = self._lib.saru_filter_run(self._h, _p(r) if r.size else 0, n, do_reverse,
+                                       chunk_value, _p(cnt))
+        if rc != SARU_OK:
+            raise SaruError(rc, last_error())
+        nc, na, npf = (int(x) for x in cnt)
+        out = FilterCalls(np.zeros(nc + 1, np.int64), np.zeros(na, np.int32),
+                          np.zeros(na, np.int32), np.zeros(na, np.int8),
+                          np.zeros(npf, np.int32), np.zeros(npf, np.int32),
+                          float(self._lib.saru_filter_last_ms(self._h)))
+        self._lib.saru_filter_results(self._h, *[_p(a) if a.size else 0 for a in
+                                                 (out.call_begin, out.ids, out.pos, out.dirs,
+                                                  out.perfect_ids, out.perfect_pos)])
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.saru_filter_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,509 @@
+// filter.cu -- the q-gram pair filter on the device.
+//
+//  index    every q-gram of the resident genome, hashed (64-bit FNV-1a of its
+//           bytes) and sorted with its position (a stable radix sort keeps
+//           each q-gram's positions in genome order, as the reference's
+//           index lists them, src/util.c:462-480); equal hashes of unequal
+//           q-grams are reported, not trusted.
+//  lookup   one thread per (read, q-gram): the q-gram of the strand-adjusted
+//           read, its run in the sorted index (checked against the genome
+//           bytes) and, by an exclusive scan per read chunk, its list's
+//           offset in the reference's data array (lists in q-gram order per
+//           read, each followed by a 0, src/hash.c:404-457).
+//  filter   one thread per read: filter_read (filter_core.cuh) over that
+//           layout, the read's kept positions into its slice of a scratch.
+//  calls    the kept positions, packed, copied back and assembled into the
+//           reference's calls on the host (filter_calls.h).
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/saruman_b200.h"
+#include "filter_calls.h"
+#include "filter_core.cuh"
+#include "server_internal.h"
+
+namespace {
+
+using namespace saru;
+
+constexpr int kHitsPerRead = 4096;   // kept positions per read and strand
+constexpr int kReadsPerLaunch = 1 << 16;
+
+__host__ __device__ inline uint64_t qgram_hash(const uint8_t *p, int q) {
+  uint64_t h = 1469598103934665603ull;  // FNV-1a 64
+  for (int i = 0; i < q; ++i) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+__device__ inline uint8_t comp_byte(uint8_t c) {
+  switch (c) {
+    case 'A': return 'T';
+    case 'C': return 'G';
+    case 'G': return 'C';
+    case 'T': return 'A';
+    default: return c;
+  }
+}
+
+__global__ void k_qgram_hash(const uint8_t *g, long npos, int q, uint64_t *hash, uint32_t *pos) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npos;
+       p += (long)gridDim.x * blockDim.x) {
+    hash[p] = qgram_hash(g + p, q);
+    pos[p] = (uint32_t)p;
+  }
+}
+
+__global__ void k_index_check(const uint64_t *hash, const uint32_t *pos, long n, const uint8_t *g,
+                              int q, int *flag) {
+  for (long i = 1 + blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    if (hash[i] != hash[i - 1]) continue;
+    const uint8_t *a = g + pos[i], *b = g + pos[i - 1];
+    for (int j = 0; j < q; ++j)
+      if (a[j] != b[j]) {
+        atomicOr(flag, 1);
+        break;
+      }
+  }
+}
+
+// byte i of the read as its strand aligns it (reverse complement for dr 4)
+__device__ inline uint8_t strand_byte(const uint8_t *read, int m, int dr, int i) {
+  return dr == 4 ? comp_byte(read[m - 1 - i]) : read[i];
+}
+
+struct LookupArgs {
+  const uint8_t *reads;  // nreads x m, as sequenced
+  long nreads;
+  int dr;
+  FilterShape S;
+  const uint8_t *genome;
+  const uint64_t *hash;
+  const uint32_t *pos;
+  long nidx;
+  long *lo;       // nreads x P: first index of the q-gram's run
+  long *count;    // nreads x P: list length + 1 (its terminating 0)
+};
+
+__global__ void k_lookup(LookupArgs a) {
+  const long total = a.nreads * a.S.P;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    const long r = t / a.S.P;
+    const int x = (int)(t % a.S.P);
+    const uint8_t *rd = a.reads + r * a.S.m;
+    uint8_t key[kFilterMaxQgrams * 4];
+    const int q = a.S.q;
+    uint64_t h = 1469598103934665603ull;
+    for (int i = 0; i < q; ++i) {
+      key[i] = strand_byte(rd, a.S.m, a.dr, a.S.qpos[x] + i);
+      h ^= key[i];
+      h *= 1099511628211ull;
+    }
+    long l = 0, u = a.nidx;  // first index with hash >= h
+    while (l < u) {
+      const long mid = (l + u) >> 1;
+      if (a.hash[mid] < h) l = mid + 1;
+      else u = mid;
+    }
+    long e = l, u2 = a.nidx;  // first index with hash > h
+    while (e < u2) {
+      const long mid = (e + u2) >> 1;
+      if (a.hash[mid] <= h) e = mid + 1;
+      else u2 = mid;
+    }
+    long len = e - l;
+    if (len > 0) {  // a hash shared with another q-gram: no list
+      const uint8_t *gq = a.genome + a.pos[l];
+      for (int i = 0; i < q; ++i)
+        if (gq[i] != key[i]) {
+          len = 0;
+          break;
+        }
+    }
+    a.lo[t] = l;
+    a.count[t] = len + 1;
+  }
+}
+
+struct FilterArgs {
+  const uint8_t *reads;
+  long r0, r1;      // reads of this launch
+  long chunk;       // reads per chunk of the reference's data array (its chunk value)
+  long nreads;
+  int dr;
+  FilterShape S;
+  const uint8_t *genome;
+  long glen;
+  const uint32_t *pos;
+  const long *lo, *count, *offs;  // per (read, q-gram); offs: exclusive scan of count
+  int32_t *hit_pos;               // (r1 - r0) x kHitsPerRead
+  int8_t *hit_flag;
+  int32_t *n, *queue;             // per read of the launch
+  int *status;
+};
+
+__global__ void __launch_bounds__(128) k_filter(FilterArgs a) {
+  const long r = a.r0 + blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (r >= a.r1) return;
+  const int P = a.S.P;
+  const long base = r * P;
+  // the data array of the read's chunk ends at cend (flattened offsets)
+  const long c0 = (r / a.chunk) * a.chunk, c1 = min(c0 + a.chunk, a.nreads);
+  const long cend = a.offs[c1 * P - 1] + a.count[c1 * P - 1];
+  struct Lists {
+    const FilterArgs *a;
+    long base, c0, c1, cend;
+    int P;
+    __device__ uint32_t len(int x) const { return (uint32_t)(a->count[base + x] - 1); }
+    __device__ uint32_t at(int x, uint32_t i) const {
+      const long t = base + x;
+      const long cnt = a->count[t];
+      if ((long)i + 1 < cnt) return a->pos[a->lo[t] + i];
+      if ((long)i + 1 == cnt) return 0u;
+      const long j = a->offs[t] + (long)i;  // past the list: what follows it
+      if (j >= cend) return 0u;
+      long l = c0 * P, u = c1 * P - 1;  // last list starting at or before j
+      while (l < u) {
+        const long mid = (l + u + 1) >> 1;
+        if (a->offs[mid] <= j) l = mid;
+        else u = mid - 1;
+      }
+      const long w = j - a->offs[l];
+      return w + 1 < a->count[l] ? a->pos[a->lo[l] + w] : 0u;
+    }
+    __device__ int find(int x, uint32_t from, uint32_t want) const {
+      const long t = base + x;
+      long l = a->lo[t] + from, u = a->lo[t] + a->count[t] - 1;  // ascending positions
+      while (l < u) {
+        const long mid = (l + u) >> 1;
+        if (a->pos[mid] < want) l = mid + 1;
+        else u = mid;
+      }
+      return (l < a->lo[t] + a->count[t] - 1 && a->pos[l] == want) ? (int)(l - a->lo[t]) : -1;
+    }
+  } lists{&a, base, c0, c1, cend, P};
+  const uint8_t *rd = a.reads + r * a.S.m;
+  const int m = a.S.m, dr = a.dr;
+  auto perfect = [&](int g1) {
+    if ((long)g1 + m > a.glen) return false;
+    for (int i = 0; i < m; ++i)
+      if (a.genome[g1 + i] != strand_byte(rd, m, dr, i)) return false;
+    return true;
+  };
+  const long lr = r - a.r0;
+  ReadHits h{a.hit_pos + lr * kHitsPerRead, a.hit_flag + lr * kHitsPerRead, kHitsPerRead, 0, 0,
+             0};
+  filter_read(a.S, dr, lists, perfect, h);
+  a.n[lr] = h.n;
+  a.queue[lr] = h.queue;
+  if (h.overflow) atomicOr(a.status, 1);
+}
+
+__global__ void k_pack(const int32_t *hit_pos, const int8_t *hit_flag, const int32_t *n,
+                       const long *at, long nr, int32_t *out_pos, int8_t *out_flag) {
+  for (long r = blockIdx.x; r < nr; r += gridDim.x)
+    for (int i = threadIdx.x; i < n[r]; i += blockDim.x) {
+      out_pos[at[r] + i] = hit_pos[r * kHitsPerRead + i];
+      out_flag[at[r] + i] = hit_flag[r * kHitsPerRead + i];
+    }
+}
+
+__global__ void k_widen(const int32_t *n, long nr, long *out) {
+  for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < nr;
+       r += (long)gridDim.x * blockDim.x)
+    out[r] = n[r];
+}
+
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t count) {
+    if (count <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    const cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 64);
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace
+
+struct saru_filter {
+  int device = 0, m = 0, k = 0;
+  FilterShape S{};
+  long glen = 0, nidx = 0;
+  cudaStream_t s = nullptr;
+  DBuf<uint8_t> genome, reads, temp;
+  DBuf<uint64_t> hash, hash_s;
+  DBuf<uint32_t> pos, pos_s;
+  DBuf<long> lo, count, offs, at, nwide;
+  DBuf<int32_t> hit_pos, n, queue, packed_pos;
+  DBuf<int8_t> hit_flag, packed_flag;
+  DBuf<int> status;
+  FilterCalls calls;
+  float last_ms = 0.f;
+};
+
+namespace {
+
+int fail(const char *what, cudaError_t e) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+  saru::set_last_error(msg.c_str());
+  return SARU_E_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t read_length,
+                                int32_t k, int32_t device) {
+  saru::set_last_error("");
+  auto *f = new saru_filter();
+  f->device = device;
+  f->m = read_length;
+  f->k = k;
+  f->glen = genome_len;
+  if (!genome || genome_len < 1 || read_length < 2 || k < 0 ||
+      !filter_shape(read_length, k, &f->S) || f->S.q > 4 * kFilterMaxQgrams) {
+    saru::set_last_error("saru_filter_create: a genome, read_length >= 2, k >= 0 and a q-gram "
+                         "layout of at most 64 q-grams");
+    delete f;
+    return nullptr;
+  }
+  const int q = f->S.q;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->s, cudaStreamNonBlocking);
+  f->nidx = genome_len >= q ? genome_len - q + 1 : 0;
+  const long n = f->nidx;
+  if (e == cudaSuccess) e = f->genome.ensure((size_t)genome_len);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(f->genome.p, genome, (size_t)genome_len, cudaMemcpyHostToDevice, f->s);
+  if (e == cudaSuccess && n > 0) {
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t *)nullptr, (uint64_t *)nullptr,
+                                    (uint32_t *)nullptr, (uint32_t *)nullptr, (int)n, 0, 64,
+                                    f->s);
+    if ((e = f->hash.ensure(n)) == cudaSuccess && (e = f->hash_s.ensure(n)) == cudaSuccess &&
+        (e = f->pos.ensure(n)) == cudaSuccess && (e = f->pos_s.ensure(n)) == cudaSuccess &&
+        (e = f->temp.ensure(tb)) == cudaSuccess && (e = f->status.ensure(1)) == cudaSuccess) {
+      k_qgram_hash<<<1184, 256, 0, f->s>>>(f->genome.p, n, q, f->hash.p, f->pos.p);
+      e = cudaGetLastError();
+      if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(f->temp.p, tb, f->hash.p, f->hash_s.p, f->pos.p,
+                                            f->pos_s.p, (int)n, 0, 64, f->s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(f->status.p, 0, sizeof(int), f->s);
+      if (e == cudaSuccess) {
+        k_index_check<<<1184, 256, 0, f->s>>>(f->hash_s.p, f->pos_s.p, n, f->genome.p, q,
+                                              f->status.p);
+        e = cudaGetLastError();
+      }
+      int flag = 0;
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&flag, f->status.p, sizeof(int), cudaMemcpyDeviceToHost, f->s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
+      if (e == cudaSuccess && flag) {
+        saru::set_last_error("saru_filter_create: two different q-grams share a 64-bit hash");
+        saru_filter_destroy(f);
+        return nullptr;
+      }
+      f->hash.release();
+      f->pos.release();
+    }
+  }
+  if (e != cudaSuccess) {
+    fail("saru_filter_create", e);
+    saru_filter_destroy(f);
+    return nullptr;
+  }
+  saru::count_launch();
+  return f;
+}
+
+int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t do_reverse,
+                    uint32_t chunk_value, int64_t *counts) {
+  saru::set_last_error("");
+  if (!f || !counts || nreads < 0 || (nreads > 0 && !reads) || chunk_value < 1 ||
+      (do_reverse != 0 && do_reverse != 4)) {
+    saru::set_last_error("saru_filter_run: reads, chunk_value >= 1, do_reverse 0 or 4");
+    return SARU_E_INVALID;
+  }
+  const long read_chunk = (long)chunk_value;  // the data array's chunk of reads
+  cudaSetDevice(f->device);
+  const FilterShape &S = f->S;
+  const long nr = nreads, P = S.P, m = f->m;
+  CallAssembler asmb(f->m, f->k, f->glen, chunk_value);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaError_t e = cudaSuccess;
+  int rc = SARU_OK;
+  float ms = 0.f;
+  if (nr > 0) {
+    const long lists = nr * P;
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, (long *)nullptr, (long *)nullptr, (int)lists,
+                                  f->s);
+    size_t tb2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb2, (long *)nullptr, (long *)nullptr,
+                                  (int)kReadsPerLaunch, f->s);
+    const long batch = std::min<long>(nr, kReadsPerLaunch);
+    if ((e = f->reads.ensure((size_t)(nr * m))) != cudaSuccess ||
+        (e = f->lo.ensure(lists)) != cudaSuccess || (e = f->count.ensure(lists)) != cudaSuccess ||
+        (e = f->offs.ensure(lists)) != cudaSuccess ||
+        (e = f->temp.ensure(std::max(tb, tb2))) != cudaSuccess ||
+        (e = f->hit_pos.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
+        (e = f->hit_flag.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
+        (e = f->n.ensure(batch)) != cudaSuccess || (e = f->queue.ensure(batch)) != cudaSuccess ||
+        (e = f->at.ensure(batch)) != cudaSuccess || (e = f->nwide.ensure(batch)) != cudaSuccess ||
+        (e = f->status.ensure(1)) != cudaSuccess)
+      return fail("saru_filter_run", e);
+    cudaEventRecord(e0, f->s);
+    e = cudaMemcpyAsync(f->reads.p, reads, (size_t)(nr * m), cudaMemcpyHostToDevice, f->s);
+    LookupArgs la{f->reads.p, nr, do_reverse, S, f->genome.p, f->hash_s.p, f->pos_s.p,
+                  f->nidx, f->lo.p, f->count.p};
+    if (e == cudaSuccess) {
+      k_lookup<<<(unsigned)std::min<long>((lists + 255) / 256, 65535), 256, 0, f->s>>>(la);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cub::DeviceScan::ExclusiveSum(f->temp.p, tb, f->count.p, f->offs.p, (int)lists, f->s);
+    // one scan over all reads: each chunk's lists stay contiguous, and the
+    // filter bounds its look past a list by its chunk's end
+    std::vector<int32_t> hn, hq;
+    std::vector<long> hat;
+    std::vector<int32_t> hpos;
+    std::vector<int8_t> hflag;
+    if (e == cudaSuccess) e = cudaMemsetAsync(f->status.p, 0, sizeof(int), f->s);
+    for (long r0 = 0; r0 < nr && e == cudaSuccess; r0 += batch) {
+      const long r1 = std::min(nr, r0 + batch), cnt = r1 - r0;
+      FilterArgs fa{f->reads.p, r0, r1, read_chunk, nr, do_reverse, S, f->genome.p,
+                    f->glen, f->pos_s.p, f->lo.p, f->count.p, f->offs.p, f->hit_pos.p,
+                    f->hit_flag.p, f->n.p, f->queue.p, f->status.p};
+      k_filter<<<(unsigned)((cnt + 127) / 128), 128, 0, f->s>>>(fa);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) break;
+      k_widen<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->n.p, cnt, f->nwide.p);
+      e = cub::DeviceScan::ExclusiveSum(f->temp.p, tb2, f->nwide.p, f->at.p, (int)cnt, f->s);
+      hn.resize((size_t)cnt);
+      hq.resize((size_t)cnt);
+      hat.resize((size_t)cnt);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hn.data(), f->n.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hq.data(), f->queue.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
+      if (e != cudaSuccess) break;
+      long total = 0;
+      for (long i = 0; i < cnt; ++i) total += hn[(size_t)i];
+      if ((e = f->packed_pos.ensure((size_t)total + 1)) != cudaSuccess ||
+          (e = f->packed_flag.ensure((size_t)total + 1)) != cudaSuccess)
+        break;
+      k_pack<<<(unsigned)std::min<long>(cnt, 65535), 128, 0, f->s>>>(
+          f->hit_pos.p, f->hit_flag.p, f->n.p, f->at.p, cnt, f->packed_pos.p, f->packed_flag.p);
+      e = cudaGetLastError();
+      hpos.resize((size_t)total + 1);
+      hflag.resize((size_t)total + 1);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hpos.data(), f->packed_pos.p, 4 * (size_t)total,
+                            cudaMemcpyDeviceToHost, f->s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hflag.data(), f->packed_flag.p, (size_t)total,
+                            cudaMemcpyDeviceToHost, f->s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
+      if (e != cudaSuccess) break;
+      long at = 0;
+      for (long i = 0; i < cnt; ++i) {
+        asmb.add_read((int32_t)(r0 + i), hpos.data() + at, hflag.data() + at, hn[(size_t)i],
+                      hq[(size_t)i]);
+        at += hn[(size_t)i];
+      }
+      saru::count_launch();
+    }
+    int flag = 0;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&flag, f->status.p, sizeof(int), cudaMemcpyDeviceToHost, f->s);
+    cudaEventRecord(e1, f->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
+    if (e != cudaSuccess) rc = fail("saru_filter_run", e);
+    else if (flag) {
+      saru::set_last_error("saru_filter_run: a read kept more positions than the filter holds");
+      rc = SARU_E_OVERFLOW;
+    }
+    if (rc == SARU_OK) cudaEventElapsedTime(&ms, e0, e1);
+  }
+  asmb.finish();
+  f->calls = std::move(asmb.out);
+  f->last_ms = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  counts[0] = (int64_t)f->calls.call_begin.size() - 1;
+  counts[1] = (int64_t)f->calls.ids.size();
+  counts[2] = (int64_t)f->calls.perfect_ids.size();
+  return rc;
+}
+
+int saru_filter_results(const saru_filter *f, int64_t *call_begin, int32_t *ids, int32_t *pos,
+                        int8_t *dirs, int32_t *perfect_ids, int32_t *perfect_pos) {
+  if (!f) return SARU_E_INVALID;
+  const FilterCalls &c = f->calls;
+  if (call_begin) memcpy(call_begin, c.call_begin.data(), c.call_begin.size() * 8);
+  if (ids) memcpy(ids, c.ids.data(), c.ids.size() * 4);
+  if (pos) memcpy(pos, c.pos.data(), c.pos.size() * 4);
+  if (dirs) memcpy(dirs, c.dirs.data(), c.dirs.size());
+  if (perfect_ids) memcpy(perfect_ids, c.perfect_ids.data(), c.perfect_ids.size() * 4);
+  if (perfect_pos) memcpy(perfect_pos, c.perfect_pos.data(), c.perfect_pos.size() * 4);
+  return SARU_OK;
+}
+
+double saru_filter_last_ms(const saru_filter *f) { return f ? f->last_ms : -1.0; }
+
+const char *saru_filter_genome(const saru_filter *f) {
+  return f ? reinterpret_cast<const char *>(f->genome.p) : nullptr;
+}
+
+void saru_filter_destroy(saru_filter *f) {
+  if (!f) return;
+  cudaSetDevice(f->device);
+  if (f->s) cudaStreamSynchronize(f->s);
+  f->genome.release();
+  f->reads.release();
+  f->temp.release();
+  f->hash.release();
+  f->hash_s.release();
+  f->pos.release();
+  f->pos_s.release();
+  f->lo.release();
+  f->count.release();
+  f->offs.release();
+  f->at.release();
+  f->nwide.release();
+  f->hit_pos.release();
+  f->n.release();
+  f->queue.release();
+  f->packed_pos.release();
+  f->hit_flag.release();
+  f->packed_flag.release();
+  f->status.release();
+  if (f->s) cudaStreamDestroy(f->s);
+  delete f;
+}
+
+}  // extern "C"

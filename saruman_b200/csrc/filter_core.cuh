@@ -112,52 +112,77 @@ SARU_HD int filter_record(ReadHits &h, int k, int tresh, int start, int flag, in
   return 2;
 }
 
+// Matches of `want` among the values a scan of the reference visits, in
+// visit order (at most two: the scan's first element can come round again).
+//  first pass, list b from index `off`: the value at off, then indices
+//    1, 2, ... up to the first 0 -- for a non-empty list, indices 1..len-1 of
+//    the list itself (ascending, so one binary search), for an empty one the
+//    lists that follow it, walked as the reference walks them;
+//  second pass, list from index 0: indices 0..len-1 unless the value at 0 is
+//    0 (an empty list, or a first position 0).
+// Lists: len(x), at(x, i) (element i of the data array from list x's start,
+// past the list included), find(x, lo, want) (an index in [lo, len(x)) of
+// list x holding want, or -1).
+template <class Lists>
+SARU_HD int scan_from(const Lists &L, int x, uint32_t off, uint32_t want) {
+  const uint32_t v0 = L.at(x, off);
+  if (v0 == 0) return 0;
+  int hits = v0 == want ? 1 : 0;
+  const uint32_t len = L.len(x);
+  if (len >= 1) return hits + (L.find(x, 1, want) >= 0 ? 1 : 0);
+  for (uint32_t i = 1;; ++i) {  // an empty list: the walk runs into the next lists
+    const uint32_t v = L.at(x, i);
+    if (v == 0) return hits;
+    if (v == want) ++hits;
+  }
+}
+
+template <class Lists>
+SARU_HD int scan_all(const Lists &L, int x, uint32_t want) {
+  if (L.at(x, 0) == 0) return 0;
+  return L.find(x, 0, want) >= 0 ? 1 : 0;
+}
+
 // One read (read bytes as sequenced; reversed and complemented here when
-// dr == 4).  val(x, i): element i of the data array from the start of this
-// read's list for q-gram x (past the list: its 0, then what follows).
-// perfect(gs1): the genome at gs1 (0-based) spells the read (strand-adjusted)
-// over m bytes.
-template <class Val, class Perfect>
-SARU_HD void filter_read(const FilterShape &S, int dr, Val val, Perfect perfect, ReadHits &h) {
+// dr == 4).  L: the read's lists (see scan_from).  perfect(gs1): the genome
+// at gs1 (0-based) spells the read (strand-adjusted) over m bytes.
+template <class Lists, class Perfect>
+SARU_HD void filter_read(const FilterShape &S, int dr, const Lists &L, Perfect perfect,
+                         ReadHits &h) {
   const int k = S.k, half = S.half, q = S.q;
   for (int a = 0; a < half; ++a) {
     const int first = a == 0 ? 1 : 0;
     const uint32_t in_read = (uint32_t)a * q + 1;
     uint32_t off = 0;
-    uint32_t pa = val(a, off);
+    uint32_t pa = L.at(a, off);
     while (pa > 0) {
       const int gs = (int)(pa - in_read);
       if (gs + 1 > 0) {
         if (perfect(gs + 1)) filter_record(h, k, S.tresh, -(gs + 1), 0, S.tresh);
         int possible = 1;
-        // pairs with the later first-half q-grams
+        // pairs with the later first-half q-grams; the reference starts each
+        // scan at a's current index
         for (int b = a + 1; b < half; ++b) {
           const uint32_t rs = (uint32_t)b * q + 1;
           for (int ez = -k; ez <= k; ++ez) {
-            const uint32_t want = (uint32_t)gs + rs + (uint32_t)ez;
-            uint32_t v = val(b, off);  // the reference starts this scan at a's index
-            uint32_t vo = 0;
-            while (v > 0) {
-              if (v == want) {
-                int flag, start;
-                if (b == half - 1 && first) {
-                  flag = 1 + dr;
-                  start = gs + 1;
-                } else if (a == half - 1) {
-                  flag = ((int)(pa + q) > S.m ? 3 : 2) + dr;
-                  start = gs - k + 1;
-                } else if (first) {
-                  flag = 1 + dr;
-                  start = gs + 1;
-                } else {
-                  flag = 3 + dr;
-                  start = gs - k + 1;
-                }
-                ++possible;
-                filter_record(h, k, S.tresh, start, flag, possible);
+            const int hits = scan_from(L, b, off, (uint32_t)gs + rs + (uint32_t)ez);
+            for (int t = 0; t < hits; ++t) {
+              int flag, start;
+              if (b == half - 1 && first) {
+                flag = 1 + dr;
+                start = gs + 1;
+              } else if (a == half - 1) {
+                flag = ((int)(pa + q) > S.m ? 3 : 2) + dr;
+                start = gs - k + 1;
+              } else if (first) {
+                flag = 1 + dr;
+                start = gs + 1;
+              } else {
+                flag = 3 + dr;
+                start = gs - k + 1;
               }
-              ++vo;
-              v = val(b, vo);
+              ++possible;
+              filter_record(h, k, S.tresh, start, flag, possible);
             }
           }
         }
@@ -168,36 +193,28 @@ SARU_HD void filter_read(const FilterShape &S, int dr, Val val, Perfect perfect,
           const uint32_t ns = (uint32_t)(half - b - 1) * q + 1 + S.rest;
           for (int err = -lim; err <= lim; ++err) {
             const int ae = (b - a < 0) ? -err : err;
-            const uint32_t want = (uint32_t)gs + ns + (uint32_t)ae;
-            uint32_t so = 0;
-            uint32_t v = val(half + b, so);
-            while (v > 0) {
-              if (v == want) {
-                int flag, start;
-                if (b == 0 && first) {
-                  flag = 1 + dr;
-                  start = gs + 1;
-                } else if (b == 0) {
-                  flag = ((int)(ns + q) > S.m ? 3 : 2) + dr;
-                  start = gs - k + 1;
-                } else if (first) {
-                  flag = 1 + dr;
-                  start = gs + 1;
-                } else {
-                  flag = 3 + dr;
-                  start = gs - k + 1;
-                }
-                ++possible;
-                filter_record(h, k, S.tresh, start, flag, possible);
-              }
-              ++so;
-              v = val(half + b, so);
+            if (!scan_all(L, half + b, (uint32_t)gs + ns + (uint32_t)ae)) continue;
+            int flag, start;
+            if (b == 0 && first) {
+              flag = 1 + dr;
+              start = gs + 1;
+            } else if (b == 0) {
+              flag = ((int)(ns + q) > S.m ? 3 : 2) + dr;
+              start = gs - k + 1;
+            } else if (first) {
+              flag = 1 + dr;
+              start = gs + 1;
+            } else {
+              flag = 3 + dr;
+              start = gs - k + 1;
             }
+            ++possible;
+            filter_record(h, k, S.tresh, start, flag, possible);
           }
         }
       }
       ++off;
-      pa = val(a, off);
+      pa = L.at(a, off);
     }
   }
 }

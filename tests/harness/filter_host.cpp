@@ -43,7 +43,7 @@ extern "C" int filter_host_calls(const uint8_t *genome, long glen, const uint8_t
   for (int run = 0; run * chunksize < nreads; ++run) {
     const int r0 = run * chunksize, r1 = std::min(nreads, r0 + chunksize);
     std::vector<uint32_t> data;
-    std::vector<size_t> offs((size_t)(r1 - r0) * S.P);
+    std::vector<size_t> offs((size_t)(r1 - r0) * S.P), lens((size_t)(r1 - r0) * S.P);
     std::vector<std::string> strand((size_t)(r1 - r0));
     for (int r = r0; r < r1; ++r) {
       std::string rd((const char *)reads + (size_t)r * m, (size_t)m);
@@ -57,21 +57,32 @@ extern "C" int filter_host_calls(const uint8_t *genome, long glen, const uint8_t
         offs[(size_t)(r - r0) * S.P + x] = data.size();
         auto it = index.find(rd.substr((size_t)S.qpos[x], (size_t)S.q));
         if (it != index.end()) data.insert(data.end(), it->second.begin(), it->second.end());
+        lens[(size_t)(r - r0) * S.P + x] = it != index.end() ? it->second.size() : 0;
         data.push_back(0);
       }
     }
     for (int r = r0; r < r1; ++r) {
       const size_t base = (size_t)(r - r0) * S.P;
-      auto val = [&](int x, uint32_t i) -> uint32_t {
-        const size_t j = offs[base + (size_t)x] + i;
-        return j < data.size() ? data[j] : 0u;
-      };
+      struct Lists {
+        const std::vector<uint32_t> *data;
+        const size_t *offs, *lens;
+        uint32_t len(int x) const { return (uint32_t)lens[x]; }
+        uint32_t at(int x, uint32_t i) const {
+          const size_t j = offs[x] + i;
+          return j < data->size() ? (*data)[j] : 0u;
+        }
+        int find(int x, uint32_t lo, uint32_t want) const {
+          for (uint32_t i = lo; i < lens[x]; ++i)  // literal scan: the checker
+            if ((*data)[offs[x] + i] == want) return (int)i;
+          return -1;
+        }
+      } lists{&data, &offs[base], &lens[base]};
       const std::string &rd = strand[(size_t)(r - r0)];
       auto perfect = [&](int g1) {
         return (long)g1 + m <= glen && memcmp(genome + g1, rd.data(), (size_t)m) == 0;
       };
       ReadHits h{hp.data(), hf.data(), cap, 0, 0, 0};
-      filter_read(S, dr, val, perfect, h);
+      filter_read(S, dr, lists, perfect, h);
       overflow |= h.overflow;
       asmb.add_read(r, h.pos, h.flag, h.n, h.queue);
     }

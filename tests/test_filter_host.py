@@ -63,7 +63,7 @@ def host_calls(lib, g, reads, m, k, dr, chunk_value):
     ppos = np.zeros_like(pids)
     cnt = np.zeros(3, np.int64)
     flat = np.ascontiguousarray(reads.reshape(-1))
-    rc = lib.filter_host_calls(P(g), C.c_long(len(g)), P(flat), n, m, k, dr, n + 1,
+    rc = lib.filter_host_calls(P(g), C.c_long(len(g)), P(flat), n, m, k, dr, chunk_value,
                                C.c_uint(chunk_value), 4096, P(cb), C.c_int64(len(cb)), P(ids),
                                P(pos), P(dirs), C.c_int64(len(ids)), P(pids), P(ppos),
                                C.c_int64(len(pids)), P(cnt))
@@ -96,3 +96,42 @@ def test_filter_calls_match_the_reference_program(tmp_path, m, k, nreads, glen, 
             assert np.array_equal(ids[lo:hi], b.ids)
             assert np.array_equal(pos[lo:hi], b.pos)
             assert np.array_equal(dirs[lo:hi], b.dirs)
+
+
+def load_golden():
+    import json
+    z = np.load(ROOT / "tests" / "golden" / "filter_calls.npz")
+    specs = json.loads(bytes(z["specs"]).decode())
+    return z, specs
+
+
+def golden_inputs(spec):
+    name, (kind, glen, gseed), nreads, m, k, rseed, chunk, rchunk = spec
+    g = (W.uniform_genome(glen, seed=gseed) if kind == "uniform"
+         else W.repeat_genome(glen, seed=gseed, copies="zipf"))
+    return g, W.sample_reads(g, nreads, m, 0.03, seed=rseed).seqs
+
+
+@pytest.mark.parametrize("name", ["f36k2", "f100k5", "f150k9", "f36k3"])
+def test_filter_calls_match_the_golden_calls(name):
+    """Against the committed calls of the reference program (read batches of
+    64 in f150k9, hundreds of calls in f36k3), no reference build needed.
+    The reference maps its reads one batch (-c) at a time, read ids from 0
+    in each batch, and chunks its data array by the queue threshold (-s)."""
+    z, specs = load_golden()
+    spec = specs[name]
+    _, _, nreads, m, k, _, chunk, rchunk = spec
+    g, reads = golden_inputs(spec)
+    lib = harness()
+    for dr, strand in ((0, "fwd"), (4, "rev")):
+        cbs, idss, poss, dirss = [np.zeros(1, np.int64)], [], [], []
+        for b0 in range(0, nreads, rchunk):
+            cb, ids, pos, dirs = host_calls(lib, g, reads[b0:b0 + rchunk], m, k, dr, chunk)
+            cbs.append(cb[1:] + cbs[-1][-1])
+            idss.append(ids)
+            poss.append(pos)
+            dirss.append(dirs)
+        assert np.array_equal(np.concatenate(cbs), z[f"{name}_{strand}_call_begin"])
+        assert np.array_equal(np.concatenate(idss), z[f"{name}_{strand}_ids"])
+        assert np.array_equal(np.concatenate(poss), z[f"{name}_{strand}_pos"])
+        assert np.array_equal(np.concatenate(dirss), z[f"{name}_{strand}_dirs"])
