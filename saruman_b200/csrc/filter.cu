@@ -151,61 +151,163 @@ struct FilterArgs {
   int *status;
 };
 
-__global__ void __launch_bounds__(128) k_filter(FilterArgs a) {
-  const long r = a.r0 + blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (r >= a.r1) return;
-  const int P = a.S.P;
-  const long base = r * P;
-  // the data array of the read's chunk ends at cend (flattened offsets)
-  const long c0 = (r / a.chunk) * a.chunk, c1 = min(c0 + a.chunk, a.nreads);
-  const long cend = a.offs[c1 * P - 1] + a.count[c1 * P - 1];
-  struct Lists {
-    const FilterArgs *a;
-    long base, c0, c1, cend;
-    int P;
-    __device__ uint32_t len(int x) const { return (uint32_t)(a->count[base + x] - 1); }
-    __device__ uint32_t at(int x, uint32_t i) const {
-      const long t = base + x;
-      const long cnt = a->count[t];
-      if ((long)i + 1 < cnt) return a->pos[a->lo[t] + i];
-      if ((long)i + 1 == cnt) return 0u;
-      const long j = a->offs[t] + (long)i;  // past the list: what follows it
-      if (j >= cend) return 0u;
-      long l = c0 * P, u = c1 * P - 1;  // last list starting at or before j
+// The read's lists on the device: the sorted index's run for each q-gram,
+// and the data array's flattened offsets for looks past a list.
+struct DevLists {
+  const FilterArgs *a;
+  long base, c0, c1, cend;
+  int P;
+  __device__ uint32_t len(int x) const { return (uint32_t)(a->count[base + x] - 1); }
+  __device__ uint32_t at(int x, uint32_t i) const {
+    const long t = base + x;
+    const long cnt = a->count[t];
+    if ((long)i + 1 < cnt) return a->pos[a->lo[t] + i];
+    if ((long)i + 1 == cnt) return 0u;
+    const long j = a->offs[t] + (long)i;  // past the list: what follows it
+    if (j >= cend) return 0u;
+    long l = t;  // the list holding j: a few lists on, or found by bisection
+    const long last = c1 * P - 1;
+    int step = 0;
+    while (l < last && a->offs[l + 1] <= j && step < 8) {
+      ++l;
+      ++step;
+    }
+    if (l < last && a->offs[l + 1] <= j) {
+      long u = last;
       while (l < u) {
         const long mid = (l + u + 1) >> 1;
         if (a->offs[mid] <= j) l = mid;
         else u = mid - 1;
       }
-      const long w = j - a->offs[l];
-      return w + 1 < a->count[l] ? a->pos[a->lo[l] + w] : 0u;
     }
-    __device__ int find(int x, uint32_t from, uint32_t want) const {
-      const long t = base + x;
-      long l = a->lo[t] + from, u = a->lo[t] + a->count[t] - 1;  // ascending positions
-      while (l < u) {
-        const long mid = (l + u) >> 1;
-        if (a->pos[mid] < want) l = mid + 1;
-        else u = mid;
-      }
-      return (l < a->lo[t] + a->count[t] - 1 && a->pos[l] == want) ? (int)(l - a->lo[t]) : -1;
+    const long w = j - a->offs[l];
+    return w + 1 < a->count[l] ? a->pos[a->lo[l] + w] : 0u;
+  }
+  __device__ int find(int x, uint32_t from, uint32_t want) const {
+    const long t = base + x;
+    long l = a->lo[t] + from, u = a->lo[t] + a->count[t] - 1;  // ascending positions
+    while (l < u) {
+      const long mid = (l + u) >> 1;
+      if (a->pos[mid] < want) l = mid + 1;
+      else u = mid;
     }
-  } lists{&a, base, c0, c1, cend, P};
-  const uint8_t *rd = a.reads + r * a.S.m;
-  const int m = a.S.m, dr = a.dr;
-  auto perfect = [&](int g1) {
-    if ((long)g1 + m > a.glen) return false;
-    for (int i = 0; i < m; ++i)
-      if (a.genome[g1 + i] != strand_byte(rd, m, dr, i)) return false;
-    return true;
-  };
-  const long lr = r - a.r0;
-  ReadHits h{a.hit_pos + lr * kHitsPerRead, a.hit_flag + lr * kHitsPerRead, kHitsPerRead, 0, 0,
+    return (l < a->lo[t] + a->count[t] - 1 && a->pos[l] == want) ? (int)(l - a->lo[t]) : -1;
+  }
+};
+
+// One warp per read: filter_read (filter_core.cuh) with its pair scans
+// spread over the lanes.  For one position of q-gram a the reference counts
+// the pairs it finds, in a fixed order (first pass b ascending, zones
+// ascending; second pass b ascending, zones ascending; a first-pass scan can
+// count its first element twice) and records only the hit that brings the
+// count to the threshold.  The lanes evaluate 32 of those items at a time; a
+// warp prefix sum over their hit counts finds that hit, and lane 0 records it
+// (and the perfect hit before it) with filter_record, in the reference's
+// order.
+__global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
+  const int lane = threadIdx.x & 31;
+  const long r = fa.r0 + (blockIdx.x * (long)blockDim.x + threadIdx.x) / 32;
+  if (r >= fa.r1) return;  // the whole warp
+  const FilterShape &S = fa.S;
+  const int P = S.P, k = S.k, half = S.half, q = S.q, m = S.m, dr = fa.dr;
+  const long c0 = (r / fa.chunk) * fa.chunk, c1 = min(c0 + fa.chunk, fa.nreads);
+  const DevLists L{&fa, r * P, c0, c1, fa.offs[c1 * P - 1] + fa.count[c1 * P - 1], P};
+  const uint8_t *rd = fa.reads + r * m;
+  const long lr = r - fa.r0;
+  ReadHits h{fa.hit_pos + lr * kHitsPerRead, fa.hit_flag + lr * kHitsPerRead, kHitsPerRead, 0, 0,
              0};
-  filter_read(a.S, dr, lists, perfect, h);
-  a.n[lr] = h.n;
-  a.queue[lr] = h.queue;
-  if (h.overflow) atomicOr(a.status, 1);
+  const int zones = 2 * k + 1;
+  const int need = S.tresh - 1;  // hits before the one that reaches the threshold
+  for (int a = 0; a < half; ++a) {
+    const int first = a == 0 ? 1 : 0;
+    const uint32_t in_read = (uint32_t)a * q + 1;
+    const int n1 = (half - 1 - a) * zones;
+    int n2 = 0;
+    for (int b = 0; b < half; ++b) n2 += 2 * abs(half - 1 - b - a) + 1;
+    uint32_t off = 0;
+    uint32_t pa = L.at(a, off);
+    while (pa > 0) {
+      const int gs = (int)(pa - in_read);
+      if (gs + 1 > 0) {
+        const long g1 = gs + 1;
+        bool eq = g1 + m <= fa.glen;
+        for (int i = lane; eq && i < m; i += 32) eq = fa.genome[g1 + i] == strand_byte(rd, m, dr, i);
+        if (__all_sync(0xffffffffu, eq) && lane == 0)
+          filter_record(h, k, S.tresh, -(int)g1, 0, S.tresh);
+        int seen = 0;
+        for (int b0 = 0; need >= 1 && b0 < n1 + n2; b0 += 32) {
+          const int item = b0 + lane;
+          int hits = 0, flag = 0, start = 0;
+          if (item < n1) {
+            const int b = a + 1 + item / zones, ez = item % zones - k;
+            const uint32_t want = (uint32_t)gs + (uint32_t)b * q + 1 + (uint32_t)ez;
+            hits = scan_from(L, b, L.at(b, off), want);
+            if (b == half - 1 && first) {
+              flag = 1 + dr;
+              start = gs + 1;
+            } else if (a == half - 1) {
+              flag = ((int)(pa + q) > m ? 3 : 2) + dr;
+              start = gs - k + 1;
+            } else if (first) {
+              flag = 1 + dr;
+              start = gs + 1;
+            } else {
+              flag = 3 + dr;
+              start = gs - k + 1;
+            }
+          } else if (item < n1 + n2) {
+            int rest = item - n1, b = 0;
+            for (;; ++b) {
+              const int w = 2 * abs(half - 1 - b - a) + 1;
+              if (rest < w) break;
+              rest -= w;
+            }
+            const int lim = abs(half - 1 - b - a);
+            const int err = rest - lim;
+            const int ae = (b - a < 0) ? -err : err;
+            const uint32_t ns = (uint32_t)(half - b - 1) * q + 1 + S.rest;
+            hits = scan_all(L, half + b, (uint32_t)gs + ns + (uint32_t)ae);
+            if (b == 0 && first) {
+              flag = 1 + dr;
+              start = gs + 1;
+            } else if (b == 0) {
+              flag = ((int)(ns + q) > m ? 3 : 2) + dr;
+              start = gs - k + 1;
+            } else if (first) {
+              flag = 1 + dr;
+              start = gs + 1;
+            } else {
+              flag = 3 + dr;
+              start = gs - k + 1;
+            }
+          }
+          int incl = hits;  // inclusive prefix over the lanes
+          for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+          }
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          if (seen + total >= need) {
+            const unsigned who = __ballot_sync(0xffffffffu, hits > 0 && seen + incl >= need &&
+                                                               seen + incl - hits < need);
+            const int src = __ffs(who) - 1;
+            const int f = __shfl_sync(0xffffffffu, flag, src);
+            const int st = __shfl_sync(0xffffffffu, start, src);
+            if (lane == 0) filter_record(h, k, S.tresh, st, f, S.tresh);
+            break;
+          }
+          seen += total;
+        }
+      }
+      ++off;
+      pa = L.at(a, off);
+    }
+  }
+  if (lane == 0) {
+    fa.n[lr] = h.n;
+    fa.queue[lr] = h.queue;
+    if (h.overflow) atomicOr(fa.status, 1);
+  }
 }
 
 __global__ void k_pack(const int32_t *hit_pos, const int8_t *hit_flag, const int32_t *n,
@@ -397,7 +499,7 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       FilterArgs fa{f->reads.p, r0, r1, read_chunk, nr, do_reverse, S, f->genome.p,
                     f->glen, f->pos_s.p, f->lo.p, f->count.p, f->offs.p, f->hit_pos.p,
                     f->hit_flag.p, f->n.p, f->queue.p, f->status.p};
-      k_filter<<<(unsigned)((cnt + 127) / 128), 128, 0, f->s>>>(fa);
+      k_filter<<<(unsigned)((cnt + 3) / 4), 128, 0, f->s>>>(fa);  // a warp per read
       e = cudaGetLastError();
       if (e != cudaSuccess) break;
       k_widen<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->n.p, cnt, f->nwide.p);

@@ -124,8 +124,8 @@ SARU_HD int filter_record(ReadHits &h, int k, int tresh, int start, int flag, in
 // past the list included), find(x, lo, want) (an index in [lo, len(x)) of
 // list x holding want, or -1).
 template <class Lists>
-SARU_HD int scan_from(const Lists &L, int x, uint32_t off, uint32_t want) {
-  const uint32_t v0 = L.at(x, off);
+SARU_HD int scan_from(const Lists &L, int x, uint32_t v0, uint32_t want) {
+  // v0: the value at the scan's first index (L.at(x, off))
   if (v0 == 0) return 0;
   int hits = v0 == want ? 1 : 0;
   const uint32_t len = L.len(x);
@@ -164,8 +164,9 @@ SARU_HD void filter_read(const FilterShape &S, int dr, const Lists &L, Perfect p
         // scan at a's current index
         for (int b = a + 1; b < half; ++b) {
           const uint32_t rs = (uint32_t)b * q + 1;
+          const uint32_t v0 = L.at(b, off);  // the same for every error zone
           for (int ez = -k; ez <= k; ++ez) {
-            const int hits = scan_from(L, b, off, (uint32_t)gs + rs + (uint32_t)ez);
+            const int hits = scan_from(L, b, v0, (uint32_t)gs + rs + (uint32_t)ez);
             for (int t = 0; t < hits; ++t) {
               int flag, start;
               if (b == half - 1 && first) {
