@@ -646,6 +646,8 @@ def main() -> None:
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--filter-reads", type=int, default=200_000,
+                    help="reads for the device filter leg (0: skip)")
     ap.add_argument("--shape", default=None,
                     help="W,C,B: install this launch shape for every bin instead of tuning")
     ap.add_argument("--requests", type=int, default=None,
@@ -681,7 +683,9 @@ def main() -> None:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
 
-    bs = build_batches(cfg, rank)
+    tables = []
+    bs = build_batches(cfg, rank, tables)
+    genome = tables.pop()
     S.load()
     dbs = [DeviceBatch(b, dev, S) for b in bs]
     n_cand = sum(b.n for b in bs)
@@ -830,6 +834,23 @@ def main() -> None:
                            "slots on the host",
                    "tsv": tsv_leg}
 
+    # ---- candidate generation on the device (the reference's q-gram filter) --
+    filt = None
+    if not multi and args.filter_reads:
+        b0, seqs = bs[0], tables[0][:args.filter_reads]
+        with S.Filter(genome, b0.m, b0.k) as f:
+            f.run(seqs[:1000], 0, 1 << 30)  # warm-up
+            runs = [f.run(seqs, dr, 4 * len(seqs) + 1000) for dr in (0, 4)]
+        ms = sum(r.ms for r in runs)
+        filt = {"reads": int(len(seqs)), "strands": 2,
+                "value": 2 * len(seqs) / (ms * 1e-3), "unit": "read-strands/s",
+                "candidates_per_s": sum(len(r.ids) for r in runs) / (ms * 1e-3),
+                "ms": ms, "candidates": sum(len(r.ids) for r in runs),
+                "perfect_hits": sum(len(r.perfect_ids) for r in runs),
+                "what": "saru_filter_run: the reference's q-gram pair filter, a warp per read, "
+                        "on the first reads of the workload, both strands, calls assembled; "
+                        "device time incl. read upload and copy-back of the kept positions"}
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -900,6 +921,8 @@ def main() -> None:
     if plain:
         line["plain"] = plain
         line["batched_over_plain"] = plain["ms_per_step"] / ms_step
+    if filt:
+        line["filter"] = filt
     if compact:
         compact["roofline_frac"] = (6 * cells / (compact["ms_per_step"] * 1e-3) / int_peak
                                     if int_peak and int_peak > 0 else None)
