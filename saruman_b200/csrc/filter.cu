@@ -157,13 +157,14 @@ struct DevLists {
   const FilterArgs *a;
   long base, c0, c1, cend;
   int P;
-  __device__ uint32_t len(int x) const { return (uint32_t)(a->count[base + x] - 1); }
+  const long *lo, *cnt, *offs;  // this read's lists (shared-memory copies)
+  __device__ uint32_t len(int x) const { return (uint32_t)(cnt[x] - 1); }
   __device__ uint32_t at(int x, uint32_t i) const {
     const long t = base + x;
-    const long cnt = a->count[t];
-    if ((long)i + 1 < cnt) return a->pos[a->lo[t] + i];
-    if ((long)i + 1 == cnt) return 0u;
-    const long j = a->offs[t] + (long)i;  // past the list: what follows it
+    const long c = cnt[x];
+    if ((long)i + 1 < c) return a->pos[lo[x] + i];
+    if ((long)i + 1 == c) return 0u;
+    const long j = offs[x] + (long)i;  // past the list: what follows it
     if (j >= cend) return 0u;
     long l = t;  // the list holding j: a few lists on, or found by bisection
     const long last = c1 * P - 1;
@@ -184,14 +185,14 @@ struct DevLists {
     return w + 1 < a->count[l] ? a->pos[a->lo[l] + w] : 0u;
   }
   __device__ int find(int x, uint32_t from, uint32_t want) const {
-    const long t = base + x;
-    long l = a->lo[t] + from, u = a->lo[t] + a->count[t] - 1;  // ascending positions
+    const long end = lo[x] + cnt[x] - 1;  // ascending positions
+    long l = lo[x] + from, u = end;
     while (l < u) {
       const long mid = (l + u) >> 1;
       if (a->pos[mid] < want) l = mid + 1;
       else u = mid;
     }
-    return (l < a->lo[t] + a->count[t] - 1 && a->pos[l] == want) ? (int)(l - a->lo[t]) : -1;
+    return (l < end && a->pos[l] == want) ? (int)(l - lo[x]) : -1;
   }
 };
 
@@ -211,7 +212,17 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
   const FilterShape &S = fa.S;
   const int P = S.P, k = S.k, half = S.half, q = S.q, m = S.m, dr = fa.dr;
   const long c0 = (r / fa.chunk) * fa.chunk, c1 = min(c0 + fa.chunk, fa.nreads);
-  const DevLists L{&fa, r * P, c0, c1, fa.offs[c1 * P - 1] + fa.count[c1 * P - 1], P};
+  __shared__ long s_lo[4][kFilterMaxQgrams], s_cnt[4][kFilterMaxQgrams],
+      s_offs[4][kFilterMaxQgrams];
+  const int w = threadIdx.x >> 5;
+  for (int x = lane; x < P; x += 32) {
+    s_lo[w][x] = fa.lo[r * P + x];
+    s_cnt[w][x] = fa.count[r * P + x];
+    s_offs[w][x] = fa.offs[r * P + x];
+  }
+  __syncwarp();
+  const DevLists L{&fa, r * P, c0, c1, fa.offs[c1 * P - 1] + fa.count[c1 * P - 1], P,
+                   s_lo[w], s_cnt[w], s_offs[w]};
   const uint8_t *rd = fa.reads + r * m;
   const long lr = r - fa.r0;
   ReadHits h{fa.hit_pos + lr * kHitsPerRead, fa.hit_flag + lr * kHitsPerRead, kHitsPerRead, 0, 0,
