@@ -10,8 +10,10 @@
 //           bytes) and, by an exclusive scan per read chunk, its list's
 //           offset in the reference's data array (lists in q-gram order per
 //           read, each followed by a 0, src/hash.c:404-457).
-//  filter   one thread per read: filter_read (filter_core.cuh) over that
-//           layout, the read's kept positions into its slice of a scratch.
+//  filter   one warp per read, reads taken most estimated work first:
+//           filter_read (filter_core.cuh) over that layout, its pair items
+//           spread over the lanes, the read's kept positions into its slice
+//           of a scratch.
 //  calls    the kept positions, packed, copied back and assembled into the
 //           reference's calls on the host (filter_calls.h).
 #include <cub/device/device_radix_sort.cuh>
@@ -149,6 +151,7 @@ struct FilterArgs {
   int8_t *hit_flag;
   int32_t *n, *queue;             // per read of the launch
   int *status;
+  const int32_t *order;           // the launch's reads (0-based in it), most work first
 };
 
 // The read's lists on the device: the sorted index's run for each q-gram,
@@ -196,19 +199,59 @@ struct DevLists {
   }
 };
 
+// filter_record (filter_core.cuh) by a whole warp: every lane carries the
+// same n, queue and overflow; the kept entries are examined 32 at a time and
+// the first that decides (dropped, flag replaced, or dropped as equal) wins,
+// as in the sequential loop; with none deciding, lane 0 appends.
+__device__ inline void warp_record(ReadHits &h, int lane, int k, int start, int flag) {
+  const int dir = flag > 3 ? 1 : 0;
+  for (int c0 = 0; c0 < h.n; c0 += 32) {
+    const int c = c0 + lane;
+    int code = 0;
+    if (c < h.n) {
+      const int pc = h.pos[c], fc = h.flag[c];
+      const int dc = fc > 3 ? 1 : 0;
+      const long d1 = (long)pc - start, d2 = -(long)pc - start;
+      if (fc <= flag && ((d1 >= -k && d1 <= k) || (d2 >= -k && d2 <= k))) code = 1;
+      else if (pc == start && dc == dir && fc > flag) code = 2;
+      else if ((pc == start || pc == -start) && dc == dir) code = 3;
+    }
+    const unsigned any = __ballot_sync(0xffffffffu, code != 0);
+    if (any) {
+      if (lane == __ffs(any) - 1 && code == 2) h.flag[c] = (int8_t)flag;
+      __syncwarp();
+      return;
+    }
+  }
+  if (h.n >= h.cap) {
+    h.overflow = 1;
+    return;
+  }
+  if (lane == 0) {
+    h.pos[h.n] = start;
+    h.flag[h.n] = (int8_t)flag;
+  }
+  ++h.n;
+  if (start > 0) ++h.queue;
+  __syncwarp();
+}
+
 // One warp per read: filter_read (filter_core.cuh) with its pair scans
 // spread over the lanes.  For one position of q-gram a the reference counts
 // the pairs it finds, in a fixed order (first pass b ascending, zones
 // ascending; second pass b ascending, zones ascending; a first-pass scan can
 // count its first element twice) and records only the hit that brings the
 // count to the threshold.  The lanes evaluate 32 of those items at a time; a
-// warp prefix sum over their hit counts finds that hit, and lane 0 records it
-// (and the perfect hit before it) with filter_record, in the reference's
-// order.
+// warp prefix sum over their hit counts finds that hit, and the warp records
+// it (and the perfect hit before it) with warp_record, in the reference's
+// order.  Warps take the launch's reads in the order `order` gives (most
+// estimated work first), so long reads start early and short ones fill in.
 __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
   const int lane = threadIdx.x & 31;
-  const long r = fa.r0 + (blockIdx.x * (long)blockDim.x + threadIdx.x) / 32;
-  if (r >= fa.r1) return;  // the whole warp
+  const long wi = (blockIdx.x * (long)blockDim.x + threadIdx.x) / 32;
+  if (wi >= fa.r1 - fa.r0) return;  // the whole warp
+  const long lr = fa.order[wi];
+  const long r = fa.r0 + lr;
   const FilterShape &S = fa.S;
   const int P = S.P, k = S.k, half = S.half, q = S.q, m = S.m, dr = fa.dr;
   const long c0 = (r / fa.chunk) * fa.chunk, c1 = min(c0 + fa.chunk, fa.nreads);
@@ -224,7 +267,6 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
   const DevLists L{&fa, r * P, c0, c1, fa.offs[c1 * P - 1] + fa.count[c1 * P - 1], P,
                    s_lo[w], s_cnt[w], s_offs[w]};
   const uint8_t *rd = fa.reads + r * m;
-  const long lr = r - fa.r0;
   ReadHits h{fa.hit_pos + lr * kHitsPerRead, fa.hit_flag + lr * kHitsPerRead, kHitsPerRead, 0, 0,
              0};
   const int zones = 2 * k + 1;
@@ -243,8 +285,7 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
         const long g1 = gs + 1;
         bool eq = g1 + m <= fa.glen;
         for (int i = lane; eq && i < m; i += 32) eq = fa.genome[g1 + i] == strand_byte(rd, m, dr, i);
-        if (__all_sync(0xffffffffu, eq) && lane == 0)
-          filter_record(h, k, S.tresh, -(int)g1, 0, S.tresh);
+        if (__all_sync(0xffffffffu, eq)) warp_record(h, lane, k, -(int)g1, 0);
         int seen = 0;
         for (int b0 = 0; need >= 1 && b0 < n1 + n2; b0 += 32) {
           const int item = b0 + lane;
@@ -304,7 +345,7 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
             const int src = __ffs(who) - 1;
             const int f = __shfl_sync(0xffffffffu, flag, src);
             const int st = __shfl_sync(0xffffffffu, start, src);
-            if (lane == 0) filter_record(h, k, S.tresh, st, f, S.tresh);
+            warp_record(h, lane, k, st, f);
             break;
           }
           seen += total;
@@ -318,6 +359,25 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
     fa.n[lr] = h.n;
     fa.queue[lr] = h.queue;
     if (h.overflow) atomicOr(fa.status, 1);
+  }
+}
+
+// A read's estimated filter work: for each first-half q-gram, its positions
+// times the warp steps of its pair items (an upper bound: a position stops
+// once its count reaches the threshold).
+__global__ void k_work(const long *count, long r0, long cnt, FilterShape S, uint32_t *key,
+                       int32_t *idx) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < cnt;
+       i += (long)gridDim.x * blockDim.x) {
+    const long r = r0 + i;
+    unsigned long long w = 0;
+    for (int a = 0; a < S.half; ++a) {
+      int items = (S.half - 1 - a) * (2 * S.k + 1);
+      for (int b = 0; b < S.half; ++b) items += 2 * abs(S.half - 1 - b - a) + 1;
+      w += (unsigned long long)(count[r * S.P + a] - 1) * (1 + (items + 31) / 32);
+    }
+    key[i] = (uint32_t)(w < 0xffffffffull ? w : 0xffffffffull);
+    idx[i] = (int32_t)i;
   }
 }
 
@@ -367,7 +427,8 @@ struct saru_filter {
   DBuf<uint64_t> hash, hash_s;
   DBuf<uint32_t> pos, pos_s;
   DBuf<long> lo, count, offs, at, nwide;
-  DBuf<int32_t> hit_pos, n, queue, packed_pos;
+  DBuf<int32_t> hit_pos, n, queue, packed_pos, widx;
+  DBuf<uint32_t> wkey;
   DBuf<int8_t> hit_flag, packed_flag;
   DBuf<int> status;
   FilterCalls calls;
@@ -477,11 +538,18 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
     size_t tb2 = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb2, (long *)nullptr, (long *)nullptr,
                                   (int)kReadsPerLaunch, f->s);
+    size_t tb3 = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tb3, (uint32_t *)nullptr,
+                                              (uint32_t *)nullptr, (int32_t *)nullptr,
+                                              (int32_t *)nullptr, (int)kReadsPerLaunch, 0, 32,
+                                              f->s);
     const long batch = std::min<long>(nr, kReadsPerLaunch);
     if ((e = f->reads.ensure((size_t)(nr * m))) != cudaSuccess ||
         (e = f->lo.ensure(lists)) != cudaSuccess || (e = f->count.ensure(lists)) != cudaSuccess ||
         (e = f->offs.ensure(lists)) != cudaSuccess ||
-        (e = f->temp.ensure(std::max(tb, tb2))) != cudaSuccess ||
+        (e = f->temp.ensure(std::max(std::max(tb, tb2), tb3))) != cudaSuccess ||
+        (e = f->wkey.ensure((size_t)batch * 2)) != cudaSuccess ||
+        (e = f->widx.ensure((size_t)batch * 2)) != cudaSuccess ||
         (e = f->hit_pos.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
         (e = f->hit_flag.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
         (e = f->n.ensure(batch)) != cudaSuccess || (e = f->queue.ensure(batch)) != cudaSuccess ||
@@ -507,9 +575,17 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
     if (e == cudaSuccess) e = cudaMemsetAsync(f->status.p, 0, sizeof(int), f->s);
     for (long r0 = 0; r0 < nr && e == cudaSuccess; r0 += batch) {
       const long r1 = std::min(nr, r0 + batch), cnt = r1 - r0;
+      k_work<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->count.p, r0, cnt, S, f->wkey.p,
+                                                              f->widx.p);
+      e = cudaGetLastError();
+      if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairsDescending(f->temp.p, tb3, f->wkey.p,
+                                                      f->wkey.p + batch, f->widx.p,
+                                                      f->widx.p + batch, (int)cnt, 0, 32, f->s);
+      if (e != cudaSuccess) break;
       FilterArgs fa{f->reads.p, r0, r1, read_chunk, nr, do_reverse, S, f->genome.p,
                     f->glen, f->pos_s.p, f->lo.p, f->count.p, f->offs.p, f->hit_pos.p,
-                    f->hit_flag.p, f->n.p, f->queue.p, f->status.p};
+                    f->hit_flag.p, f->n.p, f->queue.p, f->status.p, f->widx.p + batch};
       k_filter<<<(unsigned)((cnt + 3) / 4), 128, 0, f->s>>>(fa);  // a warp per read
       e = cudaGetLastError();
       if (e != cudaSuccess) break;
@@ -615,6 +691,8 @@ void saru_filter_destroy(saru_filter *f) {
   f->hit_flag.release();
   f->packed_flag.release();
   f->status.release();
+  f->wkey.release();
+  f->widx.release();
   if (f->s) cudaStreamDestroy(f->s);
   delete f;
 }
