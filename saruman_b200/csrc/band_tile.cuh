@@ -7,7 +7,7 @@
 // shared memory (zero-filled, as the reference's memset arena leaves them)
 // and writes the tile's slot range back with 16-byte stores.  Decision
 // planes (2 bits per band cell) go to a global scratch that stays in L2;
-// the traceback keeps the next three columns' planes in registers.
+// the traceback keeps the next four columns' planes in flight.
 //
 // The phases are separated by warp barriers in the kernel; written as
 // functions of the lane so a host harness can run them lane by lane.
@@ -190,78 +190,104 @@ SARU_HD long plane_index(int j, long pstride, long pslot, long mul) {
   return ((long)j * pstride + pslot) * mul;
 }
 
-// Traceback phase of one lane: writes the lane's two strings into its slot
-// of the output staging, in reading order (the reference emits from the
-// alignment end and reverses in place, src/cuda-functions.cu:306-307; here
-// the characters are written from the slot end downwards and the string is
-// then moved to the slot start, which leaves the same bytes).
+// Compact result record of one candidate (the alternative to its two slot
+// strings): word 0 = number of traceback steps n (bits 0-15) and an
+// overflow flag (bit 16); words 1.. = the steps in traceback order (from
+// the alignment end), 2 bits each, 16 per word: 1 DIAG (read byte against
+// window byte), 2 UP (gap in the read), 3 LEFT (gap in the window).  With
+// the call's reads and windows the host rebuilds the slot strings exactly
+// (saru_expand_compact).  A candidate with score > k has n = 0.
+constexpr int kCompactHeaderBytes = 4;
+
+// Words of 2-bit steps a traceback can need: a slot holds L + k <= m + 3k.
+SARU_HD long step_words(int max_m, int k) { return ((long)max_m + 3L * k + 15) / 16; }
+
+SARU_HD long compact_record_bytes(int max_m, int k) {
+  return (kCompactHeaderBytes + 4 * step_words(max_m, k) + 15) & ~15L;
+}
+
+// Bytes of a warp's two output strings in its shared slice.
+SARU_HD long out_area_bytes(int max_m, int k) {
+  return 2 * ((32L * (max_m + 3 * k) + 32 + 15) & ~15L);
+}
+
+// Where a traceback walk ended.
+struct WalkEnd {
+  int n;         // steps
+  int row, col;  // the cell it stopped at
+  bool bad;      // left the band or the slot
+};
+
+// The traceback walk of one lane (the reference's get_alignment,
+// src/cuda-functions.cu:108-315, over the band's decision planes).  Each
+// step is handed to emit(i, op, row, col): i counts from 0 at the alignment
+// end, op is 1 DIAG (read byte col - 1 against window byte row - 1), 2 UP
+// (gap in the read, window byte row - 1), 3 LEFT (read byte col - 1, gap in
+// the window), and (row, col) is the cell the step leaves.
 //
-// Interior cells (row >= 1, column >= 1) take a branch-free step per loop
-// iteration, so the warp stays converged: with the recorded decision as
-// bits (a, b) -- DIAG (1,0), UP (0,1), LEFT (1,1), STOP (0,0) -- the read
-// string gets a read byte iff a, the window string a window byte unless
-// a&b, the column drops iff a, the row drops unless a&b.  The planes of the
-// next column are already in registers and the column PF ahead is
-// prefetched.  Row 0 and column 0 follow the reference's border rules in a
-// short tail loop (see traceback_band in saru_core.cuh).
-template <typename T, int PF, class LoadPair, class Prefetch>
-SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
-                           const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
-                           const LaneState &ls, LoadPair ld, Prefetch prefetch) {
+// Interior cells (row >= 1, column >= 1): the recorded decision (a, b) --
+// DIAG (1,0), UP (0,1), LEFT (1,1), STOP (0,0) -- is the step; the column
+// drops iff a, the band offset moves by +1 (LEFT) or -1 (UP), and the row
+// follows from them: row = offset + column - k holds along the walk (it
+// holds at the start, row L and column m at offset L - m + k, and every
+// step keeps it).  The planes of the next four columns are in flight in
+// four registers used in turn: a register is refilled with the column four
+// ahead right after the walk leaves its column, and no register is copied
+// to another (a copy would wait for its load).  Row 0 and column 0 follow
+// the reference's border rules in a short tail loop (see traceback_band in
+// saru_core.cuh).
+template <typename T, class LoadPair, class Emit>
+SARU_HD WalkEnd lane_walk(const Cand &c, LoadPair ld, Emit emit) {
   constexpr int BITS = int(sizeof(T) * 8);
-  const long t = s.t0 + lane;
-  if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
-  const Cand &c = ls.c;
-  const int roff = (int)(ls.rs - s.r_base) - 1;  // read byte col-1 at st_reads[roff + col]
-  const int woff = (int)(ls.gs - s.g_base) - 1;  // window byte row-1 at st_win[woff + row]
-  const long slot = ls.gs + (long)a.k * t;
-  const int sr = (int)(slot - s.o_base_r);  // slot start in out_r
-  const int sg = (int)(slot - s.o_base_g);
-  const int cap = c.L + c.k;                 // slot bytes
-  int n = 0;                                 // bytes written, from the slot end down
-  int row = c.L, col = c.m, b = c.L - c.m + c.k;
-  bool bad = false, stop = false;
-  // planes of the current column and the next three to the left in
-  // registers, so a load is issued three column moves before its use
-  PlanePair<T> cur = ld(col);
-  PlanePair<T> n1 = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
-  PlanePair<T> n2 = col >= 3 ? ld(col - 2) : PlanePair<T>{};
-  PlanePair<T> n3 = col >= 4 ? ld(col - 3) : PlanePair<T>{};
-  for (int j = col - 4; j >= 1 && j > col - 4 - PF; --j) prefetch(j);
-  // interior: row >= 1 and col >= 1 hold on entry to every iteration
-  for (;;) {
-    if ((unsigned)b >= (unsigned)BITS) {
-      bad = true;
-      break;
-    }
-    const uint32_t da = (uint32_t)((cur.A >> b) & T(1));
-    const uint32_t db = (uint32_t)((cur.B >> b) & T(1));
-    if ((da | db) == 0) {
-      stop = true;
-      break;
-    }
-    if (n >= cap) {
-      bad = true;
-      break;
-    }
-    const uint8_t rch = st_reads[roff + col];
-    const uint8_t gch = st_win[woff + row];
-    ++n;
-    out_r[sr + cap - n] = da ? rch : uint8_t('_');
-    out_g[sg + cap - n] = (da & db) ? uint8_t('_') : gch;
-    row -= (int)(1u - (da & db));
-    b += (int)db * ((int)da * 2 - 1);
-    if (da) {
+  const int cap = c.L + c.k, k = c.k;
+  int n = 0;
+  int col = c.m, b = c.L - c.m + c.k;
+  int end = 0;  // 1: reached row 0 or column 0, 2: a stop decision, 3: left band or slot
+  // the steps at the current column (planes p) up to the one that leaves
+  // it; false when the walk's interior ends
+  auto column = [&](const PlanePair<T> &p) -> bool {
+    for (;;) {
+      const bool out = (unsigned)b >= (unsigned)BITS;
+      const int bb = b & (BITS - 1);
+      const uint32_t da = (uint32_t)(p.A >> bb) & 1u;
+      const uint32_t db = (uint32_t)(p.B >> bb) & 1u;
+      if (out || (da | db) == 0u || n >= cap) {
+        end = (out || (da | db) != 0u) ? 3 : 2;
+        return false;
+      }
+      emit(n++, da | (db << 1), b + col - k, col);
+      if (!da) {  // UP: same column, one row up
+        --b;
+        if (b + col == k) {
+          end = 1;
+          return false;
+        }
+        continue;
+      }
+      b += (int)db;  // LEFT +1, DIAG 0
       --col;
-      cur = n1;
-      n1 = n2;
-      n2 = n3;
-      if (col >= 4) n3 = ld(col - 3);
-      if (col - 3 - PF >= 1) prefetch(col - 3 - PF);
+      if (b + col == k || col == 0) {
+        end = 1;
+        return false;
+      }
+      return true;
     }
-    if (row == 0 || col == 0) break;
+  };
+  auto ahead = [&](int j) { return ld(j > 0 ? j : 0); };
+  PlanePair<T> p0 = ld(col), p1 = ahead(col - 1), p2 = ahead(col - 2), p3 = ahead(col - 3);
+  for (;;) {
+    if (!column(p0)) break;
+    p0 = ahead(col - 3);
+    if (!column(p1)) break;
+    p1 = ahead(col - 3);
+    if (!column(p2)) break;
+    p2 = ahead(col - 3);
+    if (!column(p3)) break;
+    p3 = ahead(col - 3);
   }
-  if (!bad && !stop) {
+  bool bad = end == 3;
+  int row = b + col - k;
+  if (end == 1) {
     // borders.  Row 0 (col >= 1): the first candidate of a call stops; later
     // ones step left to column 0 (their diagonal/top neighbours are the
     // previous matrix's last row, all > k when m > 3k).  Column 0 holds
@@ -273,9 +299,7 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
           bad = true;
           break;
         }
-        ++n;
-        out_r[sr + cap - n] = st_reads[roff + col];
-        out_g[sg + cap - n] = '_';
+        emit(n++, 3u, row, col);
         --col;
         continue;
       }
@@ -288,121 +312,78 @@ SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const
         bad = true;
         break;
       }
-      ++n;
-      out_r[sr + cap - n] = '_';
-      out_g[sg + cap - n] = st_win[woff + row];
+      emit(n++, 2u, row, col);
       --row;
     }
   }
-  // move the string to the slot start; clear what it vacated
+  return WalkEnd{n, row, col, bad};
+}
+
+// Traceback phase of one lane in slot mode: writes the lane's two strings
+// into its slot of the output staging, in reading order.  The reference
+// emits from the alignment end and reverses in place
+// (src/cuda-functions.cu:306-307); here the characters are written from the
+// slot end downwards as the walk goes and the strings are then moved to
+// the slot start, which leaves the same bytes.
+template <typename T, class LoadPair>
+SARU_HD int lane_traceback(const TileArgs &a, const TileSpan &s, int lane, const uint8_t *st_reads,
+                           const uint8_t *st_win, uint8_t *out_r, uint8_t *out_g,
+                           const LaneState &ls, LoadPair ld) {
+  const long t = s.t0 + lane;
+  if (t >= a.n || !ls.ok || ls.score > a.k) return 0;
+  const int cap = ls.c.L + ls.c.k;  // slot bytes
+  const long slot = ls.gs + (long)a.k * t;
+  uint8_t *o_r = out_r + (slot - s.o_base_r);
+  uint8_t *o_g = out_g + (slot - s.o_base_g);
+  const uint8_t *rd = st_reads + (ls.rs - s.r_base) - 1;  // read byte col - 1 at rd[col]
+  const uint8_t *wn = st_win + (ls.gs - s.g_base) - 1;    // window byte row - 1 at wn[row]
+  uint8_t *e_r = o_r + cap - 1, *e_g = o_g + cap - 1;      // step i at e_r[-i]
+  const WalkEnd e = lane_walk<T>(ls.c, ld, [&](int i, uint32_t op, int row, int col) {
+    const uint8_t rch = rd[col], gch = wn[row];
+    e_r[-i] = (op & 1u) ? rch : uint8_t('_');
+    e_g[-i] = op != 3u ? gch : uint8_t('_');
+  });
+  // move the strings to the slot start; clear what they vacated
+  const int n = e.n;
   if (n < cap) {
     const int from = cap - n;
     for (int i = 0; i < n; ++i) {
-      out_r[sr + i] = out_r[sr + from + i];
-      out_g[sg + i] = out_g[sg + from + i];
+      o_r[i] = o_r[from + i];
+      o_g[i] = o_g[from + i];
     }
     for (int i = n; i < cap; ++i) {
-      out_r[sr + i] = 0;
-      out_g[sg + i] = 0;
+      o_r[i] = 0;
+      o_g[i] = 0;
     }
   }
-  return bad ? 4 : 0;
+  return e.bad ? 4 : 0;
 }
 
-// Compact result record of one candidate (the alternative to its two slot
-// strings): word 0 = number of traceback steps n (bits 0-15) and an
-// overflow flag (bit 16); words 1.. = the steps in traceback order (from
-// the alignment end), 2 bits each, 16 per word: 1 DIAG (read byte against
-// window byte), 2 UP (gap in the read), 3 LEFT (gap in the window).  With
-// the call's reads and windows the host rebuilds the slot strings exactly
-// (saru_expand_compact).  A candidate with score > k has n = 0.
-constexpr int kCompactHeaderBytes = 4;
-
-SARU_HD long compact_record_bytes(int max_m, int k) {
-  const long steps = (long)max_m + 3L * k;  // L + k <= m + 3k
-  return (kCompactHeaderBytes + 4 * ((steps + 15) / 16) + 15) & ~15L;
-}
-
-// Traceback of one lane into its compact record (same walk and border rules
-// as lane_traceback).  store(w, v) writes word w of candidate t's record.
+// Traceback of one lane into its compact record.  store(w, v) writes word w
+// of candidate t's record.
 template <typename T, class LoadPair, class StoreWord>
 SARU_HD int lane_traceback_ops(const TileArgs &a, const TileSpan &s, int lane,
                                const LaneState &ls, LoadPair ld, StoreWord store) {
-  constexpr int BITS = int(sizeof(T) * 8);
   const long t = s.t0 + lane;
   if (t >= a.n) return 0;
   if (!ls.ok || ls.score > a.k) {
     store(0, 0u);
     return 0;
   }
-  const Cand &c = ls.c;
-  const int cap = c.L + c.k;
-  int n = 0;
   uint32_t acc = 0;
-  int row = c.L, col = c.m, b = c.L - c.m + c.k;
-  bool bad = false, stop = false;
-  auto push = [&](uint32_t op) {
-    acc |= op << (2 * (n & 15));
-    ++n;
-    if ((n & 15) == 0) {
-      store(n >> 4, acc);  // words 1.. hold steps 16(w-1) .. 16w-1
+  int sh = 0, w = 1;
+  const WalkEnd e = lane_walk<T>(ls.c, ld, [&](int, uint32_t op, int, int) {
+    acc |= op << sh;
+    sh += 2;
+    if (sh == 32) {  // words 1.. hold steps 16(w-1) .. 16w-1
+      store(w++, acc);
       acc = 0;
+      sh = 0;
     }
-  };
-  PlanePair<T> cur = ld(col);
-  PlanePair<T> nxt = ld(col - 1);  // col >= 2 here (m > 3k >= 0 and m >= 2)
-  for (;;) {
-    if ((unsigned)b >= (unsigned)BITS) {
-      bad = true;
-      break;
-    }
-    const uint32_t da = (uint32_t)((cur.A >> b) & T(1));
-    const uint32_t db = (uint32_t)((cur.B >> b) & T(1));
-    if ((da | db) == 0) {
-      stop = true;
-      break;
-    }
-    if (n >= cap) {
-      bad = true;
-      break;
-    }
-    push(da | (db << 1));
-    row -= (int)(1u - (da & db));
-    b += (int)db * ((int)da * 2 - 1);
-    if (da) {
-      --col;
-      cur = nxt;
-      if (col >= 2) nxt = ld(col - 1);
-    }
-    if (row == 0 || col == 0) break;
-  }
-  if (!bad && !stop) {
-    for (;;) {  // borders, as in lane_traceback
-      if (row == 0) {
-        if (col == 0 || c.first_of_call) break;
-        if (n >= cap) {
-          bad = true;
-          break;
-        }
-        push(3u);
-        --col;
-        continue;
-      }
-      const int v = row - 2 * c.so > 0 ? row - 2 * c.so : 0;
-      const int tp = row - 1 - 2 * c.so > 0 ? row - 1 - 2 * c.so : 0;
-      const int corr = (c.so && row - 1 <= 2 * c.so + 2) ? 1 : 0;
-      if (tp + 1 - corr != v) break;
-      if (n >= cap) {
-        bad = true;
-        break;
-      }
-      push(2u);
-      --row;
-    }
-  }
-  if (n & 15) store((n >> 4) + 1, acc);
-  store(0, (uint32_t)n | (bad ? 0x10000u : 0u));
-  return bad ? 4 : 0;
+  });
+  if (sh) store(w, acc);
+  store(0, (uint32_t)e.n | (e.bad ? 0x10000u : 0u));
+  return e.bad ? 4 : 0;
 }
 
 // Shared-memory slice sizes for a maximum read length and k.
@@ -419,7 +400,7 @@ SARU_HD SliceLayout slice_layout(int max_m, int k) {
   L.rs_bytes = (32L * max_m + 16 + 96 + 15) & ~15L;
   L.ws_bytes = (32L * (max_m + 2 * k) + 16 + 96 + 15) & ~15L;
   const long cm = 4L * 32 * (code_words + NCODES * mwords);
-  const long out = 2 * ((32L * (max_m + 3 * k) + 32 + 15) & ~15L);
+  const long out = out_area_bytes(max_m, k);
   L.region_bytes = ((cm > out ? cm : out) + 15) & ~15L;
   L.warp_smem = L.rs_bytes + L.ws_bytes + L.region_bytes;
   return L;

@@ -19,15 +19,6 @@
 
 namespace saru {
 
-// Columns ahead that the traceback prefetches into L1 beyond the next one.
-// 0 (none) measured fastest: the lanes of a warp walk different columns, and
-// prefetched lines evict each other from the L1 left beside the
-// shared-memory slices.
-#ifndef SARU_TRACE_PREFETCH
-#define SARU_TRACE_PREFETCH 0
-#endif
-constexpr int kTracePrefetch = SARU_TRACE_PREFETCH;
-
 __device__ __forceinline__ long gstart_of(const int32_t *goff, long t) { return t ? goff[t - 1] : 0; }
 
 // ---------------------------------------------------------------------------
@@ -73,18 +64,15 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
   }
   uint8_t *out_r = region;
   uint8_t *out_g = region + s.o_span_r;
+  const long out_bytes = out_area_bytes(ta.max_m, ta.k);
   {
     uint4 *p4 = reinterpret_cast<uint4 *>(region);
-    const long nv = ta.region_bytes >> 4;
+    const long nv = out_bytes >> 4;
     for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
   }
   __syncwarp();
   auto ld_pair = [&](int j) { return planes[plane_index(j, ta.pstride, pslot, mul)]; };
-  auto pf_pair = [&](int j) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(planes + plane_index(j, ta.pstride, pslot, mul)));
-  };
-  st |= lane_traceback<T, kTracePrefetch>(
-      ta, s, lane, st_reads, st_win, out_r, out_g, ls, ld_pair, pf_pair);
+  st |= lane_traceback<T>(ta, s, lane, st_reads, st_win, out_r, out_g, ls, ld_pair);
   __syncwarp();
   stage_out(ta.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
   stage_out(ta.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
@@ -94,7 +82,9 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
 
 // Persistent warps take 32-candidate tiles from a launch-wide counter; a
 // tile belongs to one segment (a call with its own m, k and band width).
-__global__ void __launch_bounds__(128, 3) saru_band_kernel(const __grid_constant__ KernelArgs a) {
+// The bounds hold the kernel to 128 registers a thread: above that an SM
+// sub-partition's register file holds 3 of these warps instead of 4.
+__global__ void __launch_bounds__(128, 4) saru_band_kernel(const __grid_constant__ KernelArgs a) {
   extern __shared__ uint4 smem_v[];
   const int lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;

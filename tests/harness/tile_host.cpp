@@ -70,13 +70,13 @@ static int run(const TileArgs &a0, int nwarps_total) {
         continue;
       }
       uint8_t *out_r = region, *out_g = region + s.o_span_r;
-      memset(region, 0, (size_t)S.region_bytes);
+      const long out_bytes = out_area_bytes(a.max_m, a.k);
+      memset(region, 0, (size_t)out_bytes);
       for (int lane = 0; lane < 32; ++lane) {
         const long pslot = (long)gwarp * 32 + lane;
-        status |= lane_traceback<T, 8>(
+        status |= lane_traceback<T>(
             a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
-            [&](int j) { return planes[plane_index(j, a.pstride, pslot, 1)]; },
-            [&](int j) { (void)planes[plane_index(j, a.pstride, pslot, 1)]; });
+            [&](int j) { return planes[plane_index(j, a.pstride, pslot, 1)]; });
       }
       for (int lane = 0; lane < 32; ++lane) {
         stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
@@ -211,14 +211,14 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
       auto trace = [&](auto tag) {
         using T = decltype(tag);
         PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
-        memset(w.region, 0, (size_t)S.region_bytes);
+        const long out_bytes = out_area_bytes(a.max_m, a.k);
+        memset(w.region, 0, (size_t)out_bytes);
         uint8_t *out_r = w.region, *out_g = w.region + w.span.o_span_r;
         for (int lane = 0; lane < 32; ++lane) {
           const long pslot = (long)gw * 32 + lane;
-          status |= lane_traceback<T, 8>(
+          status |= lane_traceback<T>(
               a, w.span, lane, w.st_reads, w.st_win, out_r, out_g, w.ls[lane],
-              [&](int j) { return planes[plane_index(j, pstride, pslot, a.pair_mul)]; },
-              [&](int j) { (void)planes[plane_index(j, pstride, pslot, a.pair_mul)]; });
+              [&](int j) { return planes[plane_index(j, pstride, pslot, a.pair_mul)]; });
         }
         for (int lane = 0; lane < 32; ++lane) {
           stage_out(a.read_aln, out_r, w.span.s_lo, w.span.s_hi, w.span.o_base_r, lane, st16);
