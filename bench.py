@@ -348,7 +348,7 @@ def tune_bins(bs, dbs, status, sample: int = 1_000_000) -> dict:
     """Autotunes the launch shape of every (read length, k) bin on the
     first `sample` candidates of the bin itself: the cost model (trained on
     the GPU from the committed B200 sweep) ranks the shapes, the tuner
-    times its top 3 and the default, and installs the fastest."""
+    times its top 6 and the default, and installs the fastest."""
     from saruman_b200 import autotune as A
     from saruman_b200 import costmodel as CM
     t0 = time.perf_counter()
@@ -357,7 +357,7 @@ def tune_bins(bs, dbs, status, sample: int = 1_000_000) -> dict:
     out = {}
     for b, d in zip(bs, dbs):
         smp = A.Sample.wrap(b, d.sb, d.sr, status).prefix(min(b.n, sample))
-        r = A.tune_bin(smp, model=model, top=3)
+        r = A.tune_bin(smp, model=model, top=6)
         out[f"{b.m},{b.k}"] = {"shape": list(r["best"]), "trials": len(r["ms"]),
                                "ms_sample": r["ms"][r["best"]],
                                "default_ms_sample": r["default_ms"]}

@@ -25,7 +25,7 @@ CACHE = Path(__file__).resolve().parent / "tuning_cache.json"
 def search_space(k: int) -> list[tuple[int, int, int]]:
     """Every shape the tuner may pick for a bin with threshold k."""
     words = (32, 64) if k <= 7 else (64,)
-    return [(w, c, b) for w in (1, 2, 4) for c in (0, 2, 3) for b in words]
+    return [(w, c, b) for w in (1, 2, 3, 4) for c in (0, 2, 3) for b in words]
 
 
 def default_shape(k: int) -> tuple[int, int, int]:

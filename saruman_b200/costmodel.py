@@ -18,7 +18,7 @@ from pathlib import Path
 
 import numpy as np
 
-N_FEATURES = 13
+N_FEATURES = 14
 SWEEP = Path(__file__).resolve().parent / "tuning_sweep_b200.json"
 
 
@@ -33,7 +33,7 @@ def features(m: int, k: int, so_frac: float, n: int, shape) -> np.ndarray:
     word64 = b == 64 or (b == 0 and k > 7)
     return np.array([
         math.log2(m) / 8.0, k / 16.0, so_frac, math.log2(max(n, 1)) / 21.0,
-        float(w == 1), float(w == 2), float(w in (0, 4)),
+        float(w == 1), float(w == 2), float(w == 3), float(w in (0, 4)),
         float(c == 0), float(c == 2), float(c == 3),
         float(word64), math.log2(band_cells(m, k, so_frac)) / 16.0,
         math.log2(max(n, 1) / 32.0 / 148.0 + 1.0) / 10.0,  # tiles per SM

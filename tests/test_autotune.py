@@ -13,7 +13,7 @@ from saruman_b200 import workloads as W
 
 
 def test_search_space():
-    assert len(A.search_space(5)) == 18 and len(A.search_space(9)) == 9
+    assert len(A.search_space(5)) == 24 and len(A.search_space(9)) == 12
     assert all(b == 64 for _, _, b in A.search_space(12))
 
 
@@ -57,6 +57,6 @@ def test_tuner_installs_its_fastest_shape(saru_lib):
         res = A.tune_bin(sample, reps=3)
         assert S.get_tuning(100, 5) == tuple(res["best"])
         assert res["ms"][res["best"]] <= res["default_ms"]
-        assert len(res["ms"]) == 19  # the search space and the default shape
+        assert len(res["ms"]) == 25  # the search space and the default shape
     finally:
         S.clear_tuning()

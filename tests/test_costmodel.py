@@ -96,7 +96,7 @@ def test_trained_model_beats_the_method_without_it(saru_lib):
     """Trained on the bins of six read lengths, the network ranks the launch
     shapes of the two held-out read lengths.  Without it the tuner either
     keeps the default shape (no trials) or times the whole search space
-    (9-18 trials per bin).  With it, its top-ranked shape alone is at
+    (12-24 trials per bin).  With it, its top-ranked shape alone is at
     least as fast as the default on average, and timing its top 3 comes
     within 3% of the exhaustive search's best."""
     data, bins = load_sweep()
