@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/saruman_b200.h"
@@ -116,8 +117,11 @@ struct DevBuf {
 
 struct Lane {
   int device = -1;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;          // copies in (and the unsplit path)
+  cudaStream_t s_run = nullptr, s_out = nullptr;  // split calls: kernels, copies out
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_run = nullptr;             // a slice aligned
+  std::vector<cudaEvent_t> ev_in;            // a slice's inputs landed (one per slice)
   DevBuf genome, reads, goff, roff, dirs, scores, ra, ga, scratch, status, eoff, arena;
   int *status_host = nullptr;  // pinned
   std::mutex mu;
@@ -126,8 +130,11 @@ struct Lane {
     if (device == dev && stream) return SARU_OK;
     SARU_CUDA(cudaSetDevice(dev));
     SARU_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    SARU_CUDA(cudaStreamCreateWithFlags(&s_run, cudaStreamNonBlocking));
+    SARU_CUDA(cudaStreamCreateWithFlags(&s_out, cudaStreamNonBlocking));
     SARU_CUDA(cudaEventCreate(&ev0));
     SARU_CUDA(cudaEventCreate(&ev1));
+    SARU_CUDA(cudaEventCreateWithFlags(&ev_run, cudaEventDisableTiming));
     SARU_CUDA(cudaMallocHost(&status_host, sizeof(int)));
     device = dev;
     return SARU_OK;
@@ -141,10 +148,15 @@ struct Lane {
     if (status_host) cudaFreeHost(status_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : ev_in) cudaEventDestroy(e);
+    ev_in.clear();
+    if (ev_run) cudaEventDestroy(ev_run);
     if (stream) cudaStreamDestroy(stream);
+    if (s_run) cudaStreamDestroy(s_run);
+    if (s_out) cudaStreamDestroy(s_out);
     status_host = nullptr;
-    ev0 = ev1 = nullptr;
-    stream = nullptr;
+    ev0 = ev1 = ev_run = nullptr;
+    stream = s_run = s_out = nullptr;
     device = -1;
   }
 };
@@ -183,35 +195,89 @@ struct Plan {
 // Host-side check of a host batch: the banded kernel needs unit costs, one
 // read length m > 3k with m <= kMaxBandM, k <= 15, and windows of exactly
 // m + so + eo bytes (the layout src/hash.c:986-1059 builds).
+// One range of candidates of plan_host's pass.
+struct PlanPart {
+  int64_t cells = 0;
+  int max_m = 0, m_first = -1, bad = -1;
+  bool uniform = true, regular = true, start_gap = false;
+};
+
+// (in locals, stored once at the end: the parts of the threads share cache
+// lines)
+void plan_range(const saru_batch *b, int lo, int hi, PlanPart *out) {
+  const int k = b->k;
+  const int32_t *go = b->genome_offsets, *ro = b->read_offsets;
+  const int8_t *dirs = b->dirs;
+  int64_t prev_g = lo ? go[lo - 1] : 0;
+  int64_t prev_r = lo ? ro[lo - 1] : 0;
+  PlanPart p;
+  for (int t = lo; t < hi; ++t) {
+    const int64_t L = (int64_t)go[t] - prev_g;
+    const int64_t m = (int64_t)ro[t] - prev_r;
+    if (L <= 0 || m <= 0 || L > 32000 || m > 32000) {
+      p.bad = t;
+      break;
+    }
+    prev_g = go[t];
+    prev_r = ro[t];
+    if (p.m_first < 0) p.m_first = (int)m;
+    p.uniform &= m == p.m_first;
+    if (m > p.max_m) p.max_m = (int)m;
+    int so, eo;
+    saru::flank_of(dirs[t], k, so, eo);
+    p.start_gap |= so != 0;
+    p.regular &= L == m + so + eo;
+    p.cells += (m + 1) * (L + 1);
+  }
+  *out = p;
+}
+
 int plan_host(const saru_batch *b, Plan *pl) {
   if (b->n < 0 || b->k < 0) {
     set_error("invalid batch: n=%d k=%d", b->n, b->k);
     return SARU_E_INVALID;
   }
   const int n = b->n, k = b->k;
-  int64_t prev_g = 0, prev_r = 0, cells = 0;
+  // one pass over the offsets, split over host threads for large calls
+  int nt = (int)std::min<long>(16, std::max<long>(1, n / 262144));
+  const int hw = (int)std::thread::hardware_concurrency();
+  if (hw > 0 && nt > hw) nt = hw;
+  std::vector<PlanPart> parts((size_t)nt);
+  auto range = [&](int i) {
+    plan_range(b, (int)((int64_t)n * i / nt), (int)((int64_t)n * (i + 1) / nt), &parts[(size_t)i]);
+  };
+  if (nt == 1) {
+    range(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int i = 1; i < nt; ++i) th.emplace_back(range, i);
+    range(0);
+    for (auto &x : th) x.join();
+  }
+  int64_t cells = 0;
   int m0 = -1;
   bool uniform = true, regular = true, any_start_gap = false;
   int max_m = 0;
-  for (int t = 0; t < n; ++t) {
-    const int64_t L = (int64_t)b->genome_offsets[t] - prev_g;
-    const int64_t m = (int64_t)b->read_offsets[t] - prev_r;
-    if (L <= 0 || m <= 0 || L > 32000 || m > 32000) {
+  for (const PlanPart &p : parts) {
+    if (p.bad >= 0) {
+      const int t = p.bad;
+      const int64_t L = (int64_t)b->genome_offsets[t] - (t ? b->genome_offsets[t - 1] : 0);
+      const int64_t m = (int64_t)b->read_offsets[t] - (t ? b->read_offsets[t - 1] : 0);
       set_error("invalid batch: candidate %d has window %lld, read %lld", t, (long long)L,
                 (long long)m);
       return SARU_E_INVALID;
     }
-    prev_g = b->genome_offsets[t];
-    prev_r = b->read_offsets[t];
-    if (m0 < 0) m0 = (int)m;
-    if (m != m0) uniform = false;
-    if (m > max_m) max_m = (int)m;
-    int so, eo;
-    saru::flank_of(b->dirs[t], k, so, eo);
-    if (so) any_start_gap = true;
-    if (L != m + so + eo) regular = false;
-    cells += (m + 1) * (L + 1);
+    cells += p.cells;
+    if (p.m_first >= 0) {
+      if (m0 < 0) m0 = p.m_first;
+      if (p.m_first != m0 || !p.uniform) uniform = false;
+    }
+    regular = regular && p.regular;
+    any_start_gap = any_start_gap || p.start_gap;
+    max_m = std::max(max_m, p.max_m);
   }
+  const int64_t prev_g = n ? b->genome_offsets[n - 1] : 0;
+  const int64_t prev_r = n ? b->read_offsets[n - 1] : 0;
   if (n > 0 && (prev_g != b->genome_bytes || prev_g > INT32_MAX || prev_r > INT32_MAX)) {
     set_error("invalid batch: genome_bytes %lld does not match offsets (%lld)",
               (long long)b->genome_bytes, (long long)prev_g);
@@ -264,11 +330,17 @@ size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
 // the tile counter, then the decision planes of the persistent grid.
 using saru::CompactOut;
 
+// t0 > 0 (a multiple of 32, one call): align candidates t0 .. n - 1 only.
 int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, const Plan &pl,
                    void *scratch, size_t scratch_bytes, int *status_dev, int dev,
-                   cudaStream_t s, long max_grid = 0, const CompactOut *cmp = nullptr) {
+                   cudaStream_t s, long max_grid = 0, const CompactOut *cmp = nullptr,
+                   long t0 = 0) {
   if (ncalls < 1 || ncalls > saru::kMaxSegs) {
     set_error("%d calls in one launch (1..%d)", ncalls, saru::kMaxSegs);
+    return SARU_E_INVALID;
+  }
+  if (t0 < 0 || (t0 & 31) || (t0 > 0 && ncalls != 1)) {
+    set_error("a slice of a call starts at a multiple of 32 (%ld)", t0);
     return SARU_E_INVALID;
   }
   // heavier segments first: the counter hands out tiles in segment order, so
@@ -306,13 +378,14 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
       g.rec_bytes = cmp[order[(size_t)q]].rec_bytes;
     }
     g.n = b->n;
+    g.t0 = t0 < b->n ? t0 : b->n;
     g.tile_begin = tiles;
     g.k = b->k;
     g.max_m = b->max_read_length;
     g.first_of_call = b->first_of_call;
     g.wide = (b->k > 7 && (ncalls > 1 || pl.wide)) || tn.word_bits == 64;
-    tiles += (b->n + 31) / 32;
-    total_n += b->n;
+    tiles += (b->n - g.t0 + 31) / 32;
+    total_n += b->n - g.t0;
     wide_any |= g.wide;
   }
   if (tiles == 0) return SARU_OK;
@@ -460,16 +533,17 @@ int run_band_classes(const saru_batch *calls, const saru_result *res, int ncalls
 
 int run_band(const saru_batch *b, const Plan &pl, const saru_result *r, void *scratch,
              size_t scratch_bytes, int *status_dev, int dev, cudaStream_t s,
-             long max_grid = 0, const CompactOut *cmp = nullptr) {
+             long max_grid = 0, const CompactOut *cmp = nullptr, long t0 = 0) {
   if (b->n == 0) return SARU_OK;
   saru_batch one = *b;
   one.max_read_length = pl.max_m;
   return run_band_multi(&one, r, 1, pl, scratch, scratch_bytes, status_dev, dev, s, max_grid,
-                        cmp);
+                        cmp, t0);
 }
 
-// Host batch -> device buffers of `lane`, returns device-side view.
-int upload(Lane &L, const saru_batch *b, saru_batch *db) {
+// Host batch -> device buffers of `lane`, returns device-side view (with
+// copy false: the buffers only, the caller copies).
+int upload(Lane &L, const saru_batch *b, saru_batch *db, bool copy = true) {
   const size_t n = (size_t)b->n;
   int rc;
   if ((rc = L.genome.ensure((size_t)b->genome_bytes + 64))) return rc;
@@ -478,7 +552,7 @@ int upload(Lane &L, const saru_batch *b, saru_batch *db) {
   if ((rc = L.roff.ensure(4 * n + 64))) return rc;
   if ((rc = L.dirs.ensure(n + 64))) return rc;
   cudaStream_t s = L.stream;
-  if (n) {
+  if (n && copy) {
     SARU_CUDA(cudaMemcpyAsync(L.genome.p, b->genome, (size_t)b->genome_bytes, cudaMemcpyHostToDevice, s));
     SARU_CUDA(cudaMemcpyAsync(L.reads.p, b->reads, (size_t)b->read_offsets[n - 1], cudaMemcpyHostToDevice, s));
     SARU_CUDA(cudaMemcpyAsync(L.goff.p, b->genome_offsets, 4 * n, cudaMemcpyHostToDevice, s));
@@ -543,10 +617,121 @@ int run_full(Lane &L, const saru_batch *hb, const saru_batch *db, const Plan &pl
   return SARU_OK;
 }
 
+// A call of at least 2 * kSplitMin candidates from host memory is split
+// into slices of whole tiles.  The copies in of every slice are issued
+// first (one event each), and the host's pass over the call (plan_host)
+// runs while they stream; then, for a banded call, the kernel of slice i
+// waits for its inputs and the copies out of slice i wait for its kernel,
+// so copies in, kernels and copies out overlap on three streams (the
+// reference copies everything in, aligns, copies everything out).  Each
+// slice is a launch over candidates [t0, t1) of the whole call on the
+// device, so its tiles, and every output byte, are the ones the unsplit
+// launch makes; only candidate 0 of the call takes the first-of-call rule.
+// With pinned host buffers the copies run asynchronously; with pageable
+// ones they are correct but serialised.
+constexpr long kSplitMin = 1L << 18;
+constexpr long kSplitParts = 32;
+
+long split_chunk(long n) {
+  const long c = ((n + kSplitParts - 1) / kSplitParts + 31) & ~31L;
+  return c < kSplitMin ? kSplitMin : c;
+}
+
+// The slice edges of a large call, checked before its copies are issued:
+// each copy reads the caller's arrays between two edges, so the offsets
+// there must not decrease and must end at the sizes the call states.
+int check_slice_edges(const saru_batch *b, long chunk) {
+  const long n = b->n;
+  int64_t pg = 0, pr = 0;
+  for (long t1 = std::min(n, chunk);; t1 = std::min(n, t1 + chunk)) {
+    const int64_t g = b->genome_offsets[t1 - 1], r = b->read_offsets[t1 - 1];
+    if (g < pg || r < pr) {
+      set_error("invalid batch: offsets decrease before candidate %ld", t1 - 1);
+      return SARU_E_INVALID;
+    }
+    pg = g;
+    pr = r;
+    if (t1 == n) break;
+  }
+  if (pg != b->genome_bytes || pg > INT32_MAX || pr > INT32_MAX) {
+    set_error("invalid batch: genome_bytes %lld does not match offsets (%lld)",
+              (long long)b->genome_bytes, (long long)pg);
+    return SARU_E_INVALID;
+  }
+  return SARU_OK;
+}
+
+// Copies in, slice by slice, on the lane's first stream.
+int upload_slices(Lane &L, const saru_batch *b, long chunk) {
+  const long n = b->n;
+  const size_t nslices = (size_t)((n + chunk - 1) / chunk);
+  while (L.ev_in.size() < nslices) {
+    cudaEvent_t e;
+    SARU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    L.ev_in.push_back(e);
+  }
+  cudaStream_t si = L.stream;
+  const int32_t *go = b->genome_offsets, *ro = b->read_offsets;
+  for (long t0 = 0, i = 0; t0 < n; t0 += chunk, ++i) {
+    const long t1 = std::min(n, t0 + chunk);
+    const long g0 = t0 ? go[t0 - 1] : 0, g1 = go[t1 - 1];
+    const long r0 = t0 ? ro[t0 - 1] : 0, r1 = ro[t1 - 1];
+    SARU_CUDA(cudaMemcpyAsync(L.genome.as<char>() + g0, b->genome + g0, (size_t)(g1 - g0),
+                              cudaMemcpyHostToDevice, si));
+    SARU_CUDA(cudaMemcpyAsync(L.reads.as<char>() + r0, b->reads + r0, (size_t)(r1 - r0),
+                              cudaMemcpyHostToDevice, si));
+    SARU_CUDA(cudaMemcpyAsync(L.goff.as<int32_t>() + t0, go + t0, 4 * (size_t)(t1 - t0),
+                              cudaMemcpyHostToDevice, si));
+    SARU_CUDA(cudaMemcpyAsync(L.roff.as<int32_t>() + t0, ro + t0, 4 * (size_t)(t1 - t0),
+                              cudaMemcpyHostToDevice, si));
+    SARU_CUDA(cudaMemcpyAsync(L.dirs.as<int8_t>() + t0, b->dirs + t0, (size_t)(t1 - t0),
+                              cudaMemcpyHostToDevice, si));
+    SARU_CUDA(cudaEventRecord(L.ev_in[(size_t)i], si));
+  }
+  return SARU_OK;
+}
+
+// Kernels and copies out of the slices (after upload_slices).
+int band_slices(Lane &L, const saru_batch *b, const Plan &pl, const saru_batch &db,
+                const saru_result &dr, const saru_result *r, int dev, long chunk) {
+  const long n = b->n, k = b->k;
+  int rc;
+  const long grid = band_grid(dev, chunk, pl.max_m, b->k);
+  if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, b->k, pl.wide)))) return rc;
+  cudaStream_t sr = L.s_run, so = L.s_out;
+  const int32_t *go = b->genome_offsets;
+  for (long t0 = 0, i = 0; t0 < n; t0 += chunk, ++i) {
+    const long t1 = std::min(n, t0 + chunk);
+    const long g0 = t0 ? go[t0 - 1] : 0, g1 = go[t1 - 1];
+    SARU_CUDA(cudaStreamWaitEvent(sr, L.ev_in[(size_t)i], 0));
+    saru_batch slice = db;
+    slice.n = (int32_t)t1;
+    if ((rc = run_band(&slice, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, sr, 0,
+                       nullptr, t0)))
+      return rc;
+    SARU_CUDA(cudaEventRecord(L.ev_run, sr));
+    SARU_CUDA(cudaStreamWaitEvent(so, L.ev_run, 0));
+    const long s0 = g0 + k * t0, s1 = g1 + k * t1;
+    SARU_CUDA(cudaMemcpyAsync(r->scores + t0, dr.scores + t0, 4 * (size_t)(t1 - t0),
+                              cudaMemcpyDeviceToHost, so));
+    SARU_CUDA(cudaMemcpyAsync(r->read_aln + s0, dr.read_aln + s0, (size_t)(s1 - s0),
+                              cudaMemcpyDeviceToHost, so));
+    SARU_CUDA(cudaMemcpyAsync(r->genome_aln + s0, dr.genome_aln + s0, (size_t)(s1 - s0),
+                              cudaMemcpyDeviceToHost, so));
+  }
+  SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, so));
+  SARU_CUDA(cudaEventRecord(L.ev1, so));
+  SARU_CUDA(cudaStreamSynchronize(so));
+  return SARU_OK;
+}
+
 int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out) {
   Plan pl;
-  int rc = plan_host(b, &pl);
-  if (rc) return rc;
+  int rc;
+  const bool big = b->n >= 2 * kSplitMin && b->k >= 0;
+  const long chunk = big ? split_chunk(b->n) : 0;
+  if (!big && (rc = plan_host(b, &pl))) return rc;
+  if (big && (rc = check_slice_edges(b, chunk))) return rc;
   const int dev = current_device();
   if (dev < 0) {
     set_error("no CUDA device");
@@ -557,17 +742,37 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
   if (b->n == 0) return SARU_OK;
   cudaStream_t s = L.stream;
   SARU_CUDA(cudaEventRecord(L.ev0, s));
-  saru_batch db;
-  if ((rc = upload(L, b, &db))) return rc;
   const size_t n = (size_t)b->n;
+  saru_batch db;
+  if ((rc = upload(L, b, &db, !big))) return rc;
   if ((rc = L.scores.ensure(4 * n + 64))) return rc;
   if ((rc = L.ra.ensure((size_t)b->total_slots + 64))) return rc;
   if ((rc = L.ga.ensure((size_t)b->total_slots + 64))) return rc;
   if ((rc = L.status.ensure(64))) return rc;
   saru_result dr{L.scores.as<int32_t>(), L.ra.as<char>(), L.ga.as<char>(), L.status.as<int32_t>()};
   SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
-  bool full = !pl.band;
-  if (pl.band) {
+  if (big) {  // copies in first; the host's pass over the call runs meanwhile
+    if ((rc = upload_slices(L, b, chunk))) return rc;
+    if ((rc = plan_host(b, &pl))) {
+      cudaStreamSynchronize(s);
+      return rc;
+    }
+  }
+  const bool split = big && pl.band;
+  bool full = !pl.band, copied = false;
+  if (split) {
+    if ((rc = band_slices(L, b, pl, db, dr, r, dev, chunk))) return rc;
+    const int st = *L.status_host;
+    if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
+      full = true;  // rare bytes or layouts: redo the call on the exact path
+      SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
+    } else if (st & saru::kStatusOverflow) {
+      set_error("banded traceback left its band (status %d)", st);
+      return SARU_E_OVERFLOW;
+    } else {
+      copied = true;
+    }
+  } else if (pl.band) {
     const long grid = band_grid(dev, b->n, pl.max_m, b->k);
     if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, b->k, pl.wide)))) return rc;
     if ((rc = run_band(&db, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, s)))
@@ -587,11 +792,13 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
     if ((rc = run_full(L, b, &db, pl, &dr))) return rc;
     SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   }
-  SARU_CUDA(cudaMemcpyAsync(r->scores, dr.scores, 4 * n, cudaMemcpyDeviceToHost, s));
-  SARU_CUDA(cudaMemcpyAsync(r->read_aln, dr.read_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
-  SARU_CUDA(cudaMemcpyAsync(r->genome_aln, dr.genome_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
-  SARU_CUDA(cudaEventRecord(L.ev1, s));
-  SARU_CUDA(cudaStreamSynchronize(s));
+  if (!copied) {
+    SARU_CUDA(cudaMemcpyAsync(r->scores, dr.scores, 4 * n, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaMemcpyAsync(r->read_aln, dr.read_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaMemcpyAsync(r->genome_aln, dr.genome_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaEventRecord(L.ev1, s));
+    SARU_CUDA(cudaStreamSynchronize(s));
+  }
   if (full && (*L.status_host & saru::kStatusOverflow)) {
     set_error("a traceback left its slot; the reference result depends on thread order");
     return SARU_E_OVERFLOW;

@@ -38,6 +38,7 @@ struct TileArgs {
   long rs_bytes, ws_bytes, region_bytes;
   uint8_t *records;  // compact result records instead of slot strings (nullptr: slots)
   long rec_bytes;    // bytes per record (compact_record_bytes)
+  long t0;           // first candidate (a multiple of 32); n is one past the last
 };
 
 // Byte ranges of a tile in the three arrays.
@@ -59,7 +60,7 @@ SARU_HD long stage_base(const void *p, long lo) {
 
 SARU_HD TileSpan tile_span(const TileArgs &a, long wt) {
   TileSpan s;
-  s.t0 = wt * 32;
+  s.t0 = a.t0 + wt * 32;
   s.t1 = s.t0 + 32 < a.n ? s.t0 + 32 : a.n;
   s.r_lo = s.t0 ? a.roff[s.t0 - 1] : 0;
   s.r_hi = a.roff[s.t1 - 1];

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(128, 4) saru_band_kernel(const __grid_constant
     const TileArgs ta{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
                       g.first_of_call, g.scores, g.read_aln, g.genome_aln, a.planes, pstride,
                       (!g.wide && a.wide_any) ? 2L : 1L, a.rs_bytes, a.ws_bytes,
-                      a.warp_smem - a.rs_bytes - a.ws_bytes, g.records, g.rec_bytes};
+                      a.warp_smem - a.rs_bytes - a.ws_bytes, g.records, g.rec_bytes, g.t0};
     const long wt = tile - g.tile_begin;
     int status = g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
                         : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);

@@ -30,7 +30,8 @@ struct Segment {
   int *status;      // this call's status word (device)
   uint8_t *records;  // compact result records instead of slot strings (nullptr: slots)
   long rec_bytes;
-  long n;
+  long n;           // candidates t0 .. n - 1 of the call's arrays are this segment's
+  long t0;          // (t0 > 0, a multiple of 32: a later slice of a call)
   long tile_begin;  // first 32-candidate tile of this segment in the launch
   int k, max_m, first_of_call, wide;
 };

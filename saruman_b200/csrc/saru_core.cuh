@@ -124,15 +124,13 @@ struct Cand {
   bool first_of_call;  // candidate 0 of a reference call: traceback stops on row 0
 };
 
+// Flags 1/5: end gap free (eo = k); 2/6: start gap (so = k); 3/7: both;
+// anything else (0/4 are perfect hits): none.  Branch-free: bit 0 of a flag
+// in 0..7 is the end gap, bit 1 the start gap.
 SARU_HD void flank_of(int dir, int k, int &so, int &eo) {
-  so = 0;
-  eo = 0;
-  switch (dir) {
-    case 1: case 5: eo = k; break;
-    case 2: case 6: so = k; break;
-    case 3: case 7: so = k; eo = k; break;
-    default: break;
-  }
+  const bool valid = (unsigned)dir <= 7u;
+  so = (valid && (dir & 2)) ? k : 0;
+  eo = (valid && (dir & 1)) ? k : 0;
 }
 
 // Builds the read-class codes (4 bits each, 8 per word) and the window

@@ -1,0 +1,57 @@
+"""The host entry point splits a large banded call into slices of whole
+32-candidate tiles whose copies in, kernels and copies out overlap on three
+streams.  Its output must be the bytes one launch over the whole call gives:
+here a 660k-candidate C2-shaped call (three slices, the last one partial)
+through saru_align_host against the same call through saru_align_device in
+a single launch."""
+from __future__ import annotations
+
+import importlib.util
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import saruman_b200 as S
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def load_bench():
+    spec = importlib.util.spec_from_file_location("bench_split", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["bench_split"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_split_host_call_equals_one_launch(saru_lib):
+    import torch
+    bench = load_bench()
+    cfg = dict(bench.CONFIGS["c2"])
+    cfg["reads"] = 70_000
+    b = bench.build_batches(cfg, 0)[0]
+    assert 2 * (1 << 18) <= b.n < 3 * (1 << 18) and b.n % 32 != 0
+    host = S.align_host(b)
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    g, r, go, ro, d = T(b.genome), T(b.reads), T(b.genome_offsets), T(b.read_offsets), T(b.dirs)
+    sc = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    sb = S.SaruBatch(g.data_ptr(), r.data_ptr(), go.data_ptr(), ro.data_ptr(), d.data_ptr(), b.n,
+                     b.k, 0, 1, 1, b.m, len(b.genome), b.total_genome)
+    sr = S.SaruResult(sc.data_ptr(), ra.data_ptr(), ga.data_ptr(), st.data_ptr())
+    nscr = S.scratch_bytes(b.n, b.m, b.k)
+    scr = torch.empty(nscr, dtype=torch.uint8, device=dev)
+    S.align_device(sb, sr, scr.data_ptr(), nscr)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    assert np.array_equal(host.scores, sc.cpu().numpy())
+    assert np.array_equal(host.read_aln, ra.cpu().numpy()[:b.total_genome])
+    assert np.array_equal(host.genome_aln, ga.cpu().numpy()[:b.total_genome])
+    assert (host.scores <= b.k).sum() > b.n // 4
+
