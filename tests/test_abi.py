@@ -68,3 +68,27 @@ def test_writer_matches_reference_writer(saru_lib, name):
 def test_load_fails_loudly_without_library(tmp_path):
     with pytest.raises(RuntimeError, match="not built"):
         S.load(tmp_path / "missing.so")
+
+
+def test_large_call_offsets_checked_before_any_copy(saru_lib):
+    """A call large enough to be streamed in slices has the offsets at its
+    slice edges checked before any copy is issued: each copy reads the
+    caller's arrays between two edges.  Host code only: the check comes
+    before the library looks for a device."""
+    n, m, k = 600_000, 36, 2
+    L = np.full(n, m + k, np.int64)
+    go = np.cumsum(L).astype(np.int32)
+    ro = (np.arange(1, n + 1) * m).astype(np.int32)
+    dirs = np.ones(n, np.int8)
+    genome = np.zeros(int(go[-1]), np.uint8)
+    reads = np.zeros(int(ro[-1]), np.uint8)
+    bad_go = go.copy()
+    bad_go[(2 << 18) - 1] = go[(1 << 18) - 1] - 7  # the second slice edge before the first
+    for offs, total, what in ((bad_go, int(go[-1]), "decrease"),
+                              (go, int(go[-1]) - 1, "genome_bytes")):
+        sb = S.SaruBatch(genome.ctypes.data, reads.ctypes.data, offs.ctypes.data, ro.ctypes.data,
+                         dirs.ctypes.data, n, k, 0, 1, 1, m, total, int(go[-1]) + k * n)
+        res = S.SaruResult(None, None, None, None)
+        rc = saru_lib.saru_align_host(C.byref(sb), C.byref(res), 0)
+        assert rc == S.SARU_E_INVALID
+        assert what in S.last_error()
