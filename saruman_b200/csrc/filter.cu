@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
           if (item < n1) {
             const int b = a + 1 + item / zones, ez = item % zones - k;
             const uint32_t want = (uint32_t)gs + (uint32_t)b * q + 1 + (uint32_t)ez;
-            hits = scan_from(L, b, L.at(b, off), want);
+            hits = scan_from_at(L, b, P, off, want);
             if (b == half - 1 && first) {
               flag = 1 + dr;
               start = gs + 1;

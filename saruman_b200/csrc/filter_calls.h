@@ -37,16 +37,14 @@ class CallAssembler {
   // The read's kept positions, in the order the filter kept them.
   void add_read(int32_t id, const int32_t *pos, const int8_t *flag, int n, int queue) {
     if (n > 0) {
-      Entry e;
-      e.id = id;
-      e.pos.assign(pos, pos + n);
-      e.flag.assign(flag, flag + n);
+      entries_.push_back(Entry{id, (uint32_t)pos_.size(), (uint32_t)n});
+      pos_.insert(pos_.end(), pos, pos + n);
+      flag_.insert(flag_.end(), flag, flag + n);
       for (int i = 0; i < n; ++i)
         if (flag[i] == 0) {  // a perfect hit (kept only with a negative position)
           out.perfect_ids.push_back(id);
           out.perfect_pos.push_back(-pos[i]);
         }
-      entries_.push_back(std::move(e));
     }
     queue_ += (uint32_t)queue;
     if (queue_ > chunk_) flush();
@@ -59,35 +57,45 @@ class CallAssembler {
   FilterCalls out;
 
  private:
+  // a read's positions: pos_/flag_[at, at + n)
   struct Entry {
     int32_t id;
-    std::vector<int32_t> pos;
-    std::vector<int8_t> flag;
+    uint32_t at, n;
   };
 
   void flush() {
     const int64_t before = (int64_t)out.ids.size();
-    size_t keep = 0;
+    size_t keep = 0, kept_values = 0;
     for (size_t e = 0; e < entries_.size(); ++e) {
-      Entry &E = entries_[e];
+      const Entry E = entries_[e];
       bool pending = false;
-      for (size_t i = 0; i < E.pos.size(); ++i) {
-        if (E.pos[i] <= 0) continue;
+      for (uint32_t i = E.at; i < E.at + E.n; ++i) {
+        if (pos_[i] <= 0) continue;
         int so = 0, eo = 0;
-        flank_of(E.flag[i], k_, so, eo);
-        if ((int64_t)(uint32_t)E.pos[i] + m_ + so + eo > glen_) {
+        flank_of(flag_[i], k_, so, eo);
+        if ((int64_t)(uint32_t)pos_[i] + m_ + so + eo > glen_) {
           pending = true;  // stays positive: looked at again by later calls
           continue;
         }
         out.ids.push_back(E.id);
-        out.pos.push_back(E.pos[i]);
-        out.dirs.push_back(E.flag[i]);
-        E.pos[i] = -E.pos[i];
+        out.pos.push_back(pos_[i]);
+        out.dirs.push_back(flag_[i]);
+        pos_[i] = -pos_[i];
       }
-      // reads left with nothing positive can never contribute again
-      if (pending) entries_[keep++] = std::move(E);
+      // reads left with nothing positive can never contribute again; the
+      // others move down to the front of the arrays
+      if (pending) {
+        for (uint32_t i = 0; i < E.n; ++i) {
+          pos_[kept_values + i] = pos_[E.at + i];
+          flag_[kept_values + i] = flag_[E.at + i];
+        }
+        entries_[keep++] = Entry{E.id, (uint32_t)kept_values, E.n};
+        kept_values += E.n;
+      }
     }
     entries_.resize(keep);
+    pos_.resize(kept_values);
+    flag_.resize(kept_values);
     if ((int64_t)out.ids.size() > before) out.call_begin.push_back((int64_t)out.ids.size());
     queue_ = 0;
   }
@@ -97,6 +105,8 @@ class CallAssembler {
   uint32_t chunk_;
   uint32_t queue_ = 0;
   std::vector<Entry> entries_;
+  std::vector<int32_t> pos_;
+  std::vector<int8_t> flag_;
 };
 
 }  // namespace saru

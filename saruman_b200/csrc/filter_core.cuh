@@ -137,6 +137,26 @@ SARU_HD int scan_from(const Lists &L, int x, uint32_t v0, uint32_t want) {
   }
 }
 
+// scan_from over list x from index `off` (nlists: the read's lists),
+// the same count in fewer reads of the data array.  An empty list x read
+// from off >= 1 starts in list x + 1, which follows its terminating 0:
+// the value at off is element off - 1 of list x + 1 (its 0 when off - 1 is
+// its length), and the walk from index 1 is list x + 1 from its start to
+// its 0.  Positions in a list ascend, so a 0 inside one can only be its
+// first element (the walk then stops at once) and the walk's match is one
+// search.  Any other case takes scan_from itself.
+template <class Lists>
+SARU_HD int scan_from_at(const Lists &L, int x, int nlists, uint32_t off, uint32_t want) {
+  if (L.len(x) >= 1 || off == 0 || x + 1 >= nlists) return scan_from(L, x, L.at(x, off), want);
+  const uint32_t len1 = L.len(x + 1);
+  const uint32_t v0 =
+      off - 1 < len1 ? L.at(x + 1, off - 1) : (off - 1 == len1 ? 0u : L.at(x, off));
+  if (v0 == 0) return 0;
+  const int hits = v0 == want ? 1 : 0;
+  if (len1 == 0 || L.at(x + 1, 0) == 0) return hits;
+  return hits + (L.find(x + 1, 0, want) >= 0 ? 1 : 0);
+}
+
 template <class Lists>
 SARU_HD int scan_all(const Lists &L, int x, uint32_t want) {
   if (L.at(x, 0) == 0) return 0;
@@ -164,9 +184,8 @@ SARU_HD void filter_read(const FilterShape &S, int dr, const Lists &L, Perfect p
         // scan at a's current index
         for (int b = a + 1; b < half; ++b) {
           const uint32_t rs = (uint32_t)b * q + 1;
-          const uint32_t v0 = L.at(b, off);  // the same for every error zone
           for (int ez = -k; ez <= k; ++ez) {
-            const int hits = scan_from(L, b, v0, (uint32_t)gs + rs + (uint32_t)ez);
+            const int hits = scan_from_at(L, b, S.P, off, (uint32_t)gs + rs + (uint32_t)ez);
             for (int t = 0; t < hits; ++t) {
               int flag, start;
               if (b == half - 1 && first) {
