@@ -275,7 +275,48 @@ int saru_filter_results(const saru_filter *f, int64_t *call_begin, int32_t *ids,
 /* Device time of the last run's filter (ms), and the resident genome (device). */
 double saru_filter_last_ms(const saru_filter *f);
 const char *saru_filter_genome(const saru_filter *f);
+/* The filter's genome as chunk of a larger genome (the reference's -G loop,
+ * src/saruman.c:181-415): `offset` is the genome position of its first
+ * byte, `limit` the position windows must end by (the reference's
+ * total_bases_read, src/hash.c:982).  The q-gram lists then hold positions
+ * in the whole genome (src/util.c:481), starts at or before the chunk's
+ * first byte are not taken (src/hash.c:545), and the calls' positions are
+ * whole-genome positions (windows at position - offset in the chunk).
+ * Default: offset 0, limit = the genome's length. */
+int saru_filter_set_chunk(saru_filter *f, int64_t offset, int64_t limit);
 void saru_filter_destroy(saru_filter *f);
+
+/* ---- input readers (host): the reference's read and genome readers -------
+ * Reads of a FASTA (fastq = 0) or FASTQ file in the reference's batches
+ * (replaces read_multiple_fasta_file, src/util.c:294-452): records of 2 or
+ * 4 lines read as fgets reads them (names into 60 bytes, sequence lines
+ * into read_length + 2), sequences cut at read_length and upper-cased;
+ * shorter reads and reads with more than max_n Ns are dropped.
+ * saru_reads_next takes up to max_entries records: the kept ones go to
+ * reads (read_length bytes each) and names (60-byte NUL-padded slots: the
+ * name line without its first and last byte), *skipped gets the dropped
+ * count; returns the kept count (read ids 0.. of this batch), 0 with
+ * *skipped == 0 at the end of the file, -1 on bad arguments. */
+typedef struct saru_reads saru_reads;
+saru_reads *saru_reads_open(const char *path, int32_t fastq, int32_t read_length, int32_t max_n);
+int32_t saru_reads_next(saru_reads *r, int32_t max_entries, char *reads, char *names,
+                        int32_t *skipped);
+void saru_reads_close(saru_reads *r);
+
+/* The genome of a FASTA file in the reference's chunks (replaces the chunk
+ * loop of src/saruman.c:139-271, -G): each chunk is chunk_value bases and
+ * an overhang of read_length bases, newlines dropped, upper-cased, the
+ * first line skipped.  saru_genome_next writes the chunk (out: at least
+ * chunk_value + read_length + 1 bytes, NUL-terminated), *len its bytes,
+ * *bases its own bases (without the overhang), *total the bases of all
+ * chunks so far (the limit windows must end by); returns 1 for a chunk, 0
+ * after the last one (the first that did not fill chunk_value bases), -1 on
+ * bad arguments.  Chunk i's bytes start at genome position i * chunk_value. */
+typedef struct saru_genome_reader saru_genome_reader;
+saru_genome_reader *saru_genome_open(const char *path, int64_t chunk_value, int32_t read_length);
+int32_t saru_genome_next(saru_genome_reader *g, char *out, int64_t *len, int64_t *bases,
+                         int64_t *total);
+void saru_genome_close(saru_genome_reader *g);
 
 /* Device scratch the banded kernel needs for a batch (bytes). */
 size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);

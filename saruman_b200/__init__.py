@@ -39,7 +39,10 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_mlp_loss_grad", "saru_mlp_adam_step", "saru_compact_record_bytes",
                  "saru_align_device_compact", "saru_expand_compact", "saru_format_tsv_compact",
                  "saru_filter_create", "saru_filter_run", "saru_filter_results",
-                 "saru_filter_last_ms", "saru_filter_genome", "saru_filter_destroy")
+                 "saru_filter_last_ms", "saru_filter_genome", "saru_filter_destroy",
+                 "saru_filter_set_chunk",
+                 "saru_reads_open", "saru_reads_next", "saru_reads_close", "saru_genome_open",
+                 "saru_genome_next", "saru_genome_close")
 ABI_DATA = ("alignment_time",)
 
 
@@ -186,6 +189,22 @@ def load(path: str | Path | None = None):
     lib.saru_filter_genome.argtypes = [C.c_void_p]
     lib.saru_filter_destroy.restype = None
     lib.saru_filter_destroy.argtypes = [C.c_void_p]
+    lib.saru_filter_set_chunk.restype = C.c_int
+    lib.saru_filter_set_chunk.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
+    lib.saru_reads_open.restype = C.c_void_p
+    lib.saru_reads_open.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32]
+    lib.saru_reads_next.restype = C.c_int32
+    lib.saru_reads_next.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_int32)]
+    lib.saru_reads_close.restype = None
+    lib.saru_reads_close.argtypes = [C.c_void_p]
+    lib.saru_genome_open.restype = C.c_void_p
+    lib.saru_genome_open.argtypes = [C.c_char_p, C.c_int64, C.c_int32]
+    lib.saru_genome_next.restype = C.c_int32
+    lib.saru_genome_next.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.saru_genome_close.restype = None
+    lib.saru_genome_close.argtypes = [C.c_void_p]
     lib.saru_int32_issue_probe.restype = C.c_double
     lib.saru_int32_issue_probe.argtypes = [C.c_int]
     if path is None:
@@ -553,16 +572,19 @@ class FilterCalls:
     perfect_pos: np.ndarray
     ms: float
 
-    def call(self, genome: np.ndarray, reads: np.ndarray, m: int, k: int, c: int) -> Batch:
-        """Call c in the reference's call layout (windows cut from the genome,
-        reads reverse-complemented for flags 4-7)."""
+    def call(self, genome: np.ndarray, reads: np.ndarray, m: int, k: int, c: int,
+             offset: int = 0) -> Batch:
+        """Call c in the reference's call layout (windows cut from the genome
+        -- a chunk starting at genome position `offset` --, reads
+        reverse-complemented for flags 4-7; pos stays the genome position)."""
         from .workloads import flank, make_batch, reverse_complement
         lo, hi = int(self.call_begin[c]), int(self.call_begin[c + 1])
         ids, pos, dirs = self.ids[lo:hi], self.pos[lo:hi], self.dirs[lo:hi]
         wins = []
         for p, d in zip(pos, dirs):
             so, eo = flank(int(d), k)
-            wins.append(genome[int(p):int(p) + m + so + eo])
+            at = int(p) - offset
+            wins.append(genome[at:at + m + so + eo])
         rd = reads[ids].copy()
         rev = dirs > 3
         if rev.any():
@@ -580,6 +602,13 @@ class Filter:
         self._h = self._lib.saru_filter_create(_p(g), g.size, m, k, device)
         if not self._h:
             raise SaruError(SARU_E_INVALID, last_error())
+
+    def set_chunk(self, offset: int, limit: int) -> None:
+        """The genome as a chunk at genome position `offset`; windows must end
+        by `limit` (saru_filter_set_chunk)."""
+        rc = self._lib.saru_filter_set_chunk(self._h, offset, limit)
+        if rc != SARU_OK:
+            raise SaruError(rc, last_error())
 
     def run(self, reads: np.ndarray, do_reverse: int, chunk_value: int) -> FilterCalls:
         """One batch of reads (ids from 0), one strand (do_reverse 0 or 4)."""
@@ -610,3 +639,74 @@ class Filter:
 
     def __exit__(self, *exc):
         self.close()
+
+
+@dataclasses.dataclass
+class ReadBatch:
+    """One batch of reads as the reference's reader leaves it."""
+    reads: np.ndarray   # uint8 (n, read_length), upper-case
+    names: list         # bytes, one per read (read id = index)
+    records: int        # records of the file this batch consumed (kept + dropped)
+
+
+def read_batches(path, read_length: int, max_n: int, batch: int, fastq: bool = False):
+    """Yields the reference's read batches of a FASTA/FASTQ file
+    (saru_reads_*): up to `batch` records each, reads with more than `max_n`
+    Ns or shorter than read_length dropped.  Like the reference, a batch
+    whose records were all dropped is followed by the next one, and the
+    batches stop after the first one that did not fill `batch` records."""
+    lib = load()
+    h = lib.saru_reads_open(str(path).encode(), 1 if fastq else 0, read_length, max_n)
+    if not h:
+        raise SaruError(SARU_E_INVALID, last_error())
+    try:
+        reads = np.zeros((batch, read_length), np.uint8)
+        names = np.zeros((batch, 60), np.uint8)
+        skipped = C.c_int32(0)
+        while True:
+            n = lib.saru_reads_next(h, batch, reads.ctypes.data, names.ctypes.data,
+                                    C.byref(skipped))
+            if n < 0:
+                raise SaruError(SARU_E_INVALID, last_error())
+            records = n + skipped.value
+            if records == 0:
+                return
+            if n > 0:
+                nm = [bytes(names[i]).split(b"\0", 1)[0] for i in range(n)]
+                yield ReadBatch(reads[:n].copy(), nm, records)
+            if records < batch:
+                return
+    finally:
+        lib.saru_reads_close(h)
+
+
+@dataclasses.dataclass
+class GenomeChunk:
+    """One genome chunk as the reference's chunk loop leaves it."""
+    seq: np.ndarray  # uint8: the chunk's bases and its overhang
+    offset: int      # genome position of seq[0]
+    bases: int       # the chunk's own bases (without the overhang)
+    total: int       # bases of all chunks so far: windows must end by it
+
+
+def genome_chunks(path, chunk_value: int, read_length: int):
+    """Yields the reference's genome chunks of a FASTA file (saru_genome_*)."""
+    lib = load()
+    h = lib.saru_genome_open(str(path).encode(), chunk_value, read_length)
+    if not h:
+        raise SaruError(SARU_E_INVALID, last_error())
+    try:
+        out = np.zeros(chunk_value + read_length + 1, np.uint8)
+        ln, bases, total = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        run = 0
+        while True:
+            rc = lib.saru_genome_next(h, out.ctypes.data, C.byref(ln), C.byref(bases),
+                                      C.byref(total))
+            if rc < 0:
+                raise SaruError(SARU_E_INVALID, last_error())
+            if rc == 0:
+                return
+            yield GenomeChunk(out[:ln.value].copy(), run * chunk_value, bases.value, total.value)
+            run += 1
+    finally:
+        lib.saru_genome_close(h)

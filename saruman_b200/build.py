@@ -20,7 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libsaruman_b200.so"
 SOURCES = ["kernels.cu", "gather.cu", "filter.cu", "abi.cu", "writer.cpp", "server.cpp", "compact.cpp",
-           "costmodel.cu", "probe.cu"]
+           "costmodel.cu", "probe.cu", "input.cpp"]
 HEADERS = ["kernels.cuh", "saru_core.cuh", "band_tile.cuh", "writer.h", "server_internal.h",
            "filter_core.cuh", "filter_calls.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -152,6 +152,7 @@ struct FilterArgs {
   int32_t *n, *queue;             // per read of the launch
   int *status;
   const int32_t *order;           // the launch's reads (0-based in it), most work first
+  uint32_t offset;                // genome position of the chunk's first byte
 };
 
 // The read's lists on the device: the sorted index's run for each q-gram,
@@ -161,11 +162,12 @@ struct DevLists {
   long base, c0, c1, cend;
   int P;
   const long *lo, *cnt, *offs;  // this read's lists (shared-memory copies)
+  uint32_t off;                 // the chunk's genome position: values are whole-genome positions
   __device__ uint32_t len(int x) const { return (uint32_t)(cnt[x] - 1); }
   __device__ uint32_t at(int x, uint32_t i) const {
     const long t = base + x;
     const long c = cnt[x];
-    if ((long)i + 1 < c) return a->pos[lo[x] + i];
+    if ((long)i + 1 < c) return a->pos[lo[x] + i] + off;
     if ((long)i + 1 == c) return 0u;
     const long j = offs[x] + (long)i;  // past the list: what follows it
     if (j >= cend) return 0u;
@@ -185,17 +187,17 @@ struct DevLists {
       }
     }
     const long w = j - a->offs[l];
-    return w + 1 < a->count[l] ? a->pos[a->lo[l] + w] : 0u;
+    return w + 1 < a->count[l] ? a->pos[a->lo[l] + w] + off : 0u;
   }
   __device__ int find(int x, uint32_t from, uint32_t want) const {
     const long end = lo[x] + cnt[x] - 1;  // ascending positions
     long l = lo[x] + from, u = end;
     while (l < u) {
       const long mid = (l + u) >> 1;
-      if (a->pos[mid] < want) l = mid + 1;
+      if (a->pos[mid] + off < want) l = mid + 1;
       else u = mid;
     }
-    return (l < end && a->pos[l] == want) ? (int)(l - lo[x]) : -1;
+    return (l < end && a->pos[l] + off == want) ? (int)(l - lo[x]) : -1;
   }
 };
 
@@ -265,7 +267,8 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
   }
   __syncwarp();
   const DevLists L{&fa, r * P, c0, c1, fa.offs[c1 * P - 1] + fa.count[c1 * P - 1], P,
-                   s_lo[w], s_cnt[w], s_offs[w]};
+                   s_lo[w], s_cnt[w], s_offs[w], fa.offset};
+  const int goff = (int)fa.offset;
   const uint8_t *rd = fa.reads + r * m;
   ReadHits h{fa.hit_pos + lr * kHitsPerRead, fa.hit_flag + lr * kHitsPerRead, kHitsPerRead, 0, 0,
              0};
@@ -281,10 +284,10 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
     uint32_t pa = L.at(a, off);
     while (pa > 0) {
       const int gs = (int)(pa - in_read);
-      if (gs + 1 > 0) {
-        const long g1 = gs + 1;
-        bool eq = g1 + m <= fa.glen;
-        for (int i = lane; eq && i < m; i += 32) eq = fa.genome[g1 + i] == strand_byte(rd, m, dr, i);
+      if (gs + 1 - goff > 0) {  // a start after the chunk's first byte
+        const long g1 = gs + 1, l1 = g1 - goff;  // in the genome, in the chunk
+        bool eq = l1 + m <= fa.glen;
+        for (int i = lane; eq && i < m; i += 32) eq = fa.genome[l1 + i] == strand_byte(rd, m, dr, i);
         if (__all_sync(0xffffffffu, eq)) warp_record(h, lane, k, -(int)g1, 0);
         int seen = 0;
         for (int b0 = 0; need >= 1 && b0 < n1 + n2; b0 += 32) {
@@ -422,6 +425,7 @@ struct saru_filter {
   int device = 0, m = 0, k = 0;
   FilterShape S{};
   long glen = 0, nidx = 0;
+  int64_t offset = 0, limit = -1;  // the chunk's genome position; windows end by limit
   cudaStream_t s = nullptr;
   DBuf<uint8_t> genome, reads, temp;
   DBuf<uint64_t> hash, hash_s;
@@ -523,7 +527,7 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
   cudaSetDevice(f->device);
   const FilterShape &S = f->S;
   const long nr = nreads, P = S.P, m = f->m;
-  CallAssembler asmb(f->m, f->k, f->glen, chunk_value);
+  CallAssembler asmb(f->m, f->k, f->limit >= 0 ? f->limit : f->glen, chunk_value);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -585,7 +589,8 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       if (e != cudaSuccess) break;
       FilterArgs fa{f->reads.p, r0, r1, read_chunk, nr, do_reverse, S, f->genome.p,
                     f->glen, f->pos_s.p, f->lo.p, f->count.p, f->offs.p, f->hit_pos.p,
-                    f->hit_flag.p, f->n.p, f->queue.p, f->status.p, f->widx.p + batch};
+                    f->hit_flag.p, f->n.p, f->queue.p, f->status.p, f->widx.p + batch,
+                    (uint32_t)f->offset};
       k_filter<<<(unsigned)((cnt + 3) / 4), 128, 0, f->s>>>(fa);  // a warp per read
       e = cudaGetLastError();
       if (e != cudaSuccess) break;
@@ -666,6 +671,17 @@ double saru_filter_last_ms(const saru_filter *f) { return f ? f->last_ms : -1.0;
 
 const char *saru_filter_genome(const saru_filter *f) {
   return f ? reinterpret_cast<const char *>(f->genome.p) : nullptr;
+}
+
+int saru_filter_set_chunk(saru_filter *f, int64_t offset, int64_t limit) {
+  saru::set_last_error("");
+  if (!f || offset < 0 || limit < offset || offset + f->glen > (int64_t)UINT32_MAX) {
+    saru::set_last_error("saru_filter_set_chunk: offset >= 0, limit >= offset, positions in 32 bits");
+    return SARU_E_INVALID;
+  }
+  f->offset = offset;
+  f->limit = limit;
+  return SARU_OK;
 }
 
 void saru_filter_destroy(saru_filter *f) {

@@ -164,11 +164,16 @@ SARU_HD int scan_all(const Lists &L, int x, uint32_t want) {
 }
 
 // One read (read bytes as sequenced; reversed and complemented here when
-// dr == 4).  L: the read's lists (see scan_from).  perfect(gs1): the genome
-// at gs1 (0-based) spells the read (strand-adjusted) over m bytes.
+// dr == 4).  L: the read's lists (see scan_from), whose values are genome
+// positions: with the genome in chunks, positions in the whole genome (the
+// chunk's position `offset` added, src/util.c:481), so only the genome's own
+// position 0 reads as a list end.  A start is taken when it lies after the
+// chunk's first byte (src/hash.c:545).  perfect(gs1): the genome at gs1 (a
+// position in the whole genome) spells the read (strand-adjusted) over m
+// bytes.  Kept positions are positions in the whole genome.
 template <class Lists, class Perfect>
 SARU_HD void filter_read(const FilterShape &S, int dr, const Lists &L, Perfect perfect,
-                         ReadHits &h) {
+                         ReadHits &h, int offset = 0) {
   const int k = S.k, half = S.half, q = S.q;
   for (int a = 0; a < half; ++a) {
     const int first = a == 0 ? 1 : 0;
@@ -177,7 +182,7 @@ SARU_HD void filter_read(const FilterShape &S, int dr, const Lists &L, Perfect p
     uint32_t pa = L.at(a, off);
     while (pa > 0) {
       const int gs = (int)(pa - in_read);
-      if (gs + 1 > 0) {
+      if (gs + 1 - offset > 0) {
         if (perfect(gs + 1)) filter_record(h, k, S.tresh, -(gs + 1), 0, S.tresh);
         int possible = 1;
         // pairs with the later first-half q-grams; the reference starts each

@@ -25,18 +25,21 @@ static uint8_t comp(uint8_t c) {
   }
 }
 
-extern "C" int filter_host_calls(const uint8_t *genome, long glen, const uint8_t *reads,
-                                 int nreads, int m, int k, int dr, int chunksize,
-                                 unsigned chunk_value, int cap, int64_t *call_begin,
-                                 int64_t cb_cap, int32_t *ids, int32_t *pos, int8_t *dirs,
-                                 int64_t cand_cap, int32_t *pids, int32_t *ppos, int64_t pcap,
-                                 int64_t *counts) {
+// The genome may be a chunk of a larger one: `offset` is the genome
+// position of its first byte, `limit` the position windows must end by.
+extern "C" int filter_host_calls_chunk(const uint8_t *genome, long glen, long offset, long limit,
+                                       const uint8_t *reads, int nreads, int m, int k, int dr,
+                                       int chunksize, unsigned chunk_value, int cap,
+                                       int64_t *call_begin, int64_t cb_cap, int32_t *ids,
+                                       int32_t *pos, int8_t *dirs, int64_t cand_cap,
+                                       int32_t *pids, int32_t *ppos, int64_t pcap,
+                                       int64_t *counts) {
   FilterShape S;
   if (!filter_shape(m, k, &S)) return -1;
   std::unordered_map<std::string, std::vector<uint32_t>> index;
   for (long p = 0; p + S.q <= glen; ++p)
-    index[std::string((const char *)genome + p, (size_t)S.q)].push_back((uint32_t)p);
-  CallAssembler asmb(m, k, glen, chunk_value);
+    index[std::string((const char *)genome + p, (size_t)S.q)].push_back((uint32_t)(p + offset));
+  CallAssembler asmb(m, k, limit, chunk_value);
   std::vector<int32_t> hp((size_t)cap);
   std::vector<int8_t> hf((size_t)cap);
   int overflow = 0;
@@ -79,10 +82,11 @@ extern "C" int filter_host_calls(const uint8_t *genome, long glen, const uint8_t
       } lists{&data, &offs[base], &lens[base]};
       const std::string &rd = strand[(size_t)(r - r0)];
       auto perfect = [&](int g1) {
-        return (long)g1 + m <= glen && memcmp(genome + g1, rd.data(), (size_t)m) == 0;
+        const long l1 = (long)g1 - offset;
+        return l1 + m <= glen && memcmp(genome + l1, rd.data(), (size_t)m) == 0;
       };
       ReadHits h{hp.data(), hf.data(), cap, 0, 0, 0};
-      filter_read(S, dr, lists, perfect, h);
+      filter_read(S, dr, lists, perfect, h, (int)offset);
       overflow |= h.overflow;
       asmb.add_read(r, h.pos, h.flag, h.n, h.queue);
     }
@@ -102,4 +106,15 @@ extern "C" int filter_host_calls(const uint8_t *genome, long glen, const uint8_t
   memcpy(pids, o.perfect_ids.data(), o.perfect_ids.size() * 4);
   memcpy(ppos, o.perfect_pos.data(), o.perfect_pos.size() * 4);
   return overflow ? 1 : 0;
+}
+
+extern "C" int filter_host_calls(const uint8_t *genome, long glen, const uint8_t *reads,
+                                 int nreads, int m, int k, int dr, int chunksize,
+                                 unsigned chunk_value, int cap, int64_t *call_begin,
+                                 int64_t cb_cap, int32_t *ids, int32_t *pos, int8_t *dirs,
+                                 int64_t cand_cap, int32_t *pids, int32_t *ppos, int64_t pcap,
+                                 int64_t *counts) {
+  return filter_host_calls_chunk(genome, glen, 0, glen, reads, nreads, m, k, dr, chunksize,
+                                 chunk_value, cap, call_begin, cb_cap, ids, pos, dirs, cand_cap,
+                                 pids, ppos, pcap, counts);
 }

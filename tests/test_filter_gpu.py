@@ -82,3 +82,55 @@ def test_filter_rejects_bad_arguments(saru_lib):
     with S.Filter(g, 36, 2) as f:
         with pytest.raises(S.SaruError):
             f.run(np.zeros((4, 36), np.uint8) + ord("A"), 1, 100)
+
+
+def map_chunked_on_gpu(genome_path, reads_path, m, k, fastq, nread, chunk_value, gchunk):
+    """map_on_gpu over the reference's genome chunks and read batches (the
+    input readers), each chunk's filter told its offset and window limit."""
+    lines = []
+    for ch in S.genome_chunks(genome_path, gchunk, m):
+        g = ch.seq
+        with S.Filter(g, m, k) as f:
+            f.set_chunk(ch.offset, ch.total)
+            for rb in S.read_batches(reads_path, m, k, nread, fastq):
+                reads = rb.reads
+                tab = S.name_table(rb.names)
+                for dr, arrow in ((0, b">>"), (4, b"<<")):
+                    out = f.run(reads, dr, chunk_value)
+                    for c in range(len(out.call_begin) - 1):
+                        b = out.call(g, reads, m, k, c, offset=ch.offset)
+                        r = S.align_host(b)
+                        text, _, _ = S.format_tsv(b, r, tab, read_length=m)
+                        lines += text.splitlines(keepends=True)
+                    for rid, g1 in zip(out.perfect_ids, out.perfect_pos):
+                        rd = reads[rid]
+                        if dr == 4:
+                            rd = W.reverse_complement(rd[None])[0]
+                        at = int(g1) - ch.offset
+                        lines.append(b"%s\t%d\t%d\t%s\t%s\t%s\t0\n" % (
+                            rb.names[rid], g1, g1 - 1 + m, arrow, g[at:at + m].tobytes(),
+                            rd.tobytes()))
+    return lines
+
+
+@pytest.mark.parametrize("fastq", [False, True])
+def test_chunked_mapping_on_the_gpu_equals_the_host_pipeline(saru_lib, tmp_path, fastq):
+    """The genome in three chunks and the reads in two batches through the
+    input readers, the device filter and the banded kernel print what the
+    host pipeline prints (the host pipeline equals the reference program's
+    output: tests/test_input.py)."""
+    import test_input as T
+    m, k = 36, 2
+    rng = np.random.default_rng(11 + fastq)
+    g = W.uniform_genome(60_000, seed=12)
+    text = bytearray(g.tobytes())
+    text[5000:5400] = bytes(text[5000:5400]).lower()
+    text[20000:20030] = b"N" * 30
+    (tmp_path / "genome.fa").write_bytes(T.genome_text(bytes(text), 70, final_nl=False))
+    rd = W.sample_reads(g, 1300, m, 0.02, seed=13).seqs
+    T.write_reads(tmp_path / "reads.fa", rd, fastq, rng)
+    args = (tmp_path / "genome.fa", tmp_path / "reads.fa", m, k, fastq, 700, 900, 25_000)
+    got = sorted(map_chunked_on_gpu(*args))
+    want = sorted(T.map_on_cpu(*args))
+    assert len(got) > 1000
+    assert got == want
