@@ -232,19 +232,16 @@ void plan_range(const saru_batch *b, int lo, int hi, PlanPart *out) {
   *out = p;
 }
 
-int plan_host(const saru_batch *b, Plan *pl) {
-  if (b->n < 0 || b->k < 0) {
-    set_error("invalid batch: n=%d k=%d", b->n, b->k);
-    return SARU_E_INVALID;
-  }
-  const int n = b->n, k = b->k;
-  // one pass over the offsets, split over host threads for large calls
-  int nt = (int)std::min<long>(16, std::max<long>(1, n / 262144));
+// plan_range over candidates [lo, hi), split over host threads for long
+// ranges; the parts merged in order (bad: the first invalid candidate).
+PlanPart plan_span(const saru_batch *b, int lo, int hi) {
+  const long n = hi - lo;
+  int nt = (int)std::min<long>(16, std::max<long>(1, n / 65536));
   const int hw = (int)std::thread::hardware_concurrency();
   if (hw > 0 && nt > hw) nt = hw;
   std::vector<PlanPart> parts((size_t)nt);
   auto range = [&](int i) {
-    plan_range(b, (int)((int64_t)n * i / nt), (int)((int64_t)n * (i + 1) / nt), &parts[(size_t)i]);
+    plan_range(b, (int)(lo + n * i / nt), (int)(lo + n * (i + 1) / nt), &parts[(size_t)i]);
   };
   if (nt == 1) {
     range(0);
@@ -254,28 +251,43 @@ int plan_host(const saru_batch *b, Plan *pl) {
     range(0);
     for (auto &x : th) x.join();
   }
-  int64_t cells = 0;
-  int m0 = -1;
-  bool uniform = true, regular = true, any_start_gap = false;
-  int max_m = 0;
+  PlanPart all;
   for (const PlanPart &p : parts) {
     if (p.bad >= 0) {
-      const int t = p.bad;
-      const int64_t L = (int64_t)b->genome_offsets[t] - (t ? b->genome_offsets[t - 1] : 0);
-      const int64_t m = (int64_t)b->read_offsets[t] - (t ? b->read_offsets[t - 1] : 0);
-      set_error("invalid batch: candidate %d has window %lld, read %lld", t, (long long)L,
-                (long long)m);
-      return SARU_E_INVALID;
+      all.bad = p.bad;
+      break;
     }
-    cells += p.cells;
+    all.cells += p.cells;
     if (p.m_first >= 0) {
-      if (m0 < 0) m0 = p.m_first;
-      if (p.m_first != m0 || !p.uniform) uniform = false;
+      if (all.m_first < 0) all.m_first = p.m_first;
+      if (p.m_first != all.m_first || !p.uniform) all.uniform = false;
     }
-    regular = regular && p.regular;
-    any_start_gap = any_start_gap || p.start_gap;
-    max_m = std::max(max_m, p.max_m);
+    all.regular = all.regular && p.regular;
+    all.start_gap = all.start_gap || p.start_gap;
+    all.max_m = std::max(all.max_m, p.max_m);
   }
+  return all;
+}
+
+int bad_candidate(const saru_batch *b, int t) {
+  const int64_t L = (int64_t)b->genome_offsets[t] - (t ? b->genome_offsets[t - 1] : 0);
+  const int64_t m = (int64_t)b->read_offsets[t] - (t ? b->read_offsets[t - 1] : 0);
+  set_error("invalid batch: candidate %d has window %lld, read %lld", t, (long long)L,
+            (long long)m);
+  return SARU_E_INVALID;
+}
+
+int plan_host(const saru_batch *b, Plan *pl) {
+  if (b->n < 0 || b->k < 0) {
+    set_error("invalid batch: n=%d k=%d", b->n, b->k);
+    return SARU_E_INVALID;
+  }
+  const int n = b->n, k = b->k;
+  const PlanPart all = plan_span(b, 0, n);
+  if (all.bad >= 0) return bad_candidate(b, all.bad);
+  const int64_t cells = all.cells;
+  const bool uniform = all.uniform, regular = all.regular, any_start_gap = all.start_gap;
+  const int max_m = all.max_m;
   const int64_t prev_g = n ? b->genome_offsets[n - 1] : 0;
   const int64_t prev_r = n ? b->read_offsets[n - 1] : 0;
   if (n > 0 && (prev_g != b->genome_bytes || prev_g > INT32_MAX || prev_r > INT32_MAX)) {
@@ -658,6 +670,11 @@ int check_slice_edges(const saru_batch *b, long chunk) {
               (long long)b->genome_bytes, (long long)pg);
     return SARU_E_INVALID;
   }
+  if (b->total_slots != pg + (int64_t)b->k * n) {
+    set_error("invalid batch: total_slots %lld != sum(L + k) = %lld", (long long)b->total_slots,
+              (long long)(pg + (int64_t)b->k * n));
+    return SARU_E_INVALID;
+  }
   return SARU_OK;
 }
 
@@ -691,17 +708,36 @@ int upload_slices(Lane &L, const saru_batch *b, long chunk) {
   return SARU_OK;
 }
 
-// Kernels and copies out of the slices (after upload_slices).
-int band_slices(Lane &L, const saru_batch *b, const Plan &pl, const saru_batch &db,
-                const saru_result &dr, const saru_result *r, int dev, long chunk) {
+// Kernels and copies out of the slices (after upload_slices), each slice
+// checked on the host (plan_range, threaded) just before its launch, so the
+// first kernels and copies out start while later slices are checked.  The
+// banded path was chosen from facts known up front (unit costs, k <= 15, the
+// first read's length); a slice whose reads differ in length or whose
+// windows are not m + so + eo sets *exact and launches stop (the call then
+// takes the exact path whole); an invalid candidate anywhere is an error.
+int band_slices(Lane &L, const saru_batch *b, int m0, const saru_batch &db,
+                const saru_result &dr, const saru_result *r, int dev, long chunk, bool *exact) {
   const long n = b->n, k = b->k;
   int rc;
-  const long grid = band_grid(dev, chunk, pl.max_m, b->k);
-  if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, b->k, pl.wide)))) return rc;
+  Plan pl;
+  pl.band = true;
+  pl.max_m = m0;
+  const long grid = band_grid(dev, chunk, m0, b->k);
+  if ((rc = L.scratch.ensure(band_scratch_bytes(grid, m0, b->k, k > 7)))) return rc;
   cudaStream_t sr = L.s_run, so = L.s_out;
   const int32_t *go = b->genome_offsets;
+  *exact = false;
+  int bad = -1;
   for (long t0 = 0, i = 0; t0 < n; t0 += chunk, ++i) {
     const long t1 = std::min(n, t0 + chunk);
+    const PlanPart part = plan_span(b, (int)t0, (int)t1);
+    if (part.bad >= 0) {
+      bad = part.bad;
+      break;
+    }
+    if (!part.uniform || part.m_first != m0 || !part.regular) *exact = true;
+    if (*exact) continue;  // check the rest, launch no more
+    pl.wide = k > 7 && part.start_gap;
     const long g0 = t0 ? go[t0 - 1] : 0, g1 = go[t1 - 1];
     SARU_CUDA(cudaStreamWaitEvent(sr, L.ev_in[(size_t)i], 0));
     saru_batch slice = db;
@@ -721,7 +757,12 @@ int band_slices(Lane &L, const saru_batch *b, const Plan &pl, const saru_batch &
   }
   SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, so));
   SARU_CUDA(cudaEventRecord(L.ev1, so));
+  // every stream of the lane is idle before returning (the copies read and
+  // write the caller's buffers)
+  SARU_CUDA(cudaStreamSynchronize(L.stream));
+  SARU_CUDA(cudaStreamSynchronize(sr));
   SARU_CUDA(cudaStreamSynchronize(so));
+  if (bad >= 0) return bad_candidate(b, bad);
   return SARU_OK;
 }
 
@@ -751,17 +792,25 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
   if ((rc = L.status.ensure(64))) return rc;
   saru_result dr{L.scores.as<int32_t>(), L.ra.as<char>(), L.ga.as<char>(), L.status.as<int32_t>()};
   SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
-  if (big) {  // copies in first; the host's pass over the call runs meanwhile
+  bool split = false;
+  if (big) {  // copies in first; the host's checks run while they stream
     if ((rc = upload_slices(L, b, chunk))) return rc;
-    if ((rc = plan_host(b, &pl))) {
-      cudaStreamSynchronize(s);
-      return rc;
+    const int m0 = b->read_offsets[0];
+    split = b->match == 0 && b->mismatch == 1 && b->k <= 15 && m0 > 3 * b->k &&
+            m0 <= saru::kMaxBandM && m0 >= 2;
+    bool exact = false;
+    if (split && (rc = band_slices(L, b, m0, db, dr, r, dev, chunk, &exact))) return rc;
+    if (!split || exact) {
+      split = false;
+      if ((rc = plan_host(b, &pl))) {
+        cudaStreamSynchronize(s);
+        return rc;
+      }
+      pl.band = false;  // the exact path, whole
     }
   }
-  const bool split = big && pl.band;
-  bool full = !pl.band, copied = false;
+  bool full = !pl.band && !split, copied = false;
   if (split) {
-    if ((rc = band_slices(L, b, pl, db, dr, r, dev, chunk))) return rc;
     const int st = *L.status_host;
     if (st & (saru::kStatusAlphabet | saru::kStatusIrregular)) {
       full = true;  // rare bytes or layouts: redo the call on the exact path
