@@ -558,8 +558,11 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
         (e = f->hit_flag.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
         (e = f->n.ensure(batch)) != cudaSuccess || (e = f->queue.ensure(batch)) != cudaSuccess ||
         (e = f->at.ensure(batch)) != cudaSuccess || (e = f->nwide.ensure(batch)) != cudaSuccess ||
-        (e = f->status.ensure(1)) != cudaSuccess)
+        (e = f->status.ensure(1)) != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
       return fail("saru_filter_run", e);
+    }
     cudaEventRecord(e0, f->s);
     e = cudaMemcpyAsync(f->reads.p, reads, (size_t)(nr * m), cudaMemcpyHostToDevice, f->s);
     LookupArgs la{f->reads.p, nr, do_reverse, S, f->genome.p, f->hash_s.p, f->pos_s.p,
