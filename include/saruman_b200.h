@@ -147,6 +147,15 @@ int saru_gather_device(const saru_gather_call *call, const char *genome, int64_t
  * (src/cuda-functions.cu:807-824).  Prints nothing.  `lane` (0 or 1)
  * selects one of two independent streams/buffer sets. */
 int saru_align_host(const saru_batch *batch, saru_result *result, int lane);
+/* saru_align_host with compact result records (see saru_align_device_compact)
+ * in place of the two slot strings: scores (n) and records (n x record_bytes,
+ * at least saru_compact_record_bytes(read length, k), a multiple of 16) in
+ * host memory.  Calls the exact path takes come back as records too.  No
+ * counterpart in the reference: its output is the slot strings; the records
+ * cut the bytes copied back 4x (saru_expand_compact rebuilds the slots,
+ * saru_format_tsv_compact the reference's TSV). */
+int saru_align_host_compact(const saru_batch *batch, int32_t *scores, uint8_t *records,
+                            int64_t record_bytes, int32_t lane);
 
 /* Device buffers in and out, enqueued on `stream` (a cudaStream_t, may be
  * NULL for the legacy stream).  Returns after enqueueing; completion is

@@ -40,7 +40,7 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_align_device_compact", "saru_expand_compact", "saru_format_tsv_compact",
                  "saru_filter_create", "saru_filter_run", "saru_filter_results",
                  "saru_filter_last_ms", "saru_filter_genome", "saru_filter_destroy",
-                 "saru_filter_set_chunk",
+                 "saru_filter_set_chunk", "saru_align_host_compact",
                  "saru_reads_open", "saru_reads_next", "saru_reads_close", "saru_genome_open",
                  "saru_genome_next", "saru_genome_close")
 ABI_DATA = ("alignment_time",)
@@ -189,6 +189,9 @@ def load(path: str | Path | None = None):
     lib.saru_filter_genome.argtypes = [C.c_void_p]
     lib.saru_filter_destroy.restype = None
     lib.saru_filter_destroy.argtypes = [C.c_void_p]
+    lib.saru_align_host_compact.restype = C.c_int
+    lib.saru_align_host_compact.argtypes = [C.POINTER(SaruBatch), C.c_void_p, C.c_void_p,
+                                            C.c_int64, C.c_int32]
     lib.saru_filter_set_chunk.restype = C.c_int
     lib.saru_filter_set_chunk.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
     lib.saru_reads_open.restype = C.c_void_p
@@ -252,6 +255,21 @@ def align_host(b: Batch, lane: int = 0, first_of_call: bool = True,
     if rc != SARU_OK:
         raise SaruError(rc, last_error())
     return AlignResult(out.scores[:b.n], out.read_aln[:tot], out.genome_aln[:tot])
+
+
+def align_host_compact(b: Batch, lane: int = 0, first_of_call: bool = True,
+                       out: tuple | None = None) -> tuple[np.ndarray, np.ndarray, int]:
+    """Host arrays in, (scores, compact records, record bytes) out
+    (saru_align_host_compact); `out` = (scores, records) to fill."""
+    lib = load()
+    sb, keep = host_batch(b, first_of_call)
+    rb = compact_record_bytes(b.m, b.k)
+    if out is None:
+        out = (np.zeros(max(b.n, 1), np.int32), np.zeros(max(b.n, 1) * rb, np.uint8))
+    rc = lib.saru_align_host_compact(C.byref(sb), _p(out[0]), _p(out[1]), rb, lane)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+    return out[0][:b.n], out[1][:b.n * rb], rb
 
 
 def scratch_bytes(n: int, max_m: int, k: int) -> int:

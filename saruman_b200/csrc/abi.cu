@@ -122,7 +122,7 @@ struct Lane {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_run = nullptr;             // a slice aligned
   std::vector<cudaEvent_t> ev_in;            // a slice's inputs landed (one per slice)
-  DevBuf genome, reads, goff, roff, dirs, scores, ra, ga, scratch, status, eoff, arena;
+  DevBuf genome, reads, goff, roff, dirs, scores, ra, ga, scratch, status, eoff, arena, records;
   int *status_host = nullptr;  // pinned
   std::mutex mu;
 
@@ -143,7 +143,7 @@ struct Lane {
     if (device < 0) return;
     cudaSetDevice(device);
     for (DevBuf *b : {&genome, &reads, &goff, &roff, &dirs, &scores, &ra, &ga, &scratch, &status,
-                      &eoff, &arena})
+                      &eoff, &arena, &records})
       b->release();
     if (status_host) cudaFreeHost(status_host);
     if (ev0) cudaEventDestroy(ev0);
@@ -715,8 +715,16 @@ int upload_slices(Lane &L, const saru_batch *b, long chunk) {
 // first read's length); a slice whose reads differ in length or whose
 // windows are not m + so + eo sets *exact and launches stop (the call then
 // takes the exact path whole); an invalid candidate anywhere is an error.
+// Host outputs of a call in compact records (saru_align_host_compact).
+struct HostCompact {
+  int32_t *scores;
+  uint8_t *records;
+  long rec_bytes;
+};
+
 int band_slices(Lane &L, const saru_batch *b, int m0, const saru_batch &db,
-                const saru_result &dr, const saru_result *r, int dev, long chunk, bool *exact) {
+                const saru_result &dr, const saru_result *r, int dev, long chunk, bool *exact,
+                const HostCompact *hc) {
   const long n = b->n, k = b->k;
   int rc;
   Plan pl;
@@ -726,6 +734,7 @@ int band_slices(Lane &L, const saru_batch *b, int m0, const saru_batch &db,
   if ((rc = L.scratch.ensure(band_scratch_bytes(grid, m0, b->k, k > 7)))) return rc;
   cudaStream_t sr = L.s_run, so = L.s_out;
   const int32_t *go = b->genome_offsets;
+  const CompactOut dcmp{L.records.as<uint8_t>(), hc ? hc->rec_bytes : 0};
   *exact = false;
   int bad = -1;
   for (long t0 = 0, i = 0; t0 < n; t0 += chunk, ++i) {
@@ -743,10 +752,18 @@ int band_slices(Lane &L, const saru_batch *b, int m0, const saru_batch &db,
     saru_batch slice = db;
     slice.n = (int32_t)t1;
     if ((rc = run_band(&slice, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, sr, 0,
-                       nullptr, t0)))
+                       hc ? &dcmp : nullptr, t0)))
       return rc;
     SARU_CUDA(cudaEventRecord(L.ev_run, sr));
     SARU_CUDA(cudaStreamWaitEvent(so, L.ev_run, 0));
+    if (hc) {
+      SARU_CUDA(cudaMemcpyAsync(hc->scores + t0, dr.scores + t0, 4 * (size_t)(t1 - t0),
+                                cudaMemcpyDeviceToHost, so));
+      SARU_CUDA(cudaMemcpyAsync(hc->records + t0 * hc->rec_bytes,
+                                L.records.as<uint8_t>() + t0 * hc->rec_bytes,
+                                (size_t)((t1 - t0) * hc->rec_bytes), cudaMemcpyDeviceToHost, so));
+      continue;
+    }
     const long s0 = g0 + k * t0, s1 = g1 + k * t1;
     SARU_CUDA(cudaMemcpyAsync(r->scores + t0, dr.scores + t0, 4 * (size_t)(t1 - t0),
                               cudaMemcpyDeviceToHost, so));
@@ -766,7 +783,9 @@ int band_slices(Lane &L, const saru_batch *b, int m0, const saru_batch &db,
   return SARU_OK;
 }
 
-int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out) {
+// A host call: slot strings into r, or (hc) compact records.
+int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out,
+                    const HostCompact *hc = nullptr) {
   Plan pl;
   int rc;
   const bool big = b->n >= 2 * kSplitMin && b->k >= 0;
@@ -790,7 +809,9 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
   if ((rc = L.ra.ensure((size_t)b->total_slots + 64))) return rc;
   if ((rc = L.ga.ensure((size_t)b->total_slots + 64))) return rc;
   if ((rc = L.status.ensure(64))) return rc;
+  if (hc && (rc = L.records.ensure(n * (size_t)hc->rec_bytes + 64))) return rc;
   saru_result dr{L.scores.as<int32_t>(), L.ra.as<char>(), L.ga.as<char>(), L.status.as<int32_t>()};
+  const CompactOut dcmp{L.records.as<uint8_t>(), hc ? hc->rec_bytes : 0};
   SARU_CUDA(cudaMemsetAsync(L.status.p, 0, sizeof(int), s));
   bool split = false;
   if (big) {  // copies in first; the host's checks run while they stream
@@ -798,8 +819,13 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
     const int m0 = b->read_offsets[0];
     split = b->match == 0 && b->mismatch == 1 && b->k <= 15 && m0 > 3 * b->k &&
             m0 <= saru::kMaxBandM && m0 >= 2;
+    if (split && hc && hc->rec_bytes < saru::compact_record_bytes(m0, b->k)) {
+      cudaStreamSynchronize(s);
+      set_error("record_bytes %ld < saru_compact_record_bytes(%d, %d)", hc->rec_bytes, m0, b->k);
+      return SARU_E_INVALID;
+    }
     bool exact = false;
-    if (split && (rc = band_slices(L, b, m0, db, dr, r, dev, chunk, &exact))) return rc;
+    if (split && (rc = band_slices(L, b, m0, db, dr, r, dev, chunk, &exact, hc))) return rc;
     if (!split || exact) {
       split = false;
       if ((rc = plan_host(b, &pl))) {
@@ -822,9 +848,15 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
       copied = true;
     }
   } else if (pl.band) {
+    if (hc && hc->rec_bytes < saru::compact_record_bytes(pl.max_m, b->k)) {
+      set_error("record_bytes %ld < saru_compact_record_bytes(%d, %d)", hc->rec_bytes, pl.max_m,
+                b->k);
+      return SARU_E_INVALID;
+    }
     const long grid = band_grid(dev, b->n, pl.max_m, b->k);
     if ((rc = L.scratch.ensure(band_scratch_bytes(grid, pl.max_m, b->k, pl.wide)))) return rc;
-    if ((rc = run_band(&db, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, s)))
+    if ((rc = run_band(&db, pl, &dr, L.scratch.p, L.scratch.n, L.status.as<int>(), dev, s, 0,
+                       hc ? &dcmp : nullptr)))
       return rc;
     SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SARU_CUDA(cudaStreamSynchronize(s));
@@ -841,7 +873,23 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out)
     if ((rc = run_full(L, b, &db, pl, &dr))) return rc;
     SARU_CUDA(cudaMemcpyAsync(L.status_host, L.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   }
-  if (!copied) {
+  if (!copied && hc && !full) {  // banded, unsplit: the records
+    SARU_CUDA(cudaMemcpyAsync(hc->scores, dr.scores, 4 * n, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaMemcpyAsync(hc->records, L.records.p, n * (size_t)hc->rec_bytes,
+                              cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaEventRecord(L.ev1, s));
+    SARU_CUDA(cudaStreamSynchronize(s));
+  } else if (!copied && hc) {  // the exact path's slots, turned into records on the host
+    std::vector<char> ra((size_t)b->total_slots + 64), ga((size_t)b->total_slots + 64);
+    SARU_CUDA(cudaMemcpyAsync(hc->scores, dr.scores, 4 * n, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaMemcpyAsync(ra.data(), dr.read_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaMemcpyAsync(ga.data(), dr.genome_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
+    SARU_CUDA(cudaEventRecord(L.ev1, s));
+    SARU_CUDA(cudaStreamSynchronize(s));
+    if ((rc = saru::records_from_slots(b, hc->scores, ra.data(), ga.data(), hc->records,
+                                       hc->rec_bytes)))
+      return rc;
+  } else if (!copied) {
     SARU_CUDA(cudaMemcpyAsync(r->scores, dr.scores, 4 * n, cudaMemcpyDeviceToHost, s));
     SARU_CUDA(cudaMemcpyAsync(r->read_aln, dr.read_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
     SARU_CUDA(cudaMemcpyAsync(r->genome_aln, dr.genome_aln, (size_t)b->total_slots, cudaMemcpyDeviceToHost, s));
@@ -972,6 +1020,21 @@ int saru_align_host(const saru_batch *batch, saru_result *result, int lane) {
   Lane &L = g_lanes[lane ? 1 : 0];
   std::lock_guard<std::mutex> lk(L.mu);
   return align_host_impl(batch, result, L, nullptr);
+}
+
+int saru_align_host_compact(const saru_batch *batch, int32_t *scores, uint8_t *records,
+                            int64_t record_bytes, int32_t lane) {
+  g_last_error.clear();
+  if (!batch || batch->n < 0 || batch->k < 0 || (batch->n > 0 && (!scores || !records)) ||
+      (record_bytes & 15) || record_bytes < 16) {
+    set_error("saru_align_host_compact: a batch, scores, records and record_bytes a multiple "
+              "of 16 (saru_compact_record_bytes)");
+    return SARU_E_INVALID;
+  }
+  Lane &L = g_lanes[lane ? 1 : 0];
+  std::lock_guard<std::mutex> lk(L.mu);
+  const HostCompact hc{scores, records, (long)record_bytes};
+  return align_host_impl(batch, nullptr, L, nullptr, &hc);
 }
 
 int saru_align_device(const saru_batch *batch, saru_result *result, void *scratch,

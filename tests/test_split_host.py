@@ -55,3 +55,33 @@ def test_split_host_call_equals_one_launch(saru_lib):
     assert np.array_equal(host.genome_aln, ga.cpu().numpy()[:b.total_genome])
     assert (host.scores <= b.k).sum() > b.n // 4
 
+
+
+def test_compact_host_call_expands_to_the_slot_strings(saru_lib):
+    """saru_align_host_compact over the same sliced call: its records,
+    expanded on the host, are the slot strings saru_align_host returns."""
+    bench = load_bench()
+    cfg = dict(bench.CONFIGS["c2"])
+    cfg["reads"] = 70_000
+    b = bench.build_batches(cfg, 0)[0]
+    slots = S.align_host(b)
+    sc, rec, rb = S.align_host_compact(b)
+    comp = S.expand_compact(b, sc, rec, rb)
+    assert np.array_equal(comp.scores, slots.scores)
+    assert np.array_equal(comp.read_aln, slots.read_aln)
+    assert np.array_equal(comp.genome_aln, slots.genome_aln)
+
+
+def test_compact_host_call_on_the_exact_path(saru_lib):
+    """A call the banded kernel hands to the exact path (a read with five
+    distinct non-ACGT bytes) still comes back as records."""
+    from saruman_b200 import workloads as W
+    b = W.random_batch(100, 5, 3000, seed=21, err=0.03)
+    b.reads[100 * 7:100 * 7 + 5] = np.frombuffer(b"NRYKM", np.uint8)
+    slots = S.align_host(b)
+    sc, rec, rb = S.align_host_compact(b)
+    comp = S.expand_compact(b, sc, rec, rb)
+    assert np.array_equal(comp.scores, slots.scores)
+    assert np.array_equal(comp.read_aln, slots.read_aln)
+    assert np.array_equal(comp.genome_aln, slots.genome_aln)
+    assert (slots.scores <= 5).sum() > 100
