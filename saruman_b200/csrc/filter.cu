@@ -153,6 +153,7 @@ struct FilterArgs {
   int *status;
   const int32_t *order;           // the launch's reads (0-based in it), most work first
   uint32_t offset;                // genome position of the chunk's first byte
+  uint32_t zone_magic;            // ceil(2^32 / (2k + 1)): item / zones by a multiply
 };
 
 // The read's lists on the device: the sorted index's run for each q-gram,
@@ -294,7 +295,10 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
           const int item = b0 + lane;
           int hits = 0, flag = 0, start = 0;
           if (item < n1) {
-            const int b = a + 1 + item / zones, ez = item % zones - k;
+            // item / zones as a multiply-high (an integer division by a
+            // variable runs on the XU pipe, the kernel's bottleneck)
+            const int zq = (int)__umulhi((uint32_t)item, fa.zone_magic);
+            const int b = a + 1 + zq, ez = item - zq * zones - k;
             const uint32_t want = (uint32_t)gs + (uint32_t)b * q + 1 + (uint32_t)ez;
             hits = scan_from_at(L, b, P, off, want);
             if (b == half - 1 && first) {
@@ -426,6 +430,7 @@ struct saru_filter {
   FilterShape S{};
   long glen = 0, nidx = 0;
   int64_t offset = 0, limit = -1;  // the chunk's genome position; windows end by limit
+  uint32_t zone_magic = 0;         // ceil(2^32 / (2k + 1)), checked exact for every item
   cudaStream_t s = nullptr;
   DBuf<uint8_t> genome, reads, temp;
   DBuf<uint64_t> hash, hash_s;
@@ -465,6 +470,18 @@ saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t 
                          "layout of at most 64 q-grams");
     delete f;
     return nullptr;
+  }
+  {  // the kernel divides pair items by 2k + 1 with a multiply-high: exact
+     // for every item index a read can have (checked here)
+    const uint32_t zones = 2u * (uint32_t)k + 1u;
+    f->zone_magic = (uint32_t)(((1ull << 32) + zones - 1) / zones);
+    const uint32_t items = (uint32_t)(f->S.half * (zones + 2u * (uint32_t)f->S.half + 1u));
+    for (uint32_t i = 0; i <= items; ++i)
+      if ((uint32_t)(((uint64_t)i * f->zone_magic) >> 32) != i / zones) {
+        saru::set_last_error("saru_filter_create: no exact multiply for the item division");
+        delete f;
+        return nullptr;
+      }
   }
   const int q = f->S.q;
   cudaError_t e = cudaSetDevice(device);
@@ -593,7 +610,7 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       FilterArgs fa{f->reads.p, r0, r1, read_chunk, nr, do_reverse, S, f->genome.p,
                     f->glen, f->pos_s.p, f->lo.p, f->count.p, f->offs.p, f->hit_pos.p,
                     f->hit_flag.p, f->n.p, f->queue.p, f->status.p, f->widx.p + batch,
-                    (uint32_t)f->offset};
+                    (uint32_t)f->offset, f->zone_magic};
       k_filter<<<(unsigned)((cnt + 3) / 4), 128, 0, f->s>>>(fa);  // a warp per read
       e = cudaGetLastError();
       if (e != cudaSuccess) break;
