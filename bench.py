@@ -885,7 +885,7 @@ def main() -> None:
     if not multi and args.filter_reads:
         b0, seqs = bs[0], tables[0][:args.filter_reads]
         with S.Filter(genome, b0.m, b0.k) as f:
-            f.run(seqs[:1000], 0, 1 << 30)  # warm-up
+            f.run(seqs, 0, 4 * len(seqs) + 1000)  # warm-up: buffers sized for the run
             runs = [f.run(seqs, dr, 4 * len(seqs) + 1000) for dr in (0, 4)]
         ms = sum(r.ms for r in runs)
         filt = {"reads": int(len(seqs)), "strands": 2,

@@ -423,6 +423,29 @@ struct DBuf {
   }
 };
 
+// Pinned host memory that grows: copies back from the device into it run
+// at full speed and without staging.
+template <typename T>
+struct HBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t count) {
+    if (count <= n) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    const size_t want = count + count / 2 + 64;
+    const cudaError_t e = cudaMallocHost(&p, want * sizeof(T));
+    if (e == cudaSuccess) n = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
 }  // namespace
 
 struct saru_filter {
@@ -440,6 +463,8 @@ struct saru_filter {
   DBuf<uint32_t> wkey;
   DBuf<int8_t> hit_flag, packed_flag;
   DBuf<int> status;
+  HBuf<int32_t> h_n, h_q, h_pos;  // a launch's counts and kept positions, copied back
+  HBuf<int8_t> h_flag;
   FilterCalls calls;
   float last_ms = 0.f;
 };
@@ -592,10 +617,6 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       e = cub::DeviceScan::ExclusiveSum(f->temp.p, tb, f->count.p, f->offs.p, (int)lists, f->s);
     // one scan over all reads: each chunk's lists stay contiguous, and the
     // filter bounds its look past a list by its chunk's end
-    std::vector<int32_t> hn, hq;
-    std::vector<long> hat;
-    std::vector<int32_t> hpos;
-    std::vector<int8_t> hflag;
     if (e == cudaSuccess) e = cudaMemsetAsync(f->status.p, 0, sizeof(int), f->s);
     for (long r0 = 0; r0 < nr && e == cudaSuccess; r0 += batch) {
       const long r1 = std::min(nr, r0 + batch), cnt = r1 - r0;
@@ -616,13 +637,14 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       if (e != cudaSuccess) break;
       k_widen<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->n.p, cnt, f->nwide.p);
       e = cub::DeviceScan::ExclusiveSum(f->temp.p, tb2, f->nwide.p, f->at.p, (int)cnt, f->s);
-      hn.resize((size_t)cnt);
-      hq.resize((size_t)cnt);
-      hat.resize((size_t)cnt);
+      if ((e = f->h_n.ensure((size_t)cnt)) != cudaSuccess ||
+          (e = f->h_q.ensure((size_t)cnt)) != cudaSuccess)
+        break;
+      int32_t *hn = f->h_n.p, *hq = f->h_q.p;
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hn.data(), f->n.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
+        e = cudaMemcpyAsync(hn, f->n.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hq.data(), f->queue.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
+        e = cudaMemcpyAsync(hq, f->queue.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
       if (e != cudaSuccess) break;
       long total = 0;
@@ -633,19 +655,20 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       k_pack<<<(unsigned)std::min<long>(cnt, 65535), 128, 0, f->s>>>(
           f->hit_pos.p, f->hit_flag.p, f->n.p, f->at.p, cnt, f->packed_pos.p, f->packed_flag.p);
       e = cudaGetLastError();
-      hpos.resize((size_t)total + 1);
-      hflag.resize((size_t)total + 1);
+      if (e != cudaSuccess || (e = f->h_pos.ensure((size_t)total + 1)) != cudaSuccess ||
+          (e = f->h_flag.ensure((size_t)total + 1)) != cudaSuccess)
+        break;
+      int32_t *hpos = f->h_pos.p;
+      int8_t *hflag = f->h_flag.p;
+      e = cudaMemcpyAsync(hpos, f->packed_pos.p, 4 * (size_t)total, cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hpos.data(), f->packed_pos.p, 4 * (size_t)total,
-                            cudaMemcpyDeviceToHost, f->s);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hflag.data(), f->packed_flag.p, (size_t)total,
+        e = cudaMemcpyAsync(hflag, f->packed_flag.p, (size_t)total,
                             cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
       if (e != cudaSuccess) break;
       long at = 0;
       for (long i = 0; i < cnt; ++i) {
-        asmb.add_read((int32_t)(r0 + i), hpos.data() + at, hflag.data() + at, hn[(size_t)i],
+        asmb.add_read((int32_t)(r0 + i), hpos + at, hflag + at, hn[(size_t)i],
                       hq[(size_t)i]);
         at += hn[(size_t)i];
       }
@@ -727,6 +750,10 @@ void saru_filter_destroy(saru_filter *f) {
   f->hit_flag.release();
   f->packed_flag.release();
   f->status.release();
+  f->h_n.release();
+  f->h_q.release();
+  f->h_pos.release();
+  f->h_flag.release();
   f->wkey.release();
   f->widx.release();
   if (f->s) cudaStreamDestroy(f->s);
