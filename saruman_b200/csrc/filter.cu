@@ -465,7 +465,7 @@ struct saru_filter {
   DBuf<int> status;
   HBuf<int32_t> h_n, h_q, h_pos;  // a launch's counts and kept positions, copied back
   HBuf<int8_t> h_flag;
-  FilterCalls calls;
+  CallAssembler asmb{0, 0, 0, 1};  // the last run's calls (asmb.out), storage kept
   float last_ms = 0.f;
 };
 
@@ -569,7 +569,8 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
   cudaSetDevice(f->device);
   const FilterShape &S = f->S;
   const long nr = nreads, P = S.P, m = f->m;
-  CallAssembler asmb(f->m, f->k, f->limit >= 0 ? f->limit : f->glen, chunk_value);
+  CallAssembler &asmb = f->asmb;
+  asmb.reset(f->m, f->k, f->limit >= 0 ? f->limit : f->glen, chunk_value);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -687,20 +688,19 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
     if (rc == SARU_OK) cudaEventElapsedTime(&ms, e0, e1);
   }
   asmb.finish();
-  f->calls = std::move(asmb.out);
   f->last_ms = ms;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  counts[0] = (int64_t)f->calls.call_begin.size() - 1;
-  counts[1] = (int64_t)f->calls.ids.size();
-  counts[2] = (int64_t)f->calls.perfect_ids.size();
+  counts[0] = (int64_t)f->asmb.out.call_begin.size() - 1;
+  counts[1] = (int64_t)f->asmb.out.ids.size();
+  counts[2] = (int64_t)f->asmb.out.perfect_ids.size();
   return rc;
 }
 
 int saru_filter_results(const saru_filter *f, int64_t *call_begin, int32_t *ids, int32_t *pos,
                         int8_t *dirs, int32_t *perfect_ids, int32_t *perfect_pos) {
   if (!f) return SARU_E_INVALID;
-  const FilterCalls &c = f->calls;
+  const FilterCalls &c = f->asmb.out;
   if (call_begin) memcpy(call_begin, c.call_begin.data(), c.call_begin.size() * 8);
   if (ids) memcpy(ids, c.ids.data(), c.ids.size() * 4);
   if (pos) memcpy(pos, c.pos.data(), c.pos.size() * 4);

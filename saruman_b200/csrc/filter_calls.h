@@ -13,6 +13,7 @@
 // printed by the filter itself and never aligned.
 #pragma once
 #include <stdint.h>
+#include <string.h>
 
 #include <vector>
 
@@ -29,17 +30,38 @@ struct FilterCalls {
 
 class CallAssembler {
  public:
-  CallAssembler(int m, int k, int64_t genome_len, uint32_t chunk_value)
-      : m_(m), k_(k), glen_(genome_len), chunk_(chunk_value) {
-    out.call_begin.push_back(0);
+  CallAssembler(int m, int k, int64_t genome_len, uint32_t chunk_value) {
+    reset(m, k, genome_len, chunk_value);
+  }
+
+  // A new run; the storage of earlier runs is kept (filling fresh memory
+  // costs as much as the assembly).
+  void reset(int m, int k, int64_t genome_len, uint32_t chunk_value) {
+    m_ = m;
+    k_ = k;
+    glen_ = genome_len;
+    chunk_ = chunk_value;
+    queue_ = 0;
+    entries_.clear();
+    pos_.clear();
+    flag_.clear();
+    out.call_begin.assign(1, 0);
+    out.ids.clear();
+    out.pos.clear();
+    out.dirs.clear();
+    out.perfect_ids.clear();
+    out.perfect_pos.clear();
   }
 
   // The read's kept positions, in the order the filter kept them.
   void add_read(int32_t id, const int32_t *pos, const int8_t *flag, int n, int queue) {
     if (n > 0) {
-      entries_.push_back(Entry{id, (uint32_t)pos_.size(), (uint32_t)n});
-      pos_.insert(pos_.end(), pos, pos + n);
-      flag_.insert(flag_.end(), flag, flag + n);
+      const size_t at = pos_.size();
+      entries_.push_back(Entry{id, (uint32_t)at, (uint32_t)n});
+      pos_.resize(at + (size_t)n);
+      flag_.resize(at + (size_t)n);
+      memcpy(&pos_[at], pos, sizeof(int32_t) * (size_t)n);
+      memcpy(&flag_[at], flag, (size_t)n);
       for (int i = 0; i < n; ++i)
         if (flag[i] == 0) {  // a perfect hit (kept only with a negative position)
           out.perfect_ids.push_back(id);
@@ -65,6 +87,9 @@ class CallAssembler {
 
   void flush() {
     const int64_t before = (int64_t)out.ids.size();
+    out.ids.reserve(out.ids.size() + pos_.size());
+    out.pos.reserve(out.pos.size() + pos_.size());
+    out.dirs.reserve(out.dirs.size() + pos_.size());
     size_t keep = 0, kept_values = 0;
     for (size_t e = 0; e < entries_.size(); ++e) {
       const Entry E = entries_[e];
@@ -100,9 +125,9 @@ class CallAssembler {
     queue_ = 0;
   }
 
-  int m_, k_;
-  int64_t glen_;
-  uint32_t chunk_;
+  int m_ = 0, k_ = 0;
+  int64_t glen_ = 0;
+  uint32_t chunk_ = 0;
   uint32_t queue_ = 0;
   std::vector<Entry> entries_;
   std::vector<int32_t> pos_;
