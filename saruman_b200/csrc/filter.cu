@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(128) k_filter(FilterArgs fa) {
           int hits = 0, flag = 0, start = 0;
           if (item < n1) {
             // item / zones as a multiply-high (an integer division by a
-            // variable runs on the XU pipe, the kernel's bottleneck)
+            // variable is a reciprocal estimate and corrections)
             const int zq = (int)__umulhi((uint32_t)item, fa.zone_magic);
             const int b = a + 1 + zq, ez = item - zq * zones - k;
             const uint32_t want = (uint32_t)gs + (uint32_t)b * q + 1 + (uint32_t)ez;
