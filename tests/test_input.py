@@ -197,16 +197,15 @@ def map_on_cpu(genome_path: Path, reads_path: Path, m: int, k: int, fastq: bool,
 
 
 @pytest.mark.skipif(not EMUL.exists(), reason="the reference's host build is not here")
-@pytest.mark.parametrize("fastq", [False, True])
-def test_chunked_mapping_prints_the_reference_output(saru_lib, tmp_path, fastq):
-    m, k = 36, 2
-    rng = np.random.default_rng(11 + fastq)
+@pytest.mark.parametrize("fastq,m,k", [(False, 36, 2), (True, 36, 2), (False, 75, 4)])
+def test_chunked_mapping_prints_the_reference_output(saru_lib, tmp_path, fastq, m, k):
+    rng = np.random.default_rng(11 + fastq + m)
     g = W.uniform_genome(60_000, seed=12)
     text = bytearray(g.tobytes())
     text[5000:5400] = bytes(text[5000:5400]).lower()
     text[20000:20030] = b"N" * 30
     (tmp_path / "genome.fa").write_bytes(genome_text(bytes(text), 70, final_nl=False))
-    rd = W.sample_reads(g, 1300, m, 0.02, seed=13).seqs
+    rd = W.sample_reads(g, 1300, m, 0.02 if m < 50 else 0.03, seed=13).seqs
     write_reads(tmp_path / "reads.fa", rd, fastq, rng)
     nread, chunk_value, gchunk = 700, 900, 25_000  # 2 read batches, 3 genome chunks
     args = [str(EMUL), "-m", "0", "-i", "1", "-l", str(m), "-e", repr((k + 0.5) / m),
