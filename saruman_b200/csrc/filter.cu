@@ -22,6 +22,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <future>
 #include <vector>
 
 #include "../../include/saruman_b200.h"
@@ -463,8 +464,10 @@ struct saru_filter {
   DBuf<uint32_t> wkey;
   DBuf<int8_t> hit_flag, packed_flag;
   DBuf<int> status;
-  HBuf<int32_t> h_n, h_q, h_pos;  // a launch's counts and kept positions, copied back
-  HBuf<int8_t> h_flag;
+  // a launch's counts and kept positions, copied back; two sets, so one
+  // launch's calls are assembled on the host while the next one runs
+  HBuf<int32_t> h_n[2], h_q[2], h_pos[2];
+  HBuf<int8_t> h_flag[2];
   CallAssembler asmb{0, 0, 0, 1};  // the last run's calls (asmb.out), storage kept
   float last_ms = 0.f;
 };
@@ -619,8 +622,15 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
     // one scan over all reads: each chunk's lists stay contiguous, and the
     // filter bounds its look past a list by its chunk's end
     if (e == cudaSuccess) e = cudaMemsetAsync(f->status.p, 0, sizeof(int), f->s);
-    for (long r0 = 0; r0 < nr && e == cudaSuccess; r0 += batch) {
+    // the calls of launch i are assembled on the host (one launch at a time,
+    // in read order) while launch i + 1 runs on the device
+    std::future<void> assembling;
+    auto wait_assembly = [&]() {
+      if (assembling.valid()) assembling.get();
+    };
+    for (long r0 = 0, li = 0; r0 < nr && e == cudaSuccess; r0 += batch, ++li) {
       const long r1 = std::min(nr, r0 + batch), cnt = r1 - r0;
+      const int set = (int)(li & 1);
       k_work<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->count.p, r0, cnt, S, f->wkey.p,
                                                               f->widx.p);
       e = cudaGetLastError();
@@ -638,10 +648,10 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       if (e != cudaSuccess) break;
       k_widen<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->n.p, cnt, f->nwide.p);
       e = cub::DeviceScan::ExclusiveSum(f->temp.p, tb2, f->nwide.p, f->at.p, (int)cnt, f->s);
-      if ((e = f->h_n.ensure((size_t)cnt)) != cudaSuccess ||
-          (e = f->h_q.ensure((size_t)cnt)) != cudaSuccess)
+      if ((e = f->h_n[set].ensure((size_t)cnt)) != cudaSuccess ||
+          (e = f->h_q[set].ensure((size_t)cnt)) != cudaSuccess)
         break;
-      int32_t *hn = f->h_n.p, *hq = f->h_q.p;
+      int32_t *hn = f->h_n[set].p, *hq = f->h_q[set].p;
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(hn, f->n.p, 4 * cnt, cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess)
@@ -656,25 +666,29 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       k_pack<<<(unsigned)std::min<long>(cnt, 65535), 128, 0, f->s>>>(
           f->hit_pos.p, f->hit_flag.p, f->n.p, f->at.p, cnt, f->packed_pos.p, f->packed_flag.p);
       e = cudaGetLastError();
-      if (e != cudaSuccess || (e = f->h_pos.ensure((size_t)total + 1)) != cudaSuccess ||
-          (e = f->h_flag.ensure((size_t)total + 1)) != cudaSuccess)
+      if (e != cudaSuccess || (e = f->h_pos[set].ensure((size_t)total + 1)) != cudaSuccess ||
+          (e = f->h_flag[set].ensure((size_t)total + 1)) != cudaSuccess)
         break;
-      int32_t *hpos = f->h_pos.p;
-      int8_t *hflag = f->h_flag.p;
+      int32_t *hpos = f->h_pos[set].p;
+      int8_t *hflag = f->h_flag[set].p;
       e = cudaMemcpyAsync(hpos, f->packed_pos.p, 4 * (size_t)total, cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(hflag, f->packed_flag.p, (size_t)total,
                             cudaMemcpyDeviceToHost, f->s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
       if (e != cudaSuccess) break;
-      long at = 0;
-      for (long i = 0; i < cnt; ++i) {
-        asmb.add_read((int32_t)(r0 + i), hpos + at, hflag + at, hn[(size_t)i],
-                      hq[(size_t)i]);
-        at += hn[(size_t)i];
-      }
+      wait_assembly();  // the last launch's calls first (and its staging set is free)
+      assembling = std::async(std::launch::async, [&asmb, r0, cnt, hpos, hflag, hn, hq]() {
+        long at = 0;
+        for (long i = 0; i < cnt; ++i) {
+          asmb.add_read((int32_t)(r0 + i), hpos + at, hflag + at, hn[(size_t)i],
+                        hq[(size_t)i]);
+          at += hn[(size_t)i];
+        }
+      });
       saru::count_launch();
     }
+    wait_assembly();
     int flag = 0;
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&flag, f->status.p, sizeof(int), cudaMemcpyDeviceToHost, f->s);
@@ -750,10 +764,12 @@ void saru_filter_destroy(saru_filter *f) {
   f->hit_flag.release();
   f->packed_flag.release();
   f->status.release();
-  f->h_n.release();
-  f->h_q.release();
-  f->h_pos.release();
-  f->h_flag.release();
+  for (int i = 0; i < 2; ++i) {
+    f->h_n[i].release();
+    f->h_q[i].release();
+    f->h_pos[i].release();
+    f->h_flag[i].release();
+  }
   f->wkey.release();
   f->widx.release();
   if (f->s) cudaStreamDestroy(f->s);
