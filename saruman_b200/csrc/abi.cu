@@ -128,6 +128,7 @@ struct Lane {
 
   int init(int dev) {
     if (device == dev && stream) return SARU_OK;
+    if (device >= 0) release();  // buffers and streams of another device
     SARU_CUDA(cudaSetDevice(dev));
     SARU_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     SARU_CUDA(cudaStreamCreateWithFlags(&s_run, cudaStreamNonBlocking));
@@ -163,15 +164,19 @@ struct Lane {
 
 Lane g_lanes[3];  // legacy forward, legacy reverse, request server
 
+// The GPU of a host call: the one the reference chose (use_gpu_value, set
+// by get_cuda_infos or -u), else the calling thread's current device (one
+// process per GPU sets its own).
 int current_device() {
-  int d = 0;
-  if (use_gpu_value < 5000) d = use_gpu_value;
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
     cudaGetLastError();
     return -1;
   }
-  if (d >= count) d = 0;
+  int d = 0;
+  if (use_gpu_value < 5000) d = use_gpu_value;
+  else if (cudaGetDevice(&d) != cudaSuccess) d = 0;
+  if (d < 0 || d >= count) d = 0;
   return d;
 }
 
