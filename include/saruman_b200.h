@@ -261,14 +261,15 @@ int64_t saru_format_tsv_compact(const saru_batch *batch, const int32_t *scores,
  * whose filter runs on the host: src/hash.c:348-839) ---------------------------
  * The reference's q-gram pair filter for one strand and one batch of reads
  * (the reads it loads at a time, its -c option; read ids count from 0 in
- * each batch), one thread per read, against a q-gram index of the genome
- * held on the device.  The kept positions are assembled into exactly the
+ * each batch), one warp per read, against a q-gram index of the genome
+ * held on the device (device < 0: the calling thread's current device).
+ * The kept positions are assembled into exactly the
  * calls the reference would submit: read ids, positions, flags and call
  * boundaries, set by chunk_value (its -s option: the queue threshold, which
  * is also the number of reads per chunk of its data array).  Perfect hits,
  * which the reference prints from the filter, come back as (read id,
- * 0-based start).  The genome must be one chunk (the reference's -G at
- * least its length). */
+ * 0-based start).  A genome read in chunks (-G) takes one filter per chunk
+ * (saru_filter_set_chunk). */
 typedef struct saru_filter saru_filter;
 saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t read_length,
                                 int32_t k, int32_t device);

@@ -613,7 +613,8 @@ class FilterCalls:
 class Filter:
     """The reference's q-gram pair filter on the device (saru_filter_*)."""
 
-    def __init__(self, genome: np.ndarray, m: int, k: int, device: int = 0):
+    def __init__(self, genome: np.ndarray, m: int, k: int, device: int = -1):
+        """device -1: the calling thread's current CUDA device."""
         self._lib = load()
         g = np.ascontiguousarray(genome, np.uint8)
         self.m, self.k = m, k

@@ -487,6 +487,7 @@ extern "C" {
 saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t read_length,
                                 int32_t k, int32_t device) {
   saru::set_last_error("");
+  if (device < 0 && cudaGetDevice(&device) != cudaSuccess) device = 0;  // the current one
   auto *f = new saru_filter();
   f->device = device;
   f->m = read_length;
