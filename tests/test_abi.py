@@ -92,3 +92,15 @@ def test_large_call_offsets_checked_before_any_copy(saru_lib):
         rc = saru_lib.saru_align_host(C.byref(sb), C.byref(res), 0)
         assert rc == S.SARU_E_INVALID
         assert what in S.last_error()
+
+
+def test_compact_host_call_refuses_bad_record_sizes(saru_lib):
+    """saru_align_host_compact checks its record size before any device work."""
+    from saruman_b200 import workloads as W
+    b = W.random_batch(36, 2, 10, seed=1)
+    sb, keep = S.host_batch(b)
+    sc = np.zeros(b.n, np.int32)
+    rec = np.zeros(b.n * 64, np.uint8)
+    for rb in (0, 8, 40):  # not a multiple of 16, or too small
+        rc = saru_lib.saru_align_host_compact(C.byref(sb), sc.ctypes.data, rec.ctypes.data, rb, 0)
+        assert rc == S.SARU_E_INVALID

@@ -220,3 +220,16 @@ def test_chunked_mapping_prints_the_reference_output(saru_lib, tmp_path, fastq, 
     assert len(want) > 1000
     assert len(got) == len(want)
     assert hashlib.sha256(b"".join(got)).hexdigest() == hashlib.sha256(b"".join(want)).hexdigest()
+
+
+def test_readers_refuse_bad_arguments(saru_lib, tmp_path):
+    with pytest.raises(S.SaruError):
+        list(S.read_batches(tmp_path / "missing.fa", 36, 2, 100))
+    with pytest.raises(S.SaruError):
+        list(S.genome_chunks(tmp_path / "missing.fa", 1000, 36))
+    p = tmp_path / "g.fa"
+    p.write_bytes(genome_text(b"ACGT" * 100, 60))
+    with pytest.raises(S.SaruError):
+        list(S.genome_chunks(p, 0, 36))
+    with pytest.raises(S.SaruError):
+        list(S.read_batches(p, 0, 2, 100))
