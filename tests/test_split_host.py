@@ -85,3 +85,37 @@ def test_compact_host_call_on_the_exact_path(saru_lib):
     assert np.array_equal(comp.read_aln, slots.read_aln)
     assert np.array_equal(comp.genome_aln, slots.genome_aln)
     assert (slots.scores <= 5).sum() > 100
+
+
+def test_split_host_call_with_64_bit_bands(saru_lib):
+    """A sliced call at k = 9 (150 bp): each slice chooses its own band word
+    (64 bits where it has start gaps); slot strings and compact records
+    equal one launch over the whole call."""
+    import torch
+    bench = load_bench()
+    cfg = dict(bench.CONFIGS["c2"], m=150, k=9, reads=60_000)
+    b = bench.build_batches(cfg, 0)[0]
+    assert b.n >= 2 * (1 << 18) and b.k == 9
+    host = S.align_host(b)
+    sc, rec, rb = S.align_host_compact(b)
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    g, r, go, ro, d = T(b.genome), T(b.reads), T(b.genome_offsets), T(b.read_offsets), T(b.dirs)
+    dsc = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    sb = S.SaruBatch(g.data_ptr(), r.data_ptr(), go.data_ptr(), ro.data_ptr(), d.data_ptr(), b.n,
+                     b.k, 0, 1, 1, b.m, len(b.genome), b.total_genome)
+    sr = S.SaruResult(dsc.data_ptr(), ra.data_ptr(), ga.data_ptr(), st.data_ptr())
+    nscr = S.scratch_bytes(b.n, b.m, b.k)
+    scr = torch.empty(nscr, dtype=torch.uint8, device=dev)
+    S.align_device(sb, sr, scr.data_ptr(), nscr)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    assert np.array_equal(host.scores, dsc.cpu().numpy())
+    assert np.array_equal(host.read_aln, ra.cpu().numpy()[:b.total_genome])
+    assert np.array_equal(host.genome_aln, ga.cpu().numpy()[:b.total_genome])
+    comp = S.expand_compact(b, sc, rec, rb)
+    assert np.array_equal(comp.read_aln, host.read_aln)
+    assert np.array_equal(comp.genome_aln, host.genome_aln)
