@@ -30,3 +30,35 @@ def test_tile_emulation_under_asan():
                        capture_output=True, text=True, env=env, timeout=900)
     assert r.returncode == 0, (r.stdout[-3000:], r.stderr[-3000:])
     assert "BAD 0" in r.stdout
+
+
+FLANK_CHECK = r'''
+#include <stdio.h>
+#include "saru_core.cuh"
+int main() {
+  for (int k = 0; k <= 15; ++k)
+    for (int dir = -300; dir <= 300; ++dir) {
+      int so, eo, wso = 0, weo = 0;  // the flag meanings of src/hash.c:938-979
+      switch (dir) {
+        case 1: case 5: weo = k; break;
+        case 2: case 6: wso = k; break;
+        case 3: case 7: wso = k; weo = k; break;
+        default: break;
+      }
+      saru::flank_of(dir, k, so, eo);
+      if (so != wso || eo != weo) { printf("dir %d k %d\n", dir, k); return 1; }
+    }
+  return 0;
+}
+'''
+
+
+def test_flank_of_matches_the_flag_table(tmp_path):
+    """The branch-free flank_of gives each flag's start/end gaps exactly as
+    the reference's flag table does, for every flag value."""
+    src = tmp_path / "flank.cpp"
+    src.write_text(FLANK_CHECK)
+    exe = tmp_path / "flank"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", str(ROOT / "saruman_b200" / "csrc"),
+                    str(src), "-o", str(exe)], check=True)
+    assert subprocess.run([str(exe)]).returncode == 0
