@@ -38,7 +38,7 @@ static int run(const TileArgs &a0, int nwarps_total) {
     memset(st_win, 0xA5, (size_t)S.ws_bytes);
     memset(region, 0xA5, (size_t)S.region_bytes);
     uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
-    for (long wt = gwarp; wt * 32 < a.n; wt += nwarps_total) {
+    for (long wt = gwarp; a.t0 + wt * 32 < a.n; wt += nwarps_total) {
       const TileSpan s = tile_span(a, wt);
       if (!s.fits) {
         for (int lane = 0; lane < 32; ++lane)
@@ -99,6 +99,22 @@ extern "C" int tile_align_batch(const uint8_t *genome, const uint8_t *reads, con
   TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, ra, ga,
              nullptr, 0, 1, 0, 0, 0};
   return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
+}
+
+// The same call in slices of `slice` candidates (a multiple of 32), each a
+// launch over candidates [t0, t1) of the whole call, as the host entry
+// point streams a large call.
+extern "C" int tile_align_slices(const uint8_t *genome, const uint8_t *reads, const int *goff,
+                                 const int *roff, const int8_t *dirs, long n, int k, int max_m,
+                                 int wide, int first_of_call, int nwarps, long slice, int *scores,
+                                 uint8_t *ra, uint8_t *ga) {
+  int status = 0;
+  for (long t0 = 0; t0 < n; t0 += slice) {
+    TileArgs a{genome, reads, goff, roff, dirs, t0 + slice < n ? t0 + slice : n, k, max_m,
+               first_of_call, scores, ra, ga, nullptr, 0, 1, 0, 0, 0, nullptr, 0, t0};
+    status |= wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
+  }
+  return status;
 }
 
 // The same call with compact records (rec_bytes per candidate) instead of

@@ -78,6 +78,18 @@ def main():
                     print("MISMATCH", m, k, seed, off, st, flush=True)
                 if off == 3:  # compact records, expanded on the host by the library
                     bad += compact_case(lib, b, g, r, go, ro, d, wide, s1, ra1, ga1)
+                if off == 9:  # the call in slices of whole tiles
+                    sc2 = np.zeros(n, np.int32)
+                    ra2 = exact(np.zeros(b.total_genome, np.uint8), 2)
+                    ga2 = exact(np.zeros(b.total_genome, np.uint8), 13)
+                    st2 = lib.tile_align_slices(P(g), P(r), P(go), P(ro), P(d), C.c_long(n),
+                                                C.c_int(k), C.c_int(m), C.c_int(wide), C.c_int(1),
+                                                C.c_int(3), C.c_long(32 * (1 + seed)), P(sc2),
+                                                P(ra2), P(ga2))
+                    if not (st2 == 0 and np.array_equal(np.minimum(s1, k + 1), sc2)
+                            and np.array_equal(ra1, ra2) and np.array_equal(ga1, ga2)):
+                        bad += 1
+                        print("SLICE MISMATCH", m, k, seed, st2, flush=True)
     # an irregular tile (window far too long) must be rejected, not staged
     b = W.random_batch(36, 2, 40, seed=1)
     go = b.genome_offsets.copy()
