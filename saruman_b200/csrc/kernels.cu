@@ -1,9 +1,12 @@
 // kernels.cu -- sm_100a kernels of the alignment stage.
 //
-//  saru_band_kernel<T, CTA>   the production path: one thread per candidate,
+//  saru_band_kernel           the production path: persistent warps over
+//                             32-candidate tiles (one lane per candidate),
 //                             bit-parallel banded fill (saru_core.cuh) with
 //                             2-bit traceback decisions, traceback and slot
-//                             output on the device.
+//                             strings or compact records on the device; a
+//                             launch covers segments (calls, or slices
+//                             [t0, t1) of one call) of 32- or 64-bit bands.
 //  saru_full_fill_kernel      the exact full-rectangle path for inputs the
 //  saru_full_trace_kernel     banded kernel does not cover (other costs,
 //                             m <= 3k, k > 15, irregular windows): the
