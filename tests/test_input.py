@@ -197,7 +197,7 @@ def map_on_cpu(genome_path: Path, reads_path: Path, m: int, k: int, fastq: bool,
 
 
 @pytest.mark.skipif(not EMUL.exists(), reason="the reference's host build is not here")
-@pytest.mark.parametrize("fastq,m,k", [(False, 36, 2), (True, 36, 2), (False, 75, 4)])
+@pytest.mark.parametrize("fastq,m,k", [(False, 36, 2), (True, 36, 2), (False, 75, 4), (True, 100, 5)])
 def test_chunked_mapping_prints_the_reference_output(saru_lib, tmp_path, fastq, m, k):
     rng = np.random.default_rng(11 + fastq + m)
     g = W.uniform_genome(60_000, seed=12)
