@@ -55,31 +55,37 @@ CONFIGS = {
     "c4": dict(workload="long-read-end stress: 10 Mbp uniform genome, 1M reads x 250 bp, 4% errors "
                "(60/20/20), 5% unmapped, k=15", genome=("uniform", 10_000_000, 401),
                reads=1_000_000, m=250, k=15, rate=0.04, mix=(0.60, 0.20, 0.20), unmapped=0.05),
-    "c3": dict(workload="batching: 5 Mbp genome with Zipf(1.5, max 500) repeat copies, 4M reads of "
-               "lengths {36,75,100,150} (1M each), 3% errors, k=ceil(0.06 m); repeat hits capped at "
-               "25 per read (~22M candidates of uneven count per read); all length bins in one launch",
-               genome=("repeat", 5_000_000, 301, "zipf"), reads=4_000_000, lengths=(36, 75, 100, 150),
-               rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0, max_hits=25),
-    "c5": dict(workload="serving: 5 Mbp genome with Zipf(1.5, max 500) repeat copies; Poisson "
-               "arrivals of requests of 1k-500k reads (log-uniform), read lengths {36,75,100,150} "
-               "in equal parts, k=ceil(0.06 m), repeat hits capped at 25 per read; 60 GB device "
-               "budget; continuous-batching server vs the plain per-request loop on one trace",
-               genome=("repeat", 5_000_000, 301, "zipf"), reads=2_000_000,
+    "c3": dict(workload="batching: 5 Mbp genome with Zipf(1.5, max 500) repeat copies (seed 313: "
+               "1-112 copies per family), 4M reads of lengths {36,75,100,150} (1M each), 3% errors, "
+               "k=ceil(0.06 m); every candidate the reference's filter makes (uneven count per "
+               "read); all length bins in one batched request",
+               genome=("repeat", 5_000_000, 313, "zipf"), reads=4_000_000, lengths=(36, 75, 100, 150),
+               rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0),
+    "c5": dict(workload="serving: 5 Mbp genome with Zipf(1.5, max 500) repeat copies (seed 313) "
+               "resident on the device; Poisson arrivals of requests of 1k-500k reads (log-uniform), "
+               "read lengths {36,75,100,150} in equal parts, k=ceil(0.06 m); requests carry reads "
+               "only (the server filters, gathers and aligns); 60 GB device budget; continuous-"
+               "batching server vs the plain per-request loop on one trace",
+               genome=("repeat", 5_000_000, 313, "zipf"), reads=2_000_000,
                lengths=(36, 75, 100, 150), rate=0.03, mix=(0.70, 0.15, 0.15), unmapped=0.0,
-               max_hits=25, requests=400, min_reads=1_000, max_reads=500_000, budget=60 << 30,
-               load=0.8),
+               requests=400, min_reads=1_000, max_reads=500_000, budget=60 << 30, load=0.8),
 }
 
 
-def build_batches(cfg: dict, rank: int, tables: list | None = None):
-    """One batch per read-length bin (one for single-length configs); the
-    sequenced reads of each bin go to `tables` when given."""
+def build_genome(cfg: dict):
     from saruman_b200 import workloads as W
     gs = cfg["genome"]
     if gs[0] == "uniform":
-        g, rmap = W.uniform_genome(gs[1], seed=gs[2]), None
-    else:
-        g, rmap = W.repeat_genome_with_map(gs[1], seed=gs[2], copies=gs[3])
+        return W.uniform_genome(gs[1], seed=gs[2]), None
+    return W.repeat_genome_with_map(gs[1], seed=gs[2], copies=gs[3])
+
+
+def build_batches(cfg: dict, rank: int, tables: list | None = None):
+    """One batch per read-length bin (one for single-length configs) with
+    candidates placed where the q-gram filter places them (synthetic, no
+    GPU needed); the sequenced reads of each bin go to `tables` when given."""
+    from saruman_b200 import workloads as W
+    g, rmap = build_genome(cfg)
     lengths = cfg.get("lengths", (cfg.get("m"),))
     per_bin = cfg["reads"] // len(lengths)
     out = []
@@ -96,8 +102,34 @@ def build_batches(cfg: dict, rank: int, tables: list | None = None):
     return out
 
 
-def build_batch(cfg: dict, rank: int):
-    return build_batches(cfg, rank)[0]
+def build_callsets(cfg: dict, rank: int, tables: list | None = None, info: dict | None = None):
+    """One CallSet per read-length bin: the calls the reference's q-gram
+    filter makes for the bin's reads on both strands (the library's device
+    filter, which reproduces the reference's calls), at the reference's
+    queue threshold for that read length.  Needs the library and a GPU (the
+    filter runs on the calling thread's current device).  `info` receives
+    the filter's device time and counts."""
+    from saruman_b200 import workloads as W
+    g, _ = build_genome(cfg)
+    lengths = cfg.get("lengths", (cfg.get("m"),))
+    per_bin = cfg["reads"] // len(lengths)
+    out = []
+    for i, m in enumerate(lengths):
+        k = cfg.get("k", W.k_for(m))
+        rd = W.sample_reads(g, per_bin, m, cfg["rate"], seed=1000 + 17 * rank + i, mix=cfg["mix"],
+                            unmapped=cfg["unmapped"])
+        cv = cfg.get("chunk_value") or W.chunk_value_for(m, k)
+        cs = W.filter_callset(g, rd.seqs, m, k, cv)
+        out.append(cs)
+        if info is not None:
+            info.setdefault("bins", []).append(
+                {"m": m, "k": k, "reads": per_bin, "chunk_value": cv, "filter_ms": cs.filter_ms,
+                 "candidates": cs.n, "calls": cs.ncalls, "perfect_hits": cs.perfect})
+        if tables is not None:
+            tables.append(rd.seqs)
+    if tables is not None:
+        tables.append(g)
+    return out
 
 
 def band_cells(b) -> int:
@@ -191,36 +223,11 @@ def profile_traffic() -> dict | None:
     return None
 
 
-class Chunker:
-    """Consecutive sub-batches of a batch, each re-based as a call of its
-    own (the layout the reference's host code would build for it)."""
-
-    def __init__(self, b):
-        from saruman_b200 import workloads as W
-        self.b = b
-        self.W = W
-        self.L = b.lengths.astype(np.int64)
-        self.gend = np.cumsum(self.L)
-
-    def take(self, start: int, count: int):
-        b, W = self.b, self.W
-        e = min(b.n, start + count)
-        gs = int(self.gend[start - 1]) if start else 0
-        ge = int(self.gend[e - 1])
-        Ls = self.L[start:e]
-        go = np.cumsum(Ls).astype(np.int32)
-        ro = ((np.arange(e - start) + 1) * b.m).astype(np.int32)
-        esz = (b.m + 1) * (Ls + 1)
-        eo = (np.cumsum(esz) - esz).astype(np.int32)
-        return W.Batch(m=b.m, k=b.k, genome=b.genome[gs:ge], reads=b.reads[start * b.m:e * b.m],
-                       genome_offsets=go, read_offsets=ro, edit_offsets=eo, dirs=b.dirs[start:e],
-                       ids=b.ids[start:e], pos=b.pos[start:e])
-
-
-def cpu_reference_rate(b, seconds: float = 10.0, nthreads: int | None = None,
-                       chunker: Chunker | None = None) -> dict:
+def cpu_reference_rate(calls, seconds: float = 10.0, nthreads: int | None = None) -> dict:
     """The reference's own kernel code on the host (oracle/_ref), all host
-    threads, over consecutive sub-batches of the workload until `seconds`."""
+    threads, over consecutive pieces of the workload's calls (each piece a
+    call of its own, the layout the reference's host code would build for
+    it) until `seconds`."""
     import ctypes as C
     lib_path = ROOT / "oracle" / "_ref" / "libref_emul.so"
     if not lib_path.exists():
@@ -228,48 +235,64 @@ def cpu_reference_rate(b, seconds: float = 10.0, nthreads: int | None = None,
     lib = C.CDLL(str(lib_path))
     lib.ref_align_batch.restype = C.c_int
     nthreads = nthreads or os.cpu_count() or 1
-    ch = chunker or Chunker(b)
     P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
     done = 0
     chunk = max(2000, 500 * nthreads)
-    start = 0
     t0 = time.perf_counter()
-    while time.perf_counter() - t0 < seconds and start < b.n:
-        sb = ch.take(start, chunk)
-        sc = np.zeros(sb.n, np.int32)
-        ra = np.zeros(sb.total_genome + 64, np.uint8)
-        ga = np.zeros(sb.total_genome + 64, np.uint8)
-        rc = lib.ref_align_batch(C.c_int(0), C.c_int(1), P(sb.genome), P(sb.reads),
-                                 P(sb.genome_offsets), P(sb.read_offsets), P(sb.edit_offsets),
-                                 C.c_int(sb.n), P(sb.dirs), C.c_int(sb.k),
-                                 C.c_size_t(sb.total_genome), C.c_int(0), C.c_int(nthreads),
-                                 C.c_int(256), P(sc), P(ra), P(ga))
-        if rc != 0:
-            return {"value": None, "unavailable": "reference host run failed"}
-        done += sb.n
-        start += sb.n
+    for b in calls:
+        L = b.lengths
+        gend = np.cumsum(L)
+        for start in range(0, b.n, chunk):
+            if time.perf_counter() - t0 >= seconds:
+                break
+            e = min(b.n, start + chunk)
+            gs = int(gend[start - 1]) if start else 0
+            Ls = L[start:e]
+            go = np.cumsum(Ls).astype(np.int32)
+            ro = ((np.arange(e - start) + 1) * b.m).astype(np.int32)
+            esz = (b.m + 1) * (Ls + 1)
+            eo = (np.cumsum(esz) - esz).astype(np.int32)
+            gbytes = np.ascontiguousarray(b.genome[gs:int(gend[e - 1])])
+            rbytes = np.ascontiguousarray(b.reads[start * b.m:e * b.m])
+            dirs = np.ascontiguousarray(b.dirs[start:e])
+            tot = int(go[-1]) + b.k * (e - start)
+            sc = np.zeros(e - start, np.int32)
+            ra = np.zeros(tot + 64, np.uint8)
+            ga = np.zeros(tot + 64, np.uint8)
+            rc = lib.ref_align_batch(C.c_int(0), C.c_int(1), P(gbytes), P(rbytes), P(go), P(ro),
+                                     P(eo), C.c_int(e - start), P(dirs), C.c_int(b.k),
+                                     C.c_size_t(tot), C.c_int(0), C.c_int(nthreads),
+                                     C.c_int(256), P(sc), P(ra), P(ga))
+            if rc != 0:
+                return {"value": None, "unavailable": "reference host run failed"}
+            done += e - start
+        if time.perf_counter() - t0 >= seconds:
+            break
     dt = time.perf_counter() - t0
     return {"value": done / dt, "cores": nthreads, "candidates": done, "seconds": dt}
+
+
+def all_calls(css) -> list:
+    return [cs.call(c) for cs in css for c in range(cs.ncalls)]
 
 
 def run_reference_arm(args, cfg, rank: int) -> None:
     if rank != 0:
         return
-    bs = build_batches(cfg, 0)
-    chs = [Chunker(b) for b in bs]
+    import torch
+    torch.cuda.set_device(0)  # the workload's calls come from the device filter
+    css = build_callsets(cfg, 0)
+    calls = all_calls(css)
     per_step = []
+    cores = None
     for i in range(args.warmup + args.steps):
-        cand, secs = 0, 0.0
-        for b, ch in zip(bs, chs):
-            r = cpu_reference_rate(b, seconds=args.ref_seconds / len(bs), chunker=ch)
-            if r.get("value") is None:
-                print(json.dumps({"impl": "reference", "unavailable": r.get("unavailable")}))
-                return
-            cand += r["candidates"]
-            secs += r["seconds"]
-            cores = r["cores"]
+        r = cpu_reference_rate(calls, seconds=args.ref_seconds)
+        if r.get("value") is None:
+            print(json.dumps({"impl": "reference", "unavailable": r.get("unavailable")}))
+            return
+        cores = r["cores"]
         if i >= args.warmup:
-            per_step.append((cand, secs))
+            per_step.append((r["candidates"], r["seconds"]))
     cand = sum(c for c, _ in per_step)
     secs = sum(t for _, t in per_step)
     value = cand / secs
@@ -278,8 +301,8 @@ def run_reference_arm(args, cfg, rank: int) -> None:
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * secs / len(per_step), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "sample": "consecutive sub-batches of the "
-                   f"workload, {args.ref_seconds:.0f} s of host work per step"},
+        "config": {"workload": cfg["workload"], "sample": "consecutive pieces of the workload's "
+                   f"calls, {args.ref_seconds:.0f} s of host work per step"},
         "cpu_baseline": {"value": value, "unit": "alignments/s", "cores": cores,
                          "kind": "reference", "sample": f"{cand} candidates"},
         "e2e": {"value": value, "unit": "alignments/s", "h2d_bytes_per_step": 0,
@@ -288,46 +311,107 @@ def run_reference_arm(args, cfg, rank: int) -> None:
     print(json.dumps(line))
 
 
-class DeviceBatch:
-    """A batch's inputs and outputs resident on the device, with the C-ABI
-    views of them."""
+class DeviceCalls:
+    """A CallSet's inputs and outputs resident on the device, with one C-ABI
+    call per reference call (pointers into the set's arrays), and pinned
+    host copies of the inputs and outputs for the end-to-end legs."""
 
-    def __init__(self, b, dev, S):
+    def __init__(self, cs, dev, S, status):
         import torch
         T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-        self.b = b
-        self.g, self.r, self.go, self.ro, self.d = (T(b.genome), T(b.reads), T(b.genome_offsets),
-                                                    T(b.read_offsets), T(b.dirs))
-        self.scores = torch.zeros(b.n, dtype=torch.int32, device=dev)
-        self.ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
-        self.ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
-        self.sb = S.SaruBatch(self.g.data_ptr(), self.r.data_ptr(), self.go.data_ptr(),
-                              self.ro.data_ptr(), self.d.data_ptr(), b.n, b.k, 0, 1, 1, b.m,
-                              len(b.genome), b.total_genome)
-        self.sr = S.SaruResult(self.scores.data_ptr(), self.ra.data_ptr(), self.ga.data_ptr(),
-                               None)
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-        self.h_in = [(self.g, pin(b.genome)), (self.r, pin(b.reads)), (self.go, pin(b.genome_offsets)),
-                     (self.ro, pin(b.read_offsets)), (self.d, pin(b.dirs))]
-        self.h_out = [(torch.empty(b.n, dtype=torch.int32).pin_memory(), self.scores),
-                      (torch.empty(b.total_genome, dtype=torch.uint8).pin_memory(),
-                       self.ra[:b.total_genome]),
-                      (torch.empty(b.total_genome, dtype=torch.uint8).pin_memory(),
-                       self.ga[:b.total_genome])]
+        self.cs, m = cs, cs.m
+        self.g, self.r, self.go, self.ro, self.d = (T(cs.genome), T(cs.reads),
+                                                    T(cs.genome_offsets), T(cs.read_offsets),
+                                                    T(cs.dirs))
+        self.scores = torch.zeros(cs.n, dtype=torch.int32, device=dev)
+        self.ra = torch.zeros(cs.total_slots + 64, dtype=torch.uint8, device=dev)
+        self.ga = torch.zeros(cs.total_slots + 64, dtype=torch.uint8, device=dev)
+        self.h_in = [pin(cs.genome), pin(cs.reads), pin(cs.genome_offsets), pin(cs.read_offsets),
+                     pin(cs.dirs)]
+        self.h_out = [torch.empty(cs.n, dtype=torch.int32).pin_memory(),
+                      torch.empty(cs.total_slots + 64, dtype=torch.uint8).pin_memory(),
+                      torch.empty(cs.total_slots + 64, dtype=torch.uint8).pin_memory()]
+        self.sbs, self.srs, self.spans = [], [], []
+        cb, gb, sbase = cs.call_begin, cs.gbase, cs.sbase
+        for c in range(cs.ncalls):
+            a, b = int(cb[c]), int(cb[c + 1])
+            g0, g1, s0, s1 = int(gb[c]), int(gb[c + 1]), int(sbase[c]), int(sbase[c + 1])
+            self.sbs.append(S.SaruBatch(self.g.data_ptr() + g0, self.r.data_ptr() + a * m,
+                                        self.go.data_ptr() + 4 * a, self.ro.data_ptr() + 4 * a,
+                                        self.d.data_ptr() + a, b - a, cs.k, 0, 1, 1, m, g1 - g0,
+                                        s1 - s0))
+            self.srs.append(S.SaruResult(self.scores.data_ptr() + 4 * a, self.ra.data_ptr() + s0,
+                                         self.ga.data_ptr() + s0, status.data_ptr()))
+            self.spans.append((a, b, g0, g1, s0, s1))
 
-    def h2d(self):
-        for d, h in self.h_in:
-            d.copy_(h, non_blocking=True)
+    def host_call(self, c: int):
+        """Call c as a Batch over the pinned host inputs, and an AlignResult
+        over the pinned host outputs."""
+        import saruman_b200 as S
+        from saruman_b200 import workloads as W
+        cs, m = self.cs, self.cs.m
+        a, b, g0, g1, s0, s1 = self.spans[c]
+        hg, hr, hgo, hro, hd = (t.numpy() for t in self.h_in)
+        bt = W.Batch(m=m, k=cs.k, genome=hg[g0:g1], reads=hr[a * m:b * m],
+                     genome_offsets=hgo[a:b], read_offsets=hro[a:b],
+                     edit_offsets=cs.edit_offsets[a:b], dirs=hd[a:b], ids=cs.ids[a:b],
+                     pos=cs.pos[a:b])
+        sc, ra, ga = (t.numpy() for t in self.h_out)
+        return bt, S.AlignResult(sc[a:b], ra[s0:s1], ga[s0:s1])
 
-    def d2h(self):
-        for h, d in self.h_out:
-            h.copy_(d, non_blocking=True)
+    def copy_in(self, c0: int, c1: int):
+        """Inputs of calls [c0, c1) (contiguous in every array), on the
+        current stream."""
+        a, g0, m = self.spans[c0][0], self.spans[c0][2], self.cs.m
+        b, g1 = self.spans[c1 - 1][1], self.spans[c1 - 1][3]
+        for d, h, lo, hi in ((self.g, self.h_in[0], g0, g1), (self.r, self.h_in[1], a * m, b * m),
+                             (self.go, self.h_in[2], a, b), (self.ro, self.h_in[3], a, b),
+                             (self.d, self.h_in[4], a, b)):
+            d[lo:hi].copy_(h[lo:hi], non_blocking=True)
 
-    def bytes_in(self):
-        return sum(int(h.numel() * h.element_size()) for _, h in self.h_in)
+    def copy_out(self, c0: int, c1: int):
+        a, s0 = self.spans[c0][0], self.spans[c0][4]
+        b, s1 = self.spans[c1 - 1][1], self.spans[c1 - 1][5]
+        for h, d, lo, hi in ((self.h_out[0], self.scores, a, b), (self.h_out[1], self.ra, s0, s1),
+                             (self.h_out[2], self.ga, s0, s1)):
+            h[lo:hi].copy_(d[lo:hi], non_blocking=True)
 
-    def bytes_out(self):
-        return sum(int(h.numel() * h.element_size()) for h, _ in self.h_out)
+    def bytes_in(self) -> int:
+        return sum(int(h.numel() * h.element_size()) for h in self.h_in)
+
+    def bytes_out(self) -> int:
+        return 4 * self.cs.n + 2 * self.cs.total_slots
+
+
+def call_groups(dcs: list, per_group: int) -> list:
+    """Consecutive calls of each set in groups of up to `per_group`:
+    (set index, first call, end call)."""
+    out = []
+    for i, d in enumerate(dcs):
+        for c0 in range(0, d.cs.ncalls, per_group):
+            out.append((i, c0, min(d.cs.ncalls, c0 + per_group)))
+    return out
+
+
+def legacy_names(n_ids: int):
+    """The caller-owned read_names table of the reference's host program for
+    read ids 0..n_ids-1 (names "read<id>"), as the library walks it: a list
+    of struct read_name_hash (src/util.h:350-354: int read_number; char
+    name[60]; UT_hash_handle hh) linked by the handle's third pointer."""
+    import ctypes as C
+    esz = 64 + 6 * 8 + 8
+    buf = np.zeros(n_ids * esz, np.uint8)
+    base = buf.ctypes.data
+    rec = buf.reshape(n_ids, esz)
+    rec[:, 0:4] = np.arange(n_ids, dtype=np.int32).view(np.uint8).reshape(n_ids, 4)
+    names = np.char.add(b"read", np.arange(n_ids).astype("S12"))
+    nb = np.frombuffer(names.astype("S60").tobytes(), np.uint8).reshape(n_ids, 60)
+    rec[:, 4:64] = nb
+    nxt = base + (np.arange(n_ids, dtype=np.uint64) + 1) * esz
+    nxt[-1] = 0
+    rec[:, 80:88] = nxt.view(np.uint8).reshape(n_ids, 8)
+    return buf, C.c_void_p(base)
 
 
 def timed(stream, fn, steps, world, dist, dev):
@@ -347,294 +431,614 @@ def timed(stream, fn, steps, world, dist, dev):
     return ms / steps
 
 
-def tune_bins(bs, dbs, status, sample: int = 1_000_000) -> dict:
-    """Autotunes the launch shape of every (read length, k) bin on the
-    first `sample` candidates of the bin itself: the cost model (trained on
-    the GPU from the committed B200 sweep) ranks the shapes, the tuner
-    times its top 6 and the default, and installs the fastest."""
+class ReadPool:
+    """Reads of every length bin, as sequenced; a request takes a contiguous
+    range of reads from each bin (reads only: the server filters them)."""
+
+    def __init__(self, tables: list, ks: list):
+        self.tables, self.ks = tables, ks
+
+    def make(self, reads: int, rng) -> list:
+        sets = []
+        for t, k in zip(self.tables, self.ks):
+            r = max(1, reads // len(self.tables))
+            off = int(rng.integers(0, max(1, t.shape[0] - r)))
+            sets.append((t[off:off + r], k, 0))
+        return sets
+
+
+def run_trace(S, genome, reqs: list, arrivals_s, pipeline: bool, budget: int,
+              compact: bool = False, warm: list | None = None) -> dict:
+    """Submits reads-only requests at their arrival times (seconds after the
+    start; None = all at once) to a fresh server and returns per-request
+    latency from arrival to results in host memory, the makespan, the
+    candidates the filter made and the server's counters."""
+    import threading
+    srv = S.Server(pipeline=pipeline, max_requests_per_launch=64, max_inflight=2,
+                   budget_bytes=budget)
+    try:
+        srv.set_genome(genome)
+        for sets in warm or []:  # builds each bin's q-gram index; not timed
+            t = srv.submit_reads(sets, compact=compact)
+            rc, _ = srv.wait(t, 3_600_000)
+            if rc != S.SARU_OK:
+                raise RuntimeError(S.last_error())
+            srv.release(t)
+        g0, l0 = srv.counters()
+        tickets = [None] * len(reqs)
+        err = []
+        lock = threading.Condition()
+        t0 = time.monotonic_ns() // 1000
+
+        def submitter():
+            try:
+                for q, sets in enumerate(reqs):
+                    if arrivals_s is not None:
+                        delay = t0 / 1e6 + arrivals_s[q] - time.monotonic()
+                        if delay > 0:
+                            time.sleep(delay)
+                    t = srv.submit_reads(sets, compact=compact)
+                    with lock:
+                        tickets[q] = t
+                        lock.notify_all()
+            except Exception as ex:  # surfaced below
+                with lock:
+                    err.append(ex)
+                    lock.notify_all()
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        done_us, cand = [0] * len(reqs), 0
+        for q in range(len(reqs)):
+            with lock:
+                while tickets[q] is None and not err:
+                    lock.wait()
+                if err:
+                    break
+                t = tickets[q]
+            rc, st = srv.wait(t, 3_600_000)
+            if rc != S.SARU_OK:
+                raise RuntimeError(f"request {q}: {rc} {S.last_error()}")
+            done_us[q] = st.done_us
+            cand += srv.candidates(t)
+            srv.release(t)
+        th.join()
+        if err:
+            raise err[0]
+        groups, launches = srv.counters()
+    finally:
+        srv.close()
+    arr_us = [t0 + (int(a * 1e6) if arrivals_s is not None else 0) for a in
+              (arrivals_s if arrivals_s is not None else [0] * len(reqs))]
+    lat_ms = [(d - a) / 1000 for d, a in zip(done_us, arr_us)]
+    return {"lat_ms": lat_ms, "makespan_s": (max(done_us) - t0) / 1e6, "candidates": cand,
+            "groups": groups - g0, "launches": launches - l0}
+
+
+def serving(S, cfg: dict, nreq: int, seed: int = 4242, compact_too: bool = False,
+            clk=None) -> dict:
+    """The serving workload: one seeded Poisson trace of reads-only requests
+    through the continuous-batching server and the plain per-request loop,
+    at `load` of the plain loop's capacity, and both at saturation."""
+    from saruman_b200 import workloads as W
+    g, _ = build_genome(cfg)
+    lengths = cfg["lengths"]
+    per_bin = cfg["reads"] // len(lengths)
+    tables = [W.sample_reads(g, per_bin, m, cfg["rate"], seed=1000 + i, mix=cfg["mix"],
+                             unmapped=cfg["unmapped"]).seqs for i, m in enumerate(lengths)]
+    pool = ReadPool(tables, [W.k_for(m) for m in lengths])
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(cfg["min_reads"]), np.log(cfg["max_reads"]), nreq))
+    sizes = sizes.astype(np.int64)
+    reqs = [pool.make(int(x), rng) for x in sizes]
+    warm = [pool.make(20_000, rng) for _ in range(3)]
+    probe = [pool.make(100_000, rng) for _ in range(6)]
+    budget = cfg["budget"]
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(budget, free - (8 << 30)))
+    # the plain loop's capacity in reads/s, closed loop
+    cap = run_trace(S, g, probe, None, False, budget, warm=warm)
+    plain_reads_s = sum(t.shape[0] for sets in probe for t, _, _ in sets) / cap["makespan_s"]
+    lam = cfg["load"] * plain_reads_s / float(sizes.mean())
+    gaps = rng.exponential(1.0 / lam, nreq)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    if clk is not None:
+        clk.__enter__()
+    try:
+        b = run_trace(S, g, reqs, arrivals, True, budget, warm=warm)
+    finally:
+        if clk is not None:
+            clk.__exit__(None, None, None)
+    p = run_trace(S, g, reqs, arrivals, False, budget, warm=warm)
+    sb = run_trace(S, g, reqs, None, True, budget, warm=warm)
+    sp = run_trace(S, g, reqs, None, False, budget, warm=warm)
+
+    def pct(v, q):
+        return float(np.percentile(np.asarray(v), q))
+
+    n_cand = b["candidates"]
+    out = {
+        "requests": nreq, "reads": int(sizes.sum()), "candidates": n_cand,
+        "offered_load": {"requests_per_s": lam, "reads_per_s": lam * float(sizes.mean()),
+                         "fraction_of_plain_capacity": cfg["load"]},
+        "latency_ms": {"p50": pct(b["lat_ms"], 50), "p99": pct(b["lat_ms"], 99),
+                       "max": max(b["lat_ms"]), "throughput": n_cand / b["makespan_s"],
+                       "groups": b["groups"], "launches": b["launches"]},
+        "plain_latency_ms": {"p50": pct(p["lat_ms"], 50), "p99": pct(p["lat_ms"], 99),
+                             "max": max(p["lat_ms"]), "throughput": n_cand / p["makespan_s"],
+                             "launches": p["launches"]},
+        "saturation": {"value": n_cand / sb["makespan_s"], "plain_value": n_cand / sp["makespan_s"],
+                       "batched_over_plain": sp["makespan_s"] / sb["makespan_s"],
+                       "makespan_s": sb["makespan_s"]},
+        "p99_plain_over_batched": pct(p["lat_ms"], 99) / pct(b["lat_ms"], 99),
+        "budget_bytes": budget,
+        "what": "requests of reads only: the server runs the reference's q-gram filter on both "
+                "strands, gathers windows from the resident genome, aligns and returns slot "
+                "strings; latency from arrival to results in host memory; plain = one request "
+                "at a time, filter, one launch per call, no overlap",
+    }
+    if compact_too:
+        sbc = run_trace(S, g, reqs, None, True, budget, compact=True, warm=warm)
+        spc = run_trace(S, g, reqs, None, False, budget, compact=True, warm=warm)
+        out["compact"] = {"value": n_cand / sbc["makespan_s"],
+                          "plain_value": n_cand / spc["makespan_s"],
+                          "batched_over_plain": spc["makespan_s"] / sbc["makespan_s"]}
+    return out
+
+
+def run_serving(args, cfg, rank: int) -> None:
+    import torch
+    import saruman_b200 as S
+    torch.cuda.set_device(0)
+    S.load()
+    nreq = args.requests or cfg["requests"]
+    clk = ClockSampler(0)
+    r = serving(S, cfg, nreq, compact_too=True, clk=clk)
+    line = {
+        "metric": "alignments/s", "value": r["saturation"]["value"], "unit": "alignments/s",
+        "n_gpus": 1, "steps": 1, "warmup": 3, "ms_per_step": 1000 * r["saturation"]["makespan_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "requests": nreq, "reads": r["reads"],
+                   "candidates": r["candidates"], "device_budget_bytes": r["budget_bytes"],
+                   "step": "the whole trace, submitted at once (saturation)",
+                   "l2": "inputs > L2"},
+        "e2e": {"value": r["saturation"]["value"], "unit": "alignments/s",
+                "h2d_bytes_per_step": r["reads"], "d2h_bytes_per_step": None},
+        "serving": r,
+        "batched_over_plain": r["saturation"]["batched_over_plain"],
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+def tune_callsets(dcs: list, status, sample_calls: int = 6) -> dict:
+    """Autotunes the launch shape of every (read length, k) bin on the bin's
+    largest call: the cost model (trained on the GPU from the committed
+    B200 sweep) ranks the shapes, the tuner times its top 6 and the
+    default, and installs the fastest."""
     from saruman_b200 import autotune as A
     from saruman_b200 import costmodel as CM
     t0 = time.perf_counter()
     model = CM.trained_on_sweep()
     t_train = time.perf_counter() - t0
     out = {}
-    for b, d in zip(bs, dbs):
-        smp = A.Sample.wrap(b, d.sb, d.sr, status).prefix(min(b.n, sample))
+    for d in dcs:
+        cs = d.cs
+        c = int(np.argmax(np.diff(cs.call_begin)))
+        smp = A.Sample.wrap(cs.call(c), d.sbs[c], d.srs[c], status)
         r = A.tune_bin(smp, model=model, top=6)
-        out[f"{b.m},{b.k}"] = {"shape": list(r["best"]), "trials": len(r["ms"]),
-                               "ms_sample": r["ms"][r["best"]],
-                               "default_ms_sample": r["default_ms"]}
+        out[f"{cs.m},{cs.k}"] = {"shape": list(r["best"]), "trials": len(r["ms"]),
+                                 "ms_sample": r["ms"][r["best"]],
+                                 "default_ms_sample": r["default_ms"],
+                                 "sample_candidates": int(cs.call_begin[c + 1] - cs.call_begin[c])}
     out["cost_model_train_s"] = t_train
     out["tune_s"] = time.perf_counter() - t0
     return out
 
 
-class RequestPool:
-    """Requests of the serving trace as C-ABI views into pinned host memory.
-    Each request takes a contiguous range of reads from every length bin of
-    a pre-generated candidate pool (the host filter's output), one gather
-    call per bin: the request's read table (reads as sequenced), and per
-    candidate its read's row, window start, flag and window end offset; the
-    server gathers windows and reads from its resident genome.  Outputs come
-    from a pinned ring that requests release in completion order."""
-
-    def __init__(self, bs, tables, S, ring_bytes: int):
-        import torch
-        self.S = S
-        self.bs = bs
-        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-        self.pt = [pin(t.reshape(-1)) for t in tables]
-        self.pp = [pin(b.pos) for b in bs]
-        self.pd = [pin(b.dirs) for b in bs]
-        self.gend = [np.concatenate([[0], b.genome_offsets.astype(np.int64)]) for b in bs]
-        self.per_bin = [t.shape[0] for t in tables]
-        self.ring = torch.empty(ring_bytes, dtype=torch.uint8).pin_memory()
-        self.ring_ptr = self.ring.data_ptr()
-        self.ring_bytes = ring_bytes
-        self.live = []  # (start, end) of outstanding requests, oldest first
-
-    def make(self, reads: int, rng) -> dict:
-        import torch
-        S = self.S
-        calls, gcalls, keep, cand, out_bytes, spans = [], [], [], 0, 0, []
-        h2d = d2h = out_compact = d2h_compact = 0
-        for i, b in enumerate(self.bs):
-            r = max(1, reads // len(self.bs))
-            r0 = int(rng.integers(0, max(1, self.per_bin[i] - r)))
-            c0, c1 = (int(x) for x in np.searchsorted(b.ids, [r0, r0 + r]))
-            n = c1 - c0
-            if n == 0:
-                continue
-            base = int(self.gend[i][c0])
-            go = (self.gend[i][c0 + 1:c1 + 1] - base).astype(np.int32)
-            ri = (b.ids[c0:c1] - r0).astype(np.int32)
-            t = torch.from_numpy(np.concatenate([go, ri])).pin_memory()
-            keep.append(t)
-            gbytes = int(go[-1])
-            slots = gbytes + b.k * n
-            recs = n * S.compact_record_bytes(b.m, b.k)
-            spans.append((4 * n, slots + 64, recs))
-            out_bytes += (4 * n + 255) // 256 * 256 + 2 * ((slots + 64 + 255) // 256 * 256)
-            out_compact += (4 * n + 255) // 256 * 256 + (recs + 255) // 256 * 256
-            d2h_compact += 4 * n + recs
-            calls.append(S.SaruBatch(0, 0, t.data_ptr(), 0, self.pd[i].data_ptr() + c0, n, b.k,
-                                     0, 1, 1, b.m, gbytes, slots))
-            gcalls.append(S.SaruGatherCall(self.pt[i].data_ptr() + r0 * b.m, t.data_ptr() + 4 * n,
-                                           self.pp[i].data_ptr() + 4 * c0,
-                                           self.pd[i].data_ptr() + c0, t.data_ptr(), n, r, b.k,
-                                           0, 1, 1, b.m, gbytes, slots))
-            cand += n
-            h2d += r * b.m + 13 * n
-            d2h += 4 * n + 2 * slots
-        return dict(calls=calls, gcalls=gcalls, keep=keep, cand=cand, out_bytes=out_bytes,
-                    out_compact=out_compact, spans=spans, h2d=h2d, d2h=d2h,
-                    d2h_compact=d2h_compact)
-
-    def alloc(self, nbytes: int) -> int | None:
-        """Start offset in the ring, or None while the oldest requests hold it."""
-        if nbytes > self.ring_bytes:
-            raise ValueError("request larger than the output ring")
-        if not self.live:
-            return 0
-        tail, head = self.live[0][0], self.live[-1][1]
-        if self.live[-1][0] >= tail:  # not wrapped: free [head, end) and [0, tail)
-            if self.ring_bytes - head >= nbytes:
-                return head
-            return 0 if tail >= nbytes else None
-        return head if tail - head >= nbytes else None  # wrapped: free [head, tail)
-
-    def bind(self, req: dict, start: int, compact: bool = False):
-        S = self.S
-        p = self.ring_ptr + start
-        res = []
-        for n4, slots, recs in req["spans"]:
-            sc = p
-            p += (n4 + 255) // 256 * 256
-            if compact:
-                res.append(S.SaruResult(sc, p, 0, None))
-                p += (recs + 255) // 256 * 256
-                continue
-            ra = p
-            p += (slots + 255) // 256 * 256
-            ga = p
-            p += (slots + 255) // 256 * 256
-            res.append(S.SaruResult(sc, ra, ga, None))
-        self.live.append((start, start + (req["out_compact"] if compact else req["out_bytes"])))
-        n = len(req["calls"])
-        import ctypes as C
-        req["arr_c"] = (S.SaruBatch * n)(*req["calls"])
-        req["arr_r"] = (S.SaruResult * n)(*res)
-        req["arr_g"] = (S.SaruGatherCall * n)(*req["gcalls"])
-        req["creq"] = S.SaruRequest(req["arr_c"], req["arr_r"], n,
-                                    C.cast(req["arr_g"], C.POINTER(S.SaruGatherCall)),
-                                    1 if compact else 0)
-
-    def release_oldest(self):
-        self.live.pop(0)
-
-
-def run_trace(S, pool: RequestPool, reqs: list, arrivals_s, pipeline: bool, budget: int,
-              max_per_launch: int = 64, compact: bool = False):
-    """Submits the requests at their arrival times (seconds after start;
-    None = all at once) to a fresh server and returns per-request latency
-    from arrival to results on the host, the makespan and the counters."""
-    import ctypes as C
+def measure_calls(S, css: list, args, dev, world: int, dist, tune: bool = True,
+                  legacy_steps: int = 0, clk_device: int | None = None) -> dict:
+    """Times one workload of calls (CallSets, all resident): the batched
+    request (every call in one saru_align_multi_device request, replayed from
+    a CUDA graph), the plain per-call kernel (one launch per call), the
+    batched end-to-end path (pinned host buffers, groups of calls overlapped
+    on three streams), the plain end-to-end path (a thread per strand,
+    saru_align_host per call) and, if asked, the drop-in entry."""
     import threading
-    srv = S.Server(pipeline=pipeline, max_requests_per_launch=max_per_launch, max_inflight=2,
-                   budget_bytes=budget)
-    srv.set_genome(pool.genome)
-    lib = S.load()
-    tickets = [None] * len(reqs)
-    done_us = [0] * len(reqs)
-    lock = threading.Condition()
-    t0 = time.monotonic_ns() // 1000
 
-    def submitter():
-        for q, r in enumerate(reqs):
-            if arrivals_s is not None:
-                delay = t0 / 1e6 + arrivals_s[q] - time.monotonic()
-                if delay > 0:
-                    time.sleep(delay)
-            with lock:
-                while True:
-                    start = pool.alloc(r["out_compact"] if compact else r["out_bytes"])
-                    if start is not None:
-                        break
-                    lock.wait()
-                pool.bind(r, start, compact)
-            t = C.c_int64()
-            rc = lib.saru_server_submit(srv._h, C.byref(r["creq"]), C.byref(t))
-            if rc != S.SARU_OK:
-                raise RuntimeError(S.last_error())
-            with lock:
-                tickets[q] = t.value
-                lock.notify_all()
-
-    th = threading.Thread(target=submitter)
-    th.start()
-    st = S.RequestStats()
-    for q in range(len(reqs)):
-        with lock:
-            while tickets[q] is None:
-                lock.wait()
-            t = tickets[q]
-        rc = lib.saru_server_wait(srv._h, t, 3_600_000, C.byref(st))
-        if rc != S.SARU_OK:
-            raise RuntimeError(f"request {q}: {rc} {S.last_error()}")
-        done_us[q] = st.done_us
-        with lock:
-            pool.release_oldest()
-            lock.notify_all()
-    th.join()
-    groups, launches = srv.counters()
-    srv.close()
-    arr_us = [t0 + (int(a * 1e6) if arrivals_s is not None else 0) for a in
-              (arrivals_s if arrivals_s is not None else [0] * len(reqs))]
-    lat_ms = [(d - a) / 1000 for d, a in zip(done_us, arr_us)]
-    makespan = (max(done_us) - t0) / 1e6
-    return lat_ms, makespan, groups, launches
-
-
-def run_serving(args, cfg, rank: int) -> None:
-    """Serving workload: the same seeded Poisson trace through the batched
-    server and the plain per-request loop, plus both at saturation."""
     import torch
-    import saruman_b200 as S
-    torch.cuda.set_device(0)
-    tables = []
-    bs = build_batches(cfg, rank, tables)
-    genome = tables.pop()
-    S.load()
-    rng = np.random.default_rng(4242)
-    nreq = args.requests or cfg["requests"]
-    sizes = np.exp(rng.uniform(np.log(cfg["min_reads"]), np.log(cfg["max_reads"]), nreq))
-    sizes = sizes.astype(np.int64)
-    pool = RequestPool(bs, tables, S, ring_bytes=6 << 30)  # largest request: ~0.7 GB out
-    pool.genome = genome
-    reqs = [pool.make(int(s), rng) for s in sizes]
-    n_cand = sum(r["cand"] for r in reqs)
-    warm = [pool.make(100_000, rng) for _ in range(max(args.warmup, 3))]
-    status = torch.zeros(1, dtype=torch.int32, device="cuda:0")
-    tuning = {}
-    if not args.no_tune:
-        dbs = [DeviceBatch(b, torch.device("cuda:0"), S) for b in bs]
-        for d in dbs:
-            d.sr.status = status.data_ptr()
-        tuning = tune_bins(bs, dbs, status)
-        del dbs
-        torch.cuda.empty_cache()
-    budget = cfg["budget"]
-    free, _ = torch.cuda.mem_get_info()
-    budget = int(min(budget, free - (8 << 30)))
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    dcs = [DeviceCalls(cs, dev, S, status) for cs in css]
+    n_cand = sum(cs.n for cs in css)
+    sbs = [sb for d in dcs for sb in d.sbs]
+    srs = [sr for d in dcs for sr in d.srs]
+    ncalls = len(sbs)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    # launch shapes first: the scratch sizes depend on them
+    if args.shape:
+        shape = tuple(int(x) for x in args.shape.split(","))
+        for cs in css:
+            S.set_tuning(cs.m, cs.k, *shape)
+        tuning = {f"{cs.m},{cs.k}": {"shape": list(shape), "trials": 0} for cs in css}
+    else:
+        tuning = tune_callsets(dcs, status) if tune else {}
+    status.zero_()
+    reqs = [(sbs[q:q + 192], srs[q:q + 192]) for q in range(0, ncalls, 192)]
+    nscr = max(S.multi_scratch_bytes(rb) for rb, _ in reqs)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
 
-    # warm-up + plain capacity, closed loop
-    _, mk, _, _ = run_trace(S, pool, warm, None, False, budget)
-    plain_cap = sum(r["cand"] for r in warm) / mk
-    run_trace(S, pool, warm, None, True, budget)
+    def step_batched():  # every call of the step in one request (one launch per length class)
+        for rb, rr in reqs:
+            S.align_multi_device(rb, rr, status.data_ptr(), scratch.data_ptr(), nscr, sptr)
 
-    mean_cand = n_cand / nreq
-    lam = cfg["load"] * plain_cap / mean_cand  # requests per second
-    gaps = rng.exponential(1.0 / lam, nreq)
-    arrivals = np.cumsum(gaps) - gaps[0]
+    nplain = max(S.scratch_bytes(sb.n, sb.max_read_length, sb.k) for sb in sbs)
+    scratch_plain = torch.empty(nplain, dtype=torch.uint8, device=dev)
+
+    def step_plain():  # one launch per call, in call order
+        for sb, sr in zip(sbs, srs):
+            S.align_device(sb, sr, scratch_plain.data_ptr(), nplain, sptr)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step_batched()
+    stream.synchronize()
+    if int(status.item()) != 0:
+        raise SystemExit(f"kernel status {int(status.item())}")
+    graph = torch.cuda.CUDAGraph()
     launches0 = S.kernel_launches()
-    with ClockSampler(0) as clk:
-        lat_b, mk_b, groups_b, launches_b = run_trace(S, pool, reqs, arrivals, True, budget)
-    lat_p, mk_p, groups_p, launches_p = run_trace(S, pool, reqs, arrivals, False, budget)
-    sat_b = run_trace(S, pool, reqs, None, True, budget)
-    sat_p = run_trace(S, pool, reqs, None, False, budget)
-    # compact records instead of slot strings, same trace and arrivals
-    lat_bc, mk_bc, _, _ = run_trace(S, pool, reqs, arrivals, True, budget, compact=True)
-    lat_pc, mk_pc, _, _ = run_trace(S, pool, reqs, arrivals, False, budget, compact=True)
-    sat_bc = run_trace(S, pool, reqs, None, True, budget, compact=True)
-    sat_pc = run_trace(S, pool, reqs, None, False, budget, compact=True)
-    launches = S.kernel_launches() - launches0
+    with torch.cuda.graph(graph, stream=stream):
+        step_batched()
+    per_step_launches = S.kernel_launches() - launches0
 
-    def pct(v, p):
-        return float(np.percentile(np.asarray(v), p))
+    def step_graph():
+        with torch.cuda.stream(stream):
+            graph.replay()
 
-    h2d = sum(r["h2d"] for r in reqs)
-    d2h = sum(r["d2h"] for r in reqs)
+    step_graph()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(clk_device) if clk_device is not None else None
+    if clk:
+        clk.__enter__()
+    try:
+        ms_step = timed(stream, step_graph, args.steps, world, dist, dev)
+    finally:
+        if clk:
+            clk.__exit__(None, None, None)
+    torch.cuda.synchronize()
+    if int(status.item()) != 0:
+        raise SystemExit(f"kernel status {int(status.item())}")
+
+    for _ in range(2):
+        step_plain()
+    stream.synchronize()
+    ms_plain = timed(stream, step_plain, args.steps, world, dist, dev)
+
+    # end to end, batched
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
+    s_in, s_run, s_out = (torch.cuda.Stream(device=dev) for _ in range(3))
+    groups = call_groups(dcs, args.calls_per_group)
+    gscr = max(S.multi_scratch_bytes(dcs[i].sbs[c0:c1]) for i, c0, c1 in groups)
+    scratch_g = torch.empty(gscr, dtype=torch.uint8, device=dev)
+
+    def e2e_batched():
+        for i, c0, c1 in groups:
+            d = dcs[i]
+            with torch.cuda.stream(s_in):
+                d.copy_in(c0, c1)
+            s_run.wait_stream(s_in)
+            S.align_multi_device(d.sbs[c0:c1], d.srs[c0:c1], status.data_ptr(),
+                                 scratch_g.data_ptr(), gscr, s_run.cuda_stream)
+            s_out.wait_stream(s_run)
+            with torch.cuda.stream(s_out):
+                d.copy_out(c0, c1)
+
+    def timed_streams(fn, steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s_in)
+        for _ in range(steps):
+            fn()
+        s_out.wait_stream(s_in)
+        s_out.wait_stream(s_run)
+        e1.record(s_out)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps
+
+    e2e_batched()
+    torch.cuda.synchronize()
+    e_ms = timed_streams(e2e_batched, e2e_steps)
+    if int(status.item()) != 0:
+        raise SystemExit(f"kernel status {int(status.item())} (e2e)")
+
+    # end to end, plain: the reference's structure -- a thread per strand,
+    # each submitting its calls one at a time through saru_align_host
+    strands = {}
+    for i, d in enumerate(dcs):
+        for c in range(d.cs.ncalls):
+            strands.setdefault(int(d.cs.strand[c]), []).append((i, c))
+    views = {(i, c): dcs[i].host_call(c) for i, d in enumerate(dcs) for c in range(d.cs.ncalls)}
+
+    def plain_strand(lane, items, err):
+        try:
+            for key in items:
+                b, out = views[key]
+                S.align_host(b, lane=lane, out=out)
+        except Exception as ex:  # surfaced after the join
+            err.append(ex)
+
+    def e2e_plain():
+        err = []
+        th = [threading.Thread(target=plain_strand, args=(0 if st == 0 else 1, items, err))
+              for st, items in strands.items()]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        if err:
+            raise err[0]
+
+    e2e_plain()
+    torch.cuda.synchronize()
+    t_p = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_plain()
+    torch.cuda.synchronize()
+    p_ms = (time.perf_counter() - t_p) * 1e3 / e2e_steps
+    if world > 1:
+        t = torch.tensor([p_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        p_ms = float(t.item())
+
+    legacy = None
+    if legacy_steps > 0:
+        # lines the reference prints: one per candidate with score <= k
+        expect = sum(int((d.h_out[0].numpy() <= d.cs.k).sum()) for d in dcs)
+        legacy = legacy_leg(S, css, strands, legacy_steps, world, dist, dev)
+        if legacy["lines_per_step"] != expect:
+            raise SystemExit(f"drop-in entry printed {legacy['lines_per_step']} lines, "
+                             f"expected {expect}")
+    out = dict(n_cand=n_cand, ncalls=ncalls, ms_step=ms_step, per_step_launches=per_step_launches,
+               ms_plain=ms_plain, e_ms=e_ms, p_ms=p_ms, e2e_steps=e2e_steps, legacy=legacy,
+               tuning=tuning, groups=len(groups), clocks=clk.summary() if clk else None,
+               h2d=sum(d.bytes_in() for d in dcs), d2h=sum(d.bytes_out() for d in dcs))
+    del graph
+    return out
+
+
+def batched_plain(r: dict, world: int) -> dict:
+    """The batched-vs-plain part of a line from measure_calls' result."""
+    n = r["n_cand"]
+    return {
+        "plain": {
+            "kernel": {"value": world * n / (r["ms_plain"] * 1e-3), "ms_per_step": r["ms_plain"],
+                       "launches_per_step": r["ncalls"],
+                       "what": "one saru_align_device launch per reference call, in call order"},
+            "e2e": {"value": world * n / (r["p_ms"] * 1e-3), "ms_per_step": r["p_ms"],
+                    "what": "the reference's structure: a thread per strand, each submitting its "
+                            "calls one at a time through saru_align_host (synchronous copies "
+                            "in, kernel, copies out), pinned host buffers, host clock"}},
+        "batched_over_plain": {"kernel": r["ms_plain"] / r["ms_step"], "e2e": r["p_ms"] / r["e_ms"]},
+    }
+
+
+def run_aligner(args, cfg: dict, rank: int, world: int, local: int) -> None:
+    import torch
+    import torch.distributed as dist
+    import saruman_b200 as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    S.load()
+    winfo = {}
+    t_build = time.perf_counter()
+    css = build_callsets(cfg, rank, info=winfo)
+    t_build = time.perf_counter() - t_build
+    int_peak = S.int32_issue_peak() if rank == 0 else None
+    r = measure_calls(S, css, args, dev, world, dist, tune=not args.no_tune,
+                      legacy_steps=args.legacy_steps, clk_device=local)
+    n_cand, ms_step = r["n_cand"], r["ms_step"]
+    launches = r["per_step_launches"] * args.steps
+    value = world * n_cand / (ms_step * 1e-3)
+    e2e_value = world * n_cand / (r["e_ms"] * 1e-3)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    # ---- mixed read lengths (a reduced C3) and serving (a reduced C5) -------
+    mixed = serve = None
+    if world == 1 and args.config == "c2" and args.mixed_reads > 0:
+        mcfg = dict(CONFIGS["c3"], reads=args.mixed_reads)
+        mcss = build_callsets(mcfg, 0)
+        mr = measure_calls(S, mcss, args, dev, 1, dist, tune=not args.no_tune)
+        mixed = {"workload": CONFIGS["c3"]["workload"] + f" (reduced to {args.mixed_reads} reads)",
+                 "candidates_per_step": mr["n_cand"], "calls_per_step": mr["ncalls"],
+                 "read_lengths": [cs.m for cs in mcss], "k": [cs.k for cs in mcss],
+                 "value": mr["n_cand"] / (mr["ms_step"] * 1e-3), "ms_per_step": mr["ms_step"],
+                 "launches_per_step": mr["per_step_launches"],
+                 "e2e": {"value": mr["n_cand"] / (mr["e_ms"] * 1e-3), "ms_per_step": mr["e_ms"]},
+                 "tuning": mr["tuning"]}
+        mixed.update(batched_plain(mr, 1))
+        del mcss
+    if world == 1 and args.config == "c2" and args.serve_requests > 0:
+        serve = serving(S, CONFIGS["c5"], args.serve_requests)
+        serve["workload"] = CONFIGS["c5"]["workload"] + \
+            f" (reduced to {args.serve_requests} requests)"
+
+    # ---- roofline --------------------------------------------------------
+    peaks = measured_peaks()
+    cells = sum(band_cells(cs) for cs in css)
+    achieved_ops = 6 * cells / (ms_step * 1e-3)
+    abytes = sum(algorithmic_bytes(cs) for cs in css)
+    prof = profile_traffic() if args.config == "c2" else None
+    traffic = None
+    if prof and prof.get("dram_bytes_per_candidate"):
+        traffic = prof["dram_bytes_per_candidate"] * n_cand
+    roofline = {
+        "bound": "int32",
+        "achieved": achieved_ops / 1e12,
+        "peak": int_peak / 1e12 if int_peak and int_peak > 0 else None,
+        "unit": "Tops/s", "frac": (achieved_ops / int_peak) if int_peak and int_peak > 0 else None,
+        "traffic": traffic,
+        "traffic_source": "profiles/band_kernel_c2.json (ncu dram bytes per candidate, small case, "
+                          "scaled by candidates)" if traffic else None,
+        "peak_source": "measured live by saru_int32_issue_probe on this GPU",
+        "ops_per_candidate_definition": "band cells x 6 (m*(2k+1) or m*(4k+1) cells)",
+        "hbm": {"achieved_gbs": abytes / (ms_step * 1e-3) / 1e9,
+                "peak_gbs": peaks.get("hbm_gbs"),
+                "frac": abytes / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                "algorithmic_bytes_per_step": abytes,
+                "peak_source": "MEASURED_PEAKS.json" if not peaks.get("fallback") else "fallback"},
+    }
+    cpu = None
+    if world == 1:
+        cr = cpu_reference_rate(all_calls(css), seconds=args.cpu_seconds)
+        if cr.get("value") is None:
+            cpu = {"value": None, "unavailable": cr.get("unavailable")}
+        else:
+            cpu = {"value": cr["value"], "unit": "alignments/s", "cores": cr["cores"],
+                   "kind": "reference",
+                   "sample": f"{cr['candidates']} candidates: consecutive pieces of the "
+                             "workload's calls, the reference's own kernel code compiled for "
+                             f"the host, {args.cpu_seconds:.0f} s"}
+    bins = winfo.get("bins", [])
+    filt_ms = sum(b["filter_ms"] for b in bins)
+    filt_reads = sum(2 * b["reads"] for b in bins)
     line = {
-        "metric": "alignments/s", "value": n_cand / sat_b[1], "unit": "alignments/s",
-        "n_gpus": 1, "steps": 1, "warmup": len(warm), "ms_per_step": 1000 * sat_b[1],
+        "metric": "alignments/s", "value": value, "unit": "alignments/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
         "data": "synthetic",
-        "config": {"workload": cfg["workload"], "requests": nreq, "candidates": n_cand,
-                   "genome": "resident on the device (saru_server_set_genome); requests carry "
-                             "reads and candidate (read, position, flag, window end) arrays",
-                   "reads": int(sizes.sum()), "device_budget_bytes": budget,
-                   "offered_load": {"requests_per_s": lam,
-                                    "alignments_per_s": lam * mean_cand,
-                                    "fraction_of_plain_capacity": cfg["load"]},
-                   "step": "the whole trace, submitted at once (saturation)",
-                   "tuning": tuning or "default shapes",
-                   "timing": "host steady clock, arrival (or submit) to results in pinned host "
-                             "memory", "l2": "inputs > L2"},
-        "e2e": {"value": n_cand / sat_b[1], "unit": "alignments/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "latency_ms": {"p50": pct(lat_b, 50), "p99": pct(lat_b, 99), "max": max(lat_b),
-                       "throughput": n_cand / mk_b, "groups": groups_b,
-                       "launches": launches_b},
-        "plain": {"value": n_cand / sat_p[1], "latency_ms": {
-            "p50": pct(lat_p, 50), "p99": pct(lat_p, 99), "max": max(lat_p),
-            "throughput": n_cand / mk_p, "launches": launches_p},
-            "what": "one request at a time, one launch per length bin, no copy/compute overlap"},
-        "batched_over_plain": sat_p[1] / sat_b[1],
-        "p99_plain_over_batched": pct(lat_p, 99) / pct(lat_b, 99),
-        "compact": {
-            "what": "the same trace with compact records (saru_request.compact) returned "
-                    "instead of slot strings",
-            "d2h_bytes_per_step": sum(r["d2h_compact"] for r in reqs),
-            "value": n_cand / sat_bc[1], "plain_value": n_cand / sat_pc[1],
-            "batched_over_plain": sat_pc[1] / sat_bc[1],
-            "latency_ms": {"p50": pct(lat_bc, 50), "p99": pct(lat_bc, 99),
-                           "throughput": n_cand / mk_bc},
-            "plain_latency_ms": {"p50": pct(lat_pc, 50), "p99": pct(lat_pc, 99),
-                                 "throughput": n_cand / mk_pc}},
+        "config": {"workload": cfg["workload"], "candidates_per_step": n_cand,
+                   "calls_per_step": r["ncalls"], "reads_per_step": cfg["reads"],
+                   "read_lengths": [cs.m for cs in css], "k": [cs.k for cs in css],
+                   "candidates": "the reference's q-gram filter on all reads, both strands "
+                                 "(the library's device filter); calls cut at the reference's "
+                                 "queue threshold", "bins": bins,
+                   "parallelism": f"replicas x{world}", "l2": "inputs 4+ GB > L2, no flush",
+                   "tuning": r["tuning"] or "default shapes", "build_s": t_build},
+        "gcups_rect": world * sum(rect_cells(cs) for cs in css) / (ms_step * 1e-3) / 1e9,
         "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "launch": "one CUDA graph replay per step "
+                  f"({r['per_step_launches']} kernel launch(es) captured for {r['ncalls']} calls)",
+        "e2e": {"value": e2e_value, "unit": "alignments/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"], "steps": r["e2e_steps"],
+                "what": f"pinned host buffers; {r['groups']} groups of up to "
+                        f"{args.calls_per_group} calls, each copied in, aligned in one batched "
+                        "request (saru_align_multi_device) and copied out, overlapped on three "
+                        "streams; CUDA events"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "filter": {"value": filt_reads / (filt_ms * 1e-3) if filt_ms else None,
+                   "unit": "read-strands/s", "reads": filt_reads // 2, "strands": 2,
+                   "ms": filt_ms, "candidates": n_cand,
+                   "what": "saru_filter_run on every read of the step, both strands: device "
+                           "time incl. read upload, copy-back and call assembly"},
+        "clocks": r["clocks"],
     }
+    line.update(batched_plain(r, world))
+    if r["legacy"]:
+        line["e2e_legacy"] = r["legacy"]
+    if mixed:
+        line["mixed_lengths"] = mixed
+    if serve:
+        line["serving"] = serve
     print(json.dumps(line))
+
+
+def legacy_leg(S, css, strands: dict, steps: int, world: int, dist, dev) -> dict:
+    """cuda_needleman_wunsch per call, as src/hash.c:1094-1108 calls it:
+    from one thread per strand, pageable host arrays, results printed by the
+    library's writer before the call returns (stdout to /dev/null here)."""
+    import ctypes as C
+    import threading
+    lib = S.load()
+    n_ids = max(int(cs.ids.max()) + 1 for cs in css if cs.n)
+    names, head = legacy_names(n_ids)
+    C.c_void_p.in_dll(lib, "read_names").value = head.value
+    C.c_ushort.in_dll(lib, "read_length_value").value = max(cs.m for cs in css)
+    ctl = [(C.c_char * n_ids)(), (C.c_char * n_ids)()]
+    C.c_void_p.in_dll(lib, "forward_output_control").value = C.addressof(ctl[0])
+    C.c_void_p.in_dll(lib, "reverse_output_control").value = C.addressof(ctl[1])
+    P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    calls = {}
+    for st in strands:
+        calls[st] = []
+        for cs in css:
+            for c in range(cs.ncalls):
+                if int(cs.strand[c]) == st:
+                    calls[st].append(cs.call(c))
+    n_cand = sum(b.n for v in calls.values() for b in v)
+
+    def strand(st, bl):
+        for b in bl:
+            lib.cuda_needleman_wunsch(C.c_int(0), C.c_int(1), P(b.genome), P(b.reads),
+                                      P(b.genome_offsets), P(b.read_offsets),
+                                      P(b.edit_offsets), C.c_int(b.n), P(b.ids), P(b.pos),
+                                      P(b.dirs), C.c_int(b.k), C.c_size_t(b.total_genome),
+                                      C.c_size_t(b.n * b.m), C.c_size_t(b.total_edit),
+                                      C.c_int(st))
+
+    def one():
+        th = [threading.Thread(target=strand, args=(st, bl)) for st, bl in calls.items()]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+
+    libc = C.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved_out, saved_err = os.dup(1), os.dup(2)
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    os.dup2(null, 2)  # the per-call banner the reference prints on stderr
+    try:
+        for name in ("forward_alignments_done", "reverse_alignments_done"):
+            C.c_uint.in_dll(lib, name).value = 0
+        one()
+        libc.fflush(None)
+        printed = sum(C.c_uint.in_dll(lib, nm).value for nm in
+                      ("forward_alignments_done", "reverse_alignments_done"))
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            one()
+        libc.fflush(None)
+        ms = (time.perf_counter() - t0) * 1e3 / steps
+    finally:
+        os.dup2(saved_out, 1)
+        os.dup2(saved_err, 2)
+        os.close(null)
+        os.close(saved_out)
+        os.close(saved_err)
+    C.c_void_p.in_dll(lib, "read_names").value = None
+    del names
+    if world > 1:
+        import torch
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return {"value": world * n_cand / (ms * 1e-3), "unit": "alignments/s", "ms_per_step": ms,
+            "steps": steps, "lines_per_step": int(printed),
+            "what": "cuda_needleman_wunsch per reference call from a thread per strand, "
+                    "pageable host arrays, TSV lines written to /dev/null before each call "
+                    "returns; host clock"}
 
 
 def main() -> None:
@@ -645,12 +1049,18 @@ def main() -> None:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--legacy-steps", type=int, default=2,
+                    help="steps of the drop-in entry leg (0: skip)")
+    ap.add_argument("--calls-per-group", type=int, default=12,
+                    help="calls per group of the batched end-to-end leg")
+    ap.add_argument("--mixed-reads", type=int, default=1_000_000,
+                    help="reads of the mixed-length leg of the default line (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=100,
+                    help="requests of the serving leg of the default line (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (no autotuning)")
-    ap.add_argument("--filter-reads", type=int, default=200_000,
-                    help="reads for the device filter leg (0: skip)")
     ap.add_argument("--shape", default=None,
                     help="W,C,B: install this launch shape for every bin instead of tuning")
     ap.add_argument("--requests", type=int, default=None,
@@ -674,307 +1084,7 @@ def main() -> None:
             raise SystemExit("the serving workload runs on one GPU")
         run_serving(args, cfg, rank)
         return
-
-    import torch
-    import torch.distributed as dist
-    import saruman_b200 as S
-
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
-
-    tables = []
-    bs = build_batches(cfg, rank, tables)
-    genome = tables.pop()
-    S.load()
-    dbs = [DeviceBatch(b, dev, S) for b in bs]
-    n_cand = sum(b.n for b in bs)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
-    for d in dbs:
-        d.sr.status = status.data_ptr()
-    stream = torch.cuda.Stream(device=dev)
-    sptr = stream.cuda_stream
-    multi = len(dbs) > 1
-    int_peak = S.int32_issue_peak() if rank == 0 else None
-    # launch shapes first: the scratch sizes depend on them
-    if args.shape:
-        shape = tuple(int(x) for x in args.shape.split(","))
-        for b in bs:
-            S.set_tuning(b.m, b.k, *shape)
-        tuning = {f"{b.m},{b.k}": {"shape": list(shape), "trials": 0} for b in bs}
-    else:
-        tuning = tune_bins(bs, dbs, status) if not args.no_tune else {}
-    status.zero_()
-    if multi:
-        nscr = S.multi_scratch_bytes([d.sb for d in dbs])
-    else:
-        nscr = S.scratch_bytes(bs[0].n, bs[0].m, bs[0].k)
-    scratch = torch.empty(nscr, dtype=torch.uint8, device=dev)
-
-    def step_batched():
-        if multi:
-            S.align_multi_device([d.sb for d in dbs], [d.sr for d in dbs], status.data_ptr(),
-                                 scratch.data_ptr(), nscr, sptr)
-        else:
-            S.align_device(dbs[0].sb, dbs[0].sr, scratch.data_ptr(), nscr, sptr)
-
-    plain_scr = [S.scratch_bytes(d.b.n, d.b.m, d.b.k) for d in dbs] if multi else []
-    scratch_plain = (torch.empty(max(plain_scr), dtype=torch.uint8, device=dev)
-                     if multi else None)
-
-    def step_plain():  # one launch per length bin, in order
-        for d, n1 in zip(dbs, plain_scr):
-            S.align_device(d.sb, d.sr, scratch_plain.data_ptr(), n1, sptr)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step_batched()
-    stream.synchronize()
-    if int(status.item()) != 0:
-        raise SystemExit(f"kernel status {int(status.item())}")
-
-    # ---- device-resident timing: the step captured once in a CUDA graph --
-    graph = torch.cuda.CUDAGraph()
-    launches0 = S.kernel_launches()
-    with torch.cuda.graph(graph, stream=stream):
-        step_batched()
-    per_step_launches = S.kernel_launches() - launches0
-
-    def step_graph():
-        with torch.cuda.stream(stream):
-            graph.replay()
-
-    step_graph()
-    stream.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        ms_step = timed(stream, step_graph, args.steps, world, dist, dev)
-    torch.cuda.synchronize()
-    if int(status.item()) != 0:
-        raise SystemExit(f"kernel status {int(status.item())}")
-    launches = per_step_launches * args.steps
-    value = world * n_cand / (ms_step * 1e-3)
-    plain = None
-    if multi:
-        for _ in range(2):
-            step_plain()
-        stream.synchronize()
-        ms_plain = timed(stream, step_plain, args.steps, world, dist, dev)
-        plain = {"value": world * n_cand / (ms_plain * 1e-3), "ms_per_step": ms_plain,
-                 "launches_per_step": len(dbs),
-                 "what": "one launch per length bin (saru_align_device), bins in sequence"}
-
-    # ---- end to end through the public API, host buffers ----------------
-    e2e_steps = args.e2e_steps or max(1, min(args.steps, 5))
-
-    if multi:
-        e2e_what = ("pinned host buffers copied in and out around the batched launch "
-                    "(saru_align_multi_device) on one stream")
-
-        def e2e_step():
-            with torch.cuda.stream(stream):
-                for d in dbs:
-                    d.h2d()
-                step_batched()
-                for d in dbs:
-                    d.d2h()
-
-        e2e_step()
-        stream.synchronize()
-        if world > 1:
-            dist.barrier()
-        e_ms = timed(stream, e2e_step, e2e_steps, world, dist, dev)
-    else:
-        # the library's host entry point (saru_align_host) on pinned host
-        # buffers: it validates the call on the host, copies it in, aligns
-        # and copies the results out, in overlapped slices; synchronous, so
-        # it is timed by the host clock between device synchronisations
-        e2e_what = ("saru_align_host on pinned host buffers (host validation, copies in, "
-                    "kernels and copies out overlapped in slices), host clock")
-        d0 = dbs[0]
-        hb = dataclasses.replace(bs[0], genome=d0.h_in[0][1].numpy(), reads=d0.h_in[1][1].numpy(),
-                                 genome_offsets=d0.h_in[2][1].numpy(),
-                                 read_offsets=d0.h_in[3][1].numpy(), dirs=d0.h_in[4][1].numpy())
-        hout = S.AlignResult(d0.h_out[0][0].numpy(), d0.h_out[1][0].numpy(),
-                             d0.h_out[2][0].numpy())
-
-        def e2e_step():
-            S.align_host(hb, out=hout)
-
-        e2e_step()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        t_e = time.perf_counter()
-        for _ in range(e2e_steps):
-            e2e_step()
-        torch.cuda.synchronize()
-        e_ms = (time.perf_counter() - t_e) * 1e3 / e2e_steps
-        if world > 1:
-            t = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-    e2e_value = world * n_cand / (e_ms * 1e-3)
-
-    # ---- compact result records instead of slot strings (single-bin) -----
-    compact = None
-    if not multi:
-        d0, b0 = dbs[0], bs[0]
-        rbytes = S.compact_record_bytes(b0.m, b0.k)
-        rec = torch.empty(b0.n * rbytes, dtype=torch.uint8, device=dev)
-        h_rec = torch.empty(b0.n * rbytes, dtype=torch.uint8).pin_memory()
-
-        def step_compact():
-            S.align_device_compact(d0.sb, d0.scores.data_ptr(), rec.data_ptr(), rbytes,
-                                   status.data_ptr(), scratch.data_ptr(), nscr, sptr)
-
-        for _ in range(2):
-            step_compact()
-        stream.synchronize()
-        c_ms = timed(stream, step_compact, args.steps, world, dist, dev)
-
-        # end to end through the host entry point (saru_align_host_compact)
-        # on pinned buffers, sliced and overlapped like saru_align_host
-        c_out = (d0.h_out[0][0].numpy(), h_rec.numpy())
-
-        def e2e_compact():
-            S.align_host_compact(hb, out=c_out)
-
-        e2e_compact()
-        torch.cuda.synchronize()
-        t_c = time.perf_counter()
-        for _ in range(e2e_steps):
-            e2e_compact()
-        torch.cuda.synchronize()
-        ce_ms = (time.perf_counter() - t_c) * 1e3 / e2e_steps
-        if world > 1:
-            t = torch.tensor([ce_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ce_ms = float(t.item())
-        if int(status.item()) != 0:
-            raise SystemExit(f"kernel status {int(status.item())} (compact)")
-        # the reference's TSV lines from the records, on the host cores
-        names = S.name_table([b"read%d" % i for i in range(int(b0.ids.max()) + 1)])
-        t0 = time.perf_counter()
-        tsv, nf, nr = S.format_tsv_compact(b0, d0.h_out[0][0].numpy(), h_rec.numpy(), rbytes,
-                                           names)
-        tsv_s = time.perf_counter() - t0
-        tsv_leg = {"value": n_cand / tsv_s, "unit": "alignments/s", "lines": nf + nr,
-                   "bytes": len(tsv), "seconds": tsv_s, "threads": os.cpu_count(),
-                   "what": "saru_format_tsv_compact on the host cores (host clock): the "
-                           "reference writer's lines straight from the records"}
-        del tsv
-        compact = {"value": world * n_cand / (c_ms * 1e-3), "ms_per_step": c_ms,
-                   "record_bytes": rbytes,
-                   "e2e": {"value": world * n_cand / (ce_ms * 1e-3), "unit": "alignments/s",
-                           "h2d_bytes_per_step": d0.bytes_in(),
-                           "d2h_bytes_per_step": 4 * b0.n + b0.n * rbytes,
-                           "what": "saru_align_host_compact on pinned host buffers, host clock"},
-                   "what": "saru_align_device_compact: 2-bit traceback records per candidate "
-                           "instead of the slot strings; saru_expand_compact rebuilds the "
-                           "slots on the host",
-                   "tsv": tsv_leg}
-
-    # ---- candidate generation on the device (the reference's q-gram filter) --
-    filt = None
-    if not multi and args.filter_reads:
-        b0, seqs = bs[0], tables[0][:args.filter_reads]
-        with S.Filter(genome, b0.m, b0.k) as f:
-            f.run(seqs, 0, 4 * len(seqs) + 1000)  # warm-up: buffers sized for the run
-            runs = [f.run(seqs, dr, 4 * len(seqs) + 1000) for dr in (0, 4)]
-        ms = sum(r.ms for r in runs)
-        filt = {"reads": int(len(seqs)), "strands": 2,
-                "value": 2 * len(seqs) / (ms * 1e-3), "unit": "read-strands/s",
-                "candidates_per_s": sum(len(r.ids) for r in runs) / (ms * 1e-3),
-                "ms": ms, "candidates": sum(len(r.ids) for r in runs),
-                "perfect_hits": sum(len(r.perfect_ids) for r in runs),
-                "what": "saru_filter_run: the reference's q-gram pair filter, a warp per read, "
-                        "on the first reads of the workload, both strands, calls assembled; "
-                        "device time incl. read upload and copy-back of the kept positions"}
-
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-
-    # ---- roofline --------------------------------------------------------
-    peaks = measured_peaks()
-    cells = sum(band_cells(b) for b in bs)
-    achieved_ops = 6 * cells / (ms_step * 1e-3)
-    abytes = sum(algorithmic_bytes(b) for b in bs)
-    prof = profile_traffic() if args.config == "c2" else None
-    traffic = None
-    if prof and prof.get("dram_bytes_per_candidate"):
-        traffic = prof["dram_bytes_per_candidate"] * n_cand
-    roofline = {
-        "bound": "int32",
-        "achieved": achieved_ops / 1e12, "peak": int_peak / 1e12 if int_peak and int_peak > 0 else None,
-        "unit": "Tops/s", "frac": (achieved_ops / int_peak) if int_peak and int_peak > 0 else None,
-        "traffic": traffic,
-        "traffic_source": "profiles/band_kernel_c2.json (ncu dram bytes per candidate, small case, "
-                          "scaled by candidates)" if traffic else None,
-        "peak_source": "measured live by saru_int32_issue_probe on this GPU",
-        "ops_per_candidate_definition": "band cells x 6 (m*(2k+1) or m*(4k+1) cells)",
-        "hbm": {"achieved_gbs": abytes / (ms_step * 1e-3) / 1e9,
-                "peak_gbs": peaks.get("hbm_gbs"),
-                "frac": abytes / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"],
-                "algorithmic_bytes_per_step": abytes,
-                "peak_source": "MEASURED_PEAKS.json" if not peaks.get("fallback") else "fallback"},
-    }
-    cpu = None
-    if world == 1:
-        cand, secs, cores = 0, 0.0, None
-        for b in bs:
-            r = cpu_reference_rate(b, seconds=args.cpu_seconds / len(bs))
-            if r.get("value") is None:
-                cpu = {"value": None, "unavailable": r.get("unavailable")}
-                break
-            cand += r["candidates"]
-            secs += r["seconds"]
-            cores = r["cores"]
-        if cpu is None:
-            cpu = {"value": cand / secs, "unit": "alignments/s", "cores": cores,
-                   "kind": "reference",
-                   "sample": f"{cand} consecutive candidates of the workload ({len(bs)} bins), "
-                             "the reference's own kernel code compiled for the host"}
-    line = {
-        "metric": "alignments/s", "value": value, "unit": "alignments/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32",
-        "data": "synthetic",
-        "config": {"workload": cfg["workload"], "candidates_per_step": n_cand,
-                   "reads_per_step": cfg["reads"], "read_lengths": [b.m for b in bs],
-                   "k": [b.k for b in bs], "parallelism": f"replicas x{world}",
-                   "l2": "inputs 4+ GB > L2, no flush",
-                   "tuning": tuning or "default shapes"},
-        "gcups_rect": world * sum(rect_cells(b) for b in bs) / (ms_step * 1e-3) / 1e9,
-        "gpu_launches": int(launches),
-        "launch": "one CUDA graph replay per step "
-                  f"({per_step_launches} kernel launch(es) captured)",
-        "e2e": {"value": e2e_value, "unit": "alignments/s",
-                "h2d_bytes_per_step": sum(d.bytes_in() for d in dbs),
-                "d2h_bytes_per_step": sum(d.bytes_out() for d in dbs), "steps": e2e_steps,
-                "what": e2e_what},
-        "roofline": roofline,
-        "cpu_baseline": cpu,
-        "clocks": clk.summary(),
-    }
-    if plain:
-        line["plain"] = plain
-        line["batched_over_plain"] = plain["ms_per_step"] / ms_step
-    if filt:
-        line["filter"] = filt
-    if compact:
-        compact["roofline_frac"] = (6 * cells / (compact["ms_per_step"] * 1e-3) / int_peak
-                                    if int_peak and int_peak > 0 else None)
-        line["compact"] = compact
-    print(json.dumps(line))
+    run_aligner(args, cfg, rank, world, local)
 
 
 if __name__ == "__main__":

@@ -175,15 +175,20 @@ int saru_align_device(const saru_batch *batch, saru_result *result, void *scratc
  * reference.  Same batch, result and stream arguments and the same outputs
  * as saru_align_device; the banded kernel's scratch comes from a device
  * array inside the library of SARU_STATIC_SCRATCH_BYTES (32 MiB), present on
- * every GPU that loads the library until the process exits.  Fewer thread
- * blocks run when the planes of a full grid do not fit in it; a batch that
- * cannot get even one block, or is outside the banded kernel's domain, is
- * refused with SARU_E_INVALID and a message.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress, with that
- * device current), so make that first call before any stream capture.  All
- * calls share the array: each call clears the work counter at its start
- * and writes every other byte it reads, so nothing from an earlier call is
- * used, but calls that overlap on the GPU race. */
+ * every GPU that loads the library until the process exits.  It runs the
+ * kernel's per-tile form (half the plane slots of the queued form the other
+ * entry points run).  Fewer thread blocks run when the planes of a full
+ * grid do not fit in the array.  A batch outside the banded kernel's domain
+ * is refused with SARU_E_INVALID and a message; so would be one that cannot
+ * get a single block, which with reads of at most 512 bases (about 0.5 MB
+ * of planes a block) cannot happen at this array size.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, with
+ * that device current), so make that first call before any stream capture;
+ * the address is kept for the life of the process, so a cudaDeviceReset
+ * after that first call is not supported.  All calls share the array: each
+ * call clears the work counter at its start and writes every other byte it
+ * reads, so nothing from an earlier call is used, but calls that overlap on
+ * the GPU race. */
 #define SARU_STATIC_SCRATCH_BYTES (32u << 20)
 int saru_align_device_static(const saru_batch *batch, saru_result *result, void *stream);
 
@@ -403,6 +408,52 @@ int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket)
  * ended with.  A ticket is forgotten once a wait returns anything else
  * than SARU_E_TIMEOUT. */
 int saru_server_wait(saru_server *s, int64_t ticket, int32_t timeout_ms, saru_request_stats *stats);
+/* Requests of reads only: the server does the reference's whole per-strand
+ * daemon work (src/hash.c:295-470, 841-851, 898-1111) for them.  For each
+ * read set it runs the q-gram pair filter against the resident genome
+ * (saru_server_set_genome) on both strands, cuts the calls at the queue
+ * threshold, gathers every call's windows and reads on the device, aligns
+ * and keeps the results for saru_server_read_results.  A filter thread
+ * works on the next request while earlier ones align, as the reference's
+ * strand daemons filter while the GPU aligns.  Not in the reference's ABI
+ * (its filter is host code calling cuda_needleman_wunsch per call). */
+typedef struct {
+  const char *reads;     /* nreads x read_length bytes, as sequenced; read ids 0..nreads-1;
+                            must stay valid until the request is waited for */
+  int32_t nreads, read_length, k;
+  uint32_t chunk_value;  /* the queue threshold (-s), candidates per call; 0: one that keeps
+                            each call under 2^31 matrix cells */
+} saru_read_set;
+/* Queues a reads-only request (1..16 sets, compact: records instead of slot
+ * strings).  Needs saru_server_set_genome first. */
+int saru_server_submit_reads(saru_server *s, const saru_read_set *sets, int32_t nsets,
+                             int32_t compact, int64_t *ticket);
+/* The results of set `set` of a reads-only request, after saru_server_wait
+ * returned SARU_OK for it: pointers into the server's memory, valid until
+ * saru_server_release.  Call c (strand call_strand[c], 0 or 4) holds
+ * candidates call_begin[c] .. call_begin[c+1]; its slot strings start at
+ * slot_begin[c] of read_aln / genome_aln (slot mode), its records at
+ * candidate call_begin[c] of records (compact mode).  Perfect hits are the
+ * filter's own output lines (never aligned). */
+typedef struct {
+  int32_t ncalls, nperfect;
+  int64_t n;                   /* candidates */
+  const int64_t *call_begin;   /* ncalls + 1 */
+  const int64_t *slot_begin;   /* ncalls + 1 */
+  const int8_t *call_strand;   /* ncalls */
+  const int32_t *ids, *pos;    /* n: read id, window start */
+  const int8_t *dirs;          /* n */
+  const int32_t *scores;       /* n */
+  const char *read_aln, *genome_aln;  /* slot mode, slot_begin[ncalls] bytes each */
+  const uint8_t *records;      /* compact mode, n x record_bytes */
+  int64_t record_bytes;
+  const int32_t *perfect_ids, *perfect_pos;  /* nperfect; pos = 0-based start */
+  const int8_t *perfect_strand;              /* nperfect */
+} saru_read_results;
+int saru_server_read_results(saru_server *s, int64_t ticket, int32_t set, saru_read_results *out);
+/* Frees a waited-for reads-only request's results. */
+void saru_server_release(saru_server *s, int64_t ticket);
+
 /* Launch groups formed and kernel launches enqueued so far. */
 void saru_server_counters(saru_server *s, int64_t *groups, int64_t *launches);
 /* Finishes queued requests, then frees everything. */
@@ -415,6 +466,19 @@ int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
                         const int32_t *read_ids, const int32_t *genome_pos, int32_t read_length,
                         const char *names, int32_t name_stride, int32_t n_names, char *out,
                         int64_t cap, int32_t *done_fwd, int32_t *done_rev);
+
+/* SAM records for the reference writer's TSV lines (tsv: len bytes, lines
+ * separated by '\n'; blank lines skipped): a header (@HD, @SQ with rname and
+ * rlen, @PG), then per line QNAME (the name up to its first blank), FLAG (16
+ * for "<<", 0 for ">>", 4 for an unmapped line), RNAME, POS (the printed
+ * 1-based start), MAPQ 255, CIGAR (M, I for '_' in the genome string, D for
+ * '_' in the read string), '*', 0, 0, SEQ (the read string without gaps),
+ * '*', NM:i:<edit distance>.  Writes up to cap bytes to out and returns the
+ * bytes the text needs, or -1 for a line of fewer than 7 tab-separated
+ * fields.  The reference leaves SAM to an external script (README.md:32);
+ * no counterpart in its code. */
+int64_t saru_tsv_to_sam(const char *tsv, int64_t len, const char *rname, int64_t rlen,
+                        char *out, int64_t cap);
 
 /* Message of the last error on the calling thread ("" if none). */
 const char *saru_last_error(void);

@@ -443,3 +443,126 @@ long saru_oracle_write_tsv(const int *scores, const char *read_aln, const char *
   if (done_rev) *done_rev = dr;
   return s.len;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Whole-call check in sub-calls (saru_oracle_check).                        */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int match, mis, k;
+  const char *g, *r;
+  const long *go, *ro;
+  long n;
+  const signed char *dirs;
+  const int *scores;
+  const char *ra, *ga;
+  long chunk, nchunks;
+  long *next;
+  pthread_mutex_t *mu;
+  long bad, first_bad;
+  int status;
+} check_t;
+
+static void *check_worker(void *arg) {
+  check_t *w = (check_t *)arg;
+  const long cap = w->chunk + 1;
+  int *go = (int *)malloc(sizeof(int) * (size_t)cap);
+  int *ro = (int *)malloc(sizeof(int) * (size_t)cap);
+  int *eo = (int *)malloc(sizeof(int) * (size_t)cap);
+  int *sc = (int *)malloc(sizeof(int) * (size_t)cap);
+  char *ra = NULL, *ga = NULL;
+  long slots_cap = 0;
+  cache_t c;
+  cache_init(&c);
+  for (;;) {
+    pthread_mutex_lock(w->mu);
+    long ci = (*w->next)++;
+    pthread_mutex_unlock(w->mu);
+    if (ci >= w->nchunks) break;
+    const long s = ci * w->chunk, e = s + w->chunk < w->n ? s + w->chunk : w->n;
+    const long a = s > 0 ? s - 1 : 0; /* the lead: the candidate before the chunk */
+    const long g0 = a ? w->go[a - 1] : 0, r0 = a ? w->ro[a - 1] : 0;
+    const long nn = e - a;
+    long esum = 0, bad_input = 0;
+    for (long i = 0; i < nn; ++i) {
+      const long t = a + i;
+      go[i] = (int)(w->go[t] - g0);
+      ro[i] = (int)(w->ro[t] - r0);
+      eo[i] = (int)esum;
+      const long m = w->ro[t] - (t ? w->ro[t - 1] : 0), L = w->go[t] - (t ? w->go[t - 1] : 0);
+      if (m <= 3 * w->k || m > 32000 || L <= 0 || L > 32000) bad_input = 1;
+      esum += (m + 1) * (L + 1);
+    }
+    if (bad_input || esum > INT_MAX) {
+      w->status |= SARU_ORACLE_BAD_INPUT;
+      continue;
+    }
+    const long slots = go[nn - 1] + (long)w->k * nn;
+    if (slots > slots_cap) {
+      free(ra);
+      free(ga);
+      ra = (char *)malloc((size_t)slots);
+      ga = (char *)malloc((size_t)slots);
+      slots_cap = slots;
+    }
+    memset(ra, 0, (size_t)slots);
+    memset(ga, 0, (size_t)slots);
+    batch_t b = {w->match, w->mis, w->k, (int)nn, w->g + g0, w->r + r0, go[nn - 1], ro[nn - 1],
+                 go, ro, eo, w->dirs + a, slots, esum, sc, ra, ga};
+    for (int i = 0; i < NCACHE; ++i) c.t[i] = -1; /* matrices of the previous chunk */
+    for (long i = s - a; i < nn; ++i) w->status |= align_one(&b, &c, i);
+    for (long i = s - a; i < nn; ++i) {
+      const long t = a + i;
+      const long L = go[i] - (i ? go[i - 1] : 0);
+      const long sub = (i ? go[i - 1] : 0) + (long)w->k * i;
+      const long full = (t ? w->go[t - 1] : 0) + (long)w->k * t;
+      const int x = sc[i] < w->k + 1 ? sc[i] : w->k + 1;
+      const int y = w->scores[t] < w->k + 1 ? w->scores[t] : w->k + 1;
+      if (x != y || memcmp(ra + sub, w->ra + full, (size_t)(L + w->k)) != 0 ||
+          memcmp(ga + sub, w->ga + full, (size_t)(L + w->k)) != 0) {
+        if (w->bad == 0 || t < w->first_bad) w->first_bad = t;
+        w->bad++;
+      }
+    }
+  }
+  cache_free(&c);
+  free(go);
+  free(ro);
+  free(eo);
+  free(sc);
+  free(ra);
+  free(ga);
+  return NULL;
+}
+
+long saru_oracle_check(int match, int mismatch, const char *genome, const char *reads,
+                       const long *genome_offsets, const long *read_offsets, long n,
+                       const signed char *dirs, int k, int nthreads, const int *scores,
+                       const char *read_aln, const char *genome_aln, long *first_bad,
+                       int *status) {
+  *first_bad = -1;
+  *status = 0;
+  if (n <= 0) return 0;
+  if (nthreads < 1) nthreads = 1;
+  long next = 0;
+  pthread_mutex_t mu = PTHREAD_MUTEX_INITIALIZER;
+  const long chunk = 2048;
+  const long nchunks = (n + chunk - 1) / chunk;
+  check_t *ws = (check_t *)calloc((size_t)nthreads, sizeof(check_t));
+  pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
+  for (int i = 0; i < nthreads; ++i) {
+    ws[i] = (check_t){match, mismatch, k, genome, reads, genome_offsets, read_offsets, n, dirs,
+                      scores, read_aln, genome_aln, chunk, nchunks, &next, &mu, 0, -1, 0};
+    pthread_create(&th[i], NULL, check_worker, &ws[i]);
+  }
+  long bad = 0;
+  for (int i = 0; i < nthreads; ++i) {
+    pthread_join(th[i], NULL);
+    bad += ws[i].bad;
+    *status |= ws[i].status;
+    if (ws[i].bad && (*first_bad < 0 || ws[i].first_bad < *first_bad)) *first_bad = ws[i].first_bad;
+  }
+  free(ws);
+  free(th);
+  return bad;
+}

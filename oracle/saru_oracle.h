@@ -46,6 +46,23 @@ long saru_oracle_write_tsv(const int *scores, const char *read_aln, const char *
                            int read_length, const char *names, int name_stride, int n_names,
                            char *out, long cap, int *status, int *done_fwd, int *done_rev);
 
+/* Checks another implementation's outputs for one whole call (candidate 0
+ * opens it) of any size against this restatement.  The call is aligned in
+ * sub-calls of a few thousand candidates, each led by the candidate before
+ * it: a traceback only reads the previous matrix's last row when m > 3k,
+ * so every candidate after the lead gets the whole call's bytes (the lead's
+ * own result is discarded).  Compares min(score, k + 1) and the candidate's
+ * L + k slot bytes of both strings.  Offsets are int64 so a call may hold
+ * more than 2^31 window bytes.  Returns the number of candidates that
+ * differ; *first_bad gets the lowest such index (-1 if none) and *status
+ * the OR of the oracle's status bits (SARU_ORACLE_BAD_INPUT if some
+ * candidate has m <= 3k, where the lead would not suffice). */
+long saru_oracle_check(int match, int mismatch, const char *genome, const char *reads,
+                       const long *genome_offsets, const long *read_offsets, long n,
+                       const signed char *dirs, int k, int nthreads, const int *scores,
+                       const char *read_aln, const char *genome_aln, long *first_bad,
+                       int *status);
+
 #ifdef __cplusplus
 }
 #endif

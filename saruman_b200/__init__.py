@@ -42,7 +42,8 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_filter_last_ms", "saru_filter_genome", "saru_filter_destroy",
                  "saru_filter_set_chunk", "saru_align_host_compact",
                  "saru_reads_open", "saru_reads_next", "saru_reads_close", "saru_genome_open",
-                 "saru_genome_next", "saru_genome_close")
+                 "saru_genome_next", "saru_genome_close", "saru_server_submit_reads",
+                 "saru_server_read_results", "saru_server_release", "saru_tsv_to_sam")
 ABI_DATA = ("alignment_time",)
 
 
@@ -99,6 +100,21 @@ class RequestStats(C.Structure):
 _lib = None
 
 
+class SaruReadSet(C.Structure):
+    _fields_ = [("reads", C.c_void_p), ("nreads", C.c_int32), ("read_length", C.c_int32),
+                ("k", C.c_int32), ("chunk_value", C.c_uint32)]
+
+
+class SaruReadResults(C.Structure):
+    _fields_ = [("ncalls", C.c_int32), ("nperfect", C.c_int32), ("n", C.c_int64),
+                ("call_begin", C.c_void_p), ("slot_begin", C.c_void_p),
+                ("call_strand", C.c_void_p), ("ids", C.c_void_p), ("pos", C.c_void_p),
+                ("dirs", C.c_void_p), ("scores", C.c_void_p), ("read_aln", C.c_void_p),
+                ("genome_aln", C.c_void_p), ("records", C.c_void_p),
+                ("record_bytes", C.c_int64), ("perfect_ids", C.c_void_p),
+                ("perfect_pos", C.c_void_p), ("perfect_strand", C.c_void_p)]
+
+
 def load(path: str | Path | None = None):
     """Loads libsaruman_b200.so (in-tree).  Raises if it is not built."""
     global _lib
@@ -141,6 +157,14 @@ def load(path: str | Path | None = None):
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.POINTER(SaruBatch), C.c_void_p]
     lib.saru_server_destroy.argtypes = [C.c_void_p]
+    lib.saru_server_submit_reads.restype = C.c_int
+    lib.saru_server_submit_reads.argtypes = [C.c_void_p, C.POINTER(SaruReadSet), C.c_int32,
+                                             C.c_int32, C.POINTER(C.c_int64)]
+    lib.saru_server_read_results.restype = C.c_int
+    lib.saru_server_read_results.argtypes = [C.c_void_p, C.c_int64, C.c_int32,
+                                             C.POINTER(SaruReadResults)]
+    lib.saru_server_release.restype = None
+    lib.saru_server_release.argtypes = [C.c_void_p, C.c_int64]
     lib.saru_tuning_set.restype = C.c_int
     lib.saru_tuning_set.argtypes = [C.c_int32, C.c_int32, C.POINTER(SaruTuning)]
     lib.saru_tuning_get.restype = C.c_int
@@ -455,6 +479,7 @@ class Server:
         if not self._h:
             raise SaruError(SARU_E_CUDA, last_error())
         self._live: dict[int, HostRequest] = {}
+        self._keep: dict[int, tuple] = {}  # reads-only requests' read arrays
 
     def set_genome(self, genome: np.ndarray) -> None:
         g = np.ascontiguousarray(genome, np.uint8)
@@ -478,6 +503,70 @@ class Server:
             raise TimeoutError(f"request {ticket} not done after {timeout_ms} ms")
         self._live.pop(ticket, None)
         return rc, st
+
+    def submit_reads(self, sets: list, compact: bool = False) -> int:
+        """Queues a reads-only request: `sets` = [(reads (n, m) uint8 as
+        sequenced, k, chunk_value or 0), ...].  The read arrays must stay
+        alive until the request is waited for (they are kept on the ticket)."""
+        arr = (SaruReadSet * len(sets))()
+        keep = []
+        for i, (reads, k, cv) in enumerate(sets):
+            r = np.ascontiguousarray(reads, np.uint8)
+            keep.append(r)
+            arr[i] = SaruReadSet(_p(r) if r.size else 0, r.shape[0], r.shape[1], k, cv)
+        t = C.c_int64()
+        rc = self._lib.saru_server_submit_reads(self._h, arr, len(sets), 1 if compact else 0,
+                                                C.byref(t))
+        if rc != SARU_OK:
+            raise SaruError(rc, last_error())
+        self._keep[t.value] = (arr, keep)
+        return t.value
+
+    def read_results(self, ticket: int, s: int) -> dict:
+        """Copies of set s's results of a finished reads-only request."""
+        out = SaruReadResults()
+        rc = self._lib.saru_server_read_results(self._h, ticket, s, C.byref(out))
+        if rc != SARU_OK:
+            raise SaruError(rc, last_error())
+
+        def arr(ptr, n, dt):
+            if n == 0 or not ptr:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dt))),
+                                         shape=(n,)).copy()
+
+        nc, n, npf = out.ncalls, out.n, out.nperfect
+        slot_begin = arr(out.slot_begin, nc + 1, np.int64)
+        tot = int(slot_begin[-1]) if nc else 0
+        res = dict(call_begin=arr(out.call_begin, nc + 1, np.int64), slot_begin=slot_begin,
+                   call_strand=arr(out.call_strand, nc, np.int8), ids=arr(out.ids, n, np.int32),
+                   pos=arr(out.pos, n, np.int32), dirs=arr(out.dirs, n, np.int8),
+                   scores=arr(out.scores, n, np.int32),
+                   perfect_ids=arr(out.perfect_ids, npf, np.int32),
+                   perfect_pos=arr(out.perfect_pos, npf, np.int32),
+                   perfect_strand=arr(out.perfect_strand, npf, np.int8),
+                   record_bytes=int(out.record_bytes))
+        if out.records:
+            res["records"] = arr(out.records, n * int(out.record_bytes), np.uint8)
+        else:
+            res["read_aln"] = arr(out.read_aln, tot, np.uint8)
+            res["genome_aln"] = arr(out.genome_aln, tot, np.uint8)
+        return res
+
+    def release(self, ticket: int) -> None:
+        self._lib.saru_server_release(self._h, ticket)
+        self._keep.pop(ticket, None)
+
+    def candidates(self, ticket: int) -> int:
+        """Candidates the filter made for a finished reads-only request (all
+        sets), without copying its results."""
+        out = SaruReadResults()
+        n = 0
+        for i in range(len(self._keep.get(ticket, ((), []))[1])):
+            if self._lib.saru_server_read_results(self._h, ticket, i, C.byref(out)) != SARU_OK:
+                raise SaruError(SARU_E_INVALID, last_error())
+            n += int(out.n)
+        return n
 
     def counters(self) -> tuple[int, int]:
         g, l_ = C.c_int64(), C.c_int64()

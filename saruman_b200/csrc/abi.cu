@@ -142,6 +142,8 @@ struct Lane {
   }
   void release() {
     if (device < 0) return;
+    int caller_dev = 0;  // the caller's current device, restored below
+    const bool had_dev = cudaGetDevice(&caller_dev) == cudaSuccess;
     cudaSetDevice(device);
     for (DevBuf *b : {&genome, &reads, &goff, &roff, &dirs, &scores, &ra, &ga, &scratch, &status,
                       &eoff, &arena, &records})
@@ -159,6 +161,7 @@ struct Lane {
     ev0 = ev1 = ev_run = nullptr;
     stream = s_run = s_out = nullptr;
     device = -1;
+    if (had_dev) cudaSetDevice(caller_dev);
   }
 };
 
@@ -193,6 +196,7 @@ int sm_count(int dev) {
 struct Plan {
   bool band = false;   // banded kernel
   bool wide = false;   // 64-bit band
+  bool queue = true;   // queued form of the banded kernel (walks on full warps)
   int max_m = 0;
   int64_t total_cells = 0;  // full-rectangle arena cells
 };
@@ -331,15 +335,15 @@ saru::Tuning tuning_for(int max_m, int k) {
   return it == g_tune.end() ? saru::Tuning{} : it->second;
 }
 
-long band_grid(int dev, long n, int max_m, int k) {
+long band_grid(int dev, long n, int max_m, int k, bool queue = true) {
   const saru::Tuning tn = tuning_for(max_m, k);
-  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k, tn.warps),
+  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k, tn.warps, queue),
                          smem_per_sm(dev), tn.ctas_per_sm);
 }
 
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, bool queue = true) {
   const saru::Tuning tn = tuning_for(max_m, k);
-  return saru::band_scratch_bytes(grid, max_m, k, wide || tn.word_bits == 64, tn.warps);
+  return saru::band_scratch_bytes(grid, max_m, k, wide || tn.word_bits == 64, tn.warps, queue);
 }
 
 // Enqueues the banded kernel on device buffers: calls[0..ncalls) as the
@@ -411,10 +415,13 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   a.max_k = max_k;
   a.wide_any = wide_any;
   a.warps_req = tn.warps;
-  a.grid = saru::band_grid(sm_count(dev), total_n, saru::band_layout(max_m, max_k, tn.warps),
+  a.queue = pl.queue ? 1 : 0;
+  a.grid = saru::band_grid(sm_count(dev), total_n,
+                           saru::band_layout(max_m, max_k, tn.warps, pl.queue),
                            smem_per_sm(dev), tn.ctas_per_sm);
   if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
-  const size_t need = saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0, tn.warps);
+  const size_t need =
+      saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0, tn.warps, pl.queue);
   if (need > scratch_bytes) {
     set_error("scratch too small: %zu < %zu", scratch_bytes, need);
     return SARU_E_INVALID;
@@ -918,28 +925,74 @@ int align_host_impl(const saru_batch *b, saru_result *r, Lane &L, float *ms_out,
 // char name[60]; UT_hash_handle hh; the handle's third pointer `next`
 // (src/uthash.h, UT_hash_handle) links the elements in insertion order.
 struct NameIndex {
-  std::vector<const char *> by_id;
+  std::vector<const char *> by_id;  // element of each read id (nullptr: none)
+  const void *head = nullptr;
   static const char *lookup(void *ctx, int32_t id) {
     auto *ni = static_cast<NameIndex *>(ctx);
-    if (id < 0 || (size_t)id >= ni->by_id.size()) return nullptr;
-    return ni->by_id[(size_t)id];
+    if (id < 0 || (size_t)id >= ni->by_id.size() || !ni->by_id[(size_t)id]) return nullptr;
+    return ni->by_id[(size_t)id] + sizeof(int);
   }
-  void build(const void *head) {
+  void build(const void *h) {
     by_id.clear();
-    const char *e = static_cast<const char *>(head);
+    head = h;
+    const char *e = static_cast<const char *>(h);
     size_t guard = 0;
     while (e && guard++ < (size_t)1 << 31) {
       const int id = *reinterpret_cast<const int *>(e);
-      const char *name = e + sizeof(int);
       if (id >= 0) {
         if ((size_t)id >= by_id.size()) by_id.resize((size_t)id + 1, nullptr);
-        by_id[(size_t)id] = name;
+        by_id[(size_t)id] = e;
       }
       const void *next = *reinterpret_cast<void *const *>(e + 64 + 2 * sizeof(void *));
       e = static_cast<const char *>(next);
     }
   }
+  // true if every read id of ids[0..n) whose candidate prints (score <= k)
+  // has an element that still holds that id
+  bool covers(const void *h, const int32_t *ids, const int32_t *scores, int n, int k) const {
+    if (h != head) return false;
+    for (int v = 0; v < n; ++v) {
+      if (scores[v] > k) continue;
+      const int32_t id = ids[v];
+      if (id < 0 || (size_t)id >= by_id.size() || !by_id[(size_t)id] ||
+          *reinterpret_cast<const int *>(by_id[(size_t)id]) != id)
+        return false;
+    }
+    return true;
+  }
 };
+
+// The caller's read_names table, walked once and kept while it still holds
+// the ids a call prints (the reference builds one table per read batch and
+// makes many calls against it; walking a list of millions of reads per call
+// would cost more than the call).
+std::mutex g_names_mu;
+NameIndex g_names;
+
+// Grow-only pinned host buffer.
+struct PinnedBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= n) return SARU_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    const size_t want = bytes + bytes / 8 + 4096;
+    if (cudaMallocHost(&p, want) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMallocHost of %zu bytes failed", want);
+      return SARU_E_NOMEM;
+    }
+    n = want;
+    return SARU_OK;
+  }
+  template <typename T>
+  T *as() const {
+    return reinterpret_cast<T *>(p);
+  }
+};
+PinnedBuf g_legacy_out[2][3];  // per legacy lane: scores, read strings, window strings
 
 }  // namespace
 
@@ -1103,6 +1156,53 @@ int static_scratch_ptr(int dev, void **out) {
 
 }  // namespace
 
+namespace {
+// The TSV lines of a legacy call, formatted on the host cores in ordered
+// ranges of candidates and written in candidate order, then the output
+// controls and counters (src/cuda-functions.cu:827-1006).
+void legacy_write(const saru_batch &b, PinnedBuf *hb, const int *read_id_array,
+                  const int *genome_pos_array, const char *direction_array, int error, int lane,
+                  float ms) {
+  const int n = b.n;
+  const int32_t *scores = hb[0].as<int32_t>();
+  std::lock_guard<std::mutex> nl(g_names_mu);
+  if (!g_names.covers(read_names, read_id_array, scores, n, error)) g_names.build(read_names);
+  saru::WriterCall w{scores, hb[1].as<char>(), hb[2].as<char>(), b.total_slots,
+                     b.genome_offsets, genome_pos_array,
+                     reinterpret_cast<const int8_t *>(direction_array), read_id_array, error,
+                     (int32_t)read_length_value, &NameIndex::lookup, &g_names};
+  const int hw = (int)std::thread::hardware_concurrency();
+  int nt = std::max(1, std::min(hw > 0 ? hw : 1, n / 16384 + 1));
+  std::vector<std::string> text((size_t)nt);
+  std::vector<int32_t> df((size_t)nt, 0), dr((size_t)nt, 0);
+  auto part = [&](int i) {
+    const int64_t lo = (int64_t)n * i / nt, hi = (int64_t)n * (i + 1) / nt;
+    text[(size_t)i].reserve((size_t)(hi - lo) * 64);
+    saru::format_range(w, lo, hi, &text[(size_t)i], &df[(size_t)i], &dr[(size_t)i]);
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < nt; ++i) th.emplace_back(part, i);
+  part(0);
+  for (auto &t : th) t.join();
+  std::lock_guard<std::mutex> lk(g_out_mu);
+  for (const std::string &t : text) fwrite(t.data(), 1, t.size(), stdout);
+  for (int v = 0; v < n; ++v) {
+    if (scores[v] > error) continue;
+    const int id = read_id_array[v];
+    if (direction_array[v] > 3) {
+      if (reverse_output_control) reverse_output_control[id] = 1;
+    } else if (forward_output_control) {
+      forward_output_control[id] = 1;
+    }
+  }
+  for (int i = 0; i < nt; ++i) {
+    forward_alignments_done += (unsigned)df[(size_t)i];
+    reverse_alignments_done += (unsigned)dr[(size_t)i];
+  }
+  alignment_time[lane] += ms;
+}
+}  // namespace
+
 extern "C" {
 
 int saru_align_device_static(const saru_batch *batch, saru_result *result, void *stream) {
@@ -1124,9 +1224,10 @@ int saru_align_device_static(const saru_batch *batch, saru_result *result, void 
   pl.band = true;
   pl.max_m = batch->max_read_length;
   pl.wide = batch->k > 7;
+  pl.queue = false;  // the per-tile form: half the plane slots of the queued one
   // as many persistent CTAs as the array holds planes for (each CTA's warps
   // need their own slice); a batch that cannot get even one CTA is refused
-  const size_t per_cta = band_scratch_bytes(1, pl.max_m, batch->k, pl.wide);
+  const size_t per_cta = band_scratch_bytes(1, pl.max_m, batch->k, pl.wide, false);
   const long max_grid = (long)(kStaticScratchBytes / (per_cta ? per_cta : 1));
   if (max_grid < 1) {
     set_error("saru_align_device_static: one thread block needs %zu bytes of scratch, the "
@@ -1264,6 +1365,8 @@ unsigned long int get_cuda_infos(void) {
   fprintf(stderr, "Detected %d GPU(s):\n\n", count);
   size_t most_free = 0;
   int best = 0, i;
+  int caller_dev = 0;  // restored after the scan: the caller's current device
+  const bool had_dev = cudaGetDevice(&caller_dev) == cudaSuccess;
   for (i = 0; i < count; ++i) {
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, i);
@@ -1283,6 +1386,7 @@ unsigned long int get_cuda_infos(void) {
     fprintf(stderr, "[%*lu/%*lu MB available]\n", 4, (unsigned long)(fr / (1024 * 1024)), 4,
             (unsigned long)(tot / (1024 * 1024)));
   }
+  if (had_dev && count > 0) cudaSetDevice(caller_dev);
   if (most_free < 128000000UL) {
     fprintf(stderr, "\n-> SARUMAN was not able to find a GPU with enough VRAM available! (available: %lu MB)\n",
             (unsigned long)(most_free / (1024 * 1024)));
@@ -1316,9 +1420,7 @@ void cuda_needleman_wunsch(int match, int mismatch, char *genome_sequences_on_ho
   if (sample_size <= 0) return;
   const int n = sample_size;
   const size_t slots = total_genome_array_size;
-  // host result arrays with zeroed slack (the writer may scan past a slot)
-  std::vector<int32_t> scores((size_t)n);
-  std::vector<char> ra(slots + 64, 0), ga(slots + 64, 0);
+  const int lane = do_reverse ? 1 : 0;
   saru_batch b{};
   b.genome = genome_sequences_on_host;
   b.reads = read_sequences_on_host;
@@ -1332,42 +1434,27 @@ void cuda_needleman_wunsch(int match, int mismatch, char *genome_sequences_on_ho
   b.first_of_call = 1;
   b.genome_bytes = genome_offsets[n - 1];
   b.total_slots = (int64_t)slots;
-  saru_result r{scores.data(), ra.data(), ga.data(), nullptr};
-  const int lane = do_reverse ? 1 : 0;
   float ms = 0.f;
   int rc;
+  PinnedBuf *hb = g_legacy_out[lane];
   {
     std::lock_guard<std::mutex> lk(g_lanes[lane].mu);
-    rc = align_host_impl(&b, &r, g_lanes[lane], &ms);
-  }
-  if (rc != SARU_OK) {
-    fprintf(stderr, "ERROR: saruman_b200 alignment failed: %s\n", g_last_error.c_str());
-    return;
-  }
-  NameIndex names;
-  names.build(read_names);
-  saru::WriterCall w{scores.data(), ra.data(), ga.data(), (int64_t)slots, genome_offsets,
-                     genome_pos_array, reinterpret_cast<const int8_t *>(direction_array),
-                     read_id_array, error, (int32_t)read_length_value, &NameIndex::lookup,
-                     &names};
-  std::string text;
-  text.reserve((size_t)n * 64);
-  int32_t df = 0, dr = 0;
-  saru::format_range(w, 0, n, &text, &df, &dr);
-  std::lock_guard<std::mutex> lk(g_out_mu);
-  fwrite(text.data(), 1, text.size(), stdout);
-  for (int v = 0; v < n; ++v) {
-    if (scores[(size_t)v] > error) continue;
-    const int id = read_id_array[v];
-    if (direction_array[v] > 3) {
-      if (reverse_output_control) reverse_output_control[id] = 1;
-    } else if (forward_output_control) {
-      forward_output_control[id] = 1;
+    // the lane's pinned result arrays, reused call after call; 64 zero bytes
+    // past the slots (the writer's scans may look past the last slot)
+    rc = hb[0].ensure(4 * (size_t)n);
+    if (!rc) rc = hb[1].ensure(slots + 64);
+    if (!rc) rc = hb[2].ensure(slots + 64);
+    if (!rc) {
+      memset(hb[1].as<char>() + slots, 0, 64);
+      memset(hb[2].as<char>() + slots, 0, 64);
+      saru_result r{hb[0].as<int32_t>(), hb[1].as<char>(), hb[2].as<char>(), nullptr};
+      rc = align_host_impl(&b, &r, g_lanes[lane], &ms);
     }
+    if (rc == SARU_OK) legacy_write(b, hb, read_id_array, genome_pos_array, direction_array,
+                                    error, lane, ms);
   }
-  forward_alignments_done += (unsigned)df;
-  reverse_alignments_done += (unsigned)dr;
-  alignment_time[lane] += ms;
+  if (rc != SARU_OK)
+    fprintf(stderr, "ERROR: saruman_b200 alignment failed: %s\n", g_last_error.c_str());
 }
 
 }  // extern "C"

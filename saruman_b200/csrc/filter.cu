@@ -744,6 +744,8 @@ int saru_filter_set_chunk(saru_filter *f, int64_t offset, int64_t limit) {
 
 void saru_filter_destroy(saru_filter *f) {
   if (!f) return;
+  int caller_dev = 0;  // the caller's current device, restored before returning
+  const bool had_dev = cudaGetDevice(&caller_dev) == cudaSuccess;
   cudaSetDevice(f->device);
   if (f->s) cudaStreamSynchronize(f->s);
   f->genome.release();
@@ -775,6 +777,7 @@ void saru_filter_destroy(saru_filter *f) {
   f->widx.release();
   if (f->s) cudaStreamDestroy(f->s);
   delete f;
+  if (had_dev) cudaSetDevice(caller_dev);
 }
 
 }  // extern "C"

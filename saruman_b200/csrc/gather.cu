@@ -46,9 +46,27 @@ __global__ void __launch_bounds__(256) saru_gather_kernel(GatherArgs a) {
       status |= kStatusGather;
       continue;
     }
-    const uint8_t *src = a.genome + pos;
     uint8_t *dst = a.windows + gbeg;
-    for (long j = lane; j < L; j += 32) dst[j] = src[j];
+    if (a.genome) {
+      const uint8_t *src = a.genome + pos;
+      for (long j = lane; j < L; j += 32) dst[j] = src[j];
+    } else {
+      for (long j = lane; j < L; j += 32) {
+        const long p = pos + j;
+        dst[j] = (uint8_t)(0x54474341u >> (8 * ((a.packed[p >> 2] >> (2 * (p & 3))) & 3u)));
+      }
+      if (a.nexc > 0) {  // the window's exceptions: first one at or after pos
+        long lo = 0, hi = a.nexc;
+        while (lo < hi) {
+          const long mid = (lo + hi) >> 1;
+          if (a.exc_pos[mid] < pos) lo = mid + 1;
+          else hi = mid;
+        }
+        __syncwarp();
+        for (long e = lo + lane; e < a.nexc && a.exc_pos[e] < pos + L; e += 32)
+          dst[a.exc_pos[e] - pos] = a.exc_byte[e];
+      }
+    }
     const uint8_t *row = a.table + ri * a.m;
     uint8_t *rd = a.reads + t * a.m;
     if (dir < 4) {
@@ -70,6 +88,58 @@ cudaError_t launch_gather(const GatherArgs &a, int sms, cudaStream_t s) {
   if (blocks > cap) blocks = cap;
   saru_gather_kernel<<<(unsigned)blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+}  // namespace saru
+
+namespace saru {
+
+int gather_packed(const saru_gather_call *c, const PackedGenome &g, char *windows, char *reads,
+                  int32_t *read_offsets, int32_t *status, saru_batch *batch, void *stream) {
+  set_last_error("");
+  if (!c || !batch || !status || c->n < 0 || c->k < 0 || c->read_length < 1 || c->nreads < 0 ||
+      (c->n > 0 && (!g.packed || !windows || !reads || !read_offsets || !c->read_table ||
+                    !c->read_index || !c->positions || !c->dirs || !c->genome_offsets))) {
+    set_last_error("gather: invalid call");
+    return SARU_E_INVALID;
+  }
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    set_last_error(cudaGetErrorString(cudaGetLastError()));
+    return SARU_E_CUDA;
+  }
+  GatherArgs a{};
+  a.genome = nullptr;
+  a.genome_len = g.len;
+  a.packed = g.packed;
+  a.exc_pos = g.exc_pos;
+  a.exc_byte = g.exc_byte;
+  a.nexc = g.nexc;
+  a.table = reinterpret_cast<const uint8_t *>(c->read_table);
+  a.nreads = c->nreads;
+  a.read_index = c->read_index;
+  a.positions = c->positions;
+  a.goff = c->genome_offsets;
+  a.dirs = c->dirs;
+  a.n = c->n;
+  a.genome_bytes = c->genome_bytes;
+  a.m = c->read_length;
+  a.k = c->k;
+  a.windows = reinterpret_cast<uint8_t *>(windows);
+  a.reads = reinterpret_cast<uint8_t *>(reads);
+  a.read_offsets = read_offsets;
+  a.status = status;
+  const cudaError_t e = launch_gather(a, sms, reinterpret_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) {
+    set_last_error(cudaGetErrorString(e));
+    return SARU_E_CUDA;
+  }
+  count_launch();
+  *batch = saru_batch{windows, reads, c->genome_offsets, read_offsets, c->dirs, c->n, c->k,
+                      c->match, c->mismatch, c->first_of_call, c->read_length, c->genome_bytes,
+                      c->total_slots};
+  return SARU_OK;
 }
 
 }  // namespace saru

@@ -48,7 +48,9 @@ struct KernelArgs {
   long grid;
   int max_m, max_k, wide_any;
   int warps_req;                       // requested warps per CTA (0: as many as fit)
+  int queue;                           // 1: queued form (saru_band_queue_kernel)
   long rs_bytes, ws_bytes, warp_smem;  // shared-memory slice layout (set by the launcher)
+  long region_bytes;
 };
 
 // Launch shape of the banded kernel for one (read length, k) class; 0 keeps
@@ -84,8 +86,15 @@ struct FullArgs {
 
 // Windows and reads of one call gathered from a resident genome (gather.cu).
 struct GatherArgs {
-  const uint8_t *genome;  // resident genome
+  const uint8_t *genome;  // resident genome, one byte a base (nullptr: packed)
   long genome_len;
+  // or 2 bits a base (A 0, C 1, G 2, T 3; base p in bits 2(p & 3) of byte
+  // p >> 2) with the bytes that are not A/C/G/T as exceptions, their genome
+  // positions ascending
+  const uint8_t *packed;
+  const int64_t *exc_pos;
+  const uint8_t *exc_byte;
+  long nexc;
   const uint8_t *table;  // read table: nreads rows of m bytes, as sequenced
   long nreads;
   const int32_t *read_index, *positions, *goff;
@@ -99,10 +108,12 @@ struct GatherArgs {
 
 cudaError_t launch_gather(const GatherArgs &a, int sms, cudaStream_t s);
 
-BandLayout band_layout(int max_m, int k, int warps_req = 0);
+// queue: the queued form's slice (band_queue.cuh) and kQueueSlots plane
+// slots per warp instead of 32.
+BandLayout band_layout(int max_m, int k, int warps_req = 0, bool queue = false);
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_cap = 0);
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide,
-                          int warps_req = 0);  // counter + planes
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req = 0,
+                          bool queue = false);  // counter + planes
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s);
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
 

@@ -31,6 +31,7 @@
 
 #include "../../include/saruman_b200.h"
 #include "kernels.cuh"
+#include "saru_core.cuh"
 #include "server_internal.h"
 
 namespace {
@@ -95,6 +96,21 @@ class Arena {
   std::map<size_t, size_t> free_;  // offset -> length
 };
 
+// Results of one read set of a reads-only request, owned by the server:
+// the filter's calls (both strands), their gather descriptors and outputs.
+struct ReadSetOut {
+  saru_read_set set{};
+  std::vector<int64_t> call_begin{0}, slot_begin{0};
+  std::vector<int8_t> call_strand;
+  std::vector<int32_t> ids, pos, goff, rindex, scores;
+  std::vector<int8_t> dirs;
+  std::vector<char> ra, ga;
+  std::vector<uint8_t> records;
+  int64_t rec_bytes = 0;
+  std::vector<int32_t> perfect_ids, perfect_pos;
+  std::vector<int8_t> perfect_strand;
+};
+
 struct Request {
   int64_t ticket = 0;
   bool gather = false;                  // calls given as saru_gather_call (resident genome)
@@ -113,6 +129,7 @@ struct Request {
   int32_t group = -1, redone = 0;
   int rc = SARU_OK;
   bool done = false;
+  std::vector<ReadSetOut> rsets;  // reads-only request: its sets and results
 };
 
 // Read bytes of call i (the gathered reads of a gather call).
@@ -165,8 +182,15 @@ struct saru_server {
   cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
-  char *genome = nullptr;  // resident genome of gather requests
+  // resident genome of gather requests: 2 bits a base, non-ACGT bytes as
+  // exceptions (device memory: one quarter of the bytes plus the exceptions)
+  uint8_t *genome = nullptr;
+  int64_t *exc_pos = nullptr;
+  uint8_t *exc_byte = nullptr;
+  saru::PackedGenome pg;
   int64_t genome_len = 0;
+  std::vector<char> genome_host;  // the same genome, for the filters' q-gram indexes
+  std::map<std::pair<int, int>, saru_filter *> filters;  // per (read length, k)
 
   struct Group {
     std::vector<std::shared_ptr<Request>> reqs;
@@ -179,9 +203,168 @@ struct saru_server {
   std::deque<std::shared_ptr<Request>> pending;
   std::deque<Group> inflight;
   std::unordered_map<int64_t, std::shared_ptr<Request>> tickets;
+  std::unordered_map<int64_t, std::shared_ptr<Request>> read_done;  // until released
+  std::deque<std::shared_ptr<Request>> filter_q;  // reads-only requests to filter
+  std::condition_variable cv_filter;
   int64_t next_ticket = 1, groups = 0, launches = 0, free_gen = 0;
-  bool stop = false, sched_done = false;
-  std::thread sched_thr, done_thr;
+  bool stop = false, sched_done = false, filter_stop = false;
+  std::thread sched_thr, done_thr, filter_thr;
+
+  void free_genome() {
+    if (genome) cudaFree(genome);
+    if (exc_pos) cudaFree(exc_pos);
+    if (exc_byte) cudaFree(exc_byte);
+    genome = nullptr;
+    exc_pos = nullptr;
+    exc_byte = nullptr;
+    pg = saru::PackedGenome{};
+    genome_len = 0;
+  }
+
+  // The filter of (m, k) on the resident genome (created on first use).
+  saru_filter *filter_for(int m, int k) {
+    auto it = filters.find({m, k});
+    if (it != filters.end()) return it->second;
+    saru_filter *f = saru_filter_create(genome_host.data(), (int64_t)genome_host.size(), m, k,
+                                        cfg.device);
+    if (f) filters[{m, k}] = f;
+    return f;
+  }
+
+  // One read set through the filter on both strands: its calls as gather
+  // calls over the set's own read table, outputs in the set's arrays.
+  int filter_set(Request &r, ReadSetOut &o) {
+    const saru_read_set &rs = o.set;
+    const int m = rs.read_length, k = rs.k;
+    saru_filter *f = filter_for(m, k);
+    if (!f) return SARU_E_INVALID;
+    const uint32_t cv = rs.chunk_value
+                            ? rs.chunk_value
+                            : (uint32_t)(0.92 * 2147483648.0 / ((m + 1.0) * (m + 2.0 * k + 1.0)) /
+                                         1000.0) * 1000u;
+    for (int dr : {0, 4}) {
+      int64_t cnt[3] = {0, 0, 0};
+      int rc = saru_filter_run(f, rs.reads, rs.nreads, dr, cv, cnt);
+      if (rc) return rc;
+      const size_t nc = (size_t)cnt[0], na = (size_t)cnt[1], np = (size_t)cnt[2];
+      std::vector<int64_t> cb(nc + 1);
+      const size_t a0 = o.ids.size(), p0 = o.perfect_ids.size();
+      o.ids.resize(a0 + na);
+      o.pos.resize(a0 + na);
+      o.dirs.resize(a0 + na);
+      o.perfect_ids.resize(p0 + np);
+      o.perfect_pos.resize(p0 + np);
+      o.perfect_strand.resize(p0 + np, (int8_t)dr);
+      if ((rc = saru_filter_results(f, cb.data(), o.ids.data() + a0, o.pos.data() + a0,
+                                    o.dirs.data() + a0, o.perfect_ids.data() + p0,
+                                    o.perfect_pos.data() + p0)))
+        return rc;
+      for (size_t c = 0; c < nc; ++c) {
+        o.call_begin.push_back((int64_t)a0 + cb[c + 1]);
+        o.call_strand.push_back((int8_t)dr);
+      }
+    }
+    const size_t n = o.ids.size(), ncalls = o.call_strand.size();
+    o.goff.resize(n);
+    o.rindex.resize(n);
+    o.scores.assign(n, 0);
+    int64_t slots = 0;
+    for (size_t c = 0; c < ncalls; ++c) {
+      const int64_t a = o.call_begin[c], b = o.call_begin[c + 1];
+      int64_t acc = 0;
+      int32_t lo = INT32_MAX, hi = -1;
+      for (int64_t t = a; t < b; ++t) {
+        int so = 0, eo = 0;
+        saru::flank_of(o.dirs[(size_t)t], k, so, eo);
+        acc += m + so + eo;
+        o.goff[(size_t)t] = (int32_t)acc;
+        lo = std::min(lo, o.ids[(size_t)t]);
+        hi = std::max(hi, o.ids[(size_t)t]);
+      }
+      for (int64_t t = a; t < b; ++t) o.rindex[(size_t)t] = o.ids[(size_t)t] - lo;
+      slots += acc + (int64_t)k * (b - a);
+      o.slot_begin.push_back(slots);
+      saru_gather_call g{};
+      g.read_table = rs.reads + (size_t)lo * (size_t)m;
+      g.read_index = o.rindex.data() + a;
+      g.positions = o.pos.data() + a;
+      g.dirs = o.dirs.data() + a;
+      g.genome_offsets = o.goff.data() + a;
+      g.n = (int32_t)(b - a);
+      g.nreads = hi - lo + 1;
+      g.k = k;
+      g.match = 0;
+      g.mismatch = 1;
+      g.first_of_call = 1;
+      g.read_length = m;
+      g.genome_bytes = acc;
+      g.total_slots = acc + (int64_t)k * (b - a);
+      r.gcalls.push_back(g);
+    }
+    if (r.compact) {
+      o.rec_bytes = saru_compact_record_bytes(m, k);
+      o.records.assign(n * (size_t)o.rec_bytes, 0);
+    } else {
+      o.ra.assign((size_t)slots + 64, 0);
+      o.ga.assign((size_t)slots + 64, 0);
+    }
+    for (size_t c = 0; c < ncalls; ++c) {
+      const int64_t a = o.call_begin[c];
+      saru_result res{o.scores.data() + a, nullptr, nullptr, nullptr};
+      if (r.compact) {
+        res.read_aln = reinterpret_cast<char *>(o.records.data() + a * o.rec_bytes);
+      } else {
+        res.read_aln = o.ra.data() + o.slot_begin[c];
+        res.genome_aln = o.ga.data() + o.slot_begin[c];
+      }
+      r.results.push_back(res);
+    }
+    return SARU_OK;
+  }
+
+  // Filter thread: reads-only requests in arrival order become gather
+  // requests on the pending queue (or finish here with an error or nothing
+  // to align), while the scheduler and completer work on earlier ones.
+  void filterer() {
+    cudaSetDevice(cfg.device);
+    for (;;) {
+      std::shared_ptr<Request> r;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_filter.wait(lk, [&] { return filter_stop || !filter_q.empty(); });
+        if (filter_q.empty()) return;
+        r = filter_q.front();
+        filter_q.pop_front();
+      }
+      int rc = SARU_OK;
+      for (auto &o : r->rsets)
+        if ((rc = filter_set(*r, o))) break;
+      if (!rc && r->gcalls.size() > (size_t)SARU_MAX_CALLS) {
+        saru::set_last_error("reads-only request: more than SARU_MAX_CALLS calls");
+        rc = SARU_E_INVALID;
+      }
+      if (!rc) {
+        for (const auto &g : r->gcalls) r->calls.push_back(shape_of(g));
+        r->dev_bytes = request_bytes(*r);
+        if (r->dev_bytes > arena.size()) {
+          saru::set_last_error("reads-only request larger than the device budget");
+          rc = SARU_E_NOMEM;
+        }
+      }
+      std::unique_lock<std::mutex> lk(mu);
+      if (rc || r->calls.empty()) {
+        r->rc = rc;
+        r->t_done = now_us();
+        r->done = true;
+        cv_done.notify_all();
+        continue;
+      }
+      pending.push_back(r);
+      cv_pending.notify_all();
+      // plain mode: the next request's filter waits for this one
+      if (!cfg.pipeline) cv_done.wait(lk, [&] { return r->done; });
+    }
+  }
 
   // Carves a request's device arrays out of its arena range and copies its
   // inputs in on s_in.
@@ -245,9 +428,9 @@ struct saru_server {
       dg.dirs = d.dirs;
       dg.genome_offsets = d.genome_offsets;
       saru_batch gathered;
-      if (saru_gather_device(&dg, genome, genome_len, reinterpret_cast<char *>(g),
-                             reinterpret_cast<char *>(rd), reinterpret_cast<int32_t *>(ro),
-                             r.dstatus + i, &gathered, s_in) != SARU_OK)
+      if (saru::gather_packed(&dg, pg, reinterpret_cast<char *>(g), reinterpret_cast<char *>(rd),
+                              reinterpret_cast<int32_t *>(ro), r.dstatus + i, &gathered,
+                              s_in) != SARU_OK)
         r.rc = SARU_E_CUDA;
     }
   }
@@ -493,7 +676,88 @@ saru_server *saru_server_create(const saru_server_config *cfg) {
   }
   s->sched_thr = std::thread([s] { s->scheduler(); });
   s->done_thr = std::thread([s] { s->completer(); });
+  s->filter_thr = std::thread([s] { s->filterer(); });
   return s;
+}
+
+int saru_server_submit_reads(saru_server *s, const saru_read_set *sets, int32_t nsets,
+                             int32_t compact, int64_t *ticket) {
+  if (!s || !sets || !ticket || nsets < 1 || nsets > 16) {
+    saru::set_last_error("saru_server_submit_reads: 1..16 read sets and a ticket");
+    return SARU_E_INVALID;
+  }
+  for (int i = 0; i < nsets; ++i) {
+    const saru_read_set &rs = sets[i];
+    if (rs.nreads < 0 || (rs.nreads > 0 && !rs.reads) || rs.k < 0 || rs.k > 15 ||
+        rs.read_length < 2 || rs.read_length > saru::kMaxBandM) {
+      saru::set_last_error("saru_server_submit_reads: every set needs reads, k <= 15 and "
+                           "2 <= read_length <= 512");
+      return SARU_E_INVALID;
+    }
+  }
+  auto r = std::make_shared<Request>();
+  r->gather = true;
+  r->compact = compact != 0;
+  r->rsets.resize((size_t)nsets);
+  for (int i = 0; i < nsets; ++i) r->rsets[(size_t)i].set = sets[i];
+  r->t_submit = now_us();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->genome) {
+      saru::set_last_error("saru_server_submit_reads: no genome (saru_server_set_genome)");
+      return SARU_E_INVALID;
+    }
+    if (s->stop || s->filter_stop) {
+      saru::set_last_error("saru_server_submit_reads: server is shutting down");
+      return SARU_E_INVALID;
+    }
+    r->ticket = s->next_ticket++;
+    s->tickets[r->ticket] = r;
+    s->read_done[r->ticket] = r;
+    s->filter_q.push_back(r);
+  }
+  *ticket = r->ticket;
+  s->cv_filter.notify_all();
+  return SARU_OK;
+}
+
+int saru_server_read_results(saru_server *s, int64_t ticket, int32_t set,
+                             saru_read_results *out) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->read_done.find(ticket);
+  if (it == s->read_done.end() || !it->second->done || it->second->rc != SARU_OK || set < 0 ||
+      (size_t)set >= it->second->rsets.size() || !out) {
+    saru::set_last_error("saru_server_read_results: not a finished reads-only request, or no "
+                         "such set");
+    return SARU_E_INVALID;
+  }
+  const ReadSetOut &o = it->second->rsets[(size_t)set];
+  *out = saru_read_results{};
+  out->ncalls = (int32_t)o.call_strand.size();
+  out->nperfect = (int32_t)o.perfect_ids.size();
+  out->n = (int64_t)o.ids.size();
+  out->call_begin = o.call_begin.data();
+  out->slot_begin = o.slot_begin.data();
+  out->call_strand = o.call_strand.data();
+  out->ids = o.ids.data();
+  out->pos = o.pos.data();
+  out->dirs = o.dirs.data();
+  out->scores = o.scores.data();
+  out->read_aln = o.ra.empty() ? nullptr : o.ra.data();
+  out->genome_aln = o.ga.empty() ? nullptr : o.ga.data();
+  out->records = o.records.empty() ? nullptr : o.records.data();
+  out->record_bytes = o.rec_bytes;
+  out->perfect_ids = o.perfect_ids.data();
+  out->perfect_pos = o.perfect_pos.data();
+  out->perfect_strand = o.perfect_strand.data();
+  return SARU_OK;
+}
+
+void saru_server_release(saru_server *s, int64_t ticket) {
+  if (!s) return;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->read_done.find(ticket);
+  if (it != s->read_done.end() && it->second->done) s->read_done.erase(it);
 }
 
 int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket) {
@@ -585,20 +849,44 @@ int saru_server_set_genome(saru_server *s, const char *genome, int64_t genome_le
     return SARU_E_INVALID;
   }
   cudaSetDevice(s->cfg.device);
-  if (s->genome) cudaFree(s->genome);
-  s->genome = nullptr;
-  s->genome_len = 0;
-  if (cudaMalloc(&s->genome, (size_t)genome_len + 64) != cudaSuccess) {
+  s->free_genome();
+  // 2 bits a base; bytes other than A/C/G/T kept as (position, byte)
+  const size_t nb = ((size_t)genome_len + 3) / 4;
+  std::vector<uint8_t> packed(nb, 0);
+  std::vector<int64_t> epos;
+  std::vector<uint8_t> ebyte;
+  for (int64_t p = 0; p < genome_len; ++p) {
+    const uint8_t c = (uint8_t)genome[p];
+    const int code = saru::base_code(c);
+    if (code < 0) {
+      epos.push_back(p);
+      ebyte.push_back(c);
+      continue;
+    }
+    packed[(size_t)(p >> 2)] |= (uint8_t)(code << (2 * (p & 3)));
+  }
+  const size_t ne = epos.size();
+  if (cudaMalloc(&s->genome, nb + 64) != cudaSuccess ||
+      (ne && (cudaMalloc(&s->exc_pos, 8 * ne) != cudaSuccess ||
+              cudaMalloc(&s->exc_byte, ne) != cudaSuccess))) {
     cudaGetLastError();
-    s->genome = nullptr;
+    s->free_genome();
     saru::set_last_error("saru_server_set_genome: device allocation failed");
     return SARU_E_NOMEM;
   }
-  if (cudaMemcpy(s->genome, genome, (size_t)genome_len, cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (cudaMemcpy(s->genome, packed.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      (ne && (cudaMemcpy(s->exc_pos, epos.data(), 8 * ne, cudaMemcpyHostToDevice) != cudaSuccess ||
+              cudaMemcpy(s->exc_byte, ebyte.data(), ne, cudaMemcpyHostToDevice) != cudaSuccess))) {
     saru::set_last_error(cudaGetErrorString(cudaGetLastError()));
+    s->free_genome();
     return SARU_E_CUDA;
   }
+  s->pg = saru::PackedGenome{s->genome, s->exc_pos, s->exc_byte, genome_len, (int64_t)ne};
   s->genome_len = genome_len;
+  s->genome_host.assign(genome, genome + genome_len);
+  for (auto &kv : s->filters) saru_filter_destroy(kv.second);  // indexes of the old genome
+  s->filters.clear();
+  cudaSetDevice(s->cfg.device);
   return SARU_OK;
 }
 
@@ -610,6 +898,12 @@ void saru_server_counters(saru_server *s, int64_t *groups, int64_t *launches) {
 
 void saru_server_destroy(saru_server *s) {
   if (!s) return;
+  {  // the filter thread first: what it has queued goes to the scheduler
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->filter_stop = true;
+  }
+  s->cv_filter.notify_all();
+  if (s->filter_thr.joinable()) s->filter_thr.join();
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
@@ -625,7 +919,9 @@ void saru_server_destroy(saru_server *s) {
   cudaSetDevice(s->cfg.device);
   cudaStreamSynchronize(s->s_comp);
   if (s->scratch) cudaFree(s->scratch);
-  if (s->genome) cudaFree(s->genome);
+  s->free_genome();
+  for (auto &kv : s->filters) saru_filter_destroy(kv.second);
+  cudaSetDevice(s->cfg.device);
   s->arena.release();
   cudaStreamDestroy(s->s_in);
   cudaStreamDestroy(s->s_comp);

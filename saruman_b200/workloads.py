@@ -399,3 +399,135 @@ def random_batch(m: int, k: int, n: int, seed: int, err: float = 0.05,
         post = alpha[rng.integers(0, len(alpha), size=eo)]
         windows.append(np.concatenate([pre, np.asarray(out, np.uint8), post]).astype(np.uint8))
     return make_batch(m, k, windows, reads, fl.astype(np.int8))
+
+
+def chunk_value_for(m: int, k: int) -> int:
+    """The reference's queue threshold (-s, candidates per call) for read
+    length m: calls stay under 2^31 matrix cells and a 4 GiB arena, as a
+    run of the reference must (about 1.2M candidates at 36 bp, 180k at
+    100 bp, 28k at 250 bp)."""
+    return int(0.92 * 2**31 / ((m + 1) * (m + 2 * k + 1))) // 1000 * 1000
+
+
+@dataclasses.dataclass
+class CallSet:
+    """Calls of one read length as the reference's q-gram filter submits
+    them (src/hash.c:840-850, 1094-1098), stored back to back: call c holds
+    candidates call_begin[c] .. call_begin[c + 1]; its offsets restart at 0
+    (each call is a reference call of its own, candidate 0 opening it), its
+    windows start at byte gbase[c], its reads at rbase[c] and its slots at
+    sbase[c] of the set's slot arrays."""
+    m: int
+    k: int
+    genome: np.ndarray          # uint8 windows of all calls
+    reads: np.ndarray           # uint8 reads of all calls, as aligned
+    genome_offsets: np.ndarray  # int32, per call inclusive prefix sums of L
+    read_offsets: np.ndarray    # int32, per call (t - begin + 1) * m
+    edit_offsets: np.ndarray    # int32, per call exclusive prefix sums of (m+1)(L+1)
+    dirs: np.ndarray
+    ids: np.ndarray
+    pos: np.ndarray
+    call_begin: np.ndarray      # int64, ncalls + 1
+    strand: np.ndarray          # int8 per call: 0 forward, 4 reverse (do_reverse)
+    gbase: np.ndarray           # int64, ncalls + 1
+    sbase: np.ndarray           # int64, ncalls + 1
+    perfect: int = 0            # perfect hits the filter printed (never aligned)
+    filter_ms: float = 0.0      # device time of the filter runs that made the calls
+
+    @property
+    def n(self) -> int:
+        return int(self.dirs.shape[0])
+
+    @property
+    def ncalls(self) -> int:
+        return int(self.call_begin.shape[0]) - 1
+
+    @property
+    def total_slots(self) -> int:
+        return int(self.sbase[-1])
+
+    @property
+    def total_genome(self) -> int:
+        """sum(L + k) over all calls (the Batch name of the slot bytes)."""
+        return self.total_slots
+
+    @property
+    def lengths(self) -> np.ndarray:
+        so = np.where(np.isin(self.dirs & 3, (2, 3)), self.k, 0)
+        eo = np.where(np.isin(self.dirs & 3, (1, 3)), self.k, 0)
+        return (self.m + so + eo).astype(np.int64)
+
+    def call(self, c: int) -> Batch:
+        """Call c as a Batch (views into the set's arrays)."""
+        a, b = int(self.call_begin[c]), int(self.call_begin[c + 1])
+        m = self.m
+        return Batch(m=m, k=self.k, genome=self.genome[self.gbase[c]:self.gbase[c + 1]],
+                     reads=self.reads[a * m:b * m], genome_offsets=self.genome_offsets[a:b],
+                     read_offsets=self.read_offsets[a:b], edit_offsets=self.edit_offsets[a:b],
+                     dirs=self.dirs[a:b], ids=self.ids[a:b], pos=self.pos[a:b])
+
+
+def callset(genome: np.ndarray, seqs: np.ndarray, m: int, k: int, ids: np.ndarray,
+            pos: np.ndarray, dirs: np.ndarray, call_begin: np.ndarray,
+            strand: np.ndarray, perfect: int = 0) -> CallSet:
+    """A CallSet from per-candidate (read id, window start, flag) in call
+    order: windows cut from `genome` (m + so + eo bytes from the start,
+    src/hash.c:986-1024), reads taken from `seqs` (as sequenced) and
+    reverse-complemented for flags 4-7 (src/hash.c:1027-1034)."""
+    dirs = np.asarray(dirs, np.int8)
+    n = len(dirs)
+    so = np.where(np.isin(dirs & 3, (2, 3)), k, 0)
+    eo = np.where(np.isin(dirs & 3, (1, 3)), k, 0)
+    L = (m + so + eo).astype(np.int64)
+    cb = np.asarray(call_begin, np.int64)
+    call_of = np.repeat(np.arange(len(cb) - 1), np.diff(cb))
+    gcum = np.cumsum(L)
+    gbase = np.concatenate([[0], gcum[cb[1:] - 1]]) if n else np.zeros(len(cb), np.int64)
+    goff = (gcum - gbase[call_of]).astype(np.int32)
+    t_in = np.arange(n, dtype=np.int64) - cb[call_of]
+    roff = ((t_in + 1) * m).astype(np.int32)
+    esz = (m + 1) * (L + 1)
+    ecum = np.cumsum(esz)
+    ebase = np.concatenate([[0], ecum[cb[1:] - 1]]) if n else np.zeros(len(cb), np.int64)
+    eoff64 = ecum - esz - ebase[call_of]
+    eoff = np.where(eoff64 + esz < 2**31, eoff64, -1).astype(np.int32)
+    rd = np.ascontiguousarray(seqs[np.asarray(ids)])
+    rev = dirs > 3
+    if rev.any():
+        rd[rev] = reverse_complement(rd[rev])
+    sbase = gbase + k * cb
+    return CallSet(m=m, k=k, genome=pack_windows(genome, np.asarray(pos, np.int64), L),
+                   reads=rd.reshape(-1), genome_offsets=goff, read_offsets=roff,
+                   edit_offsets=eoff, dirs=dirs, ids=np.asarray(ids, np.int32),
+                   pos=np.asarray(pos, np.int32), call_begin=cb,
+                   strand=np.asarray(strand, np.int8), gbase=gbase.astype(np.int64),
+                   sbase=sbase.astype(np.int64), perfect=perfect)
+
+
+def filter_callset(genome: np.ndarray, seqs: np.ndarray, m: int, k: int,
+                   chunk_value: int | None = None, device: int = -1) -> CallSet:
+    """The calls the reference's q-gram filter makes for reads `seqs` (one
+    read batch, ids from 0) on both strands, from the library's device
+    filter (saru_filter_*, the reference's filter on the GPU): forward
+    strand calls first, then the reverse strand's, as the two strand
+    threads submit them."""
+    from . import Filter
+    cv = chunk_value or chunk_value_for(m, k)
+    parts = []
+    with Filter(genome, m, k, device) as f:
+        for dr in (0, 4):
+            parts.append((dr, f.run(seqs, dr, cv)))
+    ms = sum(p.ms for _, p in parts)
+    ids = np.concatenate([p.ids for _, p in parts])
+    pos = np.concatenate([p.pos for _, p in parts])
+    dirs = np.concatenate([p.dirs for _, p in parts])
+    cb, strand, off = [0], [], 0
+    for dr, p in parts:
+        cb.extend((p.call_begin[1:] + off).tolist())
+        strand.extend([dr] * (len(p.call_begin) - 1))
+        off += len(p.ids)
+    perfect = sum(len(p.perfect_ids) for _, p in parts)
+    cs = callset(genome, seqs, m, k, ids, pos, dirs, np.asarray(cb, np.int64),
+                 np.asarray(strand, np.int8), perfect)
+    cs.filter_ms = ms
+    return cs

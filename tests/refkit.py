@@ -81,6 +81,27 @@ def oracle_align(b: Batch, nthreads: int = 1):
     return sc[:b.n], ra[:tot], ga[:tot], st
 
 
+def oracle_check(b: Batch, scores, read_aln, genome_aln, nthreads: int | None = None):
+    """Checks another implementation's outputs for the whole call `b` (any
+    size) against the oracle, in sub-calls led by their predecessor
+    (saru_oracle_check).  Returns (candidates that differ, lowest such
+    index or -1, oracle status bits)."""
+    lib = oracle_lib()
+    lib.saru_oracle_check.restype = C.c_long
+    go = np.ascontiguousarray(b.genome_offsets, np.int64)
+    ro = np.ascontiguousarray(b.read_offsets, np.int64)
+    sc = np.ascontiguousarray(scores, np.int32)
+    ra = np.ascontiguousarray(read_aln, np.uint8)
+    ga = np.ascontiguousarray(genome_aln, np.uint8)
+    assert len(sc) >= b.n and len(ra) >= b.total_genome and len(ga) >= b.total_genome
+    first, st = C.c_long(-1), C.c_int(0)
+    bad = lib.saru_oracle_check(
+        C.c_int(b.match), C.c_int(b.mismatch), _ptr(b.genome), _ptr(b.reads), _ptr(go), _ptr(ro),
+        C.c_long(b.n), _ptr(b.dirs), C.c_int(b.k), C.c_int(nthreads or os.cpu_count() or 1),
+        _ptr(sc), _ptr(ra), _ptr(ga), C.byref(first), C.byref(st))
+    return int(bad), int(first.value), int(st.value)
+
+
 def ref_align(b: Batch, strict: bool = True, nthreads: int = 1, chunk: int = 512):
     lib = ref_lib()
     sc, ra, ga = _outputs(b)

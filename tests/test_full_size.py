@@ -1,14 +1,23 @@
-"""The benchmark's full C2 step (2M reads x 100 bp, 18.95M candidates),
-checked at that size by properties that do not need the oracle on every
-candidate: the slot strings of the host entry point (slot mode) equal, byte
-for byte over all candidates, the compact records of the device entry point
-expanded on the host (two independent output paths); every slot is its
-string followed by zeros; a read string without its gaps is a suffix of
-the read; and a sample of candidates matches the oracle."""
+"""Benchmarked configurations at their full size, every candidate checked
+against the oracle.
+
+Each configuration's workload is built exactly as bench.py builds it: the
+reads of every length bin, the calls the reference's q-gram filter makes
+for them on both strands (the library's device filter), cut at the
+reference's queue threshold.  Every call goes through the host entry point
+(saru_align_host) and every candidate of every call is compared with the
+oracle (oracle/saru_oracle.c through saru_oracle_check, on all host
+threads): min(score, k + 1) and both L + k byte slots.  The TSV lines the
+library's writer prints for each call are compared with the oracle's
+writer.  Each configuration prints its candidate count and a SHA-256 of its
+outputs."""
 from __future__ import annotations
 
+import hashlib
 import importlib.util
+import os
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 import numpy as np
@@ -16,7 +25,6 @@ import pytest
 
 import refkit as R
 import saruman_b200 as S
-from nwbio import sub_batch
 
 pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
@@ -30,60 +38,92 @@ def load_bench():
     return mod
 
 
-def test_full_c2_step(saru_lib):
+def align_and_check(cs, tag: str, outputs=None) -> None:
+    """Aligns every call of CallSet `cs` on the GPU (or takes `outputs` =
+    (scores, read strings, window strings) made elsewhere) and checks every
+    candidate and every call's TSV against the oracle."""
+    k, m = cs.k, cs.m
+    cb, sb = cs.call_begin, cs.sbase
+    spans = [(int(cb[c]), int(cb[c + 1]), int(sb[c]), int(sb[c + 1])) for c in range(cs.ncalls)]
+    if outputs is None:
+        sc = np.zeros(cs.n, np.int32)
+        ra = np.zeros(cs.total_slots + 64, np.uint8)
+        ga = np.zeros(cs.total_slots + 64, np.uint8)
+        for c, (a0, a1, s0, s1) in enumerate(spans):
+            S.align_host(cs.call(c), lane=0, out=S.AlignResult(sc[a0:a1], ra[s0:s1], ga[s0:s1]))
+    else:
+        sc, ra, ga = outputs
+    bad_total = 0
+    for c, (a0, a1, s0, s1) in enumerate(spans):
+        bad, first, st = R.oracle_check(cs.call(c), sc[a0:a1], ra[s0:s1], ga[s0:s1])
+        assert st == 0, (tag, c, st)
+        assert bad == 0, f"{tag}: call {c}: {bad} candidates differ, first {first}"
+        bad_total += bad
+    # the writer's lines, call by call, against the oracle's writer
+    n_ids = int(cs.ids.max()) + 1
+    names_l = [b"read%d" % i for i in range(n_ids)]
+    lib_names, ora_names = S.name_table(names_l), R.name_table(names_l)
+
+    def tsv(c):
+        a0, a1, s0, s1 = spans[c]
+        b = cs.call(c)
+        res = S.AlignResult(sc[a0:a1], ra[s0:s1], ga[s0:s1])
+        ours, _, _ = S.format_tsv(b, res, lib_names, read_length=m)
+        theirs, st, _ = R.oracle_tsv(b, sc[a0:a1], ra[s0:s1], ga[s0:s1], ora_names,
+                                     read_length=m)
+        return ours == theirs and st == 0, len(ours)
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        res = list(ex.map(tsv, range(cs.ncalls)))
+    assert all(ok for ok, _ in res), [c for c, (ok, _) in enumerate(res) if not ok][:5]
+    h = hashlib.sha256()
+    for a in (sc, ra[:cs.total_slots], ga[:cs.total_slots]):
+        h.update(memoryview(a))
+    print(f"FULLSIZE {tag} m={m} k={k} candidates={cs.n} calls={cs.ncalls} "
+          f"aligned={int((sc <= k).sum())} tsv_bytes={sum(n for _, n in res)} "
+          f"sha256={h.hexdigest()[:16]}", flush=True)
+
+
+@pytest.mark.parametrize("name", ["c1", "c2", "c4", "c3"])
+def test_full_size_config_matches_the_oracle(saru_lib, name):
     import torch
+    torch.cuda.set_device(0)
     bench = load_bench()
-    b = bench.build_batches(dict(bench.CONFIGS["c2"]), 0)[0]
-    assert b.n > 18_000_000
-    slot = S.align_host(b)
-    # the compact path on the device, expanded on the host
-    dev = torch.device("cuda:0")
-    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    g, r, go, ro, d = T(b.genome), T(b.reads), T(b.genome_offsets), T(b.read_offsets), T(b.dirs)
-    rb = S.compact_record_bytes(b.m, b.k)
-    sc = torch.zeros(b.n, dtype=torch.int32, device=dev)
-    rec = torch.empty(b.n * rb, dtype=torch.uint8, device=dev)
-    st = torch.zeros(1, dtype=torch.int32, device=dev)
-    sb = S.SaruBatch(g.data_ptr(), r.data_ptr(), go.data_ptr(), ro.data_ptr(), d.data_ptr(), b.n,
-                     b.k, 0, 1, 1, b.m, len(b.genome), b.total_genome)
-    nscr = S.scratch_bytes(b.n, b.m, b.k)
-    scr = torch.empty(nscr, dtype=torch.uint8, device=dev)
-    S.align_device_compact(sb, sc.data_ptr(), rec.data_ptr(), rb, st.data_ptr(), scr.data_ptr(),
-                           nscr)
-    torch.cuda.synchronize()
-    assert int(st.item()) == 0
-    del g, r, go, ro, d, scr
-    comp = S.expand_compact(b, sc.cpu().numpy(), rec.cpu().numpy(), rb)
-    del rec
-    assert np.array_equal(comp.scores, slot.scores)
-    assert np.array_equal(comp.read_aln, slot.read_aln)
-    assert np.array_equal(comp.genome_aln, slot.genome_aln)
-    k = b.k
-    ok = slot.scores <= k
-    assert 0.3 < ok.mean() < 1.0
-    # every slot: its string, then zeros; unreported candidates all zeros
-    ss = b.slot_starts()
-    cap = b.lengths.astype(np.int64) + k
-    rng = np.random.default_rng(1)
-    reads = b.reads.reshape(-1, b.m)
-    for i in rng.choice(b.n, 20_000, replace=False):
-        lo, hi = int(ss[i]), int(ss[i] + cap[i])
-        s = slot.read_aln[lo:hi]
-        gsl = slot.genome_aln[lo:hi]
-        nz = np.flatnonzero(s == 0)
-        n = int(nz[0]) if nz.size else hi - lo
-        assert not s[n:].any() and not gsl[n:].any()
-        if not ok[i]:
-            assert n == 0
-        if ok[i]:
-            letters = s[:n][s[:n] != ord("_")].tobytes()
-            assert reads[i].tobytes().endswith(letters)
-    # a sample against the oracle (each candidate behind its predecessor)
-    for i in rng.choice(np.arange(1, b.n), 300, replace=False):
-        pair, _ = sub_batch(b, [b""] * b.n, int(i) - 1, 2)
-        s1, ra1, ga1, _ = R.oracle_align(pair)
-        assert int(slot.scores[i]) == min(int(s1[1]), k + 1)
-        lo, hi = int(ss[i]), int(ss[i] + cap[i])
-        o = int(pair.slot_starts()[1])
-        assert np.array_equal(slot.read_aln[lo:hi], ra1[o:o + hi - lo])
-        assert np.array_equal(slot.genome_aln[lo:hi], ga1[o:o + hi - lo])
+    cfg = dict(bench.CONFIGS[name])
+    css = bench.build_callsets(cfg, 0)
+    assert sum(cs.n for cs in css) > 0
+    for cs in css:
+        align_and_check(cs, name)
+
+
+def test_full_size_serving_request_matches_the_oracle(saru_lib):
+    """The serving workload's largest request (500k reads, a quarter of
+    them in each length bin) as a reads-only request through the server:
+    every candidate of every call the server's filter made matches the
+    oracle, and the calls equal the device filter's own."""
+    import torch
+    from saruman_b200 import workloads as W
+    torch.cuda.set_device(0)
+    bench = load_bench()
+    cfg = dict(bench.CONFIGS["c5"])
+    g, _ = bench.build_genome(cfg)
+    sets = []
+    for i, m in enumerate(cfg["lengths"]):
+        rd = W.sample_reads(g, 125_000, m, cfg["rate"], seed=1000 + i, mix=cfg["mix"]).seqs
+        sets.append((rd, W.k_for(m), 0))
+    with S.Server(pipeline=True, budget_bytes=40 << 30) as srv:
+        srv.set_genome(g)
+        t = srv.submit_reads(sets)
+        rc, _ = srv.wait(t, 1_800_000)
+        assert rc == S.SARU_OK, S.last_error()
+        res = [srv.read_results(t, i) for i in range(len(sets))]
+        srv.release(t)
+    for (rd, k, _), r in zip(sets, res):
+        m = rd.shape[1]
+        cs = W.callset(g, rd, m, k, r["ids"], r["pos"], r["dirs"], r["call_begin"],
+                       r["call_strand"])
+        np.testing.assert_array_equal(cs.sbase, r["slot_begin"])
+        pad = np.zeros(64, np.uint8)
+        align_and_check(cs, f"c5-request-m{m}",
+                        outputs=(r["scores"], np.concatenate([r["read_aln"], pad]),
+                                 np.concatenate([r["genome_aln"], pad])))

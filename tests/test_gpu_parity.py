@@ -60,6 +60,26 @@ def test_legacy_entry_prints_reference_tsv(saru_lib, name):
     assert done == int((exp["scores"] <= b.k).sum())
 
 
+def test_legacy_entry_large_call_and_new_name_table(saru_lib):
+    """A call of 120k candidates (its lines formatted on several host
+    threads, written in candidate order) through the drop-in entry prints
+    the oracle writer's lines; a second call against another read_names
+    table prints that table's names."""
+    m, k, n, seed = 100, 5, 120_000, 77
+    r = subprocess.run([sys.executable, str(ROOT / "tests" / "legacy_big.py"), str(m), str(k),
+                        str(n), str(seed)], capture_output=True, check=True)
+    first, second = r.stdout.split(b"==== second call ====\n")
+    b = W.random_batch(m, k, n, seed=seed, err=0.05, alphabet=b"ACGTN")
+    s1, ra1, ga1, st = R.oracle_align(b, nthreads=8)
+    assert st == 0
+    n_ids = int(b.ids.max()) + 1
+    for out, tag in ((first, b"A"), (second, b"B")):
+        names = R.name_table([b"%s_read%d" % (tag, i) for i in range(n_ids)])
+        exp, st, _ = R.oracle_tsv(b, s1, ra1, ga1, names, read_length=m)
+        assert st == 0 and out == exp, tag
+    assert first.count(b"\n") == int((s1 <= k).sum()) > 30_000
+
+
 RANDOM = [(36, 2), (36, 3), (75, 5), (100, 5), (100, 6), (150, 9), (250, 15), (20, 1),
           (10, 0), (40, 7), (64, 15), (50, 10), (31, 10), (512, 15), (300, 12)]
 

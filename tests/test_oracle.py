@@ -87,3 +87,28 @@ def test_reference_threaded_driver_equals_serial():
     c = R.ref_align(b, strict=False, nthreads=8, chunk=64)
     for x, y in zip(a, c):
         np.testing.assert_array_equal(x, y)
+
+
+def test_whole_call_checker_agrees_with_the_oracle_and_finds_differences():
+    """saru_oracle_check (sub-calls led by their predecessor) accepts the
+    whole-call oracle's own outputs -- so the lead reproduces the row-0
+    walks into the previous matrix -- and counts every planted difference:
+    a score, a read-string byte, a window-string byte in a slot's zero tail."""
+    for m, k, n, seed in ((36, 2, 9000, 1), (100, 5, 5000, 2), (150, 9, 4500, 3),
+                          (250, 15, 2100, 4)):
+        b = W.random_batch(m, k, n, seed=seed, err=0.05, alphabet=b"ACGTN")
+        s1, ra1, ga1, st = R.oracle_align(b, nthreads=4)
+        assert st == 0
+        bad, first, cst = R.oracle_check(b, s1, ra1, ga1, nthreads=3)
+        assert (bad, first, cst) == (0, -1, 0), (m, k)
+        sc2, ra2, ga2 = s1.copy(), ra1.copy(), ga1.copy()
+        hit = [t for t in range(n) if s1[t] <= k]
+        t1, t2, t3 = hit[3], hit[len(hit) // 2], hit[-1]
+        sc2[t1] = (sc2[t1] + 1) % (k + 1)
+        slot2 = (int(b.genome_offsets[t2 - 1]) if t2 else 0) + k * t2
+        ra2[slot2 + 1] ^= 0x20
+        slot3 = (int(b.genome_offsets[t3 - 1]) if t3 else 0) + k * t3
+        L3 = int(b.genome_offsets[t3]) - (int(b.genome_offsets[t3 - 1]) if t3 else 0)
+        ga2[slot3 + L3 + k - 1] = ord("A")
+        bad, first, cst = R.oracle_check(b, sc2, ra2, ga2, nthreads=3)
+        assert (bad, first, cst) == (3, t1, 0), (m, k, bad, first)

@@ -188,10 +188,17 @@ def gather_case_on(g, m: int, k: int, nreads: int, seed: int):
 
 
 def test_server_resident_genome_requests(saru_lib):
-    """Gather requests against the resident genome give saru_align_host's
-    bytes for the host-built calls, mixed with window requests; a call with
-    m <= 3k is redone on the exact path from its gathered windows."""
-    g = W.uniform_genome(300_000, seed=40)
+    """Gather requests against the resident genome (kept 2 bits a base on
+    the device, its N runs and other non-ACGT bytes as exceptions) give
+    saru_align_host's bytes for the host-built calls, mixed with window
+    requests; a call with m <= 3k is redone on the exact path from its
+    gathered windows."""
+    g = W.uniform_genome(300_000, seed=40).copy()
+    g[1000:1010] = ord("N")
+    g[50_000:50_003] = ord("N")
+    g[120_000] = ord("R")
+    g[7919::7919] = ord("Y")
+    g[-3:] = ord("N")
     shapes = [(36, 3, 2000), (75, 5, 1500), (100, 6, 1200), (150, 9, 800), (12, 5, 300)]
     cases = [gather_case_on(g, m, k, n, seed=40 + 7 * i) for i, (m, k, n) in enumerate(shapes)]
     with S.Server(pipeline=True, max_requests_per_launch=8, budget_bytes=1 << 30) as srv:
@@ -299,3 +306,136 @@ def test_concurrent_clients(saru_lib):
     for h, w in zip(hrs, want):
         for i in range(len(w)):
             assert_same(h.result(i), w[i])
+
+
+# ---- reads-only requests: the filter inside the request path -------------
+
+def read_lines(res: dict, g: np.ndarray, reads: np.ndarray, m: int, k: int,
+               names: list[bytes]) -> list[bytes]:
+    """Every line the reference program prints for a reads-only request's
+    set: the writer's lines of each call, and the filter's perfect hits."""
+    cs = W.callset(g, reads, m, k, res["ids"], res["pos"], res["dirs"], res["call_begin"],
+                   res["call_strand"])
+    tab = S.name_table(names)
+    lines = []
+    for c in range(cs.ncalls):
+        b = cs.call(c)
+        a0, a1 = int(res["call_begin"][c]), int(res["call_begin"][c + 1])
+        s0, s1 = int(res["slot_begin"][c]), int(res["slot_begin"][c + 1])
+        if "records" in res:
+            rb = res["record_bytes"]
+            r = S.expand_compact(b, res["scores"][a0:a1], res["records"][a0 * rb:a1 * rb], rb)
+        else:
+            r = S.AlignResult(res["scores"][a0:a1], res["read_aln"][s0:s1],
+                              res["genome_aln"][s0:s1])
+        text, _, _ = S.format_tsv(b, r, tab, read_length=m)
+        lines += text.splitlines(keepends=True)
+    for rid, g1, st in zip(res["perfect_ids"], res["perfect_pos"], res["perfect_strand"]):
+        rd = reads[rid]
+        if st == 4:
+            rd = W.reverse_complement(rd[None])[0]
+        lines.append(b"%s\t%d\t%d\t%s\t%s\t%s\t0\n" % (
+            names[rid], g1, g1 - 1 + m, b"<<" if st == 4 else b">>", g[g1:g1 + m].tobytes(),
+            rd.tobytes()))
+    return lines
+
+
+def host_pipeline(g, reads, m, k, cv):
+    """The same reads through the device filter and saru_align_host call by
+    call (the pipeline the reference's strand daemons run)."""
+    with S.Filter(g, m, k) as f:
+        outs = [(dr, f.run(reads, dr, cv)) for dr in (0, 4)]
+    ids = np.concatenate([o.ids for _, o in outs])
+    pos = np.concatenate([o.pos for _, o in outs])
+    dirs = np.concatenate([o.dirs for _, o in outs])
+    cb, strand, off = [0], [], 0
+    for dr, o in outs:
+        cb.extend((o.call_begin[1:] + off).tolist())
+        strand += [dr] * (len(o.call_begin) - 1)
+        off += len(o.ids)
+    cs = W.callset(g, reads, m, k, ids, pos, dirs, np.asarray(cb), np.asarray(strand))
+    res = [S.align_host(cs.call(c)) for c in range(cs.ncalls)]
+    return cs, res
+
+
+def test_reads_only_requests_print_the_reference_output(saru_lib):
+    """A request of reads only (the drop-in dataset's reads) through the
+    server -- filter on both strands, calls, gather, alignment -- prints
+    exactly the reference program's output (SHA-256 of the sorted lines),
+    alone and in the middle of a mix of other reads-only requests of other
+    read lengths; every request's calls equal the device filter followed by
+    saru_align_host call by call."""
+    import hashlib
+    import json
+    from pathlib import Path
+    spec = json.loads((Path(__file__).resolve().parent / "golden" /
+                       "dropin_c1small.json").read_text())
+    g = W.uniform_genome(spec["genome_len"], seed=spec["genome_seed"])
+    m = spec["m"]
+    k = int(np.floor(m * spec["e"]))
+    reads = W.sample_reads(g, spec["reads"], m, spec["rate"], seed=spec["read_seed"]).seqs
+    cv = int(spec["args"][spec["args"].index("-s") + 1])
+    names = [b"r%d" % i for i in range(reads.shape[0])]
+    others = []
+    for i, (mo, ko, nr) in enumerate([(75, 5, 900), (100, 6, 1500), (36, 3, 3000),
+                                      (150, 9, 700)]):
+        rd = W.sample_reads(g, nr, mo, 0.03, seed=300 + i).seqs
+        others.append((rd, ko, 0))
+    for compact in (False, True):
+        with S.Server(pipeline=True, max_requests_per_launch=8, max_inflight=2,
+                      budget_bytes=2 << 30) as srv:
+            srv.set_genome(g)
+            t_alone = srv.submit_reads([(reads, k, cv)], compact=compact)
+            rc, _ = srv.wait(t_alone)
+            assert rc == S.SARU_OK, S.last_error()
+            alone_res = srv.read_results(t_alone, 0)
+            srv.release(t_alone)
+            # the same request in the middle of a mix (submitted at once)
+            ts = [srv.submit_reads([others[0], others[1]], compact=compact),
+                  srv.submit_reads([(reads, k, cv)], compact=compact),
+                  srv.submit_reads([others[2], others[3]], compact=compact)]
+            for t in ts:
+                rc, _ = srv.wait(t)
+                assert rc == S.SARU_OK, S.last_error()
+            mix_res = srv.read_results(ts[1], 0)
+            other_res = [srv.read_results(ts[0], 0), srv.read_results(ts[0], 1),
+                         srv.read_results(ts[2], 0), srv.read_results(ts[2], 1)]
+            for t in ts:
+                srv.release(t)
+        for key in alone_res:
+            np.testing.assert_array_equal(alone_res[key], mix_res[key], err_msg=key)
+        lines = sorted(read_lines(mix_res, g, reads, m, k, names))
+        assert len(lines) == spec["lines"]
+        assert hashlib.sha256(b"".join(lines)).hexdigest() == spec["sha256_sorted_stdout"]
+        for (rd, ko, _), res in zip(others, other_res):
+            mo = rd.shape[1]
+            cs, want = host_pipeline(g, rd, mo, ko, W.chunk_value_for(mo, ko))
+            np.testing.assert_array_equal(res["ids"], cs.ids)
+            np.testing.assert_array_equal(res["call_begin"], cs.call_begin)
+            for c in range(cs.ncalls):
+                a0, a1 = int(cs.call_begin[c]), int(cs.call_begin[c + 1])
+                s0, s1 = int(cs.sbase[c]), int(cs.sbase[c + 1])
+                np.testing.assert_array_equal(res["scores"][a0:a1], want[c].scores)
+                if compact:
+                    rb = res["record_bytes"]
+                    got = S.expand_compact(cs.call(c), res["scores"][a0:a1],
+                                           res["records"][a0 * rb:a1 * rb], rb)
+                    assert_same(got, want[c])
+                else:
+                    np.testing.assert_array_equal(res["read_aln"][s0:s1], want[c].read_aln)
+                    np.testing.assert_array_equal(res["genome_aln"][s0:s1], want[c].genome_aln)
+
+
+def test_reads_only_request_needs_a_genome_and_valid_sets(saru_lib):
+    with S.Server(pipeline=True, budget_bytes=1 << 28) as srv:
+        rd = np.frombuffer(b"ACGT" * 25, np.uint8).reshape(1, 100)
+        with pytest.raises(S.SaruError):
+            srv.submit_reads([(rd, 5, 0)])
+        srv.set_genome(W.uniform_genome(50_000, seed=2))
+        with pytest.raises(S.SaruError):
+            srv.submit_reads([(rd, 16, 0)])  # k > 15
+        t = srv.submit_reads([(np.zeros((0, 100), np.uint8), 5, 0)])  # nothing to align
+        rc, _ = srv.wait(t)
+        assert rc == S.SARU_OK
+        assert srv.read_results(t, 0)["ids"].size == 0
+        srv.release(t)

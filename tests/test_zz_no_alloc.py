@@ -56,8 +56,14 @@ def test_static_scratch_entry_matches_device_entry(saru_lib):
                                              C.c_void_p]
     stream = torch.cuda.current_stream()
     batches = [W.random_batch(100, 5, 20000, seed=41, err=0.04),
-               W.random_batch(150, 9, 7000, seed=42, err=0.05, alphabet=b"ACGTN")]
-    for b in batches:  # two calls in a row; the second sees the first's scratch contents
+               W.random_batch(150, 9, 7000, seed=42, err=0.05, alphabet=b"ACGTN"),
+               W.random_batch(512, 15, 10000, seed=43, err=0.03)]
+    # the widest reads: the full grid's decision planes (half the queued
+    # form's, which saru_scratch_bytes sizes) do not fit in the array, so
+    # the static entry runs on a reduced grid
+    b512 = batches[2]
+    assert (S.scratch_bytes(b512.n, b512.m, b512.k) - 256) // 2 > (32 << 20)
+    for b in batches:  # calls in a row; each sees the scratch contents the last one left
         sb, keep = _device_batch(b, dev)
         want_r, want = _outputs(b, dev)
         nscr = S.scratch_bytes(b.n, b.m, b.k)
