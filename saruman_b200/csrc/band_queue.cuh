@@ -11,8 +11,10 @@
 //   32 free slots (one per lane, the lane-th free slot of the warp's mask).
 //   A lane whose candidate does not survive frees its slot after the fill;
 //   a job frees its slot after its walk.
-// * Queue entries (8 bytes) sit in the warp's shared slice behind the
-//   staging and the region: the candidate index, its plane slot, so/eo and m.
+// * Queue entries (8 bytes: the candidate index, its plane slot, so/eo and
+//   m) are held in registers, two per lane (entries l and 32 + l); a fill
+//   appends its survivors by shuffles, a pass of 32 moves the upper half
+//   down.
 // * A walk writes the job's steps as a compact record (2 bits a step; the
 //   format of lane_traceback_ops): straight to the caller's records in
 //   compact mode, into the warp's region (strided by lane) in slot mode.
@@ -33,9 +35,7 @@
 
 namespace saru {
 
-constexpr int kQueueSlots = 64;          // plane slots per warp
-constexpr long kQueueEntryBytes = 8;     // one queued job
-constexpr long kQueueBytes = kQueueSlots * kQueueEntryBytes;
+constexpr int kQueueSlots = 64;  // plane slots per warp
 
 struct QEntry {
   int32_t t;      // candidate index in its segment's arrays
@@ -181,8 +181,7 @@ SARU_HD void expand_write(Word word, int n, int base, int lane, int col, int row
 }
 
 // Shared-memory slice of the queued form: [reads staging][windows staging]
-// [region: codes + masks during a fill, walked records during a pass]
-// [queue entries].
+// [region: codes + masks during a fill, walked records during a pass].
 SARU_HD SliceLayout queue_slice_layout(int max_m, int k) {
   SliceLayout L = slice_layout(max_m, k);
   const long code_words = (max_m + 7) / 8;
@@ -190,7 +189,7 @@ SARU_HD SliceLayout queue_slice_layout(int max_m, int k) {
   const long cm = 4L * 32 * (code_words + NCODES * mwords);
   const long rec = 4L * 32 * (1 + step_words(max_m, k));
   L.region_bytes = ((cm > rec ? cm : rec) + 15) & ~15L;
-  L.warp_smem = L.rs_bytes + L.ws_bytes + L.region_bytes + kQueueBytes;
+  L.warp_smem = L.rs_bytes + L.ws_bytes + L.region_bytes;
   return L;
 }
 

@@ -1,12 +1,17 @@
 // kernels.cu -- sm_100a kernels of the alignment stage.
 //
-//  saru_band_kernel           the production path: persistent warps over
+//  saru_band_queue_kernel     the production path: persistent warps over
 //                             32-candidate tiles (one lane per candidate),
 //                             bit-parallel banded fill (saru_core.cuh) with
-//                             2-bit traceback decisions, traceback and slot
-//                             strings or compact records on the device; a
+//                             2-bit traceback decisions; the candidates that
+//                             score <= k are queued and walked 32 at a time
+//                             (band_queue.cuh), slot strings expanded by the
+//                             whole warp or compact records written; a
 //                             launch covers segments (calls, or slices
 //                             [t0, t1) of one call) of 32- or 64-bit bands.
+//  saru_band_kernel           the per-tile form (each tile walked right
+//                             after its fill), behind the no-allocation
+//                             entry point.
 //  saru_full_fill_kernel      the exact full-rectangle path for inputs the
 //  saru_full_trace_kernel     banded kernel does not cover (other costs,
 //                             m <= 3k, k > 15, irregular windows): the
@@ -148,10 +153,11 @@ __device__ __forceinline__ void report_status(const Segment &g, int status) {
                            (status & 4 ? kStatusOverflow : 0));
 }
 
-// Per-warp state of the queued form.
+// Per-warp state of the queued form.  The queue is in registers: lane l
+// holds entries l (lo) and 32 + l (hi); at most 63 entries are queued.
 struct WarpQueue {
   uint8_t *st_reads, *st_win, *region;
-  QEntry *q;
+  QEntry lo, hi;
   long pstride, slot_base;
   uint64_t free_mask;
   int qn;
@@ -195,14 +201,24 @@ __device__ __forceinline__ void queue_fill(const KernelArgs &a, const Segment &g
     zero_range(ta.genome_aln, s.s_lo, s.s_hi, lane, z16);
   }
   const uint32_t mask = __ballot_sync(0xffffffffu, surv);
-  if (surv) {
-    const int rank = __popc(mask & ((1u << lane) - 1u));
-    w.q[w.qn + rank] = make_entry(t, slot, ls.c);
-  }
+  // the survivors, in lane order, become entries qn .. qn + popc(mask) - 1:
+  // each lane pulls the ones that land in its two registers
+  const QEntry mine = make_entry(t, slot, ls.c);
+  const int ns = __popc(mask);
+  const int r_lo = lane - w.qn, r_hi = 32 + lane - w.qn;
+  const bool in_lo = r_lo >= 0 && r_lo < ns, in_hi = r_hi >= 0 && r_hi < ns;
+  const int src_lo = in_lo ? nth_set_bit(mask, r_lo) : lane;
+  const int src_hi = in_hi ? nth_set_bit(mask, r_hi) : lane;
+  const int32_t t_lo = __shfl_sync(0xffffffffu, mine.t, src_lo);
+  const uint32_t i_lo = __shfl_sync(0xffffffffu, mine.info, src_lo);
+  const int32_t t_hi = __shfl_sync(0xffffffffu, mine.t, src_hi);
+  const uint32_t i_hi = __shfl_sync(0xffffffffu, mine.info, src_hi);
+  if (in_lo) w.lo = QEntry{t_lo, i_lo};
+  if (in_hi) w.hi = QEntry{t_hi, i_hi};
   const uint32_t lo = __reduce_or_sync(0xffffffffu, surv && slot < 32 ? 1u << slot : 0u);
   const uint32_t hi = __reduce_or_sync(0xffffffffu, surv && slot >= 32 ? 1u << (slot - 32) : 0u);
   w.free_mask &= ~((uint64_t)lo | ((uint64_t)hi << 32));
-  w.qn += __popc(mask);
+  w.qn += ns;
   __syncwarp();
   report_status(g, st);
 }
@@ -215,8 +231,7 @@ __device__ __forceinline__ void queue_walk(const KernelArgs &a, const Segment &g
                                            WarpQueue &w, int lane) {
   __syncwarp();
   const bool act = lane < cnt;
-  QEntry e{0, 0};
-  if (act) e = w.q[lane];
+  const QEntry e = act ? w.lo : QEntry{0, 0};
   const Cand c = entry_cand(e, g.k, g.first_of_call);
   const int slot = entry_slot(e);
   const long pslot = w.slot_base + slot;
@@ -274,12 +289,10 @@ __device__ __forceinline__ void queue_walk(const KernelArgs &a, const Segment &g
   const uint32_t lo = __reduce_or_sync(0xffffffffu, act && slot < 32 ? 1u << slot : 0u);
   const uint32_t hi = __reduce_or_sync(0xffffffffu, act && slot >= 32 ? 1u << (slot - 32) : 0u);
   w.free_mask |= (uint64_t)lo | ((uint64_t)hi << 32);
-  const int rest = w.qn - cnt;
-  QEntry mv{0, 0};
-  if (lane < rest) mv = w.q[cnt + lane];
-  __syncwarp();
-  if (lane < rest) w.q[lane] = mv;
-  w.qn = rest;
+  // a pass takes 32 jobs (the rest, in the hi registers, move down) or all
+  // of them (a flush); no other counts occur
+  if (cnt == 32) w.lo = w.hi;
+  w.qn -= cnt;
   __syncwarp();
   report_status(g, we.bad ? 4 : 0);
 }
@@ -307,7 +320,8 @@ __global__ void __launch_bounds__(128, 4) saru_band_queue_kernel(const __grid_co
   w.st_reads = ws;
   w.st_win = ws + a.rs_bytes;
   w.region = w.st_win + a.ws_bytes;
-  w.q = reinterpret_cast<QEntry *>(w.region + a.region_bytes);
+  w.lo = QEntry{0, 0};
+  w.hi = QEntry{0, 0};
   const long gwarp = (long)blockIdx.x * WARPS + wid;
   w.pstride = (long)gridDim.x * WARPS * kQueueSlots;
   w.slot_base = gwarp * kQueueSlots;

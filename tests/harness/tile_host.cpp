@@ -305,11 +305,11 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
     w.st_reads = (uint8_t *)aligned_alloc(16, (size_t)S.rs_bytes);
     w.st_win = (uint8_t *)aligned_alloc(16, (size_t)S.ws_bytes);
     w.region = (uint8_t *)aligned_alloc(16, (size_t)S.region_bytes);
-    w.q = (QEntry *)aligned_alloc(16, (size_t)kQueueBytes);
+    w.q = (QEntry *)aligned_alloc(16, sizeof(QEntry) * kQueueSlots);  // the kernel's registers
     memset(w.st_reads, 0xA5, (size_t)S.rs_bytes);
     memset(w.st_win, 0xA5, (size_t)S.ws_bytes);
     memset(w.region, 0xA5, (size_t)S.region_bytes);
-    memset(w.q, 0xA5, (size_t)kQueueBytes);
+    memset(w.q, 0xA5, sizeof(QEntry) * kQueueSlots);
   }
   auto targs = [&](int si) {
     const QSeg &g = segs[si];
@@ -374,6 +374,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
       }
       for (int lane = 0; lane < cnt; ++lane) w.free_mask |= 1ull << entry_slot(e[lane]);
       const int rest = w.qn - cnt;
+      if (cnt != 32 && rest != 0) abort();  // the kernel's register queue needs one or the other
       for (int lane = 0; lane < rest; ++lane) w.q[lane] = w.q[cnt + lane];
       w.qn = rest;
     };
