@@ -204,6 +204,10 @@ typedef struct {
   int32_t warps_per_cta; /* 1..4: alignments per CTA = 32 x warps */
   int32_t ctas_per_sm;   /* cap on resident CTAs per SM */
   int32_t word_bits;     /* 64: 64-bit band words for k <= 7 too; 32 only for k <= 7 */
+  int32_t walks;         /* when the traceback walks run: 0 the library's default; 1 queued
+                            (a warp walks 32 queued candidates at a time); 2 right after each
+                            tile's fill (strings expanded by the whole warp); 3 per tile with
+                            each lane writing its strings */
 } saru_tuning;
 int saru_tuning_set(int32_t read_length, int32_t k, const saru_tuning *t); /* NULL: remove */
 int saru_tuning_get(int32_t read_length, int32_t k, saru_tuning *t);       /* 1 if set */

@@ -110,10 +110,11 @@ SARU_HD void zero_range(uint8_t *dst, long lo, long hi, int lane, Store16Zero st
 }
 
 // The walk of one job into a compact record: store(w, v) receives words
-// 1.. (2-bit steps, 16 a word, traceback order) and word 0 (step count,
-// bit 16 set if the walk left its band or slot).  Returns where it ended.
+// 1.. (2-bit steps, 16 a word, traceback order), zeros up to word
+// `pad_words` - 1 (0: no padding), and word 0 (step count, bit 16 set if
+// the walk left its band or slot).  Returns where it ended.
 template <typename T, class LoadPair, class StoreWord>
-SARU_HD WalkEnd walk_record(const Cand &c, LoadPair ld, StoreWord store) {
+SARU_HD WalkEnd walk_record(const Cand &c, LoadPair ld, StoreWord store, int pad_words = 0) {
   uint32_t acc = 0;
   int sh = 0, w = 1;
   const WalkEnd e = lane_walk<T>(c, ld, [&](int, uint32_t op, int, int) {
@@ -125,10 +126,16 @@ SARU_HD WalkEnd walk_record(const Cand &c, LoadPair ld, StoreWord store) {
       sh = 0;
     }
   });
-  if (sh) store(w, acc);
+  if (sh) store(w++, acc);
+  for (; w < pad_words; ++w) store(w, 0u);
   store(0, (uint32_t)e.n | (e.bad ? 0x10000u : 0u));
   return e;
 }
+
+// Words between walked records in the warp's region: record j at word
+// j * stride.  Odd, so the lanes writing the same word of their records
+// hit different banks, and the words of one record are in different banks.
+SARU_HD int rec_stride(int max_m, int k) { return (int)(1 + step_words(max_m, k)) | 1; }
 
 // Cooperative expansion of one walked job into its slot strings, round by
 // round (a round covers 128 string positions, 4 per lane).  Positions are
@@ -187,7 +194,7 @@ SARU_HD SliceLayout queue_slice_layout(int max_m, int k) {
   const long code_words = (max_m + 7) / 8;
   const long mwords = mask_words(k, max_m + 2 * k);
   const long cm = 4L * 32 * (code_words + NCODES * mwords);
-  const long rec = 4L * 32 * (1 + step_words(max_m, k));
+  const long rec = 4L * 32 * rec_stride(max_m, k);
   L.region_bytes = ((cm > rec ? cm : rec) + 15) & ~15L;
   L.warp_smem = L.rs_bytes + L.ws_bytes + L.region_bytes;
   return L;

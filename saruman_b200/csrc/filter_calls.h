@@ -87,9 +87,9 @@ class CallAssembler {
 
   void flush() {
     const int64_t before = (int64_t)out.ids.size();
-    out.ids.reserve(out.ids.size() + pos_.size());
-    out.pos.reserve(out.pos.size() + pos_.size());
-    out.dirs.reserve(out.dirs.size() + pos_.size());
+    // (no reserve of size() + pending here: an exact reserve at every flush
+    // reallocates and copies every earlier candidate; push_back grows
+    // geometrically)
     size_t keep = 0, kept_values = 0;
     for (size_t e = 0; e < entries_.size(); ++e) {
       const Entry E = entries_[e];

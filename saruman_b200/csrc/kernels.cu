@@ -159,6 +159,7 @@ struct WarpQueue {
   uint8_t *st_reads, *st_win, *region;
   QEntry lo, hi;
   long pstride, slot_base;
+  long r_base, g_base;  // staging bases of the last tile filled
   uint64_t free_mask;
   int qn;
 };
@@ -181,6 +182,8 @@ __device__ __forceinline__ void queue_fill(const KernelArgs &a, const Segment &g
   auto ld1 = [](const uint8_t *gp) -> uint8_t { return __ldg(gp); };
   stage_in(w.st_reads, ta.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
   stage_in(w.st_win, ta.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
+  w.r_base = s.r_base;
+  w.g_base = s.g_base;
   __syncwarp();
   PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(a.planes);
   const int slot = fill_slot(w.free_mask, lane);
@@ -193,8 +196,11 @@ __device__ __forceinline__ void queue_fill(const KernelArgs &a, const Segment &g
                         });
   const long t = s.t0 + lane;
   const bool surv = t < ta.n && ls.ok && ls.score <= ta.k;
-  if (ta.records) {
-    if (t < ta.n && !surv) *reinterpret_cast<uint32_t *>(ta.records + t * ta.rec_bytes) = 0u;
+  if (ta.records) {  // a record of zeros (step count 0) for every other candidate
+    if (t < ta.n && !surv) {
+      uint32_t *rec = reinterpret_cast<uint32_t *>(ta.records + t * ta.rec_bytes);
+      for (long wd = 0; wd < ta.rec_bytes / 4; ++wd) rec[wd] = 0u;
+    }
   } else {
     auto z16 = [](uint8_t *gp) { *reinterpret_cast<uint4 *>(gp) = make_uint4(0, 0, 0, 0); };
     zero_range(ta.read_aln, s.s_lo, s.s_hi, lane, z16);
@@ -239,13 +245,15 @@ __device__ __forceinline__ void queue_walk(const KernelArgs &a, const Segment &g
   const PlanePair<T> *planes = reinterpret_cast<const PlanePair<T> *>(a.planes);
   auto ld = [&](int j) { return planes[plane_index(j, w.pstride, pslot, mul)]; };
   uint32_t *region32 = reinterpret_cast<uint32_t *>(w.region);
+  const int rstride = rec_stride(g.max_m, g.k);
   WalkEnd we{0, 0, 0, false};
   if (act) {
-    if (g.records) {
+    if (g.records) {  // every word of the record written: the same bytes whatever ran before
       uint32_t *rec = reinterpret_cast<uint32_t *>(g.records + (long)e.t * g.rec_bytes);
-      we = walk_record<T>(c, ld, [&](int wd, uint32_t v) { rec[wd] = v; });
+      we = walk_record<T>(c, ld, [&](int wd, uint32_t v) { rec[wd] = v; },
+                          (int)(g.rec_bytes / 4));
     } else {
-      we = walk_record<T>(c, ld, [&](int wd, uint32_t v) { region32[wd * 32 + lane] = v; });
+      we = walk_record<T>(c, ld, [&](int wd, uint32_t v) { region32[lane * rstride + wd] = v; });
     }
   }
   __syncwarp();
@@ -258,11 +266,14 @@ __device__ __forceinline__ void queue_walk(const KernelArgs &a, const Segment &g
       const long gs = t ? g.goff[t - 1] : 0;
       const long rs = t ? g.roff[t - 1] : 0;
       const long slot0 = gs + (long)g.k * t;
-      const uint8_t *rd = g.reads + rs;
-      const uint8_t *wn = g.genome + gs;
+      // the immediate form walks the tile it just filled: its bytes are
+      // still staged; queued jobs may be of earlier tiles
+      const bool staged = a.form == kFormImmediate;
+      const uint8_t *rd = staged ? w.st_reads + (rs - w.r_base) : g.reads + rs;
+      const uint8_t *wn = staged ? w.st_win + (gs - w.g_base) : g.genome + gs;
       uint8_t *o_r = g.read_aln + slot0;
       uint8_t *o_g = g.genome_aln + slot0;
-      auto word = [&](int wd) { return region32[wd * 32 + j]; };
+      auto word = [&](int wd) { return region32[j * rstride + wd]; };
       int cc = 0, rr = 0;  // advances of the rounds before
       for (int base = 0; base < n; base += 128) {
         const uint32_t adv = expand_advance(word, n, base, lane);
@@ -275,8 +286,9 @@ __device__ __forceinline__ void queue_walk(const KernelArgs &a, const Segment &g
         const uint32_t excl = incl - adv;
         const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
         expand_write(word, n, base, lane, col0 + cc + (int)(excl & 0xFFFFu),
-                     row0 + rr + (int)(excl >> 16), [&](int i) { return __ldg(rd + i); },
-                     [&](int i) { return __ldg(wn + i); },
+                     row0 + rr + (int)(excl >> 16),
+                     [&](int i) { return staged ? rd[i] : __ldg(rd + i); },
+                     [&](int i) { return staged ? wn[i] : __ldg(wn + i); },
                      [&](int p, uint8_t x, uint8_t y) {
                        o_r[p] = x;
                        o_g[p] = y;
@@ -323,9 +335,12 @@ __global__ void __launch_bounds__(128, 4) saru_band_queue_kernel(const __grid_co
   w.lo = QEntry{0, 0};
   w.hi = QEntry{0, 0};
   const long gwarp = (long)blockIdx.x * WARPS + wid;
-  w.pstride = (long)gridDim.x * WARPS * kQueueSlots;
-  w.slot_base = gwarp * kQueueSlots;
-  w.free_mask = ~0ull;
+  const int slots = form_slots(a.form);
+  const int walk_at = a.form == kFormQueued ? 32 : 1;  // queued jobs that start a pass
+  w.pstride = (long)gridDim.x * WARPS * slots;
+  w.slot_base = gwarp * slots;
+  w.free_mask = slots == 64 ? ~0ull : 0xFFFFFFFFull;
+  w.r_base = w.g_base = 0;
   w.qn = 0;
   int qseg = -1;
   auto walk = [&](int cnt) {
@@ -334,8 +349,8 @@ __global__ void __launch_bounds__(128, 4) saru_band_queue_kernel(const __grid_co
     else queue_walk<uint32_t>(a, g, cnt, w, lane);
   };
   for (;;) {
-    if (w.qn >= 32) {
-      walk(32);
+    if (w.qn >= walk_at) {  // a pass takes 32 jobs, or all when fewer are queued
+      walk(w.qn >= 32 ? 32 : w.qn);
       continue;
     }
     int tile = 0;
@@ -470,8 +485,8 @@ __global__ void saru_full_trace_kernel(FullArgs a) {
 
 constexpr long kMaxCtaSmem = 227 * 1024;  // opt-in shared memory per block on sm_100
 
-BandLayout band_layout(int max_m, int k, int warps_req, bool queue) {
-  const SliceLayout S = queue ? queue_slice_layout(max_m, k) : slice_layout(max_m, k);
+BandLayout band_layout(int max_m, int k, int warps_req, int form) {
+  const SliceLayout S = form != kFormTile ? queue_slice_layout(max_m, k) : slice_layout(max_m, k);
   BandLayout L;
   L.rs_bytes = S.rs_bytes;
   L.ws_bytes = S.ws_bytes;
@@ -504,13 +519,14 @@ cudaError_t allow_smem(int which, const void *fn) {
 }  // namespace
 
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
-  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req, a.queue != 0);
+  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req, a.form);
   if (L.warps < 1 || a.nseg < 1 || a.nseg > kMaxSegs) return cudaErrorInvalidValue;
+  const bool queued = a.form != kFormTile;
   // allow the largest slice once per device; each launch asks for its own
   // size (a per-launch attribute would race between concurrent callers)
-  const void *fn = a.queue ? reinterpret_cast<const void *>(saru_band_queue_kernel)
-                           : reinterpret_cast<const void *>(saru_band_kernel);
-  cudaError_t e = allow_smem(a.queue ? 1 : 0, fn);
+  const void *fn = queued ? reinterpret_cast<const void *>(saru_band_queue_kernel)
+                          : reinterpret_cast<const void *>(saru_band_kernel);
+  cudaError_t e = allow_smem(queued ? 1 : 0, fn);
   if (e != cudaSuccess) return e;
   a.rs_bytes = L.rs_bytes;
   a.ws_bytes = L.ws_bytes;
@@ -518,7 +534,7 @@ cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
   a.region_bytes = L.region_bytes;
   e = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  if (a.queue) saru_band_queue_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
+  if (queued) saru_band_queue_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
   else saru_band_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
   return cudaGetLastError();
 }
@@ -534,9 +550,9 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_c
   return tiles < g ? (tiles > 0 ? tiles : 1) : g;
 }
 
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req, bool queue) {
-  const BandLayout L = band_layout(max_m, k, warps_req, queue);
-  const size_t slots = queue ? kQueueSlots : 32;  // plane slots per warp
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req, int form) {
+  const BandLayout L = band_layout(max_m, k, warps_req, form);
+  const size_t slots = (size_t)form_slots(form);  // plane slots per warp
   return kCounterBytes + (size_t)grid * slots * (L.warps > 0 ? L.warps : 1) * 2 *
                              (size_t)plane_columns(max_m) * (wide ? 8 : 4);
 }

@@ -104,11 +104,16 @@ struct ReadSetOut {
   std::vector<int8_t> call_strand;
   std::vector<int32_t> ids, pos, goff, rindex, scores;
   std::vector<int8_t> dirs;
-  std::vector<char> ra, ga;
-  std::vector<uint8_t> records;
+  // outputs, written whole by the copies out (not zero-filled first: for a
+  // large request that costs as much as the copy)
+  std::unique_ptr<char[]> ra, ga;
+  std::unique_ptr<uint8_t[]> records;
   int64_t rec_bytes = 0;
   std::vector<int32_t> perfect_ids, perfect_pos;
   std::vector<int8_t> perfect_strand;
+  std::vector<saru_gather_call> gcalls;  // this set's calls
+  std::vector<saru_result> results;
+  int rc = SARU_OK;
 };
 
 struct Request {
@@ -299,25 +304,27 @@ struct saru_server {
       g.read_length = m;
       g.genome_bytes = acc;
       g.total_slots = acc + (int64_t)k * (b - a);
-      r.gcalls.push_back(g);
+      o.gcalls.push_back(g);
     }
     if (r.compact) {
       o.rec_bytes = saru_compact_record_bytes(m, k);
-      o.records.assign(n * (size_t)o.rec_bytes, 0);
+      o.records.reset(new uint8_t[n * (size_t)o.rec_bytes + 64]);
     } else {
-      o.ra.assign((size_t)slots + 64, 0);
-      o.ga.assign((size_t)slots + 64, 0);
+      o.ra.reset(new char[(size_t)slots + 64]);
+      o.ga.reset(new char[(size_t)slots + 64]);
+      memset(o.ra.get() + slots, 0, 64);
+      memset(o.ga.get() + slots, 0, 64);
     }
     for (size_t c = 0; c < ncalls; ++c) {
       const int64_t a = o.call_begin[c];
       saru_result res{o.scores.data() + a, nullptr, nullptr, nullptr};
       if (r.compact) {
-        res.read_aln = reinterpret_cast<char *>(o.records.data() + a * o.rec_bytes);
+        res.read_aln = reinterpret_cast<char *>(o.records.get() + a * o.rec_bytes);
       } else {
-        res.read_aln = o.ra.data() + o.slot_begin[c];
-        res.genome_aln = o.ga.data() + o.slot_begin[c];
+        res.read_aln = o.ra.get() + o.slot_begin[c];
+        res.genome_aln = o.ga.get() + o.slot_begin[c];
       }
-      r.results.push_back(res);
+      o.results.push_back(res);
     }
     return SARU_OK;
   }
@@ -337,8 +344,31 @@ struct saru_server {
         filter_q.pop_front();
       }
       int rc = SARU_OK;
-      for (auto &o : r->rsets)
-        if ((rc = filter_set(*r, o))) break;
+      // the sets' filters (one per read length and k) run at once, each on
+      // its own stream; sets sharing a filter run one after the other
+      std::vector<std::pair<int, int>> keys;
+      for (auto &o : r->rsets) {
+        const std::pair<int, int> key(o.set.read_length, o.set.k);
+        if (!filter_for(key.first, key.second)) rc = SARU_E_INVALID;
+        if (std::find(keys.begin(), keys.end(), key) == keys.end()) keys.push_back(key);
+      }
+      if (!rc) {
+        std::vector<std::thread> th;
+        for (const auto &key : keys)
+          th.emplace_back([this, &r, key] {
+            cudaSetDevice(cfg.device);
+            for (auto &o : r->rsets)
+              if (o.set.read_length == key.first && o.set.k == key.second && !o.rc)
+                o.rc = filter_set(*r, o);
+          });
+        for (auto &t : th) t.join();
+        for (auto &o : r->rsets)
+          if (!rc && o.rc) rc = o.rc;
+      }
+      for (auto &o : r->rsets) {
+        r->gcalls.insert(r->gcalls.end(), o.gcalls.begin(), o.gcalls.end());
+        r->results.insert(r->results.end(), o.results.begin(), o.results.end());
+      }
       if (!rc && r->gcalls.size() > (size_t)SARU_MAX_CALLS) {
         saru::set_last_error("reads-only request: more than SARU_MAX_CALLS calls");
         rc = SARU_E_INVALID;
@@ -743,9 +773,9 @@ int saru_server_read_results(saru_server *s, int64_t ticket, int32_t set,
   out->pos = o.pos.data();
   out->dirs = o.dirs.data();
   out->scores = o.scores.data();
-  out->read_aln = o.ra.empty() ? nullptr : o.ra.data();
-  out->genome_aln = o.ga.empty() ? nullptr : o.ga.data();
-  out->records = o.records.empty() ? nullptr : o.records.data();
+  out->read_aln = o.ra.get();
+  out->genome_aln = o.ga.get();
+  out->records = o.records.get();
   out->record_bytes = o.rec_bytes;
   out->perfect_ids = o.perfect_ids.data();
   out->perfect_pos = o.perfect_pos.data();

@@ -275,7 +275,12 @@ struct QSeg {
   int k, max_m, first_of_call, wide;
 };
 
-extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
+// form: 1 queued (64 plane slots, a pass at 32 queued jobs, characters read
+// from global memory), 2 immediate (32 slots, each tile's survivors walked
+// right after its fill, characters read from the staged inputs).
+extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total, int form) {
+  const int slots = form == 1 ? 64 : 32;
+  const int walk_at = form == 1 ? 32 : 1;
   int max_m = 0, max_k = 0, wide_any = 0;
   std::vector<long> tile_begin(nseg);
   long tiles = 0;
@@ -287,7 +292,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
     wide_any |= segs[i].wide;
   }
   const SliceLayout S = queue_slice_layout(max_m, max_k);
-  const long pstride = (long)nwarps_total * kQueueSlots;
+  const long pstride = (long)nwarps_total * slots;
   std::vector<uint8_t> planes_v((size_t)plane_columns(max_m) * pstride * 2 * (wide_any ? 8 : 4));
   int status = 0;
   auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
@@ -296,7 +301,8 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
   struct Warp {
     uint8_t *st_reads, *st_win, *region;
     QEntry *q;
-    uint64_t free_mask = ~0ull;
+    uint64_t free_mask = 0;
+    long r_base = 0, g_base = 0;
     int qn = 0, qseg = -1;
     bool done = false;
   };
@@ -310,6 +316,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
     memset(w.st_win, 0xA5, (size_t)S.ws_bytes);
     memset(w.region, 0xA5, (size_t)S.region_bytes);
     memset(w.q, 0xA5, sizeof(QEntry) * kQueueSlots);
+    w.free_mask = slots == 64 ? ~0ull : 0xFFFFFFFFull;
   }
   auto targs = [&](int si) {
     const QSeg &g = segs[si];
@@ -323,6 +330,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
     const QSeg &g = segs[w.qseg];
     const TileArgs a = targs(w.qseg);
     uint32_t *region32 = reinterpret_cast<uint32_t *>(w.region);
+    const int rstride = rec_stride(g.max_m, g.k);
     auto body = [&](auto tag) {
       using T = decltype(tag);
       const PlanePair<T> *planes = reinterpret_cast<const PlanePair<T> *>(planes_v.data());
@@ -333,14 +341,15 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
         if (lane >= cnt) continue;
         e[lane] = w.q[lane];
         const Cand c = entry_cand(e[lane], g.k, g.first_of_call);
-        const long pslot = (long)gw * kQueueSlots + entry_slot(e[lane]);
+        const long pslot = (long)gw * slots + entry_slot(e[lane]);
         auto ld = [&](int j) { return planes[plane_index(j, pstride, pslot, a.pair_mul)]; };
         if (g.records) {
           uint32_t *rec = reinterpret_cast<uint32_t *>(g.records + (long)e[lane].t * g.rec_bytes);
-          we[lane] = walk_record<T>(c, ld, [&](int wd, uint32_t v) { rec[wd] = v; });
+          we[lane] = walk_record<T>(c, ld, [&](int wd, uint32_t v) { rec[wd] = v; },
+                                    (int)(g.rec_bytes / 4));
         } else {
           we[lane] = walk_record<T>(c, ld, [&](int wd, uint32_t v) {
-            region32[wd * 32 + lane] = v;
+            region32[lane * rstride + wd] = v;
           });
         }
         if (we[lane].bad) status |= 4;
@@ -350,7 +359,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
           const long t = e[j].t;
           const long gs = t ? g.goff[t - 1] : 0, rs = t ? g.roff[t - 1] : 0;
           const long slot0 = gs + (long)g.k * t;
-          auto word = [&](int wd) { return region32[wd * 32 + j]; };
+          auto word = [&](int wd) { return region32[j * rstride + wd]; };
           int cc = 0, rr = 0;
           for (int base = 0; base < we[j].n; base += 128) {
             uint32_t adv[32], incl = 0;
@@ -360,8 +369,12 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
               incl += adv[lane];
               expand_write(word, we[j].n, base, lane, we[j].col + cc + (int)(excl & 0xFFFFu),
                            we[j].row + rr + (int)(excl >> 16),
-                           [&](int i) { return g.reads[rs + i]; },
-                           [&](int i) { return g.genome[gs + i]; },
+                           [&](int i) {
+                             return form == 2 ? w.st_reads[rs - w.r_base + i] : g.reads[rs + i];
+                           },
+                           [&](int i) {
+                             return form == 2 ? w.st_win[gs - w.g_base + i] : g.genome[gs + i];
+                           },
                            [&](int p, uint8_t x, uint8_t y) {
                              g.ra[slot0 + p] = x;
                              g.ga[slot0 + p] = y;
@@ -398,12 +411,14 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
         stage_in(w.st_reads, a.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
         stage_in(w.st_win, a.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
       }
+      w.r_base = s.r_base;
+      w.g_base = s.g_base;
       int slot[32];
       bool surv[32];
       LaneState ls[32];
       for (int lane = 0; lane < 32; ++lane) {
         slot[lane] = fill_slot(w.free_mask, lane);
-        const long pslot = (long)gw * kQueueSlots + slot[lane];
+        const long pslot = (long)gw * slots + slot[lane];
         status |= lane_fill<T>(a, s, lane, w.st_reads, w.st_win,
                                reinterpret_cast<uint32_t *>(w.region), ls[lane],
                                [&](int j, T A, T B) {
@@ -413,7 +428,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
         const long t = s.t0 + lane;
         surv[lane] = t < a.n && ls[lane].ok && ls[lane].score <= a.k;
         if (a.records && t < a.n && !surv[lane])
-          *reinterpret_cast<uint32_t *>(a.records + t * a.rec_bytes) = 0u;
+          memset(a.records + t * a.rec_bytes, 0, (size_t)a.rec_bytes);
       }
       if (!a.records)
         for (int lane = 0; lane < 32; ++lane) {
@@ -422,7 +437,7 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
         }
       for (int lane = 0; lane < 32; ++lane) {
         if (!surv[lane]) continue;
-        if (w.qn >= kQueueSlots || !((w.free_mask >> slot[lane]) & 1u)) abort();
+        if (w.qn >= slots || slot[lane] >= slots || !((w.free_mask >> slot[lane]) & 1u)) abort();
         w.q[w.qn++] = make_entry(s.t0 + lane, slot[lane], ls[lane].c);
         w.free_mask &= ~(1ull << slot[lane]);
       }
@@ -434,8 +449,8 @@ extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total) {
     for (int gw = 0; gw < nwarps_total; ++gw) {
       Warp &w = W[gw];
       if (w.done) continue;
-      if (w.qn >= 32) {
-        walk(w, gw, 32);
+      if (w.qn >= walk_at) {
+        walk(w, gw, w.qn >= 32 ? 32 : w.qn);
         continue;
       }
       const long tile = counter++;

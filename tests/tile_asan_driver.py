@@ -156,6 +156,10 @@ class QSeg(C.Structure):
 
 
 def queue_cases(lib) -> int:
+    return sum(queue_cases_form(lib, form) for form in (1, 2))
+
+
+def queue_cases_form(lib, form: int) -> int:
     """The queued form (walks of 32 queued jobs, cooperative expansion of
     the slot strings): single calls at misalignments, compact records, a
     call in slices, and a launch of mixed calls and band widths, with few
@@ -187,32 +191,32 @@ def queue_cases(lib) -> int:
 
         for off, nw in ((0, 1), (3, 2), (9, 7)):
             q, sc, ra, ga = seg(off)
-            st = lib.tile_align_queue(C.byref(q), 1, nw)
+            st = lib.tile_align_queue(C.byref(q), 1, nw, form)
             if not (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
                     and np.array_equal(ra1, ra) and np.array_equal(ga1, ga)):
                 bad += 1
-                print("QUEUE MISMATCH", m, k, off, nw, st, flush=True)
+                print("QUEUE MISMATCH", form, m, k, off, nw, st, flush=True)
         # compact records
         rb = S.compact_record_bytes(m, k)
         rec = exact(np.zeros(b.n * rb, np.uint8), 0)
         q, sc, _, _ = seg(4, rec, rb)
-        st = lib.tile_align_queue(C.byref(q), 1, 3)
+        st = lib.tile_align_queue(C.byref(q), 1, 3, form)
         out = S.expand_compact(b, sc, rec, rb, nthreads=2)
         if not (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
                 and np.array_equal(ra1, out.read_aln) and np.array_equal(ga1, out.genome_aln)):
             bad += 1
-            print("QUEUE COMPACT MISMATCH", m, k, st, flush=True)
+            print("QUEUE COMPACT MISMATCH", form, m, k, st, flush=True)
         # slices [t0, t1) of the call, the same output arrays
         q0, sc, ra, ga = seg(6)
         st = 0
         for t0 in range(0, b.n, 64):
             q = QSeg(*[getattr(q0, f) for f, _ in QSeg._fields_])
             q.t0, q.n = t0, min(b.n, t0 + 64)
-            st |= lib.tile_align_queue(C.byref(q), 1, 2)
+            st |= lib.tile_align_queue(C.byref(q), 1, 2, form)
         if not (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
                 and np.array_equal(ra1, ra) and np.array_equal(ga1, ga)):
             bad += 1
-            print("QUEUE SLICE MISMATCH", m, k, st, flush=True)
+            print("QUEUE SLICE MISMATCH", form, m, k, st, flush=True)
     # mixed calls in one launch, both band widths, slots and compact records
     specs = [(36, 3, 300), (75, 5, 200), (100, 6, 250), (150, 9, 120), (250, 15, 40), (40, 2, 33)]
     for nw in (1, 4):
@@ -238,7 +242,7 @@ def queue_cases(lib) -> int:
             outs.append((b, sc, ra, ga, rec, rb))
         order = sorted(range(len(specs)), key=lambda i: -(specs[i][0] * (specs[i][1] + 1)))
         arr = (QSeg * len(segs))(*[segs[i] for i in order])
-        st = lib.tile_align_queue(arr, len(segs), nw)
+        st = lib.tile_align_queue(arr, len(segs), nw, form)
         bad += 1 if st else 0
         for b, sc, ra, ga, rec, rb in outs:
             s1, ra1, ga1, _ = R.oracle_align(b, nthreads=4)
@@ -247,7 +251,7 @@ def queue_cases(lib) -> int:
                 ra, ga = out.read_aln, out.genome_aln
             if not (np.array_equal(np.minimum(s1, b.k + 1), sc) and np.array_equal(ra1, ra)
                     and np.array_equal(ga1, ga)):
-                print("QUEUE MULTI MISMATCH", b.m, b.k, nw, flush=True)
+                print("QUEUE MULTI MISMATCH", form, b.m, b.k, nw, flush=True)
                 bad += 1
     return bad
 
