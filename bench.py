@@ -1062,8 +1062,7 @@ def main() -> None:
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--shape", default=None,
-                    help="W,C,B[,WALKS]: install this launch shape (and kernel form) for every "
-                         "bin instead of tuning")
+                    help="W,C,B: install this launch shape for every bin instead of tuning")
     ap.add_argument("--requests", type=int, default=None,
                     help="requests in the serving trace (c5)")
     ap.add_argument("--reads", type=int, default=None,

@@ -175,10 +175,8 @@ int saru_align_device(const saru_batch *batch, saru_result *result, void *scratc
  * reference.  Same batch, result and stream arguments and the same outputs
  * as saru_align_device; the banded kernel's scratch comes from a device
  * array inside the library of SARU_STATIC_SCRATCH_BYTES (32 MiB), present on
- * every GPU that loads the library until the process exits.  It runs the
- * kernel's per-tile form (half the plane slots of the queued form the other
- * entry points run).  Fewer thread blocks run when the planes of a full
- * grid do not fit in the array.  A batch outside the banded kernel's domain
+ * every GPU that loads the library until the process exits.  Fewer thread
+ * blocks run when the planes of a full grid do not fit in the array.  A batch outside the banded kernel's domain
  * is refused with SARU_E_INVALID and a message; so would be one that cannot
  * get a single block, which with reads of at most 512 bases (about 0.5 MB
  * of planes a block) cannot happen at this array size.  The first call on a
@@ -204,10 +202,6 @@ typedef struct {
   int32_t warps_per_cta; /* 1..4: alignments per CTA = 32 x warps */
   int32_t ctas_per_sm;   /* cap on resident CTAs per SM */
   int32_t word_bits;     /* 64: 64-bit band words for k <= 7 too; 32 only for k <= 7 */
-  int32_t walks;         /* when the traceback walks run: 0 the library's default; 1 queued
-                            (a warp walks 32 queued candidates at a time); 2 right after each
-                            tile's fill (strings expanded by the whole warp); 3 per tile with
-                            each lane writing its strings */
 } saru_tuning;
 int saru_tuning_set(int32_t read_length, int32_t k, const saru_tuning *t); /* NULL: remove */
 int saru_tuning_get(int32_t read_length, int32_t k, saru_tuning *t);       /* 1 if set */

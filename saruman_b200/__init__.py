@@ -68,7 +68,7 @@ class SaruResult(C.Structure):
 
 class SaruTuning(C.Structure):
     _fields_ = [("warps_per_cta", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("word_bits", C.c_int32), ("walks", C.c_int32)]
+                ("word_bits", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -586,11 +586,9 @@ class Server:
         self.close()
 
 
-def set_tuning(m: int, k: int, warps: int = 0, ctas_per_sm: int = 0, word_bits: int = 0,
-               walks: int = 0) -> None:
-    """Launch shape of the banded kernel for (read length, k) (saru_tuning_set);
-    walks: 0 default, 1 queued, 2 after each fill, 3 per tile (lane strings)."""
-    t = SaruTuning(warps, ctas_per_sm, word_bits, walks)
+def set_tuning(m: int, k: int, warps: int = 0, ctas_per_sm: int = 0, word_bits: int = 0) -> None:
+    """Launch shape of the banded kernel for (read length, k) (saru_tuning_set)."""
+    t = SaruTuning(warps, ctas_per_sm, word_bits)
     rc = load().saru_tuning_set(m, k, C.byref(t))
     if rc != SARU_OK:
         raise SaruError(rc, last_error())

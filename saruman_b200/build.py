@@ -21,7 +21,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libsaruman_b200.so"
 SOURCES = ["kernels.cu", "gather.cu", "filter.cu", "abi.cu", "writer.cpp", "server.cpp", "compact.cpp", "sam.cpp",
            "costmodel.cu", "probe.cu", "input.cpp"]
-HEADERS = ["kernels.cuh", "saru_core.cuh", "band_tile.cuh", "band_queue.cuh", "writer.h", "server_internal.h",
+HEADERS = ["kernels.cuh", "saru_core.cuh", "band_tile.cuh", "writer.h", "server_internal.h",
            "filter_core.cuh", "filter_calls.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler",

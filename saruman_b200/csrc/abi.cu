@@ -196,7 +196,6 @@ int sm_count(int dev) {
 struct Plan {
   bool band = false;   // banded kernel
   bool wide = false;   // 64-bit band
-  int form = -1;       // kernel form (kForm*); -1: the tuning table's, else the default
   int max_m = 0;
   int64_t total_cells = 0;  // full-rectangle arena cells
 };
@@ -335,33 +334,15 @@ saru::Tuning tuning_for(int max_m, int k) {
   return it == g_tune.end() ? saru::Tuning{} : it->second;
 }
 
-// The banded kernel's form when neither the caller nor the tuning table
-// names one.
-constexpr int kDefaultForm = saru::kFormTile;
-
-// The form a launch of (max_m, k) runs: `forced` (>= 0), else the tuning
-// table's (saru_tuning.walks), else the default.
-int form_for(int forced, const saru::Tuning &tn) {
-  if (forced >= 0) return forced;
-  switch (tn.walks) {
-    case 1: return saru::kFormQueued;
-    case 2: return saru::kFormImmediate;
-    case 3: return saru::kFormTile;
-    default: return kDefaultForm;
-  }
-}
-
-long band_grid(int dev, long n, int max_m, int k, int forced_form = -1) {
+long band_grid(int dev, long n, int max_m, int k) {
   const saru::Tuning tn = tuning_for(max_m, k);
-  return saru::band_grid(sm_count(dev), n,
-                         saru::band_layout(max_m, k, tn.warps, form_for(forced_form, tn)),
+  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k, tn.warps),
                          smem_per_sm(dev), tn.ctas_per_sm);
 }
 
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int forced_form = -1) {
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide) {
   const saru::Tuning tn = tuning_for(max_m, k);
-  return saru::band_scratch_bytes(grid, max_m, k, wide || tn.word_bits == 64, tn.warps,
-                                  form_for(forced_form, tn));
+  return saru::band_scratch_bytes(grid, max_m, k, wide || tn.word_bits == 64, tn.warps);
 }
 
 // Enqueues the banded kernel on device buffers: calls[0..ncalls) as the
@@ -433,13 +414,10 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   a.max_k = max_k;
   a.wide_any = wide_any;
   a.warps_req = tn.warps;
-  a.form = form_for(pl.form, tn);
-  a.grid = saru::band_grid(sm_count(dev), total_n,
-                           saru::band_layout(max_m, max_k, tn.warps, a.form),
+  a.grid = saru::band_grid(sm_count(dev), total_n, saru::band_layout(max_m, max_k, tn.warps),
                            smem_per_sm(dev), tn.ctas_per_sm);
   if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
-  const size_t need =
-      saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0, tn.warps, a.form);
+  const size_t need = saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0, tn.warps);
   if (need > scratch_bytes) {
     set_error("scratch too small: %zu < %zu", scratch_bytes, need);
     return SARU_E_INVALID;
@@ -1056,16 +1034,15 @@ int saru_tuning_set(int32_t read_length, int32_t k, const saru_tuning *t) {
   }
   if (t->warps_per_cta < 0 || t->warps_per_cta > 4 || t->ctas_per_sm < 0 ||
       t->ctas_per_sm > 16 || (t->word_bits != 0 && t->word_bits != 32 && t->word_bits != 64) ||
-      (t->word_bits == 32 && k > 7) || t->walks < 0 || t->walks > 3) {
+      (t->word_bits == 32 && k > 7)) {
     set_error("saru_tuning_set: warps_per_cta 0..4, ctas_per_sm 0..16, word_bits 0/32/64 "
-              "(32 only for k <= 7), walks 0..3");
+              "(32 only for k <= 7)");
     return SARU_E_INVALID;
   }
   saru::Tuning tn;
   tn.warps = t->warps_per_cta;
   tn.ctas_per_sm = t->ctas_per_sm;
   tn.word_bits = t->word_bits;
-  tn.walks = t->walks;
   g_tune[{read_length, k}] = tn;
   return SARU_OK;
 }
@@ -1077,9 +1054,7 @@ int saru_tuning_get(int32_t read_length, int32_t k, saru_tuning *t) {
     if (t) *t = saru_tuning{0, 0, 0};
     return 0;
   }
-  if (t)
-    *t = saru_tuning{it->second.warps, it->second.ctas_per_sm, it->second.word_bits,
-                     it->second.walks};
+  if (t) *t = saru_tuning{it->second.warps, it->second.ctas_per_sm, it->second.word_bits};
   return 1;
 }
 
@@ -1245,10 +1220,9 @@ int saru_align_device_static(const saru_batch *batch, saru_result *result, void 
   pl.band = true;
   pl.max_m = batch->max_read_length;
   pl.wide = batch->k > 7;
-  pl.form = saru::kFormTile;  // the per-tile form: 32 plane slots per warp
   // as many persistent CTAs as the array holds planes for (each CTA's warps
   // need their own slice); a batch that cannot get even one CTA is refused
-  const size_t per_cta = band_scratch_bytes(1, pl.max_m, batch->k, pl.wide, saru::kFormTile);
+  const size_t per_cta = band_scratch_bytes(1, pl.max_m, batch->k, pl.wide);
   const long max_grid = (long)(kStaticScratchBytes / (per_cta ? per_cta : 1));
   if (max_grid < 1) {
     set_error("saru_align_device_static: one thread block needs %zu bytes of scratch, the "

@@ -1,17 +1,12 @@
 // kernels.cu -- sm_100a kernels of the alignment stage.
 //
-//  saru_band_queue_kernel     the production path: persistent warps over
+//  saru_band_kernel           the production path: persistent warps over
 //                             32-candidate tiles (one lane per candidate),
 //                             bit-parallel banded fill (saru_core.cuh) with
-//                             2-bit traceback decisions; the candidates that
-//                             score <= k are queued and walked 32 at a time
-//                             (band_queue.cuh), slot strings expanded by the
-//                             whole warp or compact records written; a
+//                             2-bit traceback decisions, traceback and slot
+//                             strings or compact records on the device; a
 //                             launch covers segments (calls, or slices
 //                             [t0, t1) of one call) of 32- or 64-bit bands.
-//  saru_band_kernel           the per-tile form (each tile walked right
-//                             after its fill), behind the no-allocation
-//                             entry point.
 //  saru_full_fill_kernel      the exact full-rectangle path for inputs the
 //  saru_full_trace_kernel     banded kernel does not cover (other costs,
 //                             m <= 3k, k > 15, irregular windows): the
@@ -24,7 +19,6 @@
 #include <mutex>
 
 #include "kernels.cuh"
-#include "band_queue.cuh"
 #include "band_tile.cuh"
 #include "saru_core.cuh"
 
@@ -130,243 +124,6 @@ __global__ void __launch_bounds__(128, 4) saru_band_kernel(const __grid_constant
     if (status && lane == 0)
       atomicOr(g.status, (status & 1 ? kStatusIrregular : 0) | (status & 2 ? kStatusAlphabet : 0) |
                              (status & 4 ? kStatusOverflow : 0));
-  }
-}
-
-// ---------------------------------------------------------------------------
-// banded kernel, queued form (band_queue.cuh): fills per tile, walks 32
-// queued jobs at a time, slot strings by cooperative expansion
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ TileArgs tile_args(const KernelArgs &a, const Segment &g,
-                                              long pstride) {
-  return TileArgs{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
-                  g.first_of_call, g.scores, g.read_aln, g.genome_aln, a.planes, pstride,
-                  (!g.wide && a.wide_any) ? 2L : 1L, a.rs_bytes, a.ws_bytes, a.region_bytes,
-                  g.records, g.rec_bytes, g.t0};
-}
-
-__device__ __forceinline__ void report_status(const Segment &g, int status) {
-  status = __reduce_or_sync(0xffffffffu, status);
-  if (status && (threadIdx.x & 31) == 0)
-    atomicOr(g.status, (status & 1 ? kStatusIrregular : 0) | (status & 2 ? kStatusAlphabet : 0) |
-                           (status & 4 ? kStatusOverflow : 0));
-}
-
-// Per-warp state of the queued form.  The queue is in registers: lane l
-// holds entries l (lo) and 32 + l (hi); at most 63 entries are queued.
-struct WarpQueue {
-  uint8_t *st_reads, *st_win, *region;
-  QEntry lo, hi;
-  long pstride, slot_base;
-  long r_base, g_base;  // staging bases of the last tile filled
-  uint64_t free_mask;
-  int qn;
-};
-
-// Fill of one tile: planes into free slots, scores, survivors queued.
-template <typename T>
-__device__ __forceinline__ void queue_fill(const KernelArgs &a, const Segment &g, long wt,
-                                           WarpQueue &w, int lane) {
-  const TileArgs ta = tile_args(a, g, w.pstride);
-  const TileSpan s = tile_span(ta, wt);
-  if (!s.fits) {  // offsets no regular call can have: report, do not stage
-    const long t = s.t0 + lane;
-    if (t < ta.n) ta.scores[t] = ta.k + 1;
-    report_status(g, 1);
-    return;
-  }
-  auto ld16 = [](uint8_t *d, const uint8_t *gp) {
-    *reinterpret_cast<uint4 *>(d) = __ldg(reinterpret_cast<const uint4 *>(gp));
-  };
-  auto ld1 = [](const uint8_t *gp) -> uint8_t { return __ldg(gp); };
-  stage_in(w.st_reads, ta.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
-  stage_in(w.st_win, ta.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
-  w.r_base = s.r_base;
-  w.g_base = s.g_base;
-  __syncwarp();
-  PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(a.planes);
-  const int slot = fill_slot(w.free_mask, lane);
-  const long pslot = w.slot_base + slot;
-  const long mul = ta.pair_mul;
-  LaneState ls;
-  int st = lane_fill<T>(ta, s, lane, w.st_reads, w.st_win, reinterpret_cast<uint32_t *>(w.region),
-                        ls, [&](int j, T A, T B) {
-                          planes[plane_index(j, w.pstride, pslot, mul)] = PlanePair<T>{A, B};
-                        });
-  const long t = s.t0 + lane;
-  const bool surv = t < ta.n && ls.ok && ls.score <= ta.k;
-  if (ta.records) {  // a record of zeros (step count 0) for every other candidate
-    if (t < ta.n && !surv) {
-      uint32_t *rec = reinterpret_cast<uint32_t *>(ta.records + t * ta.rec_bytes);
-      for (long wd = 0; wd < ta.rec_bytes / 4; ++wd) rec[wd] = 0u;
-    }
-  } else {
-    auto z16 = [](uint8_t *gp) { *reinterpret_cast<uint4 *>(gp) = make_uint4(0, 0, 0, 0); };
-    zero_range(ta.read_aln, s.s_lo, s.s_hi, lane, z16);
-    zero_range(ta.genome_aln, s.s_lo, s.s_hi, lane, z16);
-  }
-  const uint32_t mask = __ballot_sync(0xffffffffu, surv);
-  // the survivors, in lane order, become entries qn .. qn + popc(mask) - 1:
-  // each lane pulls the ones that land in its two registers
-  const QEntry mine = make_entry(t, slot, ls.c);
-  const int ns = __popc(mask);
-  const int r_lo = lane - w.qn, r_hi = 32 + lane - w.qn;
-  const bool in_lo = r_lo >= 0 && r_lo < ns, in_hi = r_hi >= 0 && r_hi < ns;
-  const int src_lo = in_lo ? nth_set_bit(mask, r_lo) : lane;
-  const int src_hi = in_hi ? nth_set_bit(mask, r_hi) : lane;
-  const int32_t t_lo = __shfl_sync(0xffffffffu, mine.t, src_lo);
-  const uint32_t i_lo = __shfl_sync(0xffffffffu, mine.info, src_lo);
-  const int32_t t_hi = __shfl_sync(0xffffffffu, mine.t, src_hi);
-  const uint32_t i_hi = __shfl_sync(0xffffffffu, mine.info, src_hi);
-  if (in_lo) w.lo = QEntry{t_lo, i_lo};
-  if (in_hi) w.hi = QEntry{t_hi, i_hi};
-  const uint32_t lo = __reduce_or_sync(0xffffffffu, surv && slot < 32 ? 1u << slot : 0u);
-  const uint32_t hi = __reduce_or_sync(0xffffffffu, surv && slot >= 32 ? 1u << (slot - 32) : 0u);
-  w.free_mask &= ~((uint64_t)lo | ((uint64_t)hi << 32));
-  w.qn += ns;
-  __syncwarp();
-  report_status(g, st);
-}
-
-// Walks the first `cnt` queued jobs (all of segment g), one per lane; slot
-// mode expands them into their slot strings.  Frees their plane slots and
-// drops them from the queue.
-template <typename T>
-__device__ __forceinline__ void queue_walk(const KernelArgs &a, const Segment &g, int cnt,
-                                           WarpQueue &w, int lane) {
-  __syncwarp();
-  const bool act = lane < cnt;
-  const QEntry e = act ? w.lo : QEntry{0, 0};
-  const Cand c = entry_cand(e, g.k, g.first_of_call);
-  const int slot = entry_slot(e);
-  const long pslot = w.slot_base + slot;
-  const long mul = (!g.wide && a.wide_any) ? 2L : 1L;
-  const PlanePair<T> *planes = reinterpret_cast<const PlanePair<T> *>(a.planes);
-  auto ld = [&](int j) { return planes[plane_index(j, w.pstride, pslot, mul)]; };
-  uint32_t *region32 = reinterpret_cast<uint32_t *>(w.region);
-  const int rstride = rec_stride(g.max_m, g.k);
-  WalkEnd we{0, 0, 0, false};
-  if (act) {
-    if (g.records) {  // every word of the record written: the same bytes whatever ran before
-      uint32_t *rec = reinterpret_cast<uint32_t *>(g.records + (long)e.t * g.rec_bytes);
-      we = walk_record<T>(c, ld, [&](int wd, uint32_t v) { rec[wd] = v; },
-                          (int)(g.rec_bytes / 4));
-    } else {
-      we = walk_record<T>(c, ld, [&](int wd, uint32_t v) { region32[lane * rstride + wd] = v; });
-    }
-  }
-  __syncwarp();
-  if (!g.records) {
-    for (int j = 0; j < cnt; ++j) {
-      const int t = __shfl_sync(0xffffffffu, e.t, j);
-      const int n = __shfl_sync(0xffffffffu, we.n, j);
-      const int row0 = __shfl_sync(0xffffffffu, we.row, j);
-      const int col0 = __shfl_sync(0xffffffffu, we.col, j);
-      const long gs = t ? g.goff[t - 1] : 0;
-      const long rs = t ? g.roff[t - 1] : 0;
-      const long slot0 = gs + (long)g.k * t;
-      // the immediate form walks the tile it just filled: its bytes are
-      // still staged; queued jobs may be of earlier tiles
-      const bool staged = a.form == kFormImmediate;
-      const uint8_t *rd = staged ? w.st_reads + (rs - w.r_base) : g.reads + rs;
-      const uint8_t *wn = staged ? w.st_win + (gs - w.g_base) : g.genome + gs;
-      uint8_t *o_r = g.read_aln + slot0;
-      uint8_t *o_g = g.genome_aln + slot0;
-      auto word = [&](int wd) { return region32[j * rstride + wd]; };
-      int cc = 0, rr = 0;  // advances of the rounds before
-      for (int base = 0; base < n; base += 128) {
-        const uint32_t adv = expand_advance(word, n, base, lane);
-        uint32_t incl = adv;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-          if (lane >= d) incl += y;
-        }
-        const uint32_t excl = incl - adv;
-        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
-        expand_write(word, n, base, lane, col0 + cc + (int)(excl & 0xFFFFu),
-                     row0 + rr + (int)(excl >> 16),
-                     [&](int i) { return staged ? rd[i] : __ldg(rd + i); },
-                     [&](int i) { return staged ? wn[i] : __ldg(wn + i); },
-                     [&](int p, uint8_t x, uint8_t y) {
-                       o_r[p] = x;
-                       o_g[p] = y;
-                     });
-        cc += (int)(tot & 0xFFFFu);
-        rr += (int)(tot >> 16);
-      }
-    }
-  }
-  const uint32_t lo = __reduce_or_sync(0xffffffffu, act && slot < 32 ? 1u << slot : 0u);
-  const uint32_t hi = __reduce_or_sync(0xffffffffu, act && slot >= 32 ? 1u << (slot - 32) : 0u);
-  w.free_mask |= (uint64_t)lo | ((uint64_t)hi << 32);
-  // a pass takes 32 jobs (the rest, in the hi registers, move down) or all
-  // of them (a flush); no other counts occur
-  if (cnt == 32) w.lo = w.hi;
-  w.qn -= cnt;
-  __syncwarp();
-  report_status(g, we.bad ? 4 : 0);
-}
-
-__device__ __forceinline__ int find_segment(const KernelArgs &a, long tile) {
-  int lo = 0, hi = a.nseg - 1;  // last segment with tile_begin <= tile
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (a.segs[mid].tile_begin <= tile) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Persistent warps as in saru_band_kernel; a warp walks whenever 32 jobs
-// are queued, fills a new tile otherwise, and walks what is queued before
-// it takes a tile of another segment and when the tiles run out.
-__global__ void __launch_bounds__(128, 4) saru_band_queue_kernel(const __grid_constant__ KernelArgs a) {
-  extern __shared__ uint4 smem_v[];
-  const int lane = threadIdx.x & 31;
-  const int wid = threadIdx.x >> 5;
-  const int WARPS = blockDim.x >> 5;
-  uint8_t *ws = reinterpret_cast<uint8_t *>(smem_v) + (long)wid * a.warp_smem;
-  WarpQueue w;
-  w.st_reads = ws;
-  w.st_win = ws + a.rs_bytes;
-  w.region = w.st_win + a.ws_bytes;
-  w.lo = QEntry{0, 0};
-  w.hi = QEntry{0, 0};
-  const long gwarp = (long)blockIdx.x * WARPS + wid;
-  const int slots = form_slots(a.form);
-  const int walk_at = a.form == kFormQueued ? 32 : 1;  // queued jobs that start a pass
-  w.pstride = (long)gridDim.x * WARPS * slots;
-  w.slot_base = gwarp * slots;
-  w.free_mask = slots == 64 ? ~0ull : 0xFFFFFFFFull;
-  w.r_base = w.g_base = 0;
-  w.qn = 0;
-  int qseg = -1;
-  auto walk = [&](int cnt) {
-    const Segment &g = a.segs[qseg];
-    if (g.wide) queue_walk<uint64_t>(a, g, cnt, w, lane);
-    else queue_walk<uint32_t>(a, g, cnt, w, lane);
-  };
-  for (;;) {
-    if (w.qn >= walk_at) {  // a pass takes 32 jobs, or all when fewer are queued
-      walk(w.qn >= 32 ? 32 : w.qn);
-      continue;
-    }
-    int tile = 0;
-    if (lane == 0) tile = atomicAdd(a.counter, 1);
-    tile = __shfl_sync(0xffffffffu, tile, 0);
-    if (tile >= a.total_tiles) {
-      if (w.qn > 0) walk(w.qn);
-      break;
-    }
-    const int seg = find_segment(a, tile);
-    if (w.qn > 0 && seg != qseg) walk(w.qn);
-    qseg = seg;
-    const Segment &g = a.segs[seg];
-    const long wt = tile - g.tile_begin;
-    if (g.wide) queue_fill<uint64_t>(a, g, wt, w, lane);
-    else queue_fill<uint32_t>(a, g, wt, w, lane);
   }
 }
 
@@ -485,8 +242,8 @@ __global__ void saru_full_trace_kernel(FullArgs a) {
 
 constexpr long kMaxCtaSmem = 227 * 1024;  // opt-in shared memory per block on sm_100
 
-BandLayout band_layout(int max_m, int k, int warps_req, int form) {
-  const SliceLayout S = form != kFormTile ? queue_slice_layout(max_m, k) : slice_layout(max_m, k);
+BandLayout band_layout(int max_m, int k, int warps_req) {
+  const SliceLayout S = slice_layout(max_m, k);
   BandLayout L;
   L.rs_bytes = S.rs_bytes;
   L.ws_bytes = S.ws_bytes;
@@ -500,42 +257,38 @@ BandLayout band_layout(int max_m, int k, int warps_req, int form) {
 }
 
 namespace {
-// The opt-in shared-memory limit is an attribute of a kernel on one device:
-// set once per (kernel, device), under a lock, before the first launch there.
+// The opt-in shared-memory limit is an attribute of the kernel on one
+// device: set once per device, under a lock, before the first launch there.
 std::mutex g_attr_mu;
-uint64_t g_attr_done[2];  // [kernel]: bit d set once device d allows it
+uint64_t g_attr_done;  // bit d set once device d allows it
 
-cudaError_t allow_smem(int which, const void *fn) {
+cudaError_t allow_smem() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lk(g_attr_mu);
-  if ((g_attr_done[which] >> dev) & 1u) return cudaSuccess;
-  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxCtaSmem);
-  if (e == cudaSuccess) g_attr_done[which] |= 1ull << dev;
+  if ((g_attr_done >> dev) & 1u) return cudaSuccess;
+  e = cudaFuncSetAttribute(saru_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kMaxCtaSmem);
+  if (e == cudaSuccess) g_attr_done |= 1ull << dev;
   return e;
 }
 }  // namespace
 
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
-  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req, a.form);
+  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req);
   if (L.warps < 1 || a.nseg < 1 || a.nseg > kMaxSegs) return cudaErrorInvalidValue;
-  const bool queued = a.form != kFormTile;
   // allow the largest slice once per device; each launch asks for its own
   // size (a per-launch attribute would race between concurrent callers)
-  const void *fn = queued ? reinterpret_cast<const void *>(saru_band_queue_kernel)
-                          : reinterpret_cast<const void *>(saru_band_kernel);
-  cudaError_t e = allow_smem(queued ? 1 : 0, fn);
+  cudaError_t e = allow_smem();
   if (e != cudaSuccess) return e;
   a.rs_bytes = L.rs_bytes;
   a.ws_bytes = L.ws_bytes;
   a.warp_smem = L.warp_smem;
-  a.region_bytes = L.region_bytes;
   e = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  if (queued) saru_band_queue_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
-  else saru_band_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
+  saru_band_kernel<<<(unsigned)a.grid, 32 * L.warps, L.cta_smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -550,10 +303,9 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_c
   return tiles < g ? (tiles > 0 ? tiles : 1) : g;
 }
 
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req, int form) {
-  const BandLayout L = band_layout(max_m, k, warps_req, form);
-  const size_t slots = (size_t)form_slots(form);  // plane slots per warp
-  return kCounterBytes + (size_t)grid * slots * (L.warps > 0 ? L.warps : 1) * 2 *
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req) {
+  const BandLayout L = band_layout(max_m, k, warps_req);
+  return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 *
                              (size_t)plane_columns(max_m) * (wide ? 8 : 4);
 }
 

@@ -48,9 +48,7 @@ struct KernelArgs {
   long grid;
   int max_m, max_k, wide_any;
   int warps_req;                       // requested warps per CTA (0: as many as fit)
-  int form;                            // kFormTile, kFormQueued or kFormImmediate
   long rs_bytes, ws_bytes, warp_smem;  // shared-memory slice layout (set by the launcher)
-  long region_bytes;
 };
 
 // Launch shape of the banded kernel for one (read length, k) class; 0 keeps
@@ -60,16 +58,7 @@ struct Tuning {
   int warps = 0;        // warps per CTA, 1..4
   int ctas_per_sm = 0;  // cap on resident CTAs per SM
   int word_bits = 0;    // 64: 64-bit band words even when k <= 7
-  int walks = 0;        // saru_tuning.walks: 0 default, 1 queued, 2 immediate, 3 per tile
 };
-
-// Forms of the banded kernel (when the traceback walks run).
-constexpr int kFormTile = 0;       // saru_band_kernel: each tile walked during it, lane strings
-constexpr int kFormQueued = 1;     // saru_band_queue_kernel, walks of 32 queued jobs
-constexpr int kFormImmediate = 2;  // saru_band_queue_kernel, each tile's survivors walked
-                                   // right after its fill, strings from the staged inputs
-// plane slots per warp of a form
-constexpr int form_slots(int form) { return form == kFormQueued ? 64 : 32; }
 
 struct BandLayout {
   long rs_bytes = 0, ws_bytes = 0, region_bytes = 0, warp_smem = 0, cta_smem = 0;
@@ -117,11 +106,10 @@ struct GatherArgs {
 
 cudaError_t launch_gather(const GatherArgs &a, int sms, cudaStream_t s);
 
-// form: the slice layout and plane slots of a kernel form.
-BandLayout band_layout(int max_m, int k, int warps_req = 0, int form = kFormTile);
+BandLayout band_layout(int max_m, int k, int warps_req = 0);
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_cap = 0);
-size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req = 0,
-                          int form = kFormTile);  // counter + planes
+size_t band_scratch_bytes(long grid, int max_m, int k, bool wide,
+                          int warps_req = 0);  // counter + planes
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s);
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s);
 

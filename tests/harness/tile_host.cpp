@@ -252,230 +252,3 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
   }
   return status;
 }
-
-// ---------------------------------------------------------------------------
-// The queued form (saru_band_queue_kernel over band_queue.cuh).  Warps take
-// steps in turn -- a walk pass when 32 jobs are queued, else a fill of the
-// next tile from the shared counter -- so a warp's queued planes sit in
-// the scratch while every other warp fills and walks.  Each warp's queue
-// and slice parts are exactly-sized allocations; the planes buffer has
-// exactly the queued form's kQueueSlots slots per warp.
-// ---------------------------------------------------------------------------
-#include "../../saruman_b200/csrc/band_queue.cuh"
-
-struct QSeg {
-  const uint8_t *genome, *reads;
-  const int *goff, *roff;
-  const int8_t *dirs;
-  int *scores;
-  uint8_t *ra, *ga;
-  uint8_t *records;  // compact records (rec_bytes each) instead of slots when not null
-  long rec_bytes;
-  long n, t0;
-  int k, max_m, first_of_call, wide;
-};
-
-// form: 1 queued (64 plane slots, a pass at 32 queued jobs, characters read
-// from global memory), 2 immediate (32 slots, each tile's survivors walked
-// right after its fill, characters read from the staged inputs).
-extern "C" int tile_align_queue(const QSeg *segs, int nseg, int nwarps_total, int form) {
-  const int slots = form == 1 ? 64 : 32;
-  const int walk_at = form == 1 ? 32 : 1;
-  int max_m = 0, max_k = 0, wide_any = 0;
-  std::vector<long> tile_begin(nseg);
-  long tiles = 0;
-  for (int i = 0; i < nseg; ++i) {
-    tile_begin[i] = tiles;
-    tiles += (segs[i].n - segs[i].t0 + 31) / 32;
-    if (segs[i].max_m > max_m) max_m = segs[i].max_m;
-    if (segs[i].k > max_k) max_k = segs[i].k;
-    wide_any |= segs[i].wide;
-  }
-  const SliceLayout S = queue_slice_layout(max_m, max_k);
-  const long pstride = (long)nwarps_total * slots;
-  std::vector<uint8_t> planes_v((size_t)plane_columns(max_m) * pstride * 2 * (wide_any ? 8 : 4));
-  int status = 0;
-  auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
-  auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
-  auto z16 = [](uint8_t *g) { memset(g, 0, 16); };
-  struct Warp {
-    uint8_t *st_reads, *st_win, *region;
-    QEntry *q;
-    uint64_t free_mask = 0;
-    long r_base = 0, g_base = 0;
-    int qn = 0, qseg = -1;
-    bool done = false;
-  };
-  std::vector<Warp> W(nwarps_total);
-  for (auto &w : W) {
-    w.st_reads = (uint8_t *)aligned_alloc(16, (size_t)S.rs_bytes);
-    w.st_win = (uint8_t *)aligned_alloc(16, (size_t)S.ws_bytes);
-    w.region = (uint8_t *)aligned_alloc(16, (size_t)S.region_bytes);
-    w.q = (QEntry *)aligned_alloc(16, sizeof(QEntry) * kQueueSlots);  // the kernel's registers
-    memset(w.st_reads, 0xA5, (size_t)S.rs_bytes);
-    memset(w.st_win, 0xA5, (size_t)S.ws_bytes);
-    memset(w.region, 0xA5, (size_t)S.region_bytes);
-    memset(w.q, 0xA5, sizeof(QEntry) * kQueueSlots);
-    w.free_mask = slots == 64 ? ~0ull : 0xFFFFFFFFull;
-  }
-  auto targs = [&](int si) {
-    const QSeg &g = segs[si];
-    return TileArgs{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
-                    g.first_of_call, g.scores, g.ra, g.ga, planes_v.data(), pstride,
-                    (!g.wide && wide_any) ? 2L : 1L, S.rs_bytes, S.ws_bytes, S.region_bytes,
-                    g.records, g.rec_bytes, g.t0};
-  };
-  long counter = 0;
-  auto walk = [&](Warp &w, int gw, int cnt) {
-    const QSeg &g = segs[w.qseg];
-    const TileArgs a = targs(w.qseg);
-    uint32_t *region32 = reinterpret_cast<uint32_t *>(w.region);
-    const int rstride = rec_stride(g.max_m, g.k);
-    auto body = [&](auto tag) {
-      using T = decltype(tag);
-      const PlanePair<T> *planes = reinterpret_cast<const PlanePair<T> *>(planes_v.data());
-      QEntry e[32];
-      WalkEnd we[32];
-      for (int lane = 0; lane < 32; ++lane) {
-        we[lane] = WalkEnd{0, 0, 0, false};
-        if (lane >= cnt) continue;
-        e[lane] = w.q[lane];
-        const Cand c = entry_cand(e[lane], g.k, g.first_of_call);
-        const long pslot = (long)gw * slots + entry_slot(e[lane]);
-        auto ld = [&](int j) { return planes[plane_index(j, pstride, pslot, a.pair_mul)]; };
-        if (g.records) {
-          uint32_t *rec = reinterpret_cast<uint32_t *>(g.records + (long)e[lane].t * g.rec_bytes);
-          we[lane] = walk_record<T>(c, ld, [&](int wd, uint32_t v) { rec[wd] = v; },
-                                    (int)(g.rec_bytes / 4));
-        } else {
-          we[lane] = walk_record<T>(c, ld, [&](int wd, uint32_t v) {
-            region32[lane * rstride + wd] = v;
-          });
-        }
-        if (we[lane].bad) status |= 4;
-      }
-      if (!g.records) {
-        for (int j = 0; j < cnt; ++j) {
-          const long t = e[j].t;
-          const long gs = t ? g.goff[t - 1] : 0, rs = t ? g.roff[t - 1] : 0;
-          const long slot0 = gs + (long)g.k * t;
-          auto word = [&](int wd) { return region32[j * rstride + wd]; };
-          int cc = 0, rr = 0;
-          for (int base = 0; base < we[j].n; base += 128) {
-            uint32_t adv[32], incl = 0;
-            for (int lane = 0; lane < 32; ++lane) adv[lane] = expand_advance(word, we[j].n, base, lane);
-            for (int lane = 0; lane < 32; ++lane) {
-              const uint32_t excl = incl;
-              incl += adv[lane];
-              expand_write(word, we[j].n, base, lane, we[j].col + cc + (int)(excl & 0xFFFFu),
-                           we[j].row + rr + (int)(excl >> 16),
-                           [&](int i) {
-                             return form == 2 ? w.st_reads[rs - w.r_base + i] : g.reads[rs + i];
-                           },
-                           [&](int i) {
-                             return form == 2 ? w.st_win[gs - w.g_base + i] : g.genome[gs + i];
-                           },
-                           [&](int p, uint8_t x, uint8_t y) {
-                             g.ra[slot0 + p] = x;
-                             g.ga[slot0 + p] = y;
-                           });
-            }
-            cc += (int)(incl & 0xFFFFu);
-            rr += (int)(incl >> 16);
-          }
-        }
-      }
-      for (int lane = 0; lane < cnt; ++lane) w.free_mask |= 1ull << entry_slot(e[lane]);
-      const int rest = w.qn - cnt;
-      if (cnt != 32 && rest != 0) abort();  // the kernel's register queue needs one or the other
-      for (int lane = 0; lane < rest; ++lane) w.q[lane] = w.q[cnt + lane];
-      w.qn = rest;
-    };
-    if (g.wide) body(uint64_t(0));
-    else body(uint32_t(0));
-  };
-  auto fill = [&](Warp &w, int gw, int seg, long wt) {
-    const QSeg &g = segs[seg];
-    const TileArgs a = targs(seg);
-    const TileSpan s = tile_span(a, wt);
-    if (!s.fits) {
-      for (int lane = 0; lane < 32; ++lane)
-        if (s.t0 + lane < a.n) a.scores[s.t0 + lane] = a.k + 1;
-      status |= 1;
-      return;
-    }
-    auto body = [&](auto tag) {
-      using T = decltype(tag);
-      PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
-      for (int lane = 0; lane < 32; ++lane) {
-        stage_in(w.st_reads, a.reads, s.r_lo, s.r_hi, s.r_base, lane, ld16, ld1);
-        stage_in(w.st_win, a.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
-      }
-      w.r_base = s.r_base;
-      w.g_base = s.g_base;
-      int slot[32];
-      bool surv[32];
-      LaneState ls[32];
-      for (int lane = 0; lane < 32; ++lane) {
-        slot[lane] = fill_slot(w.free_mask, lane);
-        const long pslot = (long)gw * slots + slot[lane];
-        status |= lane_fill<T>(a, s, lane, w.st_reads, w.st_win,
-                               reinterpret_cast<uint32_t *>(w.region), ls[lane],
-                               [&](int j, T A, T B) {
-                                 planes[plane_index(j, pstride, pslot, a.pair_mul)] =
-                                     PlanePair<T>{A, B};
-                               });
-        const long t = s.t0 + lane;
-        surv[lane] = t < a.n && ls[lane].ok && ls[lane].score <= a.k;
-        if (a.records && t < a.n && !surv[lane])
-          memset(a.records + t * a.rec_bytes, 0, (size_t)a.rec_bytes);
-      }
-      if (!a.records)
-        for (int lane = 0; lane < 32; ++lane) {
-          zero_range(a.read_aln, s.s_lo, s.s_hi, lane, z16);
-          zero_range(a.genome_aln, s.s_lo, s.s_hi, lane, z16);
-        }
-      for (int lane = 0; lane < 32; ++lane) {
-        if (!surv[lane]) continue;
-        if (w.qn >= slots || slot[lane] >= slots || !((w.free_mask >> slot[lane]) & 1u)) abort();
-        w.q[w.qn++] = make_entry(s.t0 + lane, slot[lane], ls[lane].c);
-        w.free_mask &= ~(1ull << slot[lane]);
-      }
-    };
-    if (g.wide) body(uint64_t(0));
-    else body(uint32_t(0));
-  };
-  for (int live = nwarps_total; live > 0;) {
-    for (int gw = 0; gw < nwarps_total; ++gw) {
-      Warp &w = W[gw];
-      if (w.done) continue;
-      if (w.qn >= walk_at) {
-        walk(w, gw, w.qn >= 32 ? 32 : w.qn);
-        continue;
-      }
-      const long tile = counter++;
-      if (tile >= tiles) {
-        if (w.qn > 0) walk(w, gw, w.qn);
-        w.done = true;
-        --live;
-        continue;
-      }
-      int lo = 0, hi = nseg - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_begin[mid] <= tile) lo = mid;
-        else hi = mid - 1;
-      }
-      if (w.qn > 0 && lo != w.qseg) walk(w, gw, w.qn);
-      w.qseg = lo;
-      fill(w, gw, lo, tile - tile_begin[lo]);
-    }
-  }
-  for (auto &w : W) {
-    free(w.st_reads);
-    free(w.st_win);
-    free(w.region);
-    free(w.q);
-  }
-  return status;
-}

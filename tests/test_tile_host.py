@@ -18,7 +18,6 @@ SO = ROOT / "tests" / "_build" / "libtile_host_asan.so"
 def test_tile_emulation_under_asan():
     SO.parent.mkdir(exist_ok=True)
     deps = [SRC, ROOT / "saruman_b200" / "csrc" / "band_tile.cuh",
-            ROOT / "saruman_b200" / "csrc" / "band_queue.cuh",
             ROOT / "saruman_b200" / "csrc" / "saru_core.cuh"]
     if not SO.exists() or SO.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["g++", "-O1", "-g", "-std=c++17", "-shared", "-fPIC",

@@ -105,7 +105,6 @@ def main():
         bad += 1
         print("irregular tile not reported", st)
     bad += multi_launch(lib)
-    bad += queue_cases(lib)
     print("BAD", bad)
     sys.exit(1 if bad else 0)
 
@@ -144,115 +143,6 @@ def multi_launch(lib) -> int:
                 and np.array_equal(ga1, ga)):
             print("MULTI MISMATCH", spec, flush=True)
             bad += 1
-    return bad
-
-
-class QSeg(C.Structure):
-    _fields_ = [("genome", C.c_void_p), ("reads", C.c_void_p), ("goff", C.c_void_p),
-                ("roff", C.c_void_p), ("dirs", C.c_void_p), ("scores", C.c_void_p),
-                ("ra", C.c_void_p), ("ga", C.c_void_p), ("records", C.c_void_p),
-                ("rec_bytes", C.c_long), ("n", C.c_long), ("t0", C.c_long), ("k", C.c_int),
-                ("max_m", C.c_int), ("first_of_call", C.c_int), ("wide", C.c_int)]
-
-
-def queue_cases(lib) -> int:
-    return sum(queue_cases_form(lib, form) for form in (1, 2))
-
-
-def queue_cases_form(lib, form: int) -> int:
-    """The queued form (walks of 32 queued jobs, cooperative expansion of
-    the slot strings): single calls at misalignments, compact records, a
-    call in slices, and a launch of mixed calls and band widths, with few
-    warps (long queues) and many (short ones)."""
-    import saruman_b200 as S
-    bad = 0
-    cases = [(36, 2, 0.05), (100, 5, 0.04), (75, 5, 0.2), (150, 9, 0.05), (250, 15, 0.05),
-             (20, 1, 0.1), (40, 7, 0.1), (64, 15, 0.3), (512, 15, 0.03)]
-    for ci, (m, k, err) in enumerate(cases):
-        n = 300 + 37 * ci if m < 512 else 70
-        b = W.random_batch(m, k, n, seed=700 + ci, err=err,
-                           alphabet=b"ACGT" if ci % 2 else b"ACGTN")
-        s1, ra1, ga1, _ = R.oracle_align(b, nthreads=4)
-        wide = 1 if k > 7 else 0
-        keep = []
-
-        def seg(off, records=None, rbytes=0, t0=0, nn=None):
-            g = exact(b.genome, off)
-            r = exact(b.reads, (off + 5) % 16)
-            sc = np.zeros(b.n, np.int32)
-            ra = exact(np.zeros(b.total_genome, np.uint8), (off + 7) % 16)
-            ga = exact(np.zeros(b.total_genome, np.uint8), (off + 11) % 16)
-            keep.append((g, r, sc, ra, ga))
-            return QSeg(g.ctypes.data, r.ctypes.data, b.genome_offsets.ctypes.data,
-                        b.read_offsets.ctypes.data, b.dirs.ctypes.data, sc.ctypes.data,
-                        ra.ctypes.data, ga.ctypes.data,
-                        records.ctypes.data if records is not None else None, rbytes,
-                        b.n if nn is None else nn, t0, k, m, 1, wide), sc, ra, ga
-
-        for off, nw in ((0, 1), (3, 2), (9, 7)):
-            q, sc, ra, ga = seg(off)
-            st = lib.tile_align_queue(C.byref(q), 1, nw, form)
-            if not (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
-                    and np.array_equal(ra1, ra) and np.array_equal(ga1, ga)):
-                bad += 1
-                print("QUEUE MISMATCH", form, m, k, off, nw, st, flush=True)
-        # compact records
-        rb = S.compact_record_bytes(m, k)
-        rec = exact(np.zeros(b.n * rb, np.uint8), 0)
-        q, sc, _, _ = seg(4, rec, rb)
-        st = lib.tile_align_queue(C.byref(q), 1, 3, form)
-        out = S.expand_compact(b, sc, rec, rb, nthreads=2)
-        if not (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
-                and np.array_equal(ra1, out.read_aln) and np.array_equal(ga1, out.genome_aln)):
-            bad += 1
-            print("QUEUE COMPACT MISMATCH", form, m, k, st, flush=True)
-        # slices [t0, t1) of the call, the same output arrays
-        q0, sc, ra, ga = seg(6)
-        st = 0
-        for t0 in range(0, b.n, 64):
-            q = QSeg(*[getattr(q0, f) for f, _ in QSeg._fields_])
-            q.t0, q.n = t0, min(b.n, t0 + 64)
-            st |= lib.tile_align_queue(C.byref(q), 1, 2, form)
-        if not (st == 0 and np.array_equal(np.minimum(s1, k + 1), sc)
-                and np.array_equal(ra1, ra) and np.array_equal(ga1, ga)):
-            bad += 1
-            print("QUEUE SLICE MISMATCH", form, m, k, st, flush=True)
-    # mixed calls in one launch, both band widths, slots and compact records
-    specs = [(36, 3, 300), (75, 5, 200), (100, 6, 250), (150, 9, 120), (250, 15, 40), (40, 2, 33)]
-    for nw in (1, 4):
-        keep, segs, outs = [], [], []
-        for i, (m, k, n) in enumerate(specs):
-            b = W.random_batch(m, k, n, seed=900 + i, err=0.06,
-                               alphabet=b"ACGT" if i % 3 else b"ACGTN")
-            sc = np.zeros(n, np.int32)
-            g = exact(b.genome, (i + 3) % 16)
-            r = exact(b.reads, (i + 7) % 16)
-            ra = exact(np.zeros(b.total_genome, np.uint8), i % 16)
-            ga = exact(np.zeros(b.total_genome, np.uint8), (i + 5) % 16)
-            rec, rb = None, 0
-            if i % 2:
-                rb = S.compact_record_bytes(m, k)
-                rec = exact(np.zeros(n * rb, np.uint8), 0)
-            keep.append((g, r, sc, ra, ga, rec))
-            segs.append(QSeg(g.ctypes.data, r.ctypes.data, b.genome_offsets.ctypes.data,
-                             b.read_offsets.ctypes.data, b.dirs.ctypes.data, sc.ctypes.data,
-                             ra.ctypes.data, ga.ctypes.data,
-                             rec.ctypes.data if rec is not None else None, rb, n, 0, k, m, 1,
-                             1 if k > 7 else 0))
-            outs.append((b, sc, ra, ga, rec, rb))
-        order = sorted(range(len(specs)), key=lambda i: -(specs[i][0] * (specs[i][1] + 1)))
-        arr = (QSeg * len(segs))(*[segs[i] for i in order])
-        st = lib.tile_align_queue(arr, len(segs), nw, form)
-        bad += 1 if st else 0
-        for b, sc, ra, ga, rec, rb in outs:
-            s1, ra1, ga1, _ = R.oracle_align(b, nthreads=4)
-            if rec is not None:
-                out = S.expand_compact(b, sc, rec, rb, nthreads=2)
-                ra, ga = out.read_aln, out.genome_aln
-            if not (np.array_equal(np.minimum(s1, b.k + 1), sc) and np.array_equal(ra1, ra)
-                    and np.array_equal(ga1, ga)):
-                print("QUEUE MULTI MISMATCH", form, b.m, b.k, nw, flush=True)
-                bad += 1
     return bad
 
 
