@@ -332,7 +332,10 @@ class DeviceCalls:
         self.h_out = [torch.empty(cs.n, dtype=torch.int32).pin_memory(),
                       torch.empty(cs.total_slots + 64, dtype=torch.uint8).pin_memory(),
                       torch.empty(cs.total_slots + 64, dtype=torch.uint8).pin_memory()]
-        self.sbs, self.srs, self.spans = [], [], []
+        self.rb = S.compact_record_bytes(cs.m, cs.k)
+        self.rec = torch.empty(max(cs.n, 1) * self.rb, dtype=torch.uint8, device=dev)
+        self.h_rec = torch.empty(max(cs.n, 1) * self.rb, dtype=torch.uint8).pin_memory()
+        self.sbs, self.srs, self.crs, self.spans = [], [], [], []
         cb, gb, sbase = cs.call_begin, cs.gbase, cs.sbase
         for c in range(cs.ncalls):
             a, b = int(cb[c]), int(cb[c + 1])
@@ -343,6 +346,9 @@ class DeviceCalls:
                                         s1 - s0))
             self.srs.append(S.SaruResult(self.scores.data_ptr() + 4 * a, self.ra.data_ptr() + s0,
                                          self.ga.data_ptr() + s0, status.data_ptr()))
+            self.crs.append(S.SaruResult(self.scores.data_ptr() + 4 * a,
+                                         self.rec.data_ptr() + a * self.rb, None,
+                                         status.data_ptr()))
             self.spans.append((a, b, g0, g1, s0, s1))
 
     def host_call(self, c: int):
@@ -376,6 +382,12 @@ class DeviceCalls:
         for h, d, lo, hi in ((self.h_out[0], self.scores, a, b), (self.h_out[1], self.ra, s0, s1),
                              (self.h_out[2], self.ga, s0, s1)):
             h[lo:hi].copy_(d[lo:hi], non_blocking=True)
+
+    def copy_out_compact(self, c0: int, c1: int):
+        a, b = self.spans[c0][0], self.spans[c1 - 1][1]
+        self.h_out[0][a:b].copy_(self.scores[a:b], non_blocking=True)
+        self.h_rec[a * self.rb:b * self.rb].copy_(self.rec[a * self.rb:b * self.rb],
+                                                  non_blocking=True)
 
     def bytes_in(self) -> int:
         return sum(int(h.numel() * h.element_size()) for h in self.h_in)
@@ -761,6 +773,50 @@ def measure_calls(S, css: list, args, dev, world: int, dist, tune: bool = True,
     if int(status.item()) != 0:
         raise SystemExit(f"kernel status {int(status.item())} (e2e)")
 
+    # compact records instead of slot strings: the batched request on the
+    # device (graph replay), and end to end with the records copied out
+    crs = [cr for d in dcs for cr in d.crs]
+    creqs = [(sbs[q:q + 192], crs[q:q + 192]) for q in range(0, ncalls, 192)]
+
+    def step_compact():
+        for rb_, rr in creqs:
+            S.align_multi_device_compact(rb_, rr, status.data_ptr(), scratch.data_ptr(), nscr,
+                                         sptr)
+
+    with torch.cuda.stream(stream):
+        step_compact()
+    stream.synchronize()
+    cgraph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(cgraph, stream=stream):
+        step_compact()
+
+    def step_cgraph():
+        with torch.cuda.stream(stream):
+            cgraph.replay()
+
+    step_cgraph()
+    stream.synchronize()
+    ms_compact = timed(stream, step_cgraph, args.steps, world, dist, dev)
+
+    def e2e_compact():
+        for i, c0, c1 in groups:
+            d = dcs[i]
+            with torch.cuda.stream(s_in):
+                d.copy_in(c0, c1)
+            s_run.wait_stream(s_in)
+            S.align_multi_device_compact(d.sbs[c0:c1], d.crs[c0:c1], status.data_ptr(),
+                                         scratch_g.data_ptr(), gscr, s_run.cuda_stream)
+            s_out.wait_stream(s_run)
+            with torch.cuda.stream(s_out):
+                d.copy_out_compact(c0, c1)
+
+    e2e_compact()
+    torch.cuda.synchronize()
+    ec_ms = timed_streams(e2e_compact, e2e_steps)
+    if int(status.item()) != 0:
+        raise SystemExit(f"kernel status {int(status.item())} (compact)")
+    del cgraph
+
     # end to end, plain: the reference's structure -- a thread per strand,
     # each submitting its calls one at a time through saru_align_host
     strands = {}
@@ -810,6 +866,8 @@ def measure_calls(S, css: list, args, dev, world: int, dist, tune: bool = True,
                              f"expected {expect}")
     out = dict(n_cand=n_cand, ncalls=ncalls, ms_step=ms_step, per_step_launches=per_step_launches,
                ms_plain=ms_plain, e_ms=e_ms, p_ms=p_ms, e2e_steps=e2e_steps, legacy=legacy,
+               ms_compact=ms_compact, ec_ms=ec_ms,
+               d2h_compact=sum(4 * d.cs.n + d.cs.n * d.rb for d in dcs),
                tuning=tuning, groups=len(groups), clocks=clk.summary() if clk else None,
                h2d=sum(d.bytes_in() for d in dcs), d2h=sum(d.bytes_out() for d in dcs))
     del graph
@@ -953,6 +1011,15 @@ def run_aligner(args, cfg: dict, rank: int, world: int, local: int) -> None:
         "clocks": r["clocks"],
     }
     line.update(batched_plain(r, world))
+    line["compact"] = {
+        "value": world * n_cand / (r["ms_compact"] * 1e-3), "ms_per_step": r["ms_compact"],
+        "roofline_frac": (6 * cells / (r["ms_compact"] * 1e-3) / int_peak
+                          if int_peak and int_peak > 0 else None),
+        "e2e": {"value": world * n_cand / (r["ec_ms"] * 1e-3), "unit": "alignments/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h_compact"]},
+        "what": "saru_align_multi_device_compact: 2-bit traceback records per candidate instead "
+                "of the slot strings (saru_expand_compact rebuilds the slots on the host); "
+                "end to end as e2e, records copied out"}
     if r["legacy"]:
         line["e2e_legacy"] = r["legacy"]
     if mixed:

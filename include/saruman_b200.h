@@ -348,6 +348,13 @@ size_t saru_scratch_bytes(int32_t n, int32_t read_length, int32_t k, int wide);
 int saru_align_multi_device(const saru_batch *calls, saru_result *results, int32_t ncalls,
                             int32_t *status, void *scratch, size_t scratch_bytes, void *stream);
 size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls);
+/* The same request with compact records instead of slot strings: call i's
+ * records (n x saru_compact_record_bytes(max_read_length, k) bytes, device
+ * memory) go to results[i].read_aln; results[i].genome_aln is unused.  Same
+ * scratch as saru_align_multi_device. */
+int saru_align_multi_device_compact(const saru_batch *calls, saru_result *results,
+                                    int32_t ncalls, int32_t *status, void *scratch,
+                                    size_t scratch_bytes, void *stream);
 
 /* ---- request server (continuous batching on one GPU) ----------------------
  * Not in the reference, whose alignment calls are synchronous

@@ -43,7 +43,8 @@ ABI_FUNCTIONS = ("cuda_needleman_wunsch", "cuda_allocate_memory", "cuda_free_mem
                  "saru_filter_set_chunk", "saru_align_host_compact",
                  "saru_reads_open", "saru_reads_next", "saru_reads_close", "saru_genome_open",
                  "saru_genome_next", "saru_genome_close", "saru_server_submit_reads",
-                 "saru_server_read_results", "saru_server_release", "saru_tsv_to_sam")
+                 "saru_server_read_results", "saru_server_release", "saru_tsv_to_sam",
+                 "saru_align_multi_device_compact")
 ABI_DATA = ("alignment_time",)
 
 
@@ -139,6 +140,8 @@ def load(path: str | Path | None = None):
     lib.saru_align_multi_device.restype = C.c_int
     lib.saru_align_multi_device.argtypes = [C.POINTER(SaruBatch), C.POINTER(SaruResult), C.c_int32,
                                             C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+    lib.saru_align_multi_device_compact.restype = C.c_int
+    lib.saru_align_multi_device_compact.argtypes = lib.saru_align_multi_device.argtypes
     lib.saru_multi_scratch_bytes.restype = C.c_size_t
     lib.saru_multi_scratch_bytes.argtypes = [C.POINTER(SaruBatch), C.c_int32]
     lib.saru_server_create.restype = C.c_void_p
@@ -362,6 +365,19 @@ def align_multi_device(batches: list[SaruBatch], results: list[SaruResult], stat
     arr_r = (SaruResult * n)(*results)
     rc = load().saru_align_multi_device(arr_b, arr_r, n, status_ptr, scratch_ptr, scratch_len,
                                         stream_ptr)
+    if rc != SARU_OK:
+        raise SaruError(rc, last_error())
+
+
+def align_multi_device_compact(batches: list[SaruBatch], results: list[SaruResult],
+                               status_ptr: int, scratch_ptr: int, scratch_len: int,
+                               stream_ptr: int = 0) -> None:
+    """saru_align_multi_device with compact records: results[i].read_aln is
+    call i's records array (device)."""
+    n = len(batches)
+    rc = load().saru_align_multi_device_compact((SaruBatch * n)(*batches),
+                                                (SaruResult * n)(*results), n, status_ptr,
+                                                scratch_ptr, scratch_len, stream_ptr)
     if rc != SARU_OK:
         raise SaruError(rc, last_error())
 

@@ -1267,6 +1267,35 @@ int saru_align_device_compact(const saru_batch *batch, int32_t *scores, uint8_t 
                   reinterpret_cast<cudaStream_t>(stream), 0, &cmp);
 }
 
+int saru_align_multi_device_compact(const saru_batch *calls, saru_result *results,
+                                    int32_t ncalls, int32_t *status, void *scratch,
+                                    size_t scratch_bytes, void *stream) {
+  g_last_error.clear();
+  if (ncalls < 1 || ncalls > saru::kMaxSegs || !status || !results) {
+    set_error("saru_align_multi_device_compact: 1..%d calls, results and a status word",
+              saru::kMaxSegs);
+    return SARU_E_INVALID;
+  }
+  std::vector<CompactOut> cmp((size_t)ncalls);
+  for (int i = 0; i < ncalls; ++i) {
+    const saru_batch *b = &calls[i];
+    if (b->n < 0 || b->k < 0 || b->k > 15 || b->match != 0 || b->mismatch != 1 ||
+        b->max_read_length < 2 || b->max_read_length > saru::kMaxBandM ||
+        (b->n > 0 && !results[i].read_aln)) {
+      set_error("saru_align_multi_device_compact: call %d needs unit costs, k <= 15, "
+                "2 <= max_read_length <= %d and a records array",
+                i, saru::kMaxBandM);
+      return SARU_E_INVALID;
+    }
+    cmp[(size_t)i] = CompactOut{reinterpret_cast<uint8_t *>(results[i].read_aln),
+                                (long)saru::compact_record_bytes(b->max_read_length, b->k)};
+  }
+  int dev = 0;
+  SARU_CUDA(cudaGetDevice(&dev));
+  return run_band_classes(calls, results, ncalls, scratch, scratch_bytes, status, dev,
+                          reinterpret_cast<cudaStream_t>(stream), cmp.data());
+}
+
 size_t saru_multi_scratch_bytes(const saru_batch *calls, int32_t ncalls) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {

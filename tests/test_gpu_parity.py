@@ -305,6 +305,38 @@ def test_multi_call_launch_matches_each_call(saru_lib):
     _check_multi(keep, want)
 
 
+def test_multi_call_launch_with_compact_records(saru_lib):
+    """saru_align_multi_device_compact: the same mixed calls in one launch,
+    each call's compact records expanded on the host give its reference
+    bytes; every record is fully written (the same bytes on a second run
+    over records filled with other bytes)."""
+    import torch
+    sbs, srs, keep, want = _multi_call_setup()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+    nscr = S.multi_scratch_bytes(sbs)
+    scratch = torch.empty(nscr, dtype=torch.uint8, device="cuda:0")
+    recs, crs = [], []
+    for (b, *_), sr in zip(want, srs):
+        rb = S.compact_record_bytes(b.m, b.k)
+        rec = torch.full((b.n * rb,), 0x5A, dtype=torch.uint8, device="cuda:0")
+        recs.append((rec, rb))
+        crs.append(S.SaruResult(sr.scores, rec.data_ptr(), None, None))
+    outs = []
+    for fill in (0x5A, 0xC3):
+        for rec, _ in recs:
+            rec.fill_(fill)
+        S.align_multi_device_compact(sbs, crs, status.data_ptr(), scratch.data_ptr(), nscr,
+                                     torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert int(status.item()) == 0
+        outs.append([rec.cpu().numpy() for rec, _ in recs])
+    for (b, s1, ra1, ga1, _), sb, bufs, (rec, rb), r0, r1 in zip(want, sbs, keep, recs, *outs):
+        assert np.array_equal(r0, r1)
+        sc = bufs["s"].cpu().numpy()
+        ex = S.expand_compact(b, sc, r0, rb, first_of_call=bool(sb.first_of_call))
+        check_equal(b, s1, ra1, ga1, ex)
+
+
 def test_multi_call_request_replays_from_a_cuda_graph(saru_lib):
     """saru_align_multi_device captured once in a CUDA graph (its class
     launches forked onto side streams and joined back inside the capture)
