@@ -381,6 +381,9 @@ typedef struct {
   int32_t max_requests_per_launch; /* cap on a launch group (>= 1) */
   int32_t max_inflight;            /* launch groups queued on the GPU at once (>= 1) */
   int64_t device_budget_bytes;     /* arena for request inputs and outputs */
+  int64_t host_pool_bytes;         /* pinned host memory for reads-only requests' results,
+                                      allocated on first use (0: 4 GiB); results that do not
+                                      fit go to pageable memory */
 } saru_server_config;
 typedef struct {
   const saru_batch *calls;        /* host pointers */

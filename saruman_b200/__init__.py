@@ -75,7 +75,7 @@ class SaruTuning(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("pipeline", C.c_int32),
                 ("max_requests_per_launch", C.c_int32), ("max_inflight", C.c_int32),
-                ("device_budget_bytes", C.c_int64)]
+                ("device_budget_bytes", C.c_int64), ("host_pool_bytes", C.c_int64)]
 
 
 class SaruGatherCall(C.Structure):
@@ -487,10 +487,10 @@ class Server:
     """Continuous-batching request server on one GPU (saru_server_*)."""
 
     def __init__(self, device: int = 0, pipeline: bool = True, max_requests_per_launch: int = 64,
-                 max_inflight: int = 2, budget_bytes: int = 8 << 30):
+                 max_inflight: int = 2, budget_bytes: int = 8 << 30, host_pool_bytes: int = 0):
         self._lib = load()
         cfg = ServerConfig(device, 1 if pipeline else 0, max_requests_per_launch, max_inflight,
-                           budget_bytes)
+                           budget_bytes, host_pool_bytes)
         self._h = self._lib.saru_server_create(C.byref(cfg))
         if not self._h:
             raise SaruError(SARU_E_CUDA, last_error())

@@ -367,8 +367,11 @@ SARU_HD int lane_traceback_ops(const TileArgs &a, const TileSpan &s, int lane,
                                const LaneState &ls, LoadPair ld, StoreWord store) {
   const long t = s.t0 + lane;
   if (t >= a.n) return 0;
+  // every word of the record is written (steps, then zeros), so a record's
+  // bytes do not depend on what the buffer held before
+  const int nwords = (int)(a.rec_bytes / 4);
   if (!ls.ok || ls.score > a.k) {
-    store(0, 0u);
+    for (int w = 0; w < nwords; ++w) store(w, 0u);
     return 0;
   }
   uint32_t acc = 0;
@@ -382,7 +385,8 @@ SARU_HD int lane_traceback_ops(const TileArgs &a, const TileSpan &s, int lane,
       sh = 0;
     }
   });
-  if (sh) store(w, acc);
+  if (sh) store(w++, acc);
+  for (; w < nwords; ++w) store(w, 0u);
   store(0, (uint32_t)e.n | (e.bad ? 0x10000u : 0u));
   return e.bad ? 4 : 0;
 }

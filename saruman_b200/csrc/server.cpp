@@ -98,16 +98,78 @@ class Arena {
 
 // Results of one read set of a reads-only request, owned by the server:
 // the filter's calls (both strands), their gather descriptors and outputs.
+// First-fit allocator over one pinned host allocation (reads-only requests'
+// results: copies out of pinned memory run at full bus speed and take no
+// page faults).  Thread-safe.
+class HostPool {
+ public:
+  ~HostPool() {
+    if (base_) cudaFreeHost(base_);
+  }
+  long alloc(size_t bytes, size_t want_total) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!base_ && !tried_) {  // on first use
+      tried_ = true;
+      if (cudaMallocHost(&base_, want_total) != cudaSuccess) {
+        cudaGetLastError();
+        base_ = nullptr;
+      } else {
+        size_ = want_total;
+        free_[0] = want_total;
+      }
+    }
+    if (!base_) return -1;
+    bytes = up256(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const size_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > bytes) free_[off + bytes] = len - bytes;
+      return (long)off;
+    }
+    return -1;
+  }
+  void free(size_t off, size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu_);
+    bytes = up256(bytes);
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  char *ptr(size_t off) const { return static_cast<char *>(base_) + off; }
+
+ private:
+  std::mutex mu_;
+  void *base_ = nullptr;
+  size_t size_ = 0;
+  bool tried_ = false;
+  std::map<size_t, size_t> free_;
+};
+
 struct ReadSetOut {
   saru_read_set set{};
   std::vector<int64_t> call_begin{0}, slot_begin{0};
   std::vector<int8_t> call_strand;
   std::vector<int32_t> ids, pos, goff, rindex, scores;
   std::vector<int8_t> dirs;
-  // outputs, written whole by the copies out (not zero-filled first: for a
-  // large request that costs as much as the copy)
-  std::unique_ptr<char[]> ra, ga;
-  std::unique_ptr<uint8_t[]> records;
+  // outputs, written whole by the copies out (not zero-filled first): in
+  // the server's pinned pool when it has room (pool offset >= 0), else in
+  // pageable memory the set owns
+  char *ra = nullptr, *ga = nullptr;
+  uint8_t *records = nullptr;
+  long pool_off = -1;
+  size_t pool_bytes = 0;
+  std::unique_ptr<char[]> owned;
   int64_t rec_bytes = 0;
   std::vector<int32_t> perfect_ids, perfect_pos;
   std::vector<int8_t> perfect_strand;
@@ -195,6 +257,7 @@ struct saru_server {
   saru::PackedGenome pg;
   int64_t genome_len = 0;
   std::vector<char> genome_host;  // the same genome, for the filters' q-gram indexes
+  HostPool host_pool;             // pinned memory for reads-only requests' results
   std::map<std::pair<int, int>, saru_filter *> filters;  // per (read length, k)
 
   struct Group {
@@ -224,6 +287,17 @@ struct saru_server {
     exc_byte = nullptr;
     pg = saru::PackedGenome{};
     genome_len = 0;
+  }
+
+  // Returns a reads-only request's pooled result ranges to the pool.
+  void free_outputs(Request &r) {
+    for (auto &o : r.rsets)
+      if (o.pool_off >= 0) {
+        host_pool.free((size_t)o.pool_off, o.pool_bytes);
+        o.pool_off = -1;
+        o.ra = o.ga = nullptr;
+        o.records = nullptr;
+      }
   }
 
   // The filter of (m, k) on the resident genome (created on first use).
@@ -306,23 +380,35 @@ struct saru_server {
       g.total_slots = acc + (int64_t)k * (b - a);
       o.gcalls.push_back(g);
     }
+    if (r.compact) o.rec_bytes = saru_compact_record_bytes(m, k);
+    const size_t half = r.compact ? n * (size_t)o.rec_bytes + 64 : (size_t)slots + 64;
+    const size_t total = r.compact ? half : 2 * up256(half);
+    o.pool_off = host_pool.alloc(total, (size_t)(cfg.host_pool_bytes > 0 ? cfg.host_pool_bytes
+                                                                         : (int64_t)4 << 30));
+    char *base;
+    if (o.pool_off >= 0) {
+      o.pool_bytes = total;
+      base = host_pool.ptr((size_t)o.pool_off);
+    } else {  // the pool is full or unavailable: pageable memory of the set's own
+      o.owned.reset(new char[total]);
+      base = o.owned.get();
+    }
     if (r.compact) {
-      o.rec_bytes = saru_compact_record_bytes(m, k);
-      o.records.reset(new uint8_t[n * (size_t)o.rec_bytes + 64]);
+      o.records = reinterpret_cast<uint8_t *>(base);
     } else {
-      o.ra.reset(new char[(size_t)slots + 64]);
-      o.ga.reset(new char[(size_t)slots + 64]);
-      memset(o.ra.get() + slots, 0, 64);
-      memset(o.ga.get() + slots, 0, 64);
+      o.ra = base;
+      o.ga = base + up256(half);
+      memset(o.ra + slots, 0, 64);
+      memset(o.ga + slots, 0, 64);
     }
     for (size_t c = 0; c < ncalls; ++c) {
       const int64_t a = o.call_begin[c];
       saru_result res{o.scores.data() + a, nullptr, nullptr, nullptr};
       if (r.compact) {
-        res.read_aln = reinterpret_cast<char *>(o.records.get() + a * o.rec_bytes);
+        res.read_aln = reinterpret_cast<char *>(o.records + a * o.rec_bytes);
       } else {
-        res.read_aln = o.ra.get() + o.slot_begin[c];
-        res.genome_aln = o.ga.get() + o.slot_begin[c];
+        res.read_aln = o.ra + o.slot_begin[c];
+        res.genome_aln = o.ga + o.slot_begin[c];
       }
       o.results.push_back(res);
     }
@@ -773,9 +859,9 @@ int saru_server_read_results(saru_server *s, int64_t ticket, int32_t set,
   out->pos = o.pos.data();
   out->dirs = o.dirs.data();
   out->scores = o.scores.data();
-  out->read_aln = o.ra.get();
-  out->genome_aln = o.ga.get();
-  out->records = o.records.get();
+  out->read_aln = o.ra;
+  out->genome_aln = o.ga;
+  out->records = o.records;
   out->record_bytes = o.rec_bytes;
   out->perfect_ids = o.perfect_ids.data();
   out->perfect_pos = o.perfect_pos.data();
@@ -787,7 +873,10 @@ void saru_server_release(saru_server *s, int64_t ticket) {
   if (!s) return;
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->read_done.find(ticket);
-  if (it != s->read_done.end() && it->second->done) s->read_done.erase(it);
+  if (it != s->read_done.end() && it->second->done) {
+    s->free_outputs(*it->second);
+    s->read_done.erase(it);
+  }
 }
 
 int saru_server_submit(saru_server *s, const saru_request *req, int64_t *ticket) {
