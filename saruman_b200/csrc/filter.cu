@@ -23,6 +23,7 @@
 #include <string.h>
 
 #include <future>
+#include <thread>
 #include <vector>
 
 #include "../../include/saruman_b200.h"
@@ -680,12 +681,10 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       if (e != cudaSuccess) break;
       wait_assembly();  // the last launch's calls first (and its staging set is free)
       assembling = std::async(std::launch::async, [&asmb, r0, cnt, hpos, hflag, hn, hq]() {
-        long at = 0;
-        for (long i = 0; i < cnt; ++i) {
-          asmb.add_read((int32_t)(r0 + i), hpos + at, hflag + at, hn[(size_t)i],
-                        hq[(size_t)i]);
-          at += hn[(size_t)i];
-        }
+        // the launch's reads at once, counted and copied on the host cores
+        // (the same calls as read-by-read assembly: test_filter_assembly.py)
+        const int hw = (int)std::thread::hardware_concurrency();
+        asmb.add_reads((int32_t)r0, cnt, hpos, hflag, hn, hq, hw > 0 ? hw : 1);
       });
       saru::count_launch();
     }

@@ -15,6 +15,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "filter_core.cuh"
@@ -72,8 +74,103 @@ class CallAssembler {
     if (queue_ > chunk_) flush();
   }
 
+  // The reads r0 .. r0 + cnt - 1 at once, in read order: read i has hn[i]
+  // kept positions at pos/flag + (sum of hn before i) and queued hq[i]
+  // positions.  The same calls as add_read for each read in turn: a window
+  // that does not fit the genome now never fits later in the run (the limit
+  // is fixed), so the pending positions add_read keeps never reach a call
+  // and are not kept here; the queue threshold's flush points come from a
+  // running sum of hq.  The reads' positions are counted and copied on up to
+  // `nthreads` host threads.
+  void add_reads(int32_t r0, long cnt, const int32_t *pos, const int8_t *flag,
+                 const int32_t *hn, const int32_t *hq, int nthreads) {
+    if (!entries_.empty()) {  // reads added one by one before: keep their order
+      long at = 0;
+      for (long i = 0; i < cnt; ++i) {
+        add_read(r0 + (int32_t)i, pos + at, flag + at, hn[i], hq[i]);
+        at += hn[i];
+      }
+      return;
+    }
+    if (cnt <= 0) return;
+    const int nt = (int)std::max(1L, std::min<long>(nthreads, cnt / 4096 + 1));
+    std::vector<int64_t> at((size_t)cnt + 1), nc((size_t)cnt + 1), np((size_t)cnt + 1);
+    at[0] = 0;
+    for (long i = 0; i < cnt; ++i) at[(size_t)i + 1] = at[(size_t)i] + hn[i];
+    auto fits = [&](int32_t p, int8_t f) {
+      int so = 0, eo = 0;
+      flank_of(f, k_, so, eo);
+      return (int64_t)(uint32_t)p + m_ + so + eo <= glen_;
+    };
+    auto parallel = [&](auto body) {
+      std::vector<std::thread> th;
+      for (int t = 1; t < nt; ++t) th.emplace_back(body, cnt * t / nt, cnt * (t + 1) / nt);
+      body(0L, cnt / nt);
+      for (auto &x : th) x.join();
+    };
+    // per read: candidates (positions > 0 whose window fits), perfect hits
+    parallel([&](long lo, long hi) {
+      for (long i = lo; i < hi; ++i) {
+        int64_t c = 0, q = 0;
+        for (int64_t j = at[(size_t)i]; j < at[(size_t)i + 1]; ++j) {
+          if (flag[j] == 0) ++q;
+          if (pos[j] > 0 && fits(pos[j], flag[j])) ++c;
+        }
+        nc[(size_t)i + 1] = c;
+        np[(size_t)i + 1] = q;
+      }
+    });
+    nc[0] = np[0] = 0;
+    for (long i = 0; i < cnt; ++i) {
+      nc[(size_t)i + 1] += nc[(size_t)i];
+      np[(size_t)i + 1] += np[(size_t)i];
+    }
+    const int64_t c0 = (int64_t)out.ids.size(), p0 = (int64_t)out.perfect_ids.size();
+    out.ids.resize((size_t)(c0 + nc[(size_t)cnt]));
+    out.pos.resize(out.ids.size());
+    out.dirs.resize(out.ids.size());
+    out.perfect_ids.resize((size_t)(p0 + np[(size_t)cnt]));
+    out.perfect_pos.resize(out.perfect_ids.size());
+    parallel([&](long lo, long hi) {
+      for (long i = lo; i < hi; ++i) {
+        int64_t c = c0 + nc[(size_t)i], q = p0 + np[(size_t)i];
+        for (int64_t j = at[(size_t)i]; j < at[(size_t)i + 1]; ++j) {
+          if (flag[j] == 0) {
+            out.perfect_ids[(size_t)q] = r0 + (int32_t)i;
+            out.perfect_pos[(size_t)q++] = -pos[j];
+          }
+          if (pos[j] > 0 && fits(pos[j], flag[j])) {
+            out.ids[(size_t)c] = r0 + (int32_t)i;
+            out.pos[(size_t)c] = pos[j];
+            out.dirs[(size_t)c++] = flag[j];
+          }
+        }
+      }
+    });
+    // flush points: after read i once the queued positions exceed the
+    // threshold; a call ends there if it holds a candidate
+    for (long i = 0; i < cnt; ++i) {
+      queue_ += (uint32_t)hq[i];
+      if (queue_ > chunk_) close_call(c0 + nc[(size_t)i + 1]);
+    }
+  }
+
   void finish() {
-    if (queue_ > 0) flush();
+    if (!entries_.empty() || pos_.size()) {
+      if (queue_ > 0) flush();
+      return;
+    }
+    // the last call, as add_read's finish flushes it: only when positions
+    // are queued (else the candidates since the last call are never
+    // submitted, as in the reference)
+    if (queue_ > 0) {
+      close_call((int64_t)out.ids.size());
+    } else {
+      const size_t end = (size_t)out.call_begin.back();
+      out.ids.resize(end);
+      out.pos.resize(end);
+      out.dirs.resize(end);
+    }
   }
 
   FilterCalls out;
@@ -84,6 +181,12 @@ class CallAssembler {
     int32_t id;
     uint32_t at, n;
   };
+
+  // A call boundary at candidate `end` (the batched path's flush).
+  void close_call(int64_t end) {
+    if (end > out.call_begin.back()) out.call_begin.push_back(end);
+    queue_ = 0;
+  }
 
   void flush() {
     const int64_t before = (int64_t)out.ids.size();

@@ -42,3 +42,17 @@ def gpu_available() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+@pytest.fixture
+def report(pytestconfig):
+    """Writes a line to the terminal even while output is captured (the
+    full-size tests' candidate counts and content hashes)."""
+    tr = pytestconfig.pluginmanager.getplugin("terminalreporter")
+
+    def write(line: str) -> None:
+        if tr is not None:
+            tr.write_line(line)
+        else:
+            print(line)
+    return write

@@ -38,7 +38,7 @@ def load_bench():
     return mod
 
 
-def align_and_check(cs, tag: str, outputs=None) -> None:
+def align_and_check(cs, tag: str, report, outputs=None) -> None:
     """Aligns every call of CallSet `cs` on the GPU (or takes `outputs` =
     (scores, read strings, window strings) made elsewhere) and checks every
     candidate and every call's TSV against the oracle."""
@@ -79,13 +79,13 @@ def align_and_check(cs, tag: str, outputs=None) -> None:
     h = hashlib.sha256()
     for a in (sc, ra[:cs.total_slots], ga[:cs.total_slots]):
         h.update(memoryview(a))
-    print(f"FULLSIZE {tag} m={m} k={k} candidates={cs.n} calls={cs.ncalls} "
-          f"aligned={int((sc <= k).sum())} tsv_bytes={sum(n for _, n in res)} "
-          f"sha256={h.hexdigest()[:16]}", flush=True)
+    report(f"FULLSIZE {tag} m={m} k={k} candidates={cs.n} calls={cs.ncalls} "
+           f"aligned={int((sc <= k).sum())} tsv_bytes={sum(n for _, n in res)} "
+           f"sha256={h.hexdigest()[:16]} oracle: every candidate equal")
 
 
 @pytest.mark.parametrize("name", ["c1", "c2", "c4", "c3"])
-def test_full_size_config_matches_the_oracle(saru_lib, name):
+def test_full_size_config_matches_the_oracle(saru_lib, report, name):
     import torch
     torch.cuda.set_device(0)
     bench = load_bench()
@@ -93,10 +93,10 @@ def test_full_size_config_matches_the_oracle(saru_lib, name):
     css = bench.build_callsets(cfg, 0)
     assert sum(cs.n for cs in css) > 0
     for cs in css:
-        align_and_check(cs, name)
+        align_and_check(cs, name, report)
 
 
-def test_full_size_serving_request_matches_the_oracle(saru_lib):
+def test_full_size_serving_request_matches_the_oracle(saru_lib, report):
     """The serving workload's largest request (500k reads, a quarter of
     them in each length bin) as a reads-only request through the server:
     every candidate of every call the server's filter made matches the
@@ -124,6 +124,6 @@ def test_full_size_serving_request_matches_the_oracle(saru_lib):
                        r["call_strand"])
         np.testing.assert_array_equal(cs.sbase, r["slot_begin"])
         pad = np.zeros(64, np.uint8)
-        align_and_check(cs, f"c5-request-m{m}",
+        align_and_check(cs, f"c5-request-m{m}", report,
                         outputs=(r["scores"], np.concatenate([r["read_aln"], pad]),
                                  np.concatenate([r["genome_aln"], pad])))
