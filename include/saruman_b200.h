@@ -162,8 +162,8 @@ int saru_align_host_compact(const saru_batch *batch, int32_t *scores, uint8_t *r
  * ordered on the stream.  Runs the banded kernel only (unit costs, k <= 15,
  * one read length m > 3k with m <= max_read_length <= 512); candidates it
  * cannot take are reported in result->status, with score k + 1.  `scratch`
- * must hold saru_scratch_bytes(n, max_read_length, k, k > 7) bytes of
- * device memory.  Enqueues no allocation, so it can be captured in a CUDA
+ * must be 16-byte aligned and hold saru_scratch_bytes(n, max_read_length,
+ * k, k > 7) bytes of device memory.  Enqueues no allocation, so it can be captured in a CUDA
  * graph. */
 int saru_align_device(const saru_batch *batch, saru_result *result, void *scratch,
                       size_t scratch_bytes, void *stream);

@@ -422,6 +422,10 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
     set_error("scratch too small: %zu < %zu", scratch_bytes, need);
     return SARU_E_INVALID;
   }
+  if (reinterpret_cast<uintptr_t>(scratch) & 15u) {  // the kernel copies 16-byte plane pairs
+    set_error("scratch must be 16-byte aligned");
+    return SARU_E_INVALID;
+  }
   a.counter = reinterpret_cast<int *>(scratch);
   a.planes = reinterpret_cast<uint8_t *>(scratch) + saru::kCounterBytes;
   SARU_CUDA(saru::launch_band_kernel(a, s));

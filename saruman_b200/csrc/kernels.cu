@@ -35,7 +35,16 @@ template <typename T>
 __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, uint8_t *st_reads,
                                          uint8_t *st_win, uint8_t *region, void *planes_v,
                                          long pslot) {
-  PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v);
+  // this lane's plane pairs: column j at lane_planes + j * col_bytes (a
+  // column of the whole grid's lanes is a few MB, so the offset of one
+  // column is a 32-bit product widened by one multiply-add)
+  const long mul = ta.pair_mul;
+  uint8_t *lane_planes = reinterpret_cast<uint8_t *>(planes_v) +
+                         plane_index(0, ta.pstride, pslot, mul) * (long)sizeof(PlanePair<T>);
+  const uint32_t col_bytes = (uint32_t)(plane_index(1, ta.pstride, 0, mul) * (long)sizeof(PlanePair<T>));
+  auto pair_at = [&](int j) -> PlanePair<T> * {
+    return reinterpret_cast<PlanePair<T> *>(lane_planes + (unsigned long long)(uint32_t)j * col_bytes);
+  };
   uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
   auto ld16 = [](uint8_t *d, const uint8_t *g) {
     *reinterpret_cast<uint4 *>(d) = __ldg(reinterpret_cast<const uint4 *>(g));
@@ -54,19 +63,34 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
   stage_in(st_win, ta.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
   __syncwarp();
   LaneState ls;
-  const long mul = ta.pair_mul;
-  int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls, [&](int j, T A, T B) {
-    planes[plane_index(j, ta.pstride, pslot, mul)] = PlanePair<T>{A, B};
-  });
+  int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls,
+                        [&](int j, T A, T B) { *pair_at(j) = PlanePair<T>{A, B}; });
   __syncwarp();
+  // the traceback walk's plane ring in the region: asynchronous 8- or
+  // 16-byte copies from the plane scratch, one copy group per column
+  const auto ring = plane_ring<T>(
+      reinterpret_cast<PlanePair<T> *>(region) + lane,
+      [&](PlanePair<T> *dst, int j) {
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+        const size_t g = __cvta_generic_to_global(pair_at(j));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(g),
+                     "n"((int)sizeof(PlanePair<T>))
+                     : "memory");
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+      },
+      [] { asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1) : "memory"); });
   if (ta.records) {  // compact records straight to global memory
     uint32_t *rec = reinterpret_cast<uint32_t *>(ta.records + (s.t0 + lane) * ta.rec_bytes);
-    st |= lane_traceback_ops<T>(
-        ta, s, lane, ls, [&](int j) { return planes[plane_index(j, ta.pstride, pslot, mul)]; },
-        [&](int w, uint32_t v) { rec[w] = v; });
+    st |= lane_traceback_ops<T>(ta, s, lane, ls, ring, [&](int w, uint32_t v) { rec[w] = v; });
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
     return st;
   }
+  uint32_t up_r[kMaxGapRuns], left_r[kMaxGapRuns];
+  LaneWalk w;
+  st |= lane_traceback_walk<T>(ta, s, lane, ls, ring, up_r, left_r, w);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncwarp();
   uint8_t *out_r = region;
   uint8_t *out_g = region + s.o_span_r;
   const long out_bytes = out_area_bytes(ta.max_m, ta.k);
@@ -76,8 +100,7 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
     for (long i = lane; i < nv; i += 32) p4[i] = make_uint4(0, 0, 0, 0);
   }
   __syncwarp();
-  auto ld_pair = [&](int j) { return planes[plane_index(j, ta.pstride, pslot, mul)]; };
-  st |= lane_traceback<T>(ta, s, lane, st_reads, st_win, out_r, out_g, ls, ld_pair);
+  lane_write_strings(ta, s, lane, st_reads, st_win, out_r, out_g, ls, w);
   __syncwarp();
   stage_out(ta.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
   stage_out(ta.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);

@@ -105,6 +105,29 @@ SARU_HD T window_bits(P mask, int j) {
   return WindowBits<T, P>::get(mask, j);
 }
 
+// bits [s, s + BITS) of the words at p (0 <= s < 32)
+template <typename T, class P>
+SARU_HD T window_bits_at(P p, int s);
+
+template <>
+SARU_HD uint32_t window_bits_at<uint32_t, Strided>(Strided p, int s) {
+  return fshr32(p[0], p[1], (uint32_t)s);
+}
+template <>
+SARU_HD uint64_t window_bits_at<uint64_t, Strided>(Strided p, int s) {
+  const uint32_t a = p[0], b = p[1], c = p[2];
+  return (uint64_t)fshr32(a, b, (uint32_t)s) | ((uint64_t)fshr32(b, c, (uint32_t)s) << 32);
+}
+template <>
+SARU_HD uint32_t window_bits_at<uint32_t, uint32_t *>(uint32_t *p, int s) {
+  return fshr32(p[0], p[1], (uint32_t)s);
+}
+template <>
+SARU_HD uint64_t window_bits_at<uint64_t, uint32_t *>(uint32_t *p, int s) {
+  const uint32_t a = p[0], b = p[1], c = p[2];
+  return (uint64_t)fshr32(a, b, (uint32_t)s) | ((uint64_t)fshr32(b, c, (uint32_t)s) << 32);
+}
+
 SARU_HD int base_code(uint8_t c) {
   switch (c) {
     case 'A': return 0;
@@ -141,7 +164,7 @@ template <class ReadFn, class WinFn, class P>
 SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, P codes, P mask, int mwords) {
   uint8_t extra[MAX_EXTRA];
   int nextra = 0;
-  for (int w = 0; w < (c.m + 7) / 8; ++w) codes[w] = 0;
+  for (int w = 0; w <= c.m / 8; ++w) codes[w] = 0;
   for (int j = 0; j < c.m; ++j) {
     uint8_t ch = rd(j);
     int code = base_code(ch);
@@ -154,7 +177,7 @@ SARU_HD bool build_codes(const Cand &c, ReadFn rd, WinFn wn, P codes, P mask, in
       }
       code = 4 + e;
     }
-    codes[j >> 3] |= (uint32_t)code << ((j & 7) * 4);
+    codes[(j + 1) >> 3] |= (uint32_t)code << (((j + 1) & 7) * 4);
   }
   for (int w = 0; w < NCODES * mwords; ++w) mask[w] = 0;
   for (int p = 0; p < c.L; ++p) {
@@ -200,6 +223,7 @@ SARU_HD uint32_t ascii_of_nibbles(uint32_t nib) { return byte_perm(0x54474341u, 
 template <class Rd4, class Wn4, class P>
 SARU_HD bool build_codes_acgt(const Cand &c, Rd4 rd4, Wn4 wn4, P codes, P mask, int mwords) {
   uint32_t bad = 0;
+  uint32_t prev = 0;  // the previous word's codes (its last nibble moves to the next word)
   for (int w = 0; 8 * w < c.m; ++w) {
     const uint32_t x0 = rd4(8 * w), x1 = rd4(8 * w + 4);
     const uint32_t s0 = codes4_nibbles(base_codes4(x0));
@@ -208,8 +232,11 @@ SARU_HD bool build_codes_acgt(const Cand &c, Rd4 rd4, Wn4 wn4, P codes, P mask, 
     const uint32_t k0 = left >= 4 ? 0xFFFFFFFFu : ((1u << (8 * left)) - 1u);
     const uint32_t k1 = left >= 8 ? 0xFFFFFFFFu : (left > 4 ? ((1u << (8 * (left - 4))) - 1u) : 0u);
     bad |= ((ascii_of_nibbles(s0) ^ x0) & k0) | ((ascii_of_nibbles(s1) ^ x1) & k1);
-    codes[w] = s0 | (s1 << 16);
+    const uint32_t cw = s0 | (s1 << 16);
+    codes[w] = (cw << 4) | (prev >> 28);
+    prev = cw;
   }
+  if (c.m % 8 == 0) codes[c.m / 8] = prev >> 28;
   if (bad) return false;
   // window bit-planes P0/P1 (code bits) over positions, 32 per word; mask
   // bit (p + k + 1) of class c is set iff window byte p is base c
@@ -256,7 +283,7 @@ SARU_HD bool build_codes_acgt(const Cand &c, Rd4 rd4, Wn4 wn4, P codes, P mask, 
 
 template <class P>
 SARU_HD int code_at(P codes, int j) {
-  return (codes[j >> 3] >> ((j & 7) * 4)) & 15;
+  return (codes[(j + 1) >> 3] >> (((j + 1) & 7) * 4)) & 15;
 }
 
 // One column of the bit-parallel recurrence.  In: the previous column's
@@ -290,7 +317,7 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
   {
     // column 1, with the first-column quirk of the traceback: rows <= 2so+3
     // (bits <= 2so + k + 2) take the vertical test with cost 0
-    const T eq = window_bits<T>(mask + (int)(codes[0] & 15u) * mwords, 1);
+    const T eq = window_bits<T>(mask + (int)((codes[0] >> 4) & 15u) * mwords, 1);
     T d0, hp;
     myers_step<T>((Pv >> 1) | TOPBIT, Mv >> 1, eq, Pv, Mv, d0, hp);
     const T col1_corr = c.so ? lowmask<T>(2 * c.so + k + 3) : T(0);
@@ -299,16 +326,20 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
     planes(1, diag | (~up & hp), ~diag & (up | hp));
     top += (int)((~d0) & T(1));
   }
-  // columns 2..m-1; column j matches read byte j-1 (code word (j-1)/8)
-  for (int w = 0; 8 * w + 1 < m; ++w) {
+  // columns 2..m-1; column j matches read byte j-1, nibble j & 7 of code
+  // word j >> 3; the eight columns of a code word read mask words j >> 5
+  // and (j >> 5) + 1 of the read byte's class
+  for (int w = 0; 8 * w < m; ++w) {
     const uint32_t cw = codes[w];
+    const P row = mask + (w >> 2);
+    const int sh0 = 8 * (w & 3);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int j = 8 * w + i + 1;
+      const int j = 8 * w + i;
       if (j < 2) continue;
       if (j >= m) break;
       const int code = (int)((cw >> (4 * i)) & 15u);
-      const T eq = window_bits<T>(mask + code * mwords, j);
+      const T eq = window_bits_at<T>(row + code * mwords, sh0 + i);
       T d0, hp;
       myers_step<T>((Pv >> 1) | TOPBIT, Mv >> 1, eq, Pv, Mv, d0, hp);
       const T diag = ~d0 | eq;

@@ -58,26 +58,32 @@ static int run(const TileArgs &a0, int nwarps_total) {
                                  planes[plane_index(j, a.pstride, pslot, 1)] = PlanePair<T>{A, B};
                                });
       }
+      // the walk's plane ring in the region; copies land at once here
+      auto ring_of = [&](int lane) {
+        const long pslot = (long)gwarp * 32 + lane;
+        return plane_ring<T>(
+            reinterpret_cast<PlanePair<T> *>(region) + lane,
+            [=](PlanePair<T> *dst, int j) { *dst = planes[plane_index(j, a.pstride, pslot, 1)]; },
+            [] {});
+      };
       if (a.records) {  // compact records straight to the (exactly sized) output
         for (int lane = 0; lane < 32; ++lane) {
-          const long pslot = (long)gwarp * 32 + lane;
           uint32_t *rec = reinterpret_cast<uint32_t *>(a.records + (s.t0 + lane) * a.rec_bytes);
-          status |= lane_traceback_ops<T>(
-              a, s, lane, ls[lane],
-              [&](int j) { return planes[plane_index(j, a.pstride, pslot, 1)]; },
-              [&](int w, uint32_t v) { rec[w] = v; });
+          status |= lane_traceback_ops<T>(a, s, lane, ls[lane], ring_of(lane),
+                                          [&](int w, uint32_t v) { rec[w] = v; });
         }
         continue;
       }
+      uint32_t up_r[32][kMaxGapRuns], left_r[32][kMaxGapRuns];
+      LaneWalk walks[32];
+      for (int lane = 0; lane < 32; ++lane)
+        status |= lane_traceback_walk<T>(a, s, lane, ls[lane], ring_of(lane), up_r[lane],
+                                         left_r[lane], walks[lane]);
       uint8_t *out_r = region, *out_g = region + s.o_span_r;
       const long out_bytes = out_area_bytes(a.max_m, a.k);
       memset(region, 0, (size_t)out_bytes);
-      for (int lane = 0; lane < 32; ++lane) {
-        const long pslot = (long)gwarp * 32 + lane;
-        status |= lane_traceback<T>(
-            a, s, lane, st_reads, st_win, out_r, out_g, ls[lane],
-            [&](int j) { return planes[plane_index(j, a.pstride, pslot, 1)]; });
-      }
+      for (int lane = 0; lane < 32; ++lane)
+        lane_write_strings(a, s, lane, st_reads, st_win, out_r, out_g, ls[lane], walks[lane]);
       for (int lane = 0; lane < 32; ++lane) {
         stage_out(a.read_aln, out_r, s.s_lo, s.s_hi, s.o_base_r, lane, st16);
         stage_out(a.genome_aln, out_g, s.s_lo, s.s_hi, s.o_base_g, lane, st16);
@@ -227,15 +233,25 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
       auto trace = [&](auto tag) {
         using T = decltype(tag);
         PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
+        uint32_t up_r[32][kMaxGapRuns], left_r[32][kMaxGapRuns];
+        LaneWalk walks[32];
+        for (int lane = 0; lane < 32; ++lane) {
+          const long pslot = (long)gw * 32 + lane;
+          const auto ring = plane_ring<T>(
+              reinterpret_cast<PlanePair<T> *>(w.region) + lane,
+              [=](PlanePair<T> *dst, int j) {
+                *dst = planes[plane_index(j, pstride, pslot, a.pair_mul)];
+              },
+              [] {});
+          status |= lane_traceback_walk<T>(a, w.span, lane, w.ls[lane], ring, up_r[lane],
+                                           left_r[lane], walks[lane]);
+        }
         const long out_bytes = out_area_bytes(a.max_m, a.k);
         memset(w.region, 0, (size_t)out_bytes);
         uint8_t *out_r = w.region, *out_g = w.region + w.span.o_span_r;
-        for (int lane = 0; lane < 32; ++lane) {
-          const long pslot = (long)gw * 32 + lane;
-          status |= lane_traceback<T>(
-              a, w.span, lane, w.st_reads, w.st_win, out_r, out_g, w.ls[lane],
-              [&](int j) { return planes[plane_index(j, pstride, pslot, a.pair_mul)]; });
-        }
+        for (int lane = 0; lane < 32; ++lane)
+          lane_write_strings(a, w.span, lane, w.st_reads, w.st_win, out_r, out_g, w.ls[lane],
+                             walks[lane]);
         for (int lane = 0; lane < 32; ++lane) {
           stage_out(a.read_aln, out_r, w.span.s_lo, w.span.s_hi, w.span.o_base_r, lane, st16);
           stage_out(a.genome_aln, out_g, w.span.s_lo, w.span.s_hi, w.span.o_base_g, lane, st16);
