@@ -32,10 +32,8 @@ struct TileArgs {
   int k, max_m, first_of_call;
   int32_t *scores;
   uint8_t *read_aln, *genome_aln;
-  void *planes;       // plane_columns(max_m) * pstride plane pairs (plane_index)
+  void *planes;       // plane_units(max_m, wide) x pstride units of kPlaneUnit bytes
   long pstride;       // lanes of the whole grid
-  long pair_mul;      // plane-pair index multiplier: 2 when 32-bit pairs share a
-                      // launch with 64-bit ones (one slot size for every lane)
   long rs_bytes, ws_bytes, region_bytes;
   uint8_t *records;  // compact result records instead of slot strings (nullptr: slots)
   long rec_bytes;    // bytes per record (compact_record_bytes)
@@ -181,15 +179,59 @@ struct PlanePair {
   T A, B;
 };
 
-// Decision planes in the scratch: [column][lane], so the fill's store of a
-// column is one contiguous 256-byte (512-byte) run per warp.  (Runs of
-// columns per lane would give the traceback's walk better L1 locality, but
-// their fill stores touch a sector per lane and measured twice as slow.)
-// `mul` spaces 32-bit pairs like 64-bit ones when a launch mixes both.
-SARU_HD long plane_columns(int max_m) { return (long)max_m + 1; }  // columns 0..max_m
+// Decision planes in the scratch: 16-byte units, [unit][lane], so a warp's
+// store of a unit is one contiguous 512-byte run.  A unit holds the pairs
+// of two columns of a 32-bit band (column j in unit j >> 1 at byte
+// (j & 1) * 8) or of one column of a 64-bit band (unit j): the fill stores
+// 16 bytes a lane every other column of a 32-bit band.  (Runs of columns
+// per lane would give the traceback's walk better locality, but their fill
+// stores touch a sector per lane and measured twice as slow.)
+constexpr long kPlaneUnit = 16;
 
-SARU_HD long plane_index(int j, long pstride, long pslot, long mul) {
-  return ((long)j * pstride + pslot) * mul;
+// Units a lane needs for columns 0..max_m.
+SARU_HD long plane_units(int max_m, bool wide) {
+  return wide ? (long)max_m + 1 : (long)(max_m >> 1) + 1;
+}
+
+// Byte offset of column j's pair in unit row 0 of a lane (add the lane's
+// slot * kPlaneUnit and the unit row's bytes).
+template <typename T>
+SARU_HD long plane_unit_of(int j) {
+  return sizeof(T) == 4 ? (long)(j >> 1) : (long)j;
+}
+template <typename T>
+SARU_HD long plane_half_of(int j) {
+  return sizeof(T) == 4 ? (long)(j & 1) * 8 : 0L;
+}
+
+// The fill's plane sink for one lane: put(unit, x, y, z, w) stores one
+// 16-byte unit.  A 32-bit band's even column waits in (pa, pb) for the odd
+// one; the last column (`last`), if even, goes out with a zero partner.
+// Column 0 has no planes (the walk never reads it), so unit 0 carries zeros
+// in its first half.
+template <typename T, class Put16>
+struct PlaneWriter {
+  Put16 put;
+  uint32_t pa, pb;
+  SARU_HD void operator()(int j, T A, T B, bool last) {
+    if (sizeof(T) == 4) {
+      if (j & 1) {
+        put(j >> 1, pa, pb, (uint32_t)A, (uint32_t)B);
+      } else {
+        pa = (uint32_t)A;
+        pb = (uint32_t)B;
+        if (last) put(j >> 1, pa, pb, 0u, 0u);
+      }
+    } else {
+      const uint64_t a = (uint64_t)A, b = (uint64_t)B;
+      put(j, (uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+    }
+  }
+};
+
+template <typename T, class Put16>
+SARU_HD PlaneWriter<T, Put16> plane_writer(Put16 put) {
+  return PlaneWriter<T, Put16>{put, 0u, 0u};
 }
 
 // Compact result record of one candidate (the alternative to its two slot

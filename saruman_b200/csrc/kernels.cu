@@ -35,15 +35,15 @@ template <typename T>
 __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, uint8_t *st_reads,
                                          uint8_t *st_win, uint8_t *region, void *planes_v,
                                          long pslot) {
-  // this lane's plane pairs: column j at lane_planes + j * col_bytes (a
-  // column of the whole grid's lanes is a few MB, so the offset of one
-  // column is a 32-bit product widened by one multiply-add)
-  const long mul = ta.pair_mul;
-  uint8_t *lane_planes = reinterpret_cast<uint8_t *>(planes_v) +
-                         plane_index(0, ta.pstride, pslot, mul) * (long)sizeof(PlanePair<T>);
-  const uint32_t col_bytes = (uint32_t)(plane_index(1, ta.pstride, 0, mul) * (long)sizeof(PlanePair<T>));
+  // this lane's plane units: unit u at lane_units + u * row_bytes (a unit
+  // row of the whole grid's lanes is a few MB, so the offset of a unit is a
+  // 32-bit product widened by one multiply-add)
+  uint8_t *lane_units = reinterpret_cast<uint8_t *>(planes_v) + pslot * kPlaneUnit;
+  const uint32_t row_bytes = (uint32_t)(ta.pstride * kPlaneUnit);
   auto pair_at = [&](int j) -> PlanePair<T> * {
-    return reinterpret_cast<PlanePair<T> *>(lane_planes + (unsigned long long)(uint32_t)j * col_bytes);
+    return reinterpret_cast<PlanePair<T> *>(
+        lane_units + (unsigned long long)(uint32_t)plane_unit_of<T>(j) * row_bytes +
+        plane_half_of<T>(j));
   };
   uint32_t *region32 = reinterpret_cast<uint32_t *>(region);
   auto ld16 = [](uint8_t *d, const uint8_t *g) {
@@ -63,8 +63,13 @@ __device__ __forceinline__ int band_tile(const TileArgs &ta, long wt, int lane, 
   stage_in(st_win, ta.genome, s.g_lo, s.g_hi, s.g_base, lane, ld16, ld1);
   __syncwarp();
   LaneState ls;
-  int st = lane_fill<T>(ta, s, lane, st_reads, st_win, region32, ls,
-                        [&](int j, T A, T B) { *pair_at(j) = PlanePair<T>{A, B}; });
+  int st = lane_fill<T>(
+      ta, s, lane, st_reads, st_win, region32, ls,
+      plane_writer<T>(
+          [&](long u, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+            *reinterpret_cast<uint4 *>(lane_units + (unsigned long long)(uint32_t)u * row_bytes) =
+                make_uint4(x, y, z, w);
+          }));
   __syncwarp();
   // the traceback walk's plane ring in the region: asynchronous 8- or
   // 16-byte copies from the plane scratch, one copy group per column
@@ -138,8 +143,8 @@ __global__ void __launch_bounds__(128, 4) saru_band_kernel(const __grid_constant
     const Segment &g = a.segs[lo];
     const TileArgs ta{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
                       g.first_of_call, g.scores, g.read_aln, g.genome_aln, a.planes, pstride,
-                      (!g.wide && a.wide_any) ? 2L : 1L, a.rs_bytes, a.ws_bytes,
-                      a.warp_smem - a.rs_bytes - a.ws_bytes, g.records, g.rec_bytes, g.t0};
+                      a.rs_bytes, a.ws_bytes, a.warp_smem - a.rs_bytes - a.ws_bytes,
+                      g.records, g.rec_bytes, g.t0};
     const long wt = tile - g.tile_begin;
     int status = g.wide ? band_tile<uint64_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot)
                         : band_tile<uint32_t>(ta, wt, lane, st_reads, st_win, region, a.planes, pslot);
@@ -328,8 +333,8 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_c
 
 size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req) {
   const BandLayout L = band_layout(max_m, k, warps_req);
-  return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) * 2 *
-                             (size_t)plane_columns(max_m) * (wide ? 8 : 4);
+  return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) *
+                             (size_t)plane_units(max_m, wide) * kPlaneUnit;
 }
 
 cudaError_t launch_full_kernels(const FullArgs &a, cudaStream_t s) {

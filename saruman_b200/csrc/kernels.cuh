@@ -44,7 +44,7 @@ struct KernelArgs {
   int nseg;
   long total_tiles;
   int *counter;  // zeroed before the launch: next tile to take
-  void *planes;  // decision planes: plane_columns(max_m) x lanes pairs of the widest band word
+  void *planes;  // decision planes: plane_units(max_m, wide_any) x lanes units (band_tile.cuh)
   long grid;
   int max_m, max_k, wide_any;
   int warps_req;                       // requested warps per CTA (0: as many as fit)

@@ -286,6 +286,19 @@ SARU_HD int code_at(P codes, int j) {
   return (codes[(j + 1) >> 3] >> (((j + 1) & 7) * 4)) & 15;
 }
 
+// x >> 1 with the top bit set (one funnel shift a 32-bit word).
+template <typename T>
+SARU_HD T shr1_top(T x);
+template <>
+SARU_HD uint32_t shr1_top<uint32_t>(uint32_t x) {
+  return fshr32(x, 1u, 1);
+}
+template <>
+SARU_HD uint64_t shr1_top<uint64_t>(uint64_t x) {
+  return (uint64_t)fshr32((uint32_t)x, (uint32_t)(x >> 32), 1) |
+         ((uint64_t)fshr32((uint32_t)(x >> 32), 1u, 1) << 32);
+}
+
 // One column of the bit-parallel recurrence.  In: the previous column's
 // vertical-delta vectors realigned to this column's rows (pv, mv) and the
 // match vector eq.  Out: this column's vectors (Pv, Mv), the diagonal-zero
@@ -302,7 +315,7 @@ SARU_HD void myers_step(T pv, T mv, T eq, T &Pv, T &Mv, T &d0, T &hp) {
   Mv = hp1 & d0;
 }
 
-// Fill of one candidate.  `planes(j, A, B)` receives the decision planes of
+// Fill of one candidate.  `planes(j, A, B, last)` receives the decision planes of
 // read column j (1..m): code = A | 2B per band bit.  Returns D[L][m] if it
 // is <= k, otherwise k + 1.
 template <typename T, class P, class PlaneSink>
@@ -323,7 +336,7 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
     const T col1_corr = c.so ? lowmask<T>(2 * c.so + k + 3) : T(0);
     const T up = (Pv & ~col1_corr) | (~(Pv | Mv) & col1_corr);
     const T diag = ~d0 | eq;
-    planes(1, diag | (~up & hp), ~diag & (up | hp));
+    planes(1, diag | (~up & hp), ~diag & (up | hp), false);
     top += (int)((~d0) & T(1));
   }
   // columns 2..m-1; column j matches read byte j-1, nibble j & 7 of code
@@ -341,9 +354,9 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
       const int code = (int)((cw >> (4 * i)) & 15u);
       const T eq = window_bits_at<T>(row + code * mwords, sh0 + i);
       T d0, hp;
-      myers_step<T>((Pv >> 1) | TOPBIT, Mv >> 1, eq, Pv, Mv, d0, hp);
+      myers_step<T>(shr1_top<T>(Pv), Mv >> 1, eq, Pv, Mv, d0, hp);
       const T diag = ~d0 | eq;
-      planes(j, diag | (~Pv & hp), ~diag & (Pv | hp));
+      planes(j, diag | (~Pv & hp), ~diag & (Pv | hp), false);
       top += (int)((~d0) & T(1));
     }
   }
@@ -375,7 +388,7 @@ SARU_HD int fill_band(const Cand &c, P codes, P mask, int mwords, PlaneSink plan
     vb = vb1;
     if (b == bmax) score = v;
   }
-  planes(m, A, B);
+  planes(m, A, B, true);
   return score <= k ? score : k + 1;
 }
 

@@ -31,7 +31,7 @@ static int run(const Cand &c, const uint8_t *read, const uint8_t *win, int *scor
                    codes.data(), mask.data(), mw))
     return 1;
   std::vector<T> PA(c.m + 1), PB(c.m + 1);
-  int s = fill_band<T>(c, codes.data(), mask.data(), mw, [&](int j, T A, T B) {
+  int s = fill_band<T>(c, codes.data(), mask.data(), mw, [&](int j, T A, T B, bool) {
     PA[j] = A;
     PB[j] = B;
   });

@@ -14,6 +14,12 @@
 
 using namespace saru;
 
+// Byte offset of column j's plane pair of lane pslot (the kernel's layout).
+template <typename T>
+static long pair_off(int j, long pstride, long pslot) {
+  return (plane_unit_of<T>(j) * pstride + pslot) * kPlaneUnit + plane_half_of<T>(j);
+}
+
 template <typename T>
 static int run(const TileArgs &a0, int nwarps_total) {
   TileArgs a = a0;
@@ -22,8 +28,9 @@ static int run(const TileArgs &a0, int nwarps_total) {
   a.ws_bytes = S.ws_bytes;
   a.region_bytes = S.region_bytes;
   a.pstride = (long)nwarps_total * 32;
-  std::vector<PlanePair<T>> planes_v((size_t)plane_columns(a.max_m) * a.pstride);
-  PlanePair<T> *planes = planes_v.data();
+  std::vector<uint8_t> planes_v((size_t)plane_units(a.max_m, sizeof(T) == 8) * a.pstride *
+                                kPlaneUnit);
+  uint8_t *planes = planes_v.data();
   int status = 0;
   auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
   auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
@@ -53,17 +60,22 @@ static int run(const TileArgs &a0, int nwarps_total) {
       LaneState ls[32];
       for (int lane = 0; lane < 32; ++lane) {
         const long pslot = (long)gwarp * 32 + lane;
-        status |= lane_fill<T>(a, s, lane, st_reads, st_win, region32, ls[lane],
-                               [&](int j, T A, T B) {
-                                 planes[plane_index(j, a.pstride, pslot, 1)] = PlanePair<T>{A, B};
-                               });
+        status |= lane_fill<T>(
+            a, s, lane, st_reads, st_win, region32, ls[lane],
+            plane_writer<T>(
+                [&](long u, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+                  const uint32_t v[4] = {x, y, z, w};
+                  memcpy(planes + (u * a.pstride + pslot) * kPlaneUnit, v, 16);
+                }));
       }
       // the walk's plane ring in the region; copies land at once here
       auto ring_of = [&](int lane) {
         const long pslot = (long)gwarp * 32 + lane;
         return plane_ring<T>(
             reinterpret_cast<PlanePair<T> *>(region) + lane,
-            [=](PlanePair<T> *dst, int j) { *dst = planes[plane_index(j, a.pstride, pslot, 1)]; },
+            [=](PlanePair<T> *dst, int j) {
+              memcpy(dst, planes + pair_off<T>(j, a.pstride, pslot), sizeof(PlanePair<T>));
+            },
             [] {});
       };
       if (a.records) {  // compact records straight to the (exactly sized) output
@@ -103,7 +115,7 @@ extern "C" int tile_align_batch(const uint8_t *genome, const uint8_t *reads, con
                                 int wide, int first_of_call, int nwarps, int *scores,
                                 uint8_t *ra, uint8_t *ga) {
   TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, ra, ga,
-             nullptr, 0, 1, 0, 0, 0};
+             nullptr, 0, 0, 0, 0};
   return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
 }
 
@@ -117,7 +129,7 @@ extern "C" int tile_align_slices(const uint8_t *genome, const uint8_t *reads, co
   int status = 0;
   for (long t0 = 0; t0 < n; t0 += slice) {
     TileArgs a{genome, reads, goff, roff, dirs, t0 + slice < n ? t0 + slice : n, k, max_m,
-               first_of_call, scores, ra, ga, nullptr, 0, 1, 0, 0, 0, nullptr, 0, t0};
+               first_of_call, scores, ra, ga, nullptr, 0, 0, 0, 0, nullptr, 0, t0};
     status |= wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
   }
   return status;
@@ -130,7 +142,7 @@ extern "C" int tile_align_compact(const uint8_t *genome, const uint8_t *reads, c
                                   int wide, int first_of_call, int nwarps, int *scores,
                                   uint8_t *records, long rec_bytes) {
   TileArgs a{genome, reads, goff, roff, dirs, n, k, max_m, first_of_call, scores, nullptr,
-             nullptr, nullptr, 0, 1, 0, 0, 0, records, rec_bytes};
+             nullptr, nullptr, 0, 0, 0, 0, records, rec_bytes};
   return wide ? run<uint64_t>(a, nwarps) : run<uint32_t>(a, nwarps);
 }
 
@@ -161,7 +173,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
   const SliceLayout S = slice_layout(max_m, max_k);
   const long pstride = (long)nwarps_total * 32;
   // exactly the bytes the launcher reserves for the planes
-  std::vector<uint8_t> planes_v((size_t)plane_columns(max_m) * pstride * 2 * (wide_any ? 8 : 4));
+  std::vector<uint8_t> planes_v((size_t)plane_units(max_m, wide_any != 0) * pstride * kPlaneUnit);
   int status = 0;
   auto ld16 = [](uint8_t *d, const uint8_t *g) { memcpy(d, g, 16); };
   auto ld1 = [](const uint8_t *g) -> uint8_t { return *g; };
@@ -183,7 +195,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
     const HostSeg &g = segs[si];
     return TileArgs{g.genome, g.reads, g.goff, g.roff, g.dirs, g.n, g.k, g.max_m,
                     g.first_of_call, g.scores, g.ra, g.ga, planes_v.data(), pstride,
-                    (!g.wide && wide_any) ? 2L : 1L, S.rs_bytes, S.ws_bytes, S.region_bytes};
+                    S.rs_bytes, S.ws_bytes, S.region_bytes};
   };
   // rounds: every warp takes a tile, all fills run, then all tracebacks --
   // the interleaving in which one lane's planes could clobber another's
@@ -208,19 +220,21 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
       }
       auto fill = [&](auto tag) {
         using T = decltype(tag);
-        PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
+        uint8_t *planes = planes_v.data();
         for (int lane = 0; lane < 32; ++lane) {
           stage_in(w.st_reads, a.reads, w.span.r_lo, w.span.r_hi, w.span.r_base, lane, ld16, ld1);
           stage_in(w.st_win, a.genome, w.span.g_lo, w.span.g_hi, w.span.g_base, lane, ld16, ld1);
         }
         for (int lane = 0; lane < 32; ++lane) {
           const long pslot = (long)gw * 32 + lane;
-          status |= lane_fill<T>(a, w.span, lane, w.st_reads, w.st_win,
-                                 reinterpret_cast<uint32_t *>(w.region), w.ls[lane],
-                                 [&](int j, T A, T B) {
-                                   planes[plane_index(j, pstride, pslot, a.pair_mul)] =
-                                       PlanePair<T>{A, B};
-                                 });
+          status |= lane_fill<T>(
+              a, w.span, lane, w.st_reads, w.st_win, reinterpret_cast<uint32_t *>(w.region),
+              w.ls[lane],
+              plane_writer<T>(
+                  [&](long u, uint32_t x, uint32_t y, uint32_t z, uint32_t q) {
+                    const uint32_t v[4] = {x, y, z, q};
+                    memcpy(planes + (u * pstride + pslot) * kPlaneUnit, v, 16);
+                  }));
         }
       };
       if (segs[lo].wide) fill(uint64_t(0));
@@ -232,7 +246,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
       const TileArgs a = targs(w.seg);
       auto trace = [&](auto tag) {
         using T = decltype(tag);
-        PlanePair<T> *planes = reinterpret_cast<PlanePair<T> *>(planes_v.data());
+        uint8_t *planes = planes_v.data();
         uint32_t up_r[32][kMaxGapRuns], left_r[32][kMaxGapRuns];
         LaneWalk walks[32];
         for (int lane = 0; lane < 32; ++lane) {
@@ -240,7 +254,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
           const auto ring = plane_ring<T>(
               reinterpret_cast<PlanePair<T> *>(w.region) + lane,
               [=](PlanePair<T> *dst, int j) {
-                *dst = planes[plane_index(j, pstride, pslot, a.pair_mul)];
+                memcpy(dst, planes + pair_off<T>(j, pstride, pslot), sizeof(PlanePair<T>));
               },
               [] {});
           status |= lane_traceback_walk<T>(a, w.span, lane, w.ls[lane], ring, up_r[lane],
