@@ -544,7 +544,13 @@ def serving(S, cfg: dict, nreq: int, seed: int = 4242, compact_too: bool = False
     sizes = sizes.astype(np.int64)
     reqs = [pool.make(int(x), rng) for x in sizes]
     warm = [pool.make(20_000, rng) for _ in range(3)]
-    probe = [pool.make(100_000, rng) for _ in range(6)]
+    # the capacity probe draws its requests from the trace's own size
+    # distribution (a fixed request size misjudges the plain loop's capacity
+    # for the trace's mix of small and large requests)
+    prng = np.random.default_rng(seed + 1)
+    psizes = np.exp(prng.uniform(np.log(cfg["min_reads"]), np.log(cfg["max_reads"]),
+                                 max(16, nreq // 4))).astype(np.int64)
+    probe = [pool.make(int(x), prng) for x in psizes]
     budget = cfg["budget"]
     import torch
     free, _ = torch.cuda.mem_get_info()

@@ -44,6 +44,11 @@ int64_t now_us() {
 
 size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// How long the filter thread waits for room in the pinned result pool
+// before it gives a request pageable memory instead (a client that keeps
+// its results does not stall the server for longer).
+constexpr int kPoolWaitMs = 200;
+
 // First-fit allocator over one device allocation (the admission budget).
 class Arena {
  public:
@@ -108,6 +113,25 @@ class HostPool {
   }
   long alloc(size_t bytes, size_t want_total) {
     std::lock_guard<std::mutex> lk(mu_);
+    return alloc_locked(bytes, want_total);
+  }
+  // As alloc, but when the pool has no room for `bytes` now (and could hold
+  // them), waits up to wait_ms for results to be freed.  The filter thread
+  // runs ahead of the aligner; without this it fills the pool with results
+  // of requests far ahead and the rest go to pageable memory.
+  long alloc_wait(size_t bytes, size_t want_total, int wait_ms) {
+    std::unique_lock<std::mutex> lk(mu_);
+    const auto until = std::chrono::steady_clock::now() + std::chrono::milliseconds(wait_ms);
+    for (;;) {
+      const long off = alloc_locked(bytes, want_total);
+      if (off >= 0 || !base_ || up256(bytes) > size_) return off;
+      if (freed_.wait_until(lk, until) == std::cv_status::timeout)
+        return alloc_locked(bytes, want_total);
+    }
+  }
+
+ private:
+  long alloc_locked(size_t bytes, size_t want_total) {
     if (!base_ && !tried_) {  // on first use
       tried_ = true;
       if (cudaMallocHost(&base_, want_total) != cudaSuccess) {
@@ -129,8 +153,11 @@ class HostPool {
     }
     return -1;
   }
+
+ public:
   void free(size_t off, size_t bytes) {
     std::lock_guard<std::mutex> lk(mu_);
+    freed_.notify_all();
     bytes = up256(bytes);
     auto it = free_.emplace(off, bytes).first;
     auto nx = std::next(it);
@@ -150,6 +177,7 @@ class HostPool {
 
  private:
   std::mutex mu_;
+  std::condition_variable freed_;
   void *base_ = nullptr;
   size_t size_ = 0;
   bool tried_ = false;
@@ -258,7 +286,11 @@ struct saru_server {
   int64_t genome_len = 0;
   std::vector<char> genome_host;  // the same genome, for the filters' q-gram indexes
   HostPool host_pool;             // pinned memory for reads-only requests' results
-  std::map<std::pair<int, int>, saru_filter *> filters;  // per (read length, k)
+  // filters per worker and (read length, k): the filter stage runs
+  // kFilterWorkers requests at once in pipeline mode (one request's host
+  // call assembly overlaps another's kernel and copies), one in plain mode
+  static constexpr int kFilterWorkers = 2;
+  std::map<std::pair<int, int>, saru_filter *> filters[kFilterWorkers];
 
   struct Group {
     std::vector<std::shared_ptr<Request>> reqs;
@@ -274,9 +306,14 @@ struct saru_server {
   std::unordered_map<int64_t, std::shared_ptr<Request>> read_done;  // until released
   std::deque<std::shared_ptr<Request>> filter_q;  // reads-only requests to filter
   std::condition_variable cv_filter;
+  // filtered requests wait here until those that arrived before them have
+  // gone on (to the pending queue, or done): arrival order is kept
+  std::map<int64_t, std::shared_ptr<Request>> filtered;
+  int64_t filter_taken = 0, filter_next = 0;  // sequence numbers
   int64_t next_ticket = 1, groups = 0, launches = 0, free_gen = 0;
   bool stop = false, sched_done = false, filter_stop = false;
-  std::thread sched_thr, done_thr, filter_thr;
+  std::thread sched_thr, done_thr;
+  std::vector<std::thread> filter_thrs;
 
   void free_genome() {
     if (genome) cudaFree(genome);
@@ -301,21 +338,27 @@ struct saru_server {
   }
 
   // The filter of (m, k) on the resident genome (created on first use).
-  saru_filter *filter_for(int m, int k) {
-    auto it = filters.find({m, k});
-    if (it != filters.end()) return it->second;
+  saru_filter *filter_for(int m, int k, int w) {
+    auto it = filters[w].find({m, k});
+    if (it != filters[w].end()) return it->second;
     saru_filter *f = saru_filter_create(genome_host.data(), (int64_t)genome_host.size(), m, k,
                                         cfg.device);
-    if (f) filters[{m, k}] = f;
+    if (f) filters[w][{m, k}] = f;
     return f;
+  }
+  void destroy_filters() {
+    for (auto &fw : filters) {
+      for (auto &kv : fw) saru_filter_destroy(kv.second);
+      fw.clear();
+    }
   }
 
   // One read set through the filter on both strands: its calls as gather
   // calls over the set's own read table, outputs in the set's arrays.
-  int filter_set(Request &r, ReadSetOut &o) {
+  int filter_set(Request &r, ReadSetOut &o, int w) {
     const saru_read_set &rs = o.set;
     const int m = rs.read_length, k = rs.k;
-    saru_filter *f = filter_for(m, k);
+    saru_filter *f = filter_for(m, k, w);
     if (!f) return SARU_E_INVALID;
     const uint32_t cv = rs.chunk_value
                             ? rs.chunk_value
@@ -383,8 +426,9 @@ struct saru_server {
     if (r.compact) o.rec_bytes = saru_compact_record_bytes(m, k);
     const size_t half = r.compact ? n * (size_t)o.rec_bytes + 64 : (size_t)slots + 64;
     const size_t total = r.compact ? half : 2 * up256(half);
-    o.pool_off = host_pool.alloc(total, (size_t)(cfg.host_pool_bytes > 0 ? cfg.host_pool_bytes
-                                                                         : (int64_t)4 << 30));
+    o.pool_off = host_pool.alloc_wait(
+        total, (size_t)(cfg.host_pool_bytes > 0 ? cfg.host_pool_bytes : (int64_t)4 << 30),
+        kPoolWaitMs);
     char *base;
     if (o.pool_off >= 0) {
       o.pool_bytes = total;
@@ -415,19 +459,25 @@ struct saru_server {
     return SARU_OK;
   }
 
-  // Filter thread: reads-only requests in arrival order become gather
-  // requests on the pending queue (or finish here with an error or nothing
-  // to align), while the scheduler and completer work on earlier ones.
-  void filterer() {
+  // Filter workers: reads-only requests become gather requests on the
+  // pending queue (or finish here with an error or nothing to align), while
+  // the scheduler and completer work on earlier ones.  In pipeline mode
+  // kFilterWorkers requests are filtered at once, each worker with its own
+  // filters; a filtered request goes on only after every request that
+  // arrived before it, so the pending queue keeps arrival order.  Plain mode
+  // has one worker, and the next request's filter waits for this one.
+  void filterer(int w) {
     cudaSetDevice(cfg.device);
     for (;;) {
       std::shared_ptr<Request> r;
+      int64_t seq = 0;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_filter.wait(lk, [&] { return filter_stop || !filter_q.empty(); });
         if (filter_q.empty()) return;
         r = filter_q.front();
         filter_q.pop_front();
+        seq = filter_taken++;
       }
       int rc = SARU_OK;
       // the sets' filters (one per read length and k) run at once, each on
@@ -435,17 +485,17 @@ struct saru_server {
       std::vector<std::pair<int, int>> keys;
       for (auto &o : r->rsets) {
         const std::pair<int, int> key(o.set.read_length, o.set.k);
-        if (!filter_for(key.first, key.second)) rc = SARU_E_INVALID;
+        if (!filter_for(key.first, key.second, w)) rc = SARU_E_INVALID;
         if (std::find(keys.begin(), keys.end(), key) == keys.end()) keys.push_back(key);
       }
       if (!rc) {
         std::vector<std::thread> th;
         for (const auto &key : keys)
-          th.emplace_back([this, &r, key] {
+          th.emplace_back([this, &r, key, w] {
             cudaSetDevice(cfg.device);
             for (auto &o : r->rsets)
               if (o.set.read_length == key.first && o.set.k == key.second && !o.rc)
-                o.rc = filter_set(*r, o);
+                o.rc = filter_set(*r, o, w);
           });
         for (auto &t : th) t.join();
         for (auto &o : r->rsets)
@@ -467,17 +517,24 @@ struct saru_server {
           rc = SARU_E_NOMEM;
         }
       }
+      r->rc = rc;
       std::unique_lock<std::mutex> lk(mu);
-      if (rc || r->calls.empty()) {
-        r->rc = rc;
-        r->t_done = now_us();
-        r->done = true;
-        cv_done.notify_all();
-        continue;
+      filtered[seq] = r;
+      // hand on, in arrival order, every request whose predecessors have gone
+      for (auto it = filtered.find(filter_next); it != filtered.end();
+           it = filtered.find(filter_next)) {
+        std::shared_ptr<Request> q = it->second;
+        filtered.erase(it);
+        ++filter_next;
+        if (q->rc || q->calls.empty()) {
+          q->t_done = now_us();
+          q->done = true;
+          cv_done.notify_all();
+        } else {
+          pending.push_back(q);
+          cv_pending.notify_all();
+        }
       }
-      pending.push_back(r);
-      cv_pending.notify_all();
-      // plain mode: the next request's filter waits for this one
       if (!cfg.pipeline) cv_done.wait(lk, [&] { return r->done; });
     }
   }
@@ -792,7 +849,8 @@ saru_server *saru_server_create(const saru_server_config *cfg) {
   }
   s->sched_thr = std::thread([s] { s->scheduler(); });
   s->done_thr = std::thread([s] { s->completer(); });
-  s->filter_thr = std::thread([s] { s->filterer(); });
+  const int nf = cfg->pipeline ? saru_server::kFilterWorkers : 1;
+  for (int w = 0; w < nf; ++w) s->filter_thrs.emplace_back([s, w] { s->filterer(w); });
   return s;
 }
 
@@ -1003,8 +1061,7 @@ int saru_server_set_genome(saru_server *s, const char *genome, int64_t genome_le
   s->pg = saru::PackedGenome{s->genome, s->exc_pos, s->exc_byte, genome_len, (int64_t)ne};
   s->genome_len = genome_len;
   s->genome_host.assign(genome, genome + genome_len);
-  for (auto &kv : s->filters) saru_filter_destroy(kv.second);  // indexes of the old genome
-  s->filters.clear();
+  s->destroy_filters();  // indexes of the old genome
   cudaSetDevice(s->cfg.device);
   return SARU_OK;
 }
@@ -1022,7 +1079,8 @@ void saru_server_destroy(saru_server *s) {
     s->filter_stop = true;
   }
   s->cv_filter.notify_all();
-  if (s->filter_thr.joinable()) s->filter_thr.join();
+  for (auto &t : s->filter_thrs)
+    if (t.joinable()) t.join();
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
@@ -1039,7 +1097,7 @@ void saru_server_destroy(saru_server *s) {
   cudaStreamSynchronize(s->s_comp);
   if (s->scratch) cudaFree(s->scratch);
   s->free_genome();
-  for (auto &kv : s->filters) saru_filter_destroy(kv.second);
+  s->destroy_filters();
   cudaSetDevice(s->cfg.device);
   s->arena.release();
   cudaStreamDestroy(s->s_in);
