@@ -20,6 +20,56 @@ static long pair_off(int j, long pstride, long pslot) {
   return (plane_unit_of<T>(j) * pstride + pslot) * kPlaneUnit + plane_half_of<T>(j);
 }
 
+// A lane's asynchronous copies (cp.async in the kernel), emulated: a copy
+// takes its source bytes when issued and lands only at a wait that covers
+// its group; copies landing at one wait land newest first.  So a slot
+// refilled before the copy that held it has landed ends up with the older
+// bytes, and the oracle comparison fails.
+struct AsyncCopies {
+  struct C {
+    uint8_t *dst;
+    uint8_t data[16];
+    size_t n;
+    long group;
+  };
+  std::vector<C> pending;
+  long open = 0;  // the group the copies issued since the last commit join
+  void copy(void *dst, const void *src, size_t n) {
+    C c;
+    c.dst = static_cast<uint8_t *>(dst);
+    memcpy(c.data, src, n);
+    c.n = n;
+    c.group = open;
+    pending.push_back(c);
+  }
+  void commit() { ++open; }
+  void wait(long keep) {  // at most `keep` committed groups stay in flight
+    const long limit = open - keep;
+    for (long i = (long)pending.size() - 1; i >= 0; --i)
+      if (pending[(size_t)i].group < limit)
+        memcpy(pending[(size_t)i].dst, pending[(size_t)i].data, pending[(size_t)i].n);
+    std::vector<C> rest;
+    for (const C &c : pending)
+      if (c.group >= limit) rest.push_back(c);
+    pending.swap(rest);
+  }
+  void wait_all() { wait(-1); }
+};
+
+// The walk's plane ring of one lane over emulated asynchronous copies (one
+// copy group a column, as in the kernel).
+template <typename T>
+static auto host_ring(uint8_t *region, int lane, const uint8_t *planes, long pstride, long pslot,
+                      AsyncCopies *ac) {
+  return plane_ring<T>(
+      reinterpret_cast<PlanePair<T> *>(region) + lane,
+      [=](PlanePair<T> *dst, int j) {
+        ac->copy(dst, planes + pair_off<T>(j, pstride, pslot), sizeof(PlanePair<T>));
+        ac->commit();
+      },
+      [=] { ac->wait(kRing - 1); });
+}
+
 template <typename T>
 static int run(const TileArgs &a0, int nwarps_total) {
   TileArgs a = a0;
@@ -68,29 +118,29 @@ static int run(const TileArgs &a0, int nwarps_total) {
                   memcpy(planes + (u * a.pstride + pslot) * kPlaneUnit, v, 16);
                 }));
       }
-      // the walk's plane ring in the region; copies land at once here
-      auto ring_of = [&](int lane) {
-        const long pslot = (long)gwarp * 32 + lane;
-        return plane_ring<T>(
-            reinterpret_cast<PlanePair<T> *>(region) + lane,
-            [=](PlanePair<T> *dst, int j) {
-              memcpy(dst, planes + pair_off<T>(j, a.pstride, pslot), sizeof(PlanePair<T>));
-            },
-            [] {});
-      };
+      // the walk's plane ring in the region, over emulated asynchronous copies
       if (a.records) {  // compact records straight to the (exactly sized) output
         for (int lane = 0; lane < 32; ++lane) {
           uint32_t *rec = reinterpret_cast<uint32_t *>(a.records + (s.t0 + lane) * a.rec_bytes);
-          status |= lane_traceback_ops<T>(a, s, lane, ls[lane], ring_of(lane),
-                                          [&](int w, uint32_t v) { rec[w] = v; });
+          AsyncCopies ac;
+          status |= lane_traceback_ops<T>(
+              a, s, lane, ls[lane],
+              host_ring<T>(region, lane, planes, a.pstride, (long)gwarp * 32 + lane, &ac),
+              [&](int w, uint32_t v) { rec[w] = v; });
+          ac.wait_all();
         }
         continue;
       }
       uint32_t up_r[32][kMaxGapRuns], left_r[32][kMaxGapRuns];
       LaneWalk walks[32];
-      for (int lane = 0; lane < 32; ++lane)
-        status |= lane_traceback_walk<T>(a, s, lane, ls[lane], ring_of(lane), up_r[lane],
-                                         left_r[lane], walks[lane]);
+      for (int lane = 0; lane < 32; ++lane) {
+        AsyncCopies ac;
+        status |= lane_traceback_walk<T>(
+            a, s, lane, ls[lane],
+            host_ring<T>(region, lane, planes, a.pstride, (long)gwarp * 32 + lane, &ac),
+            up_r[lane], left_r[lane], walks[lane]);
+        ac.wait_all();
+      }
       uint8_t *out_r = region, *out_g = region + s.o_span_r;
       const long out_bytes = out_area_bytes(a.max_m, a.k);
       memset(region, 0, (size_t)out_bytes);
@@ -251,14 +301,12 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
         LaneWalk walks[32];
         for (int lane = 0; lane < 32; ++lane) {
           const long pslot = (long)gw * 32 + lane;
-          const auto ring = plane_ring<T>(
-              reinterpret_cast<PlanePair<T> *>(w.region) + lane,
-              [=](PlanePair<T> *dst, int j) {
-                memcpy(dst, planes + pair_off<T>(j, pstride, pslot), sizeof(PlanePair<T>));
-              },
-              [] {});
-          status |= lane_traceback_walk<T>(a, w.span, lane, w.ls[lane], ring, up_r[lane],
-                                           left_r[lane], walks[lane]);
+          AsyncCopies ac;
+          status |= lane_traceback_walk<T>(
+              a, w.span, lane, w.ls[lane],
+              host_ring<T>(w.region, lane, planes, pstride, pslot, &ac), up_r[lane],
+              left_r[lane], walks[lane]);
+          ac.wait_all();
         }
         const long out_bytes = out_area_bytes(a.max_m, a.k);
         memset(w.region, 0, (size_t)out_bytes);
