@@ -109,7 +109,7 @@ typedef struct {
 
 /* Status bits the device entry point ORs into result->status. */
 #define SARU_S_IRREGULAR 1  /* a window is not m + so + eo long, or m <= 3k */
-#define SARU_S_ALPHABET 2   /* a read holds more than 4 distinct non-ACGT bytes */
+#define SARU_S_ALPHABET 2   /* a read holds more than 2 distinct non-ACGT bytes */
 #define SARU_S_OVERFLOW 4   /* a traceback left its band */
 #define SARU_S_GATHER 16    /* saru_gather_device: a candidate outside the genome or read
                                table, a bad flag, or a window length that does not match */

@@ -336,7 +336,9 @@ saru::Tuning tuning_for(int max_m, int k) {
 
 long band_grid(int dev, long n, int max_m, int k) {
   const saru::Tuning tn = tuning_for(max_m, k);
-  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k, tn.warps),
+  // the band may be 64-bit when k > 7 or when the tuning asks for it
+  const bool wide = k > 7 || tn.word_bits == 64;
+  return saru::band_grid(sm_count(dev), n, saru::band_layout(max_m, k, tn.warps, wide),
                          smem_per_sm(dev), tn.ctas_per_sm);
 }
 
@@ -414,7 +416,8 @@ int run_band_multi(const saru_batch *calls, const saru_result *res, int ncalls, 
   a.max_k = max_k;
   a.wide_any = wide_any;
   a.warps_req = tn.warps;
-  a.grid = saru::band_grid(sm_count(dev), total_n, saru::band_layout(max_m, max_k, tn.warps),
+  a.grid = saru::band_grid(sm_count(dev), total_n,
+                           saru::band_layout(max_m, max_k, tn.warps, wide_any != 0),
                            smem_per_sm(dev), tn.ctas_per_sm);
   if (max_grid > 0 && a.grid > max_grid) a.grid = max_grid;
   const size_t need = saru::band_scratch_bytes(a.grid, max_m, max_k, wide_any != 0, tn.warps);

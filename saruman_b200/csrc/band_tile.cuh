@@ -317,9 +317,9 @@ SARU_HD bool add_gap_step(uint32_t *r, int &n, uint32_t &open, int step, uint32_
 // column's slot is refilled only after the walk has left that column.
 constexpr int kRing = 16;
 
-// Region bytes the ring may take: 16-byte plane pairs (64-bit bands, which
-// a launch shape can ask for at any k).
-SARU_HD long ring_bytes() { return (long)kRing * 32 * 16; }
+// Region bytes the ring takes: 8-byte plane pairs of a 32-bit band, 16-byte
+// ones of a 64-bit band (which a launch shape can ask for at any k).
+SARU_HD long ring_bytes(bool wide) { return (long)kRing * 32 * (wide ? 16 : 8); }
 
 template <typename T, class Copy, class Wait>
 struct PlaneRing {
@@ -671,18 +671,19 @@ struct SliceLayout {
   long rs_bytes, ws_bytes, region_bytes, warp_smem;
 };
 
-SARU_HD SliceLayout slice_layout(int max_m, int k) {
+SARU_HD SliceLayout slice_layout(int max_m, int k, bool wide) {
   SliceLayout L;
   const long code_words = max_m / 8 + 1;
   const long mwords = mask_words(k, max_m + 2 * k);
-  // staged bytes, 16 bytes of alignment head and 96 of slack for the word
-  // readers (load4 and the 32-position chunks of build_codes_acgt)
-  L.rs_bytes = (32L * max_m + 16 + 96 + 15) & ~15L;
-  L.ws_bytes = (32L * (max_m + 2 * k) + 16 + 96 + 15) & ~15L;
+  // staged bytes, 16 bytes of alignment head and 48 of slack for the word
+  // readers (load4 reads up to 7 bytes past its position; the 32-position
+  // chunks of build_codes_acgt reach 31 positions past a window's end)
+  L.rs_bytes = (32L * max_m + 16 + 48 + 15) & ~15L;
+  L.ws_bytes = (32L * (max_m + 2 * k) + 16 + 48 + 15) & ~15L;
   const long cm = 4L * 32 * (code_words + NCODES * mwords);
   const long out = out_area_bytes(max_m, k);
   long r = cm > out ? cm : out;
-  if (r < ring_bytes()) r = ring_bytes();
+  if (r < ring_bytes(wide)) r = ring_bytes(wide);
   L.region_bytes = (r + 15) & ~15L;
   L.warp_smem = L.rs_bytes + L.ws_bytes + L.region_bytes;
   return L;

@@ -270,8 +270,8 @@ __global__ void saru_full_trace_kernel(FullArgs a) {
 
 constexpr long kMaxCtaSmem = 227 * 1024;  // opt-in shared memory per block on sm_100
 
-BandLayout band_layout(int max_m, int k, int warps_req) {
-  const SliceLayout S = slice_layout(max_m, k);
+BandLayout band_layout(int max_m, int k, int warps_req, bool wide) {
+  const SliceLayout S = slice_layout(max_m, k, wide);
   BandLayout L;
   L.rs_bytes = S.rs_bytes;
   L.ws_bytes = S.ws_bytes;
@@ -305,7 +305,7 @@ cudaError_t allow_smem() {
 }  // namespace
 
 cudaError_t launch_band_kernel(KernelArgs &a, cudaStream_t s) {
-  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req);
+  const BandLayout L = band_layout(a.max_m, a.max_k, a.warps_req, a.wide_any != 0);
   if (L.warps < 1 || a.nseg < 1 || a.nseg > kMaxSegs) return cudaErrorInvalidValue;
   // allow the largest slice once per device; each launch asks for its own
   // size (a per-launch attribute would race between concurrent callers)
@@ -332,7 +332,7 @@ long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_c
 }
 
 size_t band_scratch_bytes(long grid, int max_m, int k, bool wide, int warps_req) {
-  const BandLayout L = band_layout(max_m, k, warps_req);
+  const BandLayout L = band_layout(max_m, k, warps_req, wide);
   return kCounterBytes + (size_t)grid * 32 * (L.warps > 0 ? L.warps : 1) *
                              (size_t)plane_units(max_m, wide) * kPlaneUnit;
 }

@@ -106,7 +106,7 @@ struct GatherArgs {
 
 cudaError_t launch_gather(const GatherArgs &a, int sms, cudaStream_t s);
 
-BandLayout band_layout(int max_m, int k, int warps_req = 0);
+BandLayout band_layout(int max_m, int k, int warps_req = 0, bool wide = true);
 long band_grid(int sms, long n, const BandLayout &L, int smem_per_sm, int ctas_cap = 0);
 size_t band_scratch_bytes(long grid, int max_m, int k, bool wide,
                           int warps_req = 0);  // counter + planes

@@ -47,7 +47,7 @@ namespace saru {
 enum : int { OP_STOP = 0, OP_DIAG = 1, OP_UP = 2, OP_LEFT = 3 };
 
 // read-byte classes: A C G T, then up to MAX_EXTRA other bytes of the read
-constexpr int MAX_EXTRA = 4;
+constexpr int MAX_EXTRA = 2;
 constexpr int NCODES = 4 + MAX_EXTRA;
 
 SARU_HD uint32_t fshr32(uint32_t lo, uint32_t hi, uint32_t s) {

@@ -73,7 +73,7 @@ static auto host_ring(uint8_t *region, int lane, const uint8_t *planes, long pst
 template <typename T>
 static int run(const TileArgs &a0, int nwarps_total) {
   TileArgs a = a0;
-  const SliceLayout S = slice_layout(a.max_m, a.k);
+  const SliceLayout S = slice_layout(a.max_m, a.k, sizeof(T) == 8);
   a.rs_bytes = S.rs_bytes;
   a.ws_bytes = S.ws_bytes;
   a.region_bytes = S.region_bytes;
@@ -220,7 +220,7 @@ extern "C" int tile_align_multi(const HostSeg *segs, int nseg, int nwarps_total)
     if (segs[i].k > max_k) max_k = segs[i].k;
     wide_any |= segs[i].wide;
   }
-  const SliceLayout S = slice_layout(max_m, max_k);
+  const SliceLayout S = slice_layout(max_m, max_k, wide_any != 0);
   const long pstride = (long)nwarps_total * 32;
   // exactly the bytes the launcher reserves for the planes
   std::vector<uint8_t> planes_v((size_t)plane_units(max_m, wide_any != 0) * pstride * kPlaneUnit);

@@ -206,6 +206,33 @@ def test_device_entry_matches_host_entry(saru_lib):
     assert np.array_equal(ga[:tot].cpu().numpy(), host.genome_aln)
 
 
+def test_misaligned_scratch_is_refused(saru_lib):
+    """The kernel copies 16-byte plane units through the scratch: a scratch
+    pointer off a 16-byte boundary is refused before anything is enqueued."""
+    import torch
+    b = W.random_batch(100, 5, 64, seed=22, err=0.05)
+    dev = torch.device("cuda:0")
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in
+         dict(genome=b.genome, reads=b.reads, goff=b.genome_offsets, roff=b.read_offsets,
+              dirs=b.dirs).items()}
+    scores = torch.zeros(b.n, dtype=torch.int32, device=dev)
+    ra = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    ga = torch.zeros(b.total_genome + 64, dtype=torch.uint8, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    nbytes = S.scratch_bytes(b.n, b.m, b.k)
+    scratch = torch.empty(nbytes + 64, dtype=torch.uint8, device=dev)
+    sb = S.SaruBatch(t["genome"].data_ptr(), t["reads"].data_ptr(), t["goff"].data_ptr(),
+                     t["roff"].data_ptr(), t["dirs"].data_ptr(), b.n, b.k, 0, 1, 1, b.m,
+                     len(b.genome), b.total_genome)
+    sr = S.SaruResult(scores.data_ptr(), ra.data_ptr(), ga.data_ptr(), status.data_ptr())
+    with pytest.raises(S.SaruError, match="16-byte aligned"):
+        S.align_device(sb, sr, scratch.data_ptr() + 8, nbytes, 0)
+    torch.cuda.synchronize()
+    S.align_device(sb, sr, scratch.data_ptr(), nbytes, 0)  # the aligned pointer runs
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+
+
 @pytest.mark.parametrize("shape", [("c2", 100, 5, 0.03), ("c4", 250, 15, 0.04)])
 def test_full_size_batch_sampled_against_oracle(saru_lib, shape):
     """A batch of the benchmark's shape and size; every candidate is
