@@ -338,13 +338,23 @@ struct saru_server {
   }
 
   // The filter of (m, k) on the resident genome (created on first use).
+  // The filter of (m, k) for worker w.  The first use of (m, k) by any
+  // worker builds it for every worker: a worker that built its own on its
+  // first request of that length would stall that request (and, through
+  // the in-order hand-off, every one behind it) for the index build.
+  std::mutex filters_mu;
   saru_filter *filter_for(int m, int k, int w) {
+    std::lock_guard<std::mutex> lk(filters_mu);
     auto it = filters[w].find({m, k});
     if (it != filters[w].end()) return it->second;
-    saru_filter *f = saru_filter_create(genome_host.data(), (int64_t)genome_host.size(), m, k,
-                                        cfg.device);
-    if (f) filters[w][{m, k}] = f;
-    return f;
+    for (auto &fv : filters) {
+      if (fv.count({m, k})) continue;
+      saru_filter *f = saru_filter_create(genome_host.data(), (int64_t)genome_host.size(), m,
+                                          k, cfg.device);
+      if (!f) return nullptr;
+      fv[{m, k}] = f;
+    }
+    return filters[w][{m, k}];
   }
   void destroy_filters() {
     for (auto &fw : filters) {
