@@ -104,7 +104,7 @@ GENERAL = [
     (20, 8, 0.3, b"ACGT", 0, 1, (1, 2, 3, 5, 6, 7)),   # m <= 3k
     (12, 6, 0.4, b"AC", 0, 1, (1, 2, 3, 5, 6, 7)),
     (40, 16, 0.3, b"ACGT", 0, 1, (1, 3, 5, 7)),         # k > 15
-    (36, 2, 0.05, b"ACGTNRYKMSWBDHV", 0, 1, (1, 3)),     # > 4 distinct non-ACGT read bytes
+    (36, 2, 0.05, b"ACGTNRYKMSWBDHV", 0, 1, (1, 3)),     # > 2 distinct non-ACGT read bytes
 ]
 
 
