@@ -405,21 +405,28 @@ __global__ void k_widen(const int32_t *n, long nr, long *out) {
     out[r] = n[r];
 }
 
+// Device memory that grows, stream-ordered on the filter's stream: a
+// growth neither waits for the device's other work (a plain cudaFree
+// synchronizes the whole device, so one filter's growth stalled the
+// aligner and the other filters of a server) nor for the host.  `slack`
+// extra elements are taken on a growth, for buffers sized by the request.
 template <typename T>
 struct DBuf {
   T *p = nullptr;
   size_t n = 0;
-  cudaError_t ensure(size_t count) {
+  cudaError_t ensure(size_t count, cudaStream_t s, size_t slack = 0) {
     if (count <= n) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     n = 0;
-    const cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 64);
-    if (e == cudaSuccess) n = count;
+    const size_t want = count + slack;
+    const cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&p), want * sizeof(T) + 64, s);
+    if (e == cudaSuccess) n = want;
+    else p = nullptr;
     return e;
   }
-  void release() {
-    if (p) cudaFree(p);
+  void release(cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     n = 0;
   }
@@ -436,7 +443,7 @@ struct HBuf {
     if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
-    const size_t want = count + count / 2 + 64;
+    const size_t want = std::max(count + count / 2, 2 * n) + 64;
     const cudaError_t e = cudaMallocHost(&p, want * sizeof(T));
     if (e == cudaSuccess) n = want;
     return e;
@@ -518,7 +525,7 @@ saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t 
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->s, cudaStreamNonBlocking);
   f->nidx = genome_len >= q ? genome_len - q + 1 : 0;
   const long n = f->nidx;
-  if (e == cudaSuccess) e = f->genome.ensure((size_t)genome_len);
+  if (e == cudaSuccess) e = f->genome.ensure((size_t)genome_len, f->s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(f->genome.p, genome, (size_t)genome_len, cudaMemcpyHostToDevice, f->s);
   if (e == cudaSuccess && n > 0) {
@@ -526,9 +533,12 @@ saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t 
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t *)nullptr, (uint64_t *)nullptr,
                                     (uint32_t *)nullptr, (uint32_t *)nullptr, (int)n, 0, 64,
                                     f->s);
-    if ((e = f->hash.ensure(n)) == cudaSuccess && (e = f->hash_s.ensure(n)) == cudaSuccess &&
-        (e = f->pos.ensure(n)) == cudaSuccess && (e = f->pos_s.ensure(n)) == cudaSuccess &&
-        (e = f->temp.ensure(tb)) == cudaSuccess && (e = f->status.ensure(1)) == cudaSuccess) {
+    if ((e = f->hash.ensure(n, f->s)) == cudaSuccess &&
+        (e = f->hash_s.ensure(n, f->s)) == cudaSuccess &&
+        (e = f->pos.ensure(n, f->s)) == cudaSuccess &&
+        (e = f->pos_s.ensure(n, f->s)) == cudaSuccess &&
+        (e = f->temp.ensure(tb, f->s)) == cudaSuccess &&
+        (e = f->status.ensure(1, f->s)) == cudaSuccess) {
       k_qgram_hash<<<1184, 256, 0, f->s>>>(f->genome.p, n, q, f->hash.p, f->pos.p);
       e = cudaGetLastError();
       if (e == cudaSuccess)
@@ -549,8 +559,8 @@ saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t 
         saru_filter_destroy(f);
         return nullptr;
       }
-      f->hash.release();
-      f->pos.release();
+      f->hash.release(f->s);
+      f->pos.release(f->s);
     }
   }
   if (e != cudaSuccess) {
@@ -596,17 +606,21 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
                                               (int32_t *)nullptr, (int)kReadsPerLaunch, 0, 32,
                                               f->s);
     const long batch = std::min<long>(nr, kReadsPerLaunch);
-    if ((e = f->reads.ensure((size_t)(nr * m))) != cudaSuccess ||
-        (e = f->lo.ensure(lists)) != cudaSuccess || (e = f->count.ensure(lists)) != cudaSuccess ||
-        (e = f->offs.ensure(lists)) != cudaSuccess ||
-        (e = f->temp.ensure(std::max(std::max(tb, tb2), tb3))) != cudaSuccess ||
-        (e = f->wkey.ensure((size_t)batch * 2)) != cudaSuccess ||
-        (e = f->widx.ensure((size_t)batch * 2)) != cudaSuccess ||
-        (e = f->hit_pos.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
-        (e = f->hit_flag.ensure((size_t)batch * kHitsPerRead)) != cudaSuccess ||
-        (e = f->n.ensure(batch)) != cudaSuccess || (e = f->queue.ensure(batch)) != cudaSuccess ||
-        (e = f->at.ensure(batch)) != cudaSuccess || (e = f->nwide.ensure(batch)) != cudaSuccess ||
-        (e = f->status.ensure(1)) != cudaSuccess) {
+    // buffers sized by the request's reads take half again on a growth;
+    // those sized by a launch stop growing at kReadsPerLaunch reads
+    cudaStream_t s = f->s;
+    if ((e = f->reads.ensure((size_t)(nr * m), s, (size_t)(nr * m) / 2)) != cudaSuccess ||
+        (e = f->lo.ensure(lists, s, lists / 2)) != cudaSuccess ||
+        (e = f->count.ensure(lists, s, lists / 2)) != cudaSuccess ||
+        (e = f->offs.ensure(lists, s, lists / 2)) != cudaSuccess ||
+        (e = f->temp.ensure(std::max(std::max(tb, tb2), tb3), s)) != cudaSuccess ||
+        (e = f->wkey.ensure((size_t)batch * 2, s)) != cudaSuccess ||
+        (e = f->widx.ensure((size_t)batch * 2, s)) != cudaSuccess ||
+        (e = f->hit_pos.ensure((size_t)batch * kHitsPerRead, s)) != cudaSuccess ||
+        (e = f->hit_flag.ensure((size_t)batch * kHitsPerRead, s)) != cudaSuccess ||
+        (e = f->n.ensure(batch, s)) != cudaSuccess || (e = f->queue.ensure(batch, s)) != cudaSuccess ||
+        (e = f->at.ensure(batch, s)) != cudaSuccess || (e = f->nwide.ensure(batch, s)) != cudaSuccess ||
+        (e = f->status.ensure(1, s)) != cudaSuccess) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       return fail("saru_filter_run", e);
@@ -650,8 +664,8 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       if (e != cudaSuccess) break;
       k_widen<<<(unsigned)((cnt + 255) / 256), 256, 0, f->s>>>(f->n.p, cnt, f->nwide.p);
       e = cub::DeviceScan::ExclusiveSum(f->temp.p, tb2, f->nwide.p, f->at.p, (int)cnt, f->s);
-      if ((e = f->h_n[set].ensure((size_t)cnt)) != cudaSuccess ||
-          (e = f->h_q[set].ensure((size_t)cnt)) != cudaSuccess)
+      if ((e = f->h_n[set].ensure((size_t)batch)) != cudaSuccess ||
+          (e = f->h_q[set].ensure((size_t)batch)) != cudaSuccess)
         break;
       int32_t *hn = f->h_n[set].p, *hq = f->h_q[set].p;
       if (e == cudaSuccess)
@@ -662,8 +676,8 @@ int saru_filter_run(saru_filter *f, const char *reads, int32_t nreads, int32_t d
       if (e != cudaSuccess) break;
       long total = 0;
       for (long i = 0; i < cnt; ++i) total += hn[(size_t)i];
-      if ((e = f->packed_pos.ensure((size_t)total + 1)) != cudaSuccess ||
-          (e = f->packed_flag.ensure((size_t)total + 1)) != cudaSuccess)
+      if ((e = f->packed_pos.ensure((size_t)total + 1, s, (size_t)total / 2)) != cudaSuccess ||
+          (e = f->packed_flag.ensure((size_t)total + 1, s, (size_t)total / 2)) != cudaSuccess)
         break;
       k_pack<<<(unsigned)std::min<long>(cnt, 65535), 128, 0, f->s>>>(
           f->hit_pos.p, f->hit_flag.p, f->n.p, f->at.p, cnt, f->packed_pos.p, f->packed_flag.p);
@@ -747,34 +761,37 @@ void saru_filter_destroy(saru_filter *f) {
   const bool had_dev = cudaGetDevice(&caller_dev) == cudaSuccess;
   cudaSetDevice(f->device);
   if (f->s) cudaStreamSynchronize(f->s);
-  f->genome.release();
-  f->reads.release();
-  f->temp.release();
-  f->hash.release();
-  f->hash_s.release();
-  f->pos.release();
-  f->pos_s.release();
-  f->lo.release();
-  f->count.release();
-  f->offs.release();
-  f->at.release();
-  f->nwide.release();
-  f->hit_pos.release();
-  f->n.release();
-  f->queue.release();
-  f->packed_pos.release();
-  f->hit_flag.release();
-  f->packed_flag.release();
-  f->status.release();
+  f->genome.release(f->s);
+  f->reads.release(f->s);
+  f->temp.release(f->s);
+  f->hash.release(f->s);
+  f->hash_s.release(f->s);
+  f->pos.release(f->s);
+  f->pos_s.release(f->s);
+  f->lo.release(f->s);
+  f->count.release(f->s);
+  f->offs.release(f->s);
+  f->at.release(f->s);
+  f->nwide.release(f->s);
+  f->hit_pos.release(f->s);
+  f->n.release(f->s);
+  f->queue.release(f->s);
+  f->packed_pos.release(f->s);
+  f->hit_flag.release(f->s);
+  f->packed_flag.release(f->s);
+  f->status.release(f->s);
   for (int i = 0; i < 2; ++i) {
     f->h_n[i].release();
     f->h_q[i].release();
     f->h_pos[i].release();
     f->h_flag[i].release();
   }
-  f->wkey.release();
-  f->widx.release();
-  if (f->s) cudaStreamDestroy(f->s);
+  f->wkey.release(f->s);
+  f->widx.release(f->s);
+  if (f->s) {
+    cudaStreamSynchronize(f->s);  // the stream-ordered frees
+    cudaStreamDestroy(f->s);
+  }
   delete f;
   if (had_dev) cudaSetDevice(caller_dev);
 }

@@ -224,6 +224,7 @@ struct Request {
   int32_t group = -1, redone = 0;
   int rc = SARU_OK;
   bool done = false;
+  size_t pooled = 0;  // pinned pool bytes of its results (reads-only requests)
   std::vector<ReadSetOut> rsets;  // reads-only request: its sets and results
 };
 
@@ -310,6 +311,11 @@ struct saru_server {
   // gone on (to the pending queue, or done): arrival order is kept
   std::map<int64_t, std::shared_ptr<Request>> filtered;
   int64_t filter_taken = 0, filter_next = 0;  // sequence numbers
+  // pinned pool bytes held by filtered requests that are not done yet; in
+  // pipeline mode a filter worker takes no new request while they exceed
+  // ahead_limit (half the pool), so the filter cannot fill the pool with
+  // results of requests far ahead of the aligner
+  size_t ahead_bytes = 0, ahead_limit = 0;
   int64_t next_ticket = 1, groups = 0, launches = 0, free_gen = 0;
   bool stop = false, sched_done = false, filter_stop = false;
   std::thread sched_thr, done_thr;
@@ -337,7 +343,10 @@ struct saru_server {
       }
   }
 
-  // The filter of (m, k) on the resident genome (created on first use).
+  size_t pool_bytes() const {
+    return (size_t)(cfg.host_pool_bytes > 0 ? cfg.host_pool_bytes : (int64_t)4 << 30);
+  }
+
   // The filter of (m, k) for worker w.  The first use of (m, k) by any
   // worker builds it for every worker: a worker that built its own on its
   // first request of that length would stall that request (and, through
@@ -436,9 +445,7 @@ struct saru_server {
     if (r.compact) o.rec_bytes = saru_compact_record_bytes(m, k);
     const size_t half = r.compact ? n * (size_t)o.rec_bytes + 64 : (size_t)slots + 64;
     const size_t total = r.compact ? half : 2 * up256(half);
-    o.pool_off = host_pool.alloc_wait(
-        total, (size_t)(cfg.host_pool_bytes > 0 ? cfg.host_pool_bytes : (int64_t)4 << 30),
-        kPoolWaitMs);
+    o.pool_off = host_pool.alloc_wait(total, pool_bytes(), kPoolWaitMs);
     char *base;
     if (o.pool_off >= 0) {
       o.pool_bytes = total;
@@ -483,7 +490,10 @@ struct saru_server {
       int64_t seq = 0;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_filter.wait(lk, [&] { return filter_stop || !filter_q.empty(); });
+        cv_filter.wait(lk, [&] {
+          return filter_stop ||
+                 (!filter_q.empty() && (!cfg.pipeline || ahead_bytes < ahead_limit));
+        });
         if (filter_q.empty()) return;
         r = filter_q.front();
         filter_q.pop_front();
@@ -528,8 +538,11 @@ struct saru_server {
         }
       }
       r->rc = rc;
+      for (auto &o : r->rsets)
+        if (o.pool_off >= 0) r->pooled += o.pool_bytes;
       std::unique_lock<std::mutex> lk(mu);
       filtered[seq] = r;
+      ahead_bytes += r->pooled;
       // hand on, in arrival order, every request whose predecessors have gone
       for (auto it = filtered.find(filter_next); it != filtered.end();
            it = filtered.find(filter_next)) {
@@ -539,7 +552,9 @@ struct saru_server {
         if (q->rc || q->calls.empty()) {
           q->t_done = now_us();
           q->done = true;
+          ahead_bytes -= q->pooled;
           cv_done.notify_all();
+          cv_filter.notify_all();
         } else {
           pending.push_back(q);
           cv_pending.notify_all();
@@ -653,12 +668,14 @@ struct saru_server {
 
   int ensure_scratch(size_t bytes) {
     if (bytes <= scratch_bytes) return SARU_OK;
-    // launches already enqueued on s_comp may still use the old scratch
-    cudaStreamSynchronize(s_comp);
-    if (scratch) cudaFree(scratch);
+    // stream-ordered on s_comp: the old scratch is freed after the launches
+    // already enqueued there, and nothing waits (a plain cudaFree would
+    // synchronize the whole device, the filters' work and copies included)
+    if (scratch) cudaFreeAsync(scratch, s_comp);
     scratch = nullptr;
     scratch_bytes = 0;
-    if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+    if (cudaMallocAsync(&scratch, bytes, s_comp) != cudaSuccess) {
+      scratch = nullptr;
       cudaGetLastError();
       saru::set_last_error("request server: scratch allocation failed");
       return SARU_E_NOMEM;
@@ -824,12 +841,14 @@ struct saru_server {
           arena.free((size_t)r->dev_off, r->dev_bytes);
           r->t_done = t;
           r->done = true;
+          ahead_bytes -= r->pooled;
         }
         free_gen += 1;
       }
       cv_inflight.notify_all();
       cv_freed.notify_all();
       cv_done.notify_all();
+      cv_filter.notify_all();
     }
   }
 };
@@ -845,6 +864,7 @@ saru_server *saru_server_create(const saru_server_config *cfg) {
   }
   auto *s = new saru_server();
   s->cfg = *cfg;
+  s->ahead_limit = s->pool_bytes() / 2;
   if (cudaSetDevice(cfg->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->s_in, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->s_comp, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1104,8 +1124,8 @@ void saru_server_destroy(saru_server *s) {
   s->cv_inflight.notify_all();
   if (s->done_thr.joinable()) s->done_thr.join();
   cudaSetDevice(s->cfg.device);
+  if (s->scratch) cudaFreeAsync(s->scratch, s->s_comp);
   cudaStreamSynchronize(s->s_comp);
-  if (s->scratch) cudaFree(s->scratch);
   s->free_genome();
   s->destroy_filters();
   cudaSetDevice(s->cfg.device);
