@@ -555,7 +555,10 @@ def serving(S, cfg: dict, nreq: int, seed: int = 4242, compact_too: bool = False
     import torch
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(budget, free - (8 << 30)))
-    # the plain loop's capacity in reads/s, closed loop
+    # the plain loop's capacity in reads/s, closed loop; measured on the
+    # second pass: the first server trace of a process measured up to 3x
+    # slower than the same trace run again, which understated capacity
+    run_trace(S, g, probe, None, False, budget, warm=warm)
     cap = run_trace(S, g, probe, None, False, budget, warm=warm)
     plain_reads_s = sum(t.shape[0] for sets in probe for t, _, _ in sets) / cap["makespan_s"]
     lam = cfg["load"] * plain_reads_s / float(sizes.mean())
