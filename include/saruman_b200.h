@@ -272,7 +272,10 @@ int64_t saru_format_tsv_compact(const saru_batch *batch, const int32_t *scores,
  * is also the number of reads per chunk of its data array).  Perfect hits,
  * which the reference prints from the filter, come back as (read id,
  * 0-based start).  A genome read in chunks (-G) takes one filter per chunk
- * (saru_filter_set_chunk). */
+ * (saru_filter_set_chunk).  The filter's device buffers grow with the
+ * largest batch it has run, stream-ordered on its own stream
+ * (cudaMallocAsync from the device's current memory pool), so a growth
+ * does not wait for other work on the device. */
 typedef struct saru_filter saru_filter;
 saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t read_length,
                                 int32_t k, int32_t device);
