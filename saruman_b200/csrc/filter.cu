@@ -563,6 +563,8 @@ saru_filter *saru_filter_create(const char *genome, int64_t genome_len, int32_t 
       f->pos.release(f->s);
     }
   }
+  // the genome (saru_filter_genome) is usable on any stream once this returns
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->s);
   if (e != cudaSuccess) {
     fail("saru_filter_create", e);
     saru_filter_destroy(f);
