@@ -45,6 +45,25 @@ struct ByteView {
   inline char operator[](int64_t i) const {
     return (uint64_t)(i - lo) < len ? a[i - lo] : 0;
   }
+  // Bytes from i up to (not including) the first 0 byte, at most `limit`
+  // (limit < 0: no limit); bytes outside the window read as 0.
+  inline int64_t run_to_nul(int64_t i, int64_t limit) const {
+    const uint64_t off = (uint64_t)(i - lo);
+    if (off >= len) return 0;
+    uint64_t room = len - off;
+    if (limit >= 0 && (uint64_t)limit < room) room = (uint64_t)limit;
+    const void *z = memchr(a + off, 0, (size_t)room);
+    return z ? (int64_t)(static_cast<const char *>(z) - (a + off)) : (int64_t)room;
+  }
+  // Byte i's address; valid for bytes inside the window (run_to_nul
+  // counted them there).
+  inline const char *ptr(int64_t i) const { return a + (i - lo); }
+  // Copies bytes [i, i + n) to out; the caller has checked they are
+  // inside the window (run_to_nul counted them there).
+  inline char *copy(char *out, int64_t i, int64_t n) const {
+    memcpy(out, a + (i - lo), (size_t)n);
+    return out + n;
+  }
 };
 
 static inline ByteView view(const WriterCall &w, const char *a) {
@@ -85,27 +104,32 @@ bool line_fields(const WriterCall &w, int64_t v, LineFields *f) {
     if (ch != '_' && ch != 0) break;
     if (ch == '_') stop_corr++;
   }
+  // The forward scan reads position i (from the first non-gap byte) while
+  // i < L - stop_corr - start_corr + z, z being the gaps met so far, and
+  // stops at a 0 byte (end_of_read).  z only grows, so every position below
+  // the bound known when a stretch starts is read: a stretch is counted at
+  // once and the bound moves by the gaps it held.
+  const int64_t p0 = slot + start_corr, base = (int64_t)L - stop_corr - start_corr;
   int64_t i = 0, z = 0;
   short end_of_read = 0;
-  while (i < (int64_t)L - stop_corr - start_corr + z) {
-    const char rc = ra[slot + start_corr + i];
-    if (rc == 0) {
+  while (i < base + z) {
+    const int64_t want = base + z - i;
+    const int64_t run = ra.run_to_nul(p0 + i, want);  // bytes before a 0 (or the window's end)
+    const char *rp = ra.ptr(p0 + i), *gp = ga.ptr(p0 + i);
+    unsigned int dl = 0, in = 0;
+    for (int64_t q = 0; q < run; ++q) {
+      const unsigned int gr = rp[q] == '_';
+      dl += gr;
+      in += (gr ^ 1u) & (unsigned int)(gp[q] == '_');
+    }
+    deletion = (unsigned short)(deletion + dl);
+    insertion = (unsigned short)(insertion + in);
+    z += dl + in;
+    i += run;
+    if (run < want) {  // a 0 byte at position i
       end_of_read = (short)i;
       break;
     }
-    if (rc == '_') {
-      deletion++;
-      z++;
-      i++;
-      continue;
-    }
-    if (ga[slot + start_corr + i] == '_') {
-      insertion++;
-      z++;
-      i++;
-      continue;
-    }
-    i++;
   }
   const short chars =
       end_of_read > 0 ? (short)(end_of_read - stop_corr) : (short)(w.read_length + deletion);
@@ -117,9 +141,7 @@ bool line_fields(const WriterCall &w, int64_t v, LineFields *f) {
   f->stop = (int)((unsigned int)(chars - insertion) + start - 1u);
   f->from = slot + start_corr;
   // "%.*s": up to chars bytes, or to the NUL (a negative precision is no limit)
-  int64_t la = 0, lb = 0;
-  while ((chars < 0 || la < chars) && ra[f->from + la]) ++la;
-  while ((chars < 0 || lb < chars) && ga[f->from + lb]) ++lb;
+  const int64_t la = ra.run_to_nul(f->from, chars), lb = ga.run_to_nul(f->from, chars);
   f->len_read = la;
   f->len_genome = lb;
   f->reverse = w.dirs[v] > 3;
@@ -141,9 +163,9 @@ int64_t line_write(const WriterCall &w, const LineFields &f, char *out) {
   p = put_int(p, f.stop);
   memcpy(p, f.reverse ? "\t<<\t" : "\t>>\t", 4);
   p += 4;
-  for (int64_t q = 0; q < f.len_read; ++q) *p++ = ra[f.from + q];
+  p = ra.copy(p, f.from, f.len_read);
   *p++ = '\t';
-  for (int64_t q = 0; q < f.len_genome; ++q) *p++ = ga[f.from + q];
+  p = ga.copy(p, f.from, f.len_genome);
   *p++ = '\t';
   p = put_int(p, f.score);
   *p++ = '\n';

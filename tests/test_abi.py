@@ -65,6 +65,58 @@ def test_writer_matches_reference_writer(saru_lib, name):
     assert df + dr == int((exp["scores"] <= b.k).sum())
 
 
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_writer_matches_oracle_writer_on_irregular_slots(saru_lib, seed):
+    """The writer's scans (leading gaps, the trailing gap/NUL run read
+    backwards across slots, the forward gap count with its growing bound,
+    the NUL-cut strings) against the oracle's byte-by-byte restatement of
+    src/cuda-functions.cu:827-1006, on slots the aligner would not write:
+    gap runs anywhere, NULs inside slots, all-gap and all-NUL slots."""
+    import refkit as R
+    from saruman_b200.workloads import Batch
+
+    rng = np.random.default_rng(seed)
+    n, m, k = 3000, 40, 4
+    L = rng.integers(m - k, m + 2 * k + 1, n)
+    go = np.cumsum(L).astype(np.int32)
+    total = int(go[-1]) + k * n
+    alphabet = np.frombuffer(b"ACGT_", np.uint8)
+    ra = alphabet[rng.choice(5, total, p=[0.22, 0.22, 0.22, 0.22, 0.12])].copy()
+    ga = alphabet[rng.choice(5, total, p=[0.22, 0.22, 0.22, 0.22, 0.12])].copy()
+    for v in range(n):
+        s0 = int(go[v - 1]) + k * v if v else 0
+        s1 = s0 + int(L[v]) + k
+        kind = rng.integers(0, 8)
+        if kind == 0:
+            ra[s0:s1] = ord("_")
+        elif kind == 1:
+            ra[s0:s1] = 0
+        elif kind == 2:
+            ra[s0 + rng.integers(0, s1 - s0):s1] = 0
+            ga[s0 + rng.integers(0, s1 - s0):s1] = 0
+        elif kind == 3:
+            ra[s0:s0 + rng.integers(0, 12)] = ord("_")
+            ra[s1 - rng.integers(0, 12):s1] = ord("_")
+        elif kind == 4:
+            ra[s1 - k:s1] = 0
+            ga[s1 - k:s1] = 0
+        elif kind == 5:
+            ra[s0 + rng.integers(0, s1 - s0)] = 0
+    b = Batch(m=m, k=k, genome=np.zeros(int(go[-1]), np.uint8), reads=np.zeros(n * m, np.uint8),
+              genome_offsets=go, read_offsets=(np.arange(1, n + 1) * m).astype(np.int32),
+              edit_offsets=np.zeros(n, np.int32),
+              dirs=rng.choice(np.array([1, 2, 3, 5, 6, 7], np.int8), n),
+              ids=rng.integers(0, 50, n).astype(np.int32),
+              pos=rng.integers(0, 1 << 20, n).astype(np.int32))
+    scores = rng.integers(0, k + 2, n).astype(np.int32)
+    names = {i: f"read_{seed}_{i}".encode() for i in range(50)}
+    tsv, df, dr = S.format_tsv(b, S.AlignResult(scores, ra, ga), S.name_table(names),
+                               read_length=m)
+    want, _, (wf, wr) = R.oracle_tsv(b, scores, ra, ga, R.name_table(names), read_length=m)
+    assert tsv == want
+    assert (df, dr) == (wf, wr)
+
+
 def test_load_fails_loudly_without_library(tmp_path):
     with pytest.raises(RuntimeError, match="not built"):
         S.load(tmp_path / "missing.so")
