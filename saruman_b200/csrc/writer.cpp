@@ -115,12 +115,14 @@ bool line_fields(const WriterCall &w, int64_t v, LineFields *f) {
   while (i < base + z) {
     const int64_t want = base + z - i;
     const int64_t run = ra.run_to_nul(p0 + i, want);  // bytes before a 0 (or the window's end)
-    const char *rp = ra.ptr(p0 + i), *gp = ga.ptr(p0 + i);
     unsigned int dl = 0, in = 0;
-    for (int64_t q = 0; q < run; ++q) {
-      const unsigned int gr = rp[q] == '_';
-      dl += gr;
-      in += (gr ^ 1u) & (unsigned int)(gp[q] == '_');
+    if (run > 0) {
+      const char *rp = ra.ptr(p0 + i), *gp = ga.ptr(p0 + i);
+      for (int64_t q = 0; q < run; ++q) {
+        const unsigned int gr = rp[q] == '_';
+        dl += gr;
+        in += (gr ^ 1u) & (unsigned int)(gp[q] == '_');
+      }
     }
     deletion = (unsigned short)(deletion + dl);
     insertion = (unsigned short)(insertion + in);
