@@ -471,8 +471,9 @@ void saru_server_counters(saru_server *s, int64_t *groups, int64_t *launches);
 void saru_server_destroy(saru_server *s);
 
 /* Formats the reference's TSV lines for one aligned call into `out`
- * (capacity cap) and returns the bytes needed.  names: n_names entries of
- * name_stride bytes, indexed by read id. */
+ * (capacity cap) and returns the bytes needed (ordered ranges of candidates
+ * on the host cores).  names: n_names entries of name_stride bytes, indexed
+ * by read id. */
 int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
                         const int32_t *read_ids, const int32_t *genome_pos, int32_t read_length,
                         const char *names, int32_t name_stride, int32_t n_names, char *out,

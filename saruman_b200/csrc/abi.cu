@@ -1350,13 +1350,33 @@ int64_t saru_format_tsv(const saru_batch *batch, const saru_result *result,
   saru::WriterCall w{result->scores, result->read_aln, result->genome_aln, batch->total_slots,
                      batch->genome_offsets, genome_pos, batch->dirs, read_ids, batch->k,
                      read_length, &Tab::get, &tab};
-  std::string text;
-  int32_t df = 0, dr = 0;
-  saru::format_range(w, 0, batch->n, &text, &df, &dr);
-  if (done_fwd) *done_fwd = df;
-  if (done_rev) *done_rev = dr;
-  if (out && cap > 0) memcpy(out, text.data(), (size_t)((int64_t)text.size() < cap ? (int64_t)text.size() : cap));
-  return (int64_t)text.size();
+  // ordered ranges of candidates on the host cores, concatenated in order
+  const int64_t n = batch->n;
+  const int hw = (int)std::thread::hardware_concurrency();
+  const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(hw > 0 ? hw : 1, n / 16384 + 1));
+  std::vector<std::string> text((size_t)nt);
+  std::vector<int32_t> df((size_t)nt, 0), dr((size_t)nt, 0);
+  auto part = [&](int i) {
+    saru::format_range(w, n * i / nt, n * (i + 1) / nt, &text[(size_t)i], &df[(size_t)i],
+                       &dr[(size_t)i]);
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < nt; ++i) th.emplace_back(part, i);
+  part(0);
+  for (auto &t : th) t.join();
+  int64_t total = 0;
+  int32_t f = 0, r = 0;
+  for (int i = 0; i < nt; ++i) {
+    const std::string &t = text[(size_t)i];
+    if (out && total < cap)
+      memcpy(out + total, t.data(), (size_t)std::min<int64_t>((int64_t)t.size(), cap - total));
+    total += (int64_t)t.size();
+    f += df[(size_t)i];
+    r += dr[(size_t)i];
+  }
+  if (done_fwd) *done_fwd = f;
+  if (done_rev) *done_rev = r;
+  return total;
 }
 
 void cuda_allocate_memory(int do_reverse) {

@@ -65,18 +65,19 @@ def test_writer_matches_reference_writer(saru_lib, name):
     assert df + dr == int((exp["scores"] <= b.k).sum())
 
 
-@pytest.mark.parametrize("seed", [0, 1, 2])
-def test_writer_matches_oracle_writer_on_irregular_slots(saru_lib, seed):
+@pytest.mark.parametrize("seed,n", [(0, 3000), (1, 3000), (2, 3000), (3, 70000)])
+def test_writer_matches_oracle_writer_on_irregular_slots(saru_lib, seed, n):
     """The writer's scans (leading gaps, the trailing gap/NUL run read
     backwards across slots, the forward gap count with its growing bound,
     the NUL-cut strings) against the oracle's byte-by-byte restatement of
     src/cuda-functions.cu:827-1006, on slots the aligner would not write:
-    gap runs anywhere, NULs inside slots, all-gap and all-NUL slots."""
+    gap runs anywhere, NULs inside slots, all-gap and all-NUL slots.  70k
+    candidates take several host threads (ordered ranges)."""
     import refkit as R
     from saruman_b200.workloads import Batch
 
     rng = np.random.default_rng(seed)
-    n, m, k = 3000, 40, 4
+    m, k = 40, 4
     L = rng.integers(m - k, m + 2 * k + 1, n)
     go = np.cumsum(L).astype(np.int32)
     total = int(go[-1]) + k * n
