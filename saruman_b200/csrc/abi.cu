@@ -22,6 +22,7 @@
 #include <chrono>
 #include <map>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -969,7 +970,9 @@ struct NameIndex {
 // the ids a call prints (the reference builds one table per read batch and
 // makes many calls against it; walking a list of millions of reads per call
 // would cost more than the call).
-std::mutex g_names_mu;
+// Shared while a call's lines are formatted (the two strands' calls format
+// at once), exclusive while the index is rebuilt.
+std::shared_mutex g_names_mu;
 NameIndex g_names;
 
 // Grow-only pinned host buffer.
@@ -1168,8 +1171,15 @@ void legacy_write(const saru_batch &b, PinnedBuf *hb, const int *read_id_array,
                   float ms) {
   const int n = b.n;
   const int32_t *scores = hb[0].as<int32_t>();
-  std::lock_guard<std::mutex> nl(g_names_mu);
-  if (!g_names.covers(read_names, read_id_array, scores, n, error)) g_names.build(read_names);
+  std::shared_lock<std::shared_mutex> names_lk(g_names_mu);
+  if (!g_names.covers(read_names, read_id_array, scores, n, error)) {
+    names_lk.unlock();
+    {
+      std::unique_lock<std::shared_mutex> build_lk(g_names_mu);
+      if (!g_names.covers(read_names, read_id_array, scores, n, error)) g_names.build(read_names);
+    }
+    names_lk.lock();
+  }
   saru::WriterCall w{scores, hb[1].as<char>(), hb[2].as<char>(), b.total_slots,
                      b.genome_offsets, genome_pos_array,
                      reinterpret_cast<const int8_t *>(direction_array), read_id_array, error,
