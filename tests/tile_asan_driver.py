@@ -50,7 +50,8 @@ def main():
     lib = C.CDLL(sys.argv[1])
     P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
     cases = [(36, 2, 0.05), (100, 5, 0.04), (75, 5, 0.2), (150, 9, 0.05), (250, 15, 0.05),
-             (20, 1, 0.1), (40, 7, 0.1), (64, 15, 0.3)]
+             (20, 1, 0.1), (40, 7, 0.1), (64, 15, 0.3), (512, 15, 0.03), (2, 0, 0.1),
+             (8, 1, 0.1)]
     bad = 0
     for ci, (m, k, err) in enumerate(cases):
         for seed in range(2):
