@@ -47,7 +47,7 @@ def run_core(lib, b, first=True):
 
 
 CASES = [(36, 2), (36, 3), (75, 5), (100, 5), (100, 6), (150, 9), (250, 15), (20, 1), (10, 0),
-         (40, 7), (64, 15), (50, 10), (31, 10)]
+         (40, 7), (64, 15), (50, 10), (31, 10), (512, 15), (2, 0), (4, 1)]
 
 
 @pytest.mark.parametrize("m,k", CASES)
